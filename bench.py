@@ -1,0 +1,409 @@
+"""Delay-and-sum benchmark: one JSON line on rank 0.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the 3-D diverging-wave volume (32x32 = 1024-channel matrix array,
+16 diverging transmits, 4096 samples, batch 1, 128^3 voxels, FP32), seeded
+synthetic channel data built on the device.  A step is one ffdas das call on
+that volume (ingest + delay-and-sum kernel); its inputs (268 MB of channel
+data, 2 x 134 MB of delays/weights) exceed the 126 MB L2, so no flush is
+needed between steps.  Metric: voxel x channel x transmit x batch units per
+second (Gvox.ch.tx/s), whole job, all ranks.
+
+N > 1 (torchrun): every rank beamforms its own volume (independent frames,
+weak scaling, no collective on the data path); the timed region is bracketed
+by a barrier and synchronize on both sides and the time is the max over ranks.
+
+Extra keys: `roofline` for the delay-and-sum kernel (FP32 work, 5 flop/unit,
+against the FP32 FMA peak measured on this GPU; the HBM figure beside it),
+`cpu_baseline` (the FP32 C/OpenMP loop of the same formula on a voxel subset,
+all host threads), `e2e` (through the public Python API with the channel data
+copied from pinned host memory and the image read back each step), `bf16` /
+`fp16` (reduced-precision pair storage: throughput, speed-up over FP32 and
+error against the FP64 oracle), `bwd_fwd` (backward / forward time on the
+differentiable 128-channel, 8-plane-wave, batch-4 workload) and `reference_gpu`
+parity.  `--impl reference` times the reference implementation (its CUDA das,
+built from its sources into oracle/_ref) on the same workload and GPU.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+import torch.distributed as dist
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "DAS Gvox·ch·tx/s: bf16-in vs plain FP32 at ≤1e-3 rel err; bwd/fwd time ratio"
+UNIT = "Gvox·ch·tx/s"
+FLOP_PER_UNIT = 5.0
+
+
+# ----------------------------------------------------------------- clocks ---
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (200 ms period)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        load = [s for s in sm if smax and s > 0.5 * max(smax)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ utils ---
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profile_traffic(name: str):
+    """Per-launch DRAM bytes of the kernel from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / f"{name}.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get("dram_bytes_per_launch")
+        except Exception:
+            return None
+    return None
+
+
+def timed(fn, steps: int, warmup: int, stream, world: int):
+    for _ in range(warmup):
+        fn()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = a.elapsed_time(b) / steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
+def algorithmic_bytes(wl, x_bytes_per_sample: int) -> int:
+    x = wl["x"]
+    V = int(np.prod(wl["dstpos"].shape[:-1]))
+    C, S = x.shape[-3], x.shape[-2]
+    B = x.shape[0]
+    n_ev = wl["offsets"].shape[0]
+    return int(x.numel() * x_bytes_per_sample + 2 * n_ev * V * 4 + V * 12 + C * 12 + B * V * 4)
+
+
+# ------------------------------------------------------------ CPU baseline ---
+def cpu_baseline(wl, budget_s: float = 12.0) -> dict:
+    from oracle import oracle
+    x = wl["x"][0].cpu().numpy()
+    srcpos = wl["srcpos"].cpu().numpy()
+    dst = wl["dstpos"].cpu().numpy()
+    offs = wl["offsets"].cpu().numpy()
+    w = wl["weights"].cpu().numpy()
+    nz = dst.shape[0]
+    C, S = x.shape[0], x.shape[1]
+    threads = oracle.num_threads()
+    per_plane = int(np.prod(dst.shape[1:-1])) * C * S
+
+    def run(planes):
+        t0 = time.perf_counter()
+        oracle.das_f32(x[None], srcpos, dst[:planes], offs[:, :planes], w[:, :planes])
+        return time.perf_counter() - t0
+
+    run(1)                                   # warm-up (page-in, thread pool)
+    t1 = run(1)
+    planes = int(max(1, min(nz, budget_s / max(t1, 1e-3))))
+    # take planes spread over depth so near and far voxels are both sampled
+    sel = np.linspace(0, nz - 1, planes).astype(int)
+    t0 = time.perf_counter()
+    oracle.das_f32(x[None], srcpos, dst[sel], offs[:, sel], w[:, sel])
+    dt = time.perf_counter() - t0
+    units = planes * per_plane
+    return {"value": units / dt / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{planes} of {nz} depth planes ({units:.3g} units), FP32 C/OpenMP loop, "
+                      f"{threads} threads, {dt:.1f} s"}
+
+
+# ------------------------------------------------------------ reference ---
+def run_reference(args, rank, world) -> dict:
+    from ffdas_b200 import workloads as W
+    from oracle import reference
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    wl = W.diverging3d(device=dev)
+    units = wl["units"]
+    if not reference.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libffdas_ref.so was not built "
+                "(the reference sources were absent at build time)"}
+    call = reference.Prepared(wl["x"], wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"], alg=1)
+    stream = torch.cuda.current_stream(dev)
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    ms = timed(call, args.steps, args.warmup, stream, 1)
+    ck = clocks.stop()
+    # e2e: channel data from pinned host memory, image back, every step
+    xh = wl["x"].cpu().pin_memory()
+    out_h = torch.empty(call.out.shape, dtype=torch.float32).pin_memory()
+
+    def e2e():
+        call.x.copy_(xh, non_blocking=True)
+        call()
+        out_h.copy_(call.out, non_blocking=True)
+    ms_e2e = timed(e2e, args.steps, args.warmup, stream, 1)
+    call.close()
+    value = units / (ms * 1e-3) / 1e9
+    cpu = cpu_baseline(wl) if args.cpu_baseline else None
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "diverging3d: 32x32 matrix array (1024 ch), 16 diverging transmits, "
+                       "4096 samples, batch 1, 128^3 voxels, FP32", "units_per_step": units,
+                       "l2": "inputs larger than L2 (no flush)", "reference": "ffdas ALG1 (DEFAULT) "
+                       "built for sm_100a from the reference sources, run on the same GPU"},
+            "device": "gpu",
+            "e2e": {"value": units / (ms_e2e * 1e-3) / 1e9, "unit": UNIT,
+                    "h2d_bytes_per_step": int(wl["x"].numel() * 4), "d2h_bytes_per_step": int(call.out.numel() * 4)},
+            "clocks": ck}
+    if cpu:
+        line["cpu_baseline"] = cpu
+    return line
+
+
+# ------------------------------------------------------------------ ours ---
+def run_ours(args, rank, world) -> dict:
+    import ffdas_b200
+    from ffdas_b200 import workloads as W
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    wl = W.diverging3d(device=dev, seed=1 + rank)
+    x, srcpos, dstpos, offs, w = wl["x"], wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"]
+    units = wl["units"]
+    stream = torch.cuda.current_stream(dev)
+    out = torch.empty((1, *dstpos.shape[:-1]), device=dev)
+    h = ffdas_b200.get_library_handle(dev)
+
+    def step():
+        ffdas_b200.das(x, srcpos, dstpos, offs, w, out=out)
+
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    ms = timed(step, args.steps, args.warmup, stream, world)
+    ck = clocks.stop()
+    value = units * world / (ms * 1e-3) / 1e9
+
+    # kernel-only duration of the delay-and-sum kernel (events inside the library)
+    h.set_kernel_timing(True)
+    kms = []
+    for _ in range(max(3, args.steps)):
+        step()
+        kms.append(h.last_kernel_ms())
+    h.set_kernel_timing(False)
+    info = h.last_kernel_info()
+    kernel_ms = statistics.mean(kms[1:]) if len(kms) > 1 else kms[0]
+    fp32_peak = h.measure_fp32_peak()
+    pk = peaks()
+    achieved_tf = FLOP_PER_UNIT * units / (kernel_ms * 1e-3) / 1e12
+    bytes_alg = algorithmic_bytes(wl, 4)
+    roofline = {"bound": "fp32", "achieved": achieved_tf, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved_tf / fp32_peak, "traffic": profile_traffic("das_gather_diverging3d"),
+                "kernel": "das_gather_kernel<f32 pairs>", "kernel_ms": kernel_ms,
+                "peak_source": "FP32 FMA throughput measured on this GPU by ffdas_measure_fp32_peak",
+                "flop_per_unit": FLOP_PER_UNIT, "units_per_launch": units,
+                "hbm": {"algorithmic_bytes": bytes_alg, "achieved_gbs": bytes_alg / (kernel_ms * 1e-3) / 1e9,
+                        "peak_gbs": pk["hbm_gbs"], "peak_source": pk["source"] + " (MEASURED_PEAKS.json hbm_gbs)"}}
+
+    # e2e through the public API: pinned host channel data in, image out
+    xh = x.cpu().pin_memory()
+    xd = torch.empty_like(x)
+    out_h = torch.empty(out.shape, dtype=torch.float32).pin_memory()
+
+    def e2e():
+        xd.copy_(xh, non_blocking=True)
+        ffdas_b200.das(xd, srcpos, dstpos, offs, w, out=out)
+        out_h.copy_(out, non_blocking=True)
+    ms_e2e = timed(e2e, args.steps, args.warmup, stream, world)
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "diverging3d: 32x32 matrix array (1024 ch), 16 diverging transmits, "
+                       "4096 samples, batch 1, 128^3 voxels, FP32", "units_per_step": units * world,
+                       "parallelism": f"replicas x{world} (independent volumes)" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (no flush)", "schedule": info},
+            "roofline": roofline,
+            "e2e": {"value": units * world / (ms_e2e * 1e-3) / 1e9, "unit": UNIT,
+                    "h2d_bytes_per_step": int(x.numel() * 4), "d2h_bytes_per_step": int(out.numel() * 4)},
+            "gpu_launches": 2 * args.steps,
+            "clocks": ck}
+
+    if rank == 0 and world == 1 and not args.quick:
+        line.update(extras(args, wl, ms, h))
+        if args.cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(wl)
+    return line
+
+
+def extras(args, wl, ms_fp32, h) -> dict:
+    """Reduced-precision storage, errors against the FP64 oracle, backward/forward."""
+    import ffdas_b200
+    from ffdas_b200 import workloads as W
+    from oracle import oracle
+    dev = wl["x"].device
+    srcpos, dstpos, offs, w = wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"]
+    units = wl["units"]
+    xn = W.normalize_channels(wl["x"])          # per-channel peak 1
+    stream = torch.cuda.current_stream(dev)
+    res = {}
+    # FP64 oracle on depth planes spread over the volume
+    nz = dstpos.shape[0]
+    sel = np.linspace(0, nz - 1, 6).astype(int)
+    ref = oracle.das_f64(xn.cpu().numpy(), srcpos.cpu().numpy(), dstpos[sel].cpu().numpy(),
+                         offs[:, sel].cpu().numpy(), w[:, sel].cpu().numpy())
+
+    def measure(x, **kw):
+        out = torch.empty((1, *dstpos.shape[:-1]), device=dev)
+        ms = timed(lambda: ffdas_b200.das(x, srcpos, dstpos, offs, w, out=out, **kw), args.steps, args.warmup,
+                   stream, 1)
+        img = out[:, sel].cpu().numpy()
+        return ms, oracle.error_report(img, ref)
+
+    ms32, err32 = measure(xn)
+    res["fp32_error_vs_fp64_oracle"] = err32
+    for name, x in (("bf16", xn.to(torch.bfloat16)), ("fp16", xn.to(torch.float16))):
+        msr, err = measure(x)
+        res[name] = {"value": units / (msr * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": msr,
+                     "speedup_vs_fp32": ms32 / msr, "error_vs_fp64_oracle": err,
+                     "input": f"channel data stored as {name} (per-channel peak 1), FP32 geometry and accumulation"}
+    # backward / forward on the differentiable workload
+    af = W.autofocus(device=dev)
+    xa = af["x"]
+    args_f = (af["srcpos"], af["dstpos"], af["offsets"], af["weights"])
+    gout = torch.randn((xa.shape[0], *af["dstpos"].shape[:-1]), device=dev)
+    from ffdas_b200 import _lib
+    from ffdas_b200._lib import DataType
+
+    def fwd():
+        ffdas_b200.das(xa, *args_f)
+
+    gx = torch.zeros(xa.shape, device=dev)
+    go = torch.empty_like(af["offsets"])
+    gw = torch.empty_like(af["weights"])
+    gd = torch.empty_like(af["dstpos"])
+    gs = torch.empty_like(af["srcpos"])
+    xdsc = _lib.TensorDesc(list(xa.shape), list(xa.stride()), DataType.R_32F)
+    gdsc = _lib.TensorDesc(list(gout.shape), None, DataType.R_32F)
+    L = _lib.load()
+    hh = ffdas_b200.get_library_handle(dev)
+
+    def bwd():
+        hh.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+        _lib.check(L.ffdas_das_backward(hh.h, af["srcpos"].data_ptr(), None, 0.0, xdsc.desc, xa.data_ptr(),
+                                        af["dstpos"].data_ptr(), af["offsets"].data_ptr(), af["weights"].data_ptr(),
+                                        0, None, gdsc.desc, gout.data_ptr(), gx.data_ptr(), go.data_ptr(),
+                                        gw.data_ptr(), gd.data_ptr(), gs.data_ptr()))
+    msf = timed(fwd, args.steps, args.warmup, stream, 1)
+    msb = timed(bwd, args.steps, args.warmup, stream, 1)
+    res["bwd_fwd"] = {"ratio": msb / msf, "fwd_ms": msf, "bwd_ms": msb,
+                      "workload": "autofocus: 128 ch, 8 plane waves, batch 4, 2048 samples, 256x256 voxels; "
+                                  "backward = grads of x, offsets, weights, voxel and channel positions"}
+    return res
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--quick", action="store_true", help="main metric only")
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            if rank != 0:
+                line = None
+            else:
+                line = run_reference(args, rank, world)
+        else:
+            line = run_ours(args, rank, world)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,447 @@
+// das.cu -- ffdas_das / ffdas_das_sparse entry points and forward dispatch.
+//
+// Validation order and error codes follow the reference: handle, device,
+// descriptors (src/das/das.cu:25-28), dtype combination (:40-82), int32
+// index guard and algorithm (src/das/das_impl.cuh:34-54), problem dims
+// (src/das/das_utils.h:32-69), compute-type support
+// (src/das/das_alg1.cu:172-178), sparse count (das_alg1.cu:267).
+// After validation every call runs: ingest (x -> pair rows) then the
+// forward kernel chosen by the planner or the handle's config.
+#include <algorithm>
+#include <cstring>
+
+#include "core.h"
+#include "das_problem.h"
+#include "das_gather.cuh"
+
+namespace ffdas {
+
+bool fits_int32_indexing(const ffdas_tensor_desc &d) {
+    int64_t max_off = 0;
+    for (int64_t i = 0; i < d.ndim; i++)
+        if (d.dims[i] > 1) max_off += (d.dims[i] - 1) * (d.strides[i] < 0 ? -d.strides[i] : d.strides[i]);
+    return max_off <= INT32_MAX && d.numel() <= INT32_MAX;
+}
+
+ffdas_error_t make_problem(const ffdas_tensor_desc &x, const ffdas_tensor_desc &out, das_problem &p) {
+    if (x.ndim != 3 && x.ndim != 4) return FFDAS_ERROR_INVALID_DIMS;
+    if (out.ndim < 1) return FFDAS_ERROR_INVALID_DIMS;
+    p.have_batch = (x.ndim == 4);
+    const int o = p.have_batch ? 1 : 0;
+    for (int64_t i = 0; i < x.ndim; i++)
+        if (x.dims[i] < 0) return FFDAS_ERROR_INVALID_DIMS;
+    for (int64_t i = 0; i < out.ndim; i++)
+        if (out.dims[i] < 0) return FFDAS_ERROR_INVALID_DIMS;
+    p.B = p.have_batch ? (int)x.dims[0] : 1;
+    p.C = (int)x.dims[o + 0];
+    p.S = (int)x.dims[o + 1];
+    p.N = (int)x.dims[o + 2];
+    if (p.have_batch && (out.ndim < 2 || out.dims[0] != p.B)) return FFDAS_ERROR_INVALID_DIMS;
+    p.V = 1;
+    for (int64_t i = o; i < out.ndim; i++) p.V *= out.dims[i];
+    p.x_bstride = p.have_batch ? x.strides[0] : 0;
+    p.x_cstride = x.strides[o + 0];
+    p.x_sstride = x.strides[o + 1];
+    if (x.strides[o + 2] != 1 && p.N > 1) return FFDAS_ERROR_INVALID_ARGUMENT;
+    p.out_bstride = p.have_batch ? out.strides[0] : 0;
+
+    // Spatial dims of out must be C-contiguous (the reference assumes it
+    // without checking, das_alg1_kernels.cuh:104).
+    int64_t s = 1;
+    for (int64_t i = out.ndim - 1; i >= o; i--) {
+        if (out.dims[i] > 1 && out.strides[i] != s) return FFDAS_ERROR_NON_CONTIGUOUS;
+        s *= out.dims[i];
+    }
+    // Collapse spatial dims (dropping size-1 dims) into (D2, D1, D0).
+    int64_t sp[FFDAS_MAX_DIMS];
+    int ns = 0;
+    for (int64_t i = o; i < out.ndim; i++)
+        if (out.dims[i] != 1) sp[ns++] = out.dims[i];
+    int64_t d0 = 1, d1 = 1, d2 = 1;
+    if (ns >= 1) d0 = sp[ns - 1];
+    if (ns >= 2) d1 = sp[ns - 2];
+    for (int i = 0; i < ns - 2; i++) d2 *= sp[i];
+    if (p.V == 0) d0 = d1 = d2 = 0;
+    p.D0 = (int)d0;
+    p.D1 = (int)d1;
+    p.D2 = (int)d2;
+    return FFDAS_SUCCESS;
+}
+
+int select_storage(ffdas_datatype_t xt, ffdas_datatype_t ot, ffdas_compute_type_t ct) {
+    switch (xt) {
+        case FFDAS_R_16F:
+            if (ot != FFDAS_R_32F) return -1;
+            // reference: a half-precision compute request on half input is
+            // rejected (das_alg1.cu:172-178)
+            if (ct == FFDAS_COMPUTE_16F) return -1;
+            return ct == FFDAS_COMPUTE_16BF ? ST_BF16 : ST_F16;
+        case FFDAS_R_16BF:
+            if (ot != FFDAS_R_32F) return -1;
+            if (ct == FFDAS_COMPUTE_16F) return ST_F16;
+            return ST_BF16;
+        case FFDAS_R_32F:
+            if (ot != FFDAS_R_32F) return -1;
+            if (ct == FFDAS_COMPUTE_16F) return ST_F16;
+            if (ct == FFDAS_COMPUTE_16BF) return ST_BF16;
+            return ST_F32;
+        case FFDAS_C_16F:
+            if (ot != FFDAS_C_32F) return -1;
+            if (ct == FFDAS_COMPUTE_16F || ct == FFDAS_COMPUTE_16BF) return -1;
+            return ST_C16;
+        case FFDAS_C_32F:
+            if (ot != FFDAS_C_32F) return -1;
+            if (ct == FFDAS_COMPUTE_16F) return ST_C16;
+            if (ct == FFDAS_COMPUTE_16BF) return -1;
+            return ST_C32;
+        case FFDAS_R_64F:
+            if (ot != FFDAS_R_64F) return -1;
+            if (ct == FFDAS_COMPUTE_16F || ct == FFDAS_COMPUTE_16BF) return -1;
+            return ct == FFDAS_COMPUTE_32F ? ST_F32 : ST_F64;
+        case FFDAS_C_64F:
+            if (ot != FFDAS_C_64F) return -1;
+            if (ct == FFDAS_COMPUTE_16F || ct == FFDAS_COMPUTE_16BF) return -1;
+            return ct == FFDAS_COMPUTE_32F ? ST_C32 : ST_C64;
+        default:
+            return -1;
+    }
+}
+
+static size_t storage_bytes(int kind) {
+    switch (kind) {
+        case ST_F32: return 8;
+        case ST_F16: return 4;
+        case ST_BF16: return 4;
+        case ST_F64: return 16;
+        case ST_C32: return 16;
+        case ST_C16: return 8;
+        case ST_C64: return 32;
+        default: return 0;
+    }
+}
+
+// ---------------------------------------------------------------- ingest ---
+template <typename Tin, int K>
+static ffdas_error_t launch_ingest_t(ffdas_context &h, const das_problem &pb, const void *x,
+                                     int64_t npad, void *P) {
+    const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
+    if (rows == 0) return FFDAS_SUCCESS;
+    dim3 block(256);
+    dim3 grid((unsigned)((npad + 255) / 256), (unsigned)std::min<int64_t>(rows, 65535));
+    ingest_pairs_kernel<Tin, K><<<grid, block, 0, h.stream>>>(
+        static_cast<const Tin *>(x), pb.x_bstride, pb.x_cstride, pb.x_sstride, pb.C, pb.S, pb.N,
+        rows, npad, static_cast<typename pair_traits<K>::storage *>(P));
+    return ffdas_launch_check(h.stream);
+}
+
+static ffdas_error_t launch_ingest(ffdas_context &h, const das_problem &pb, ffdas_datatype_t xt,
+                                   int kind, const void *x, int64_t npad, void *P) {
+    switch (xt) {
+        case FFDAS_R_32F:
+            if (kind == ST_F32) return launch_ingest_t<float, ST_F32>(h, pb, x, npad, P);
+            if (kind == ST_F16) return launch_ingest_t<float, ST_F16>(h, pb, x, npad, P);
+            if (kind == ST_BF16) return launch_ingest_t<float, ST_BF16>(h, pb, x, npad, P);
+            break;
+        case FFDAS_R_16F:
+            if (kind == ST_F16) return launch_ingest_t<__half, ST_F16>(h, pb, x, npad, P);
+            if (kind == ST_BF16) return launch_ingest_t<__half, ST_BF16>(h, pb, x, npad, P);
+            break;
+        case FFDAS_R_16BF:
+            if (kind == ST_BF16) return launch_ingest_t<__nv_bfloat16, ST_BF16>(h, pb, x, npad, P);
+            if (kind == ST_F16) return launch_ingest_t<__nv_bfloat16, ST_F16>(h, pb, x, npad, P);
+            break;
+        case FFDAS_R_64F:
+            if (kind == ST_F64) return launch_ingest_t<double, ST_F64>(h, pb, x, npad, P);
+            if (kind == ST_F32) return launch_ingest_t<double, ST_F32>(h, pb, x, npad, P);
+            break;
+        case FFDAS_C_32F:
+            if (kind == ST_C32) return launch_ingest_t<float2, ST_C32>(h, pb, x, npad, P);
+            if (kind == ST_C16) return launch_ingest_t<float2, ST_C16>(h, pb, x, npad, P);
+            break;
+        case FFDAS_C_16F:
+            if (kind == ST_C16) return launch_ingest_t<__half2, ST_C16>(h, pb, x, npad, P);
+            break;
+        case FFDAS_C_64F:
+            if (kind == ST_C64) return launch_ingest_t<double2, ST_C64>(h, pb, x, npad, P);
+            if (kind == ST_C32) return launch_ingest_t<double2, ST_C32>(h, pb, x, npad, P);
+            break;
+        default:
+            break;
+    }
+    return FFDAS_ERROR_INTERNAL;
+}
+
+ffdas_error_t ingest_for_backward(ffdas_context &h, const das_problem &pb, ffdas_datatype_t xt, int kind,
+                                  const void *x, int64_t npad, void *P) {
+    return launch_ingest(h, pb, xt, kind, x, npad, P);
+}
+
+// ---------------------------------------------------------------- gather ---
+struct schedule {
+    int variant = 1;
+    int T0 = 16, T1 = 16, T2 = 1;
+    int BT = 1;
+    int SC = 16;
+};
+
+static int floor_pow2(int v) {
+    int p = 1;
+    while (p * 2 <= v) p *= 2;
+    return p;
+}
+
+static schedule plan_schedule(const ffdas_context &h, const das_problem &pb, int kind) {
+    schedule s;
+    const bool real = (kind == ST_F32 || kind == ST_F16 || kind == ST_BF16);
+    // batch tile: amortise geometry over batch items, bounded by registers
+    s.BT = real ? std::min(8, floor_pow2(std::max(1, pb.B))) : (pb.B >= 4 ? 4 : 1);
+    s.SC = (real && pb.n_events > 4) ? 16 : 4;
+    // tile: 2-D patch over the two innermost grid dims, 256 threads
+    if (pb.D1 <= 1) {
+        s.T0 = 256; s.T1 = 1; s.T2 = 1;
+    } else if (pb.D0 >= 16 && pb.D1 >= 16) {
+        s.T0 = 16; s.T1 = 16; s.T2 = 1;
+    } else if (pb.D0 >= 32) {
+        s.T0 = 32; s.T1 = 8; s.T2 = 1;
+    } else {
+        s.T0 = std::max(1, floor_pow2(pb.D0)); s.T1 = 256 / s.T0; s.T2 = 1;
+    }
+    if (h.has_config) {
+        const ffdas_das_config_t &c = h.config;
+        if (c.variant) s.variant = c.variant;
+        if (c.tile_x || c.tile_y || c.tile_z) {
+            s.T0 = c.tile_x ? c.tile_x : 1;
+            s.T1 = c.tile_y ? c.tile_y : 1;
+            s.T2 = c.tile_z ? c.tile_z : 1;
+        }
+        if (c.batch_tile) s.BT = c.batch_tile;
+        if (c.event_chunk) s.SC = c.event_chunk <= 4 ? 4 : 16;
+    }
+    if (!real && s.BT != 1) s.BT = 4;
+    if (s.T0 * s.T1 * s.T2 != 256) {  // the gather kernel runs 256-thread CTAs
+        s.T0 = 16; s.T1 = 16; s.T2 = 1;
+        if (pb.D1 <= 1) { s.T0 = 256; s.T1 = 1; }
+    }
+    return s;
+}
+
+template <int K, typename OutT, int BT, int SC, bool SPARSE>
+static ffdas_error_t launch_gather_t(ffdas_context &h, const gather_params &gp, dim3 grid) {
+    das_gather_kernel<K, OutT, BT, SC, SPARSE><<<grid, 256, 0, h.stream>>>(gp);
+    return ffdas_launch_check(h.stream);
+}
+
+template <int K, typename OutT, bool SPARSE>
+static ffdas_error_t launch_gather_bt(ffdas_context &h, const gather_params &gp, const schedule &s,
+                                      dim3 grid) {
+    constexpr bool real = (K == ST_F32 || K == ST_F16 || K == ST_BF16);
+    if constexpr (real) {
+        if (s.SC == 16) {
+            switch (s.BT) {
+                case 1: return launch_gather_t<K, OutT, 1, 16, SPARSE>(h, gp, grid);
+                case 2: return launch_gather_t<K, OutT, 2, 16, SPARSE>(h, gp, grid);
+                case 4: return launch_gather_t<K, OutT, 4, 16, SPARSE>(h, gp, grid);
+                case 8: return launch_gather_t<K, OutT, 8, 16, SPARSE>(h, gp, grid);
+                default: break;
+            }
+        } else {
+            switch (s.BT) {
+                case 1: return launch_gather_t<K, OutT, 1, 4, SPARSE>(h, gp, grid);
+                case 2: return launch_gather_t<K, OutT, 2, 4, SPARSE>(h, gp, grid);
+                case 4: return launch_gather_t<K, OutT, 4, 4, SPARSE>(h, gp, grid);
+                case 8: return launch_gather_t<K, OutT, 8, 4, SPARSE>(h, gp, grid);
+                default: break;
+            }
+        }
+    } else {
+        if (s.BT == 4) return launch_gather_t<K, OutT, 4, 4, SPARSE>(h, gp, grid);
+        return launch_gather_t<K, OutT, 1, 4, SPARSE>(h, gp, grid);
+    }
+    return FFDAS_ERROR_INVALID_ARGUMENT;
+}
+
+template <bool SPARSE>
+static ffdas_error_t launch_gather(ffdas_context &h, int kind, ffdas_datatype_t ot,
+                                   const gather_params &gp, const schedule &s, dim3 grid) {
+    switch (kind) {
+        case ST_F32:
+            if (ot == FFDAS_R_64F) return launch_gather_bt<ST_F32, double, SPARSE>(h, gp, s, grid);
+            return launch_gather_bt<ST_F32, float, SPARSE>(h, gp, s, grid);
+        case ST_F16: return launch_gather_bt<ST_F16, float, SPARSE>(h, gp, s, grid);
+        case ST_BF16: return launch_gather_bt<ST_BF16, float, SPARSE>(h, gp, s, grid);
+        case ST_F64: return launch_gather_bt<ST_F64, double, SPARSE>(h, gp, s, grid);
+        case ST_C32:
+            if (ot == FFDAS_C_64F) return launch_gather_bt<ST_C32, double2, SPARSE>(h, gp, s, grid);
+            return launch_gather_bt<ST_C32, float2, SPARSE>(h, gp, s, grid);
+        case ST_C16: return launch_gather_bt<ST_C16, float2, SPARSE>(h, gp, s, grid);
+        case ST_C64: return launch_gather_bt<ST_C64, double2, SPARSE>(h, gp, s, grid);
+        default: return FFDAS_ERROR_INTERNAL;
+    }
+}
+
+static void read_beta(ffdas_datatype_t ot, const void *beta, double &re, double &im, int &zero) {
+    re = 0.0;
+    im = 0.0;
+    if (beta) {
+        switch (ot) {
+            case FFDAS_R_32F: re = *static_cast<const float *>(beta); break;
+            case FFDAS_R_64F: re = *static_cast<const double *>(beta); break;
+            case FFDAS_C_32F: {
+                const float *b = static_cast<const float *>(beta);
+                re = b[0]; im = b[1];
+                break;
+            }
+            case FFDAS_C_64F: {
+                const double *b = static_cast<const double *>(beta);
+                re = b[0]; im = b[1];
+                break;
+            }
+            default: break;
+        }
+    }
+    zero = (re == 0.0 && im == 0.0) ? 1 : 0;
+}
+
+ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
+    const ffdas_tensor_desc &xd = *a.x_desc;
+    const ffdas_tensor_desc &od = *a.out_desc;
+
+    const int kind = select_storage(xd.dtype, od.dtype, a.compute_type);
+    // dtype combination first (reference das.cu:40-82); compute-type
+    // rejections are reported at the same code, after the dims checks below.
+    const bool combo_ok =
+        (xd.dtype == FFDAS_R_16F && od.dtype == FFDAS_R_32F) ||
+        (xd.dtype == FFDAS_R_16BF && od.dtype == FFDAS_R_32F) ||
+        (xd.dtype == FFDAS_R_32F && od.dtype == FFDAS_R_32F) ||
+        (xd.dtype == FFDAS_C_16F && od.dtype == FFDAS_C_32F) ||
+        (xd.dtype == FFDAS_C_32F && od.dtype == FFDAS_C_32F) ||
+        (xd.dtype == FFDAS_R_64F && od.dtype == FFDAS_R_64F) ||
+        (xd.dtype == FFDAS_C_64F && od.dtype == FFDAS_C_64F);
+    if (!combo_ok) return FFDAS_ERROR_UNSUPPORTED_TYPE;
+
+    if (!fits_int32_indexing(xd) || !fits_int32_indexing(od)) return FFDAS_ERROR_INVALID_DIMS;
+
+    const bool f64 = (od.dtype == FFDAS_R_64F || od.dtype == FFDAS_C_64F);
+    if (a.sparse) {
+        if (a.alg != FFDAS_ALG_DEFAULT && a.alg != FFDAS_ALG1) return FFDAS_ERROR_INVALID_ARGUMENT;
+    } else {
+        if (f64 && a.alg != FFDAS_ALG_DEFAULT && a.alg != FFDAS_ALG1) return FFDAS_ERROR_UNSUPPORTED_TYPE;
+        if (a.alg != FFDAS_ALG_DEFAULT && a.alg != FFDAS_ALG1 && a.alg != FFDAS_ALG2 && a.alg != FFDAS_ALG4)
+            return FFDAS_ERROR_INVALID_ARGUMENT;
+    }
+
+    das_problem pb;
+    FFDAS_TRY(make_problem(xd, od, pb));
+    if (a.sparse) {
+        if (a.sparse_count <= 0) return FFDAS_ERROR_INVALID_ARGUMENT;
+        pb.n_events = a.sparse_count;
+        pb.sparse = true;
+    } else {
+        pb.n_events = pb.S;
+    }
+    if (kind < 0) return FFDAS_ERROR_UNSUPPORTED_TYPE;
+    if (pb.N >= (1 << 22)) return FFDAS_ERROR_DIMS_TOO_LARGE;  // floor split is exact below 2^22
+
+    if (pb.V == 0 || pb.B == 0) return FFDAS_SUCCESS;
+    if (!a.out || !a.dstpos || !a.offsets || !a.weights) return FFDAS_ERROR_NULL_POINTER;
+    if (pb.C > 0 && !a.srcpos) return FFDAS_ERROR_NULL_POINTER;
+    if ((int64_t)pb.B * pb.C * pb.S * pb.N > 0 && !a.x) return FFDAS_ERROR_NULL_POINTER;
+    if (a.sparse && !a.sparse_indices) return FFDAS_ERROR_NULL_POINTER;
+
+    // ---- ingest: x -> pair rows (workspace) ----
+    const int64_t npad = std::max<int64_t>(2, ((int64_t)pb.N + 1) & ~int64_t(1));
+    const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
+    workspace P(h);
+    FFDAS_TRY(P.alloc((size_t)std::max<int64_t>(rows, 1) * npad * storage_bytes(kind)));
+    FFDAS_TRY(launch_ingest(h, pb, xd.dtype, kind, a.x, npad, P.get<void>()));
+
+    // ---- forward kernel ----
+    const schedule s = plan_schedule(h, pb, kind);
+    gather_params gp;
+    std::memset(&gp, 0, sizeof(gp));
+    gp.P = P.get<void>();
+    gp.npad = npad;
+    gp.C = pb.C;
+    gp.S = pb.S;
+    gp.n_events = pb.n_events;
+    gp.B = pb.B;
+    gp.V = pb.V;
+    gp.D0 = pb.D0; gp.D1 = pb.D1; gp.D2 = pb.D2;
+    gp.T0 = s.T0; gp.T1 = s.T1; gp.T2 = s.T2;
+    gp.n0 = (pb.D0 + s.T0 - 1) / s.T0;
+    gp.n1 = (pb.D1 + s.T1 - 1) / s.T1;
+    const int n2 = (pb.D2 + s.T2 - 1) / s.T2;
+    gp.srcpos = a.srcpos;
+    gp.srcdir = reinterpret_cast<const float4 *>(a.srcdir);
+    gp.dstpos = a.dstpos;
+    gp.offsets = a.offsets;
+    gp.weights = a.weights;
+    gp.sparse_idx = a.sparse_indices;
+    gp.wavenum = a.wavenum;
+    gp.out = a.out;
+    gp.out_bstride = pb.out_bstride;
+    read_beta(od.dtype, a.beta, gp.beta_re, gp.beta_im, gp.beta_zero);
+
+    const int64_t tiles = (int64_t)gp.n0 * gp.n1 * n2;
+    const int bchunks = (pb.B + s.BT - 1) / s.BT;
+    if (tiles > INT32_MAX || bchunks > 65535) return FFDAS_ERROR_DIMS_TOO_LARGE;
+    dim3 grid((unsigned)tiles, (unsigned)bchunks);
+
+    h.last = ffdas_kernel_info_t{};
+    h.last.variant = 1;
+    h.last.tile_x = s.T0; h.last.tile_y = s.T1; h.last.tile_z = s.T2;
+    h.last.batch_tile = s.BT;
+    h.last.event_chunk = s.SC;
+    h.last.storage = kind;
+    h.last.kernels = 2;
+    h.last.grid = tiles * bchunks;
+
+    h.mark_start();
+    const ffdas_error_t err = a.sparse ? launch_gather<true>(h, kind, od.dtype, gp, s, grid)
+                                       : launch_gather<false>(h, kind, od.dtype, gp, s, grid);
+    h.mark_stop();
+    return err;
+}
+
+}  // namespace ffdas
+
+using namespace ffdas;
+
+static ffdas_error_t das_entry(ffdas_handle_t handle, das_call &a) {
+    if (!handle) return FFDAS_ERROR_INVALID_HANDLE;
+    FFDAS_TRY(handle->check_device());
+    if (!a.x_desc || !a.out_desc) return FFDAS_ERROR_NULL_POINTER;
+    return das_forward(*handle, a);
+}
+
+extern "C" {
+
+ffdas_error_t ffdas_das(ffdas_handle_t handle, const float *srcpos, const float *srcdir,
+                        float wavenum, ffdas_tensor_desc_t x_desc, const void *x,
+                        const float *dstpos, const float *offsets, const float *weights,
+                        const void *beta, ffdas_tensor_desc_t out_desc, void *out,
+                        ffdas_compute_type_t compute_type, ffdas_alg_t alg) {
+    das_call a;
+    a.srcpos = srcpos; a.srcdir = srcdir; a.wavenum = wavenum;
+    a.x_desc = x_desc; a.x = x; a.dstpos = dstpos; a.offsets = offsets; a.weights = weights;
+    a.beta = beta; a.out_desc = out_desc; a.out = out;
+    a.compute_type = compute_type; a.alg = alg; a.sparse = false;
+    return das_entry(handle, a);
+}
+
+ffdas_error_t ffdas_das_sparse(ffdas_handle_t handle, const float *srcpos, const float *srcdir,
+                               float wavenum, ffdas_tensor_desc_t x_desc, const void *x,
+                               const float *dstpos, const float *offsets, const float *weights,
+                               int sparse_count, const int *sparse_indices, const void *beta,
+                               ffdas_tensor_desc_t out_desc, void *out,
+                               ffdas_compute_type_t compute_type, ffdas_alg_t alg) {
+    das_call a;
+    a.srcpos = srcpos; a.srcdir = srcdir; a.wavenum = wavenum;
+    a.x_desc = x_desc; a.x = x; a.dstpos = dstpos; a.offsets = offsets; a.weights = weights;
+    a.sparse_count = sparse_count; a.sparse_indices = sparse_indices;
+    a.beta = beta; a.out_desc = out_desc; a.out = out;
+    a.compute_type = compute_type; a.alg = alg; a.sparse = true;
+    return das_entry(handle, a);
+}
+
+}  // extern "C"

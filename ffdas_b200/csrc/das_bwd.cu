@@ -1,0 +1,381 @@
+// das_bwd.cu -- ffdas_das_backward: adjoint of the delay-and-sum forward.
+//
+// For each unit (b, v, c, e) the forward adds w * L with
+//   L = x0 + t d,  d = x1 - x0,  t = tau - floor(tau),  tau = ofs[e,v] + r(v,c)
+// so, with g = dLoss/dout[b,v]:
+//   dLoss/dweights[e,v] += g L
+//   dLoss/doffsets[e,v] += g w d               (slope of the interpolant)
+//   dLoss/ddstpos[v]    += g w d (v - c) / r
+//   dLoss/dsrcpos[c]    -= g w d (v - c) / r
+//   dLoss/dx[b,c,s,k]   += g w (1 - t),  dLoss/dx[b,c,s,k+1] += g w t
+// One kernel recomputes (k, t) from the same pair rows the forward reads (no
+// stored indices), keeps the per-voxel gradients in registers, and scatters
+// the channel-data adjoint through a shared-memory window per (channel,
+// event) that is flushed to global memory with one red.add per touched
+// sample.  Voxel tiles are the forward's compact tiles, so a window covers
+// only the few tens of samples the tile's voxels touch.
+#include <algorithm>
+#include <climits>
+#include <cstring>
+
+#include "core.h"
+#include "das_problem.h"
+#include "das_pairs.cuh"
+
+namespace ffdas {
+
+struct bwd_params {
+    const void *P;
+    int64_t npad;
+    int C, S, N, n_events, B;
+    int64_t V;
+    int D0, D1, D2, T0, T1, T2, n0, n1;
+    const float *srcpos, *dstpos, *offsets, *weights;
+    const int *sparse_idx;
+    const float *gout;          // (B, V) with batch stride gout_bstride
+    int64_t gout_bstride;
+    float *gx;                  // (B, C, S, N) contiguous
+    float *goff, *gw, *gdst, *gsrc;
+};
+
+constexpr int kBwdThreads = 256;
+constexpr int kBwdWin = 128;   // samples per shared window (per event, per batch item)
+
+template <int K, int BT, int SC, bool SPARSE>
+__global__ void __launch_bounds__(kBwdThreads) das_bwd_kernel(const bwd_params p) {
+    using tr = pair_traits<K>;
+    using st = typename tr::storage;
+    __shared__ float win[SC][BT][kBwdWin];
+    __shared__ int kmin_s[SC], kmax_s[SC];
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int tile = blockIdx.x;
+    const int t0 = tile % p.n0, t1 = (tile / p.n0) % p.n1, t2 = tile / (p.n0 * p.n1);
+    const int i0 = tid % p.T0, i1 = (tid / p.T0) % p.T1, i2 = tid / (p.T0 * p.T1);
+    const int g0 = t0 * p.T0 + i0, g1 = t1 * p.T1 + i1, g2 = t2 * p.T2 + i2;
+    const bool active = (g0 < p.D0 && g1 < p.D1 && g2 < p.D2);
+    const int64_t v = active ? ((int64_t)g2 * p.D1 + g1) * p.D0 + g0 : 0;
+    const int b0 = blockIdx.y * BT;
+    const bool do_gx = p.gx != nullptr;
+    // A CTA that owns several batch chunks writes the voxel-side gradients
+    // only from chunk 0 after reducing across chunks with atomics; with one
+    // chunk it stores them directly.
+    const bool multi_chunk = gridDim.y > 1;
+
+    for (int i = tid; i < SC * BT * kBwdWin; i += kBwdThreads) (&win[0][0][0])[i] = 0.f;
+    if (tid < SC) { kmin_s[tid] = INT_MAX; kmax_s[tid] = INT_MIN; }
+    __syncthreads();
+
+    float vx = 0.f, vy = 0.f, vz = 0.f;
+    if (active) {
+        vx = __ldg(p.dstpos + 3 * v); vy = __ldg(p.dstpos + 3 * v + 1); vz = __ldg(p.dstpos + 3 * v + 2);
+    }
+    float g[BT];
+#pragma unroll
+    for (int b = 0; b < BT; b++)
+        g[b] = (active && b0 + b < p.B) ? __ldg(p.gout + (int64_t)(b0 + b) * p.gout_bstride + v) : 0.f;
+
+    const st *__restrict__ P = static_cast<const st *>(p.P);
+    const uint32_t kmax_pair = (uint32_t)(p.npad - 1);
+    const int64_t row_b = (int64_t)p.C * p.S * p.npad;
+    float gpx = 0.f, gpy = 0.f, gpz = 0.f;
+
+    for (int e0 = 0; e0 < p.n_events; e0 += SC) {
+        const int sc = min(SC, p.n_events - e0);
+        float ofs[SC], w[SC], gwa[SC], goa[SC];
+        int srow[SC];
+#pragma unroll
+        for (int j = 0; j < SC; j++) {
+            gwa[j] = 0.f; goa[j] = 0.f;
+            if (active && j < sc) {
+                const int64_t idx = (int64_t)(e0 + j) * p.V + v;
+                ofs[j] = __ldg(p.offsets + idx);
+                w[j] = __ldg(p.weights + idx);
+                int s = e0 + j;
+                if constexpr (SPARSE) {
+                    s = __ldg(p.sparse_idx + idx);
+                    if ((unsigned)s >= (unsigned)p.S) { s = 0; w[j] = 0.f; ofs[j] = 1e30f; }
+                }
+                srow[j] = s;
+            } else {
+                ofs[j] = 1e30f; w[j] = 0.f; srow[j] = 0;
+            }
+        }
+
+        for (int c = 0; c < p.C; c++) {
+            const float cx = __ldg(p.srcpos + 3 * c), cy = __ldg(p.srcpos + 3 * c + 1),
+                        cz = __ldg(p.srcpos + 3 * c + 2);
+            const recv_geom gm = receive_geometry(vx, vy, vz, cx, cy, cz);
+            const st *Pc = P + (int64_t)c * p.S * p.npad;
+            float q = 0.f;      // sum_j w_j sum_b g_b d_b  (for the position gradients)
+            uint32_t kk[SC];
+            float tt[SC];
+#pragma unroll
+            for (int j = 0; j < SC; j++) {
+                const float tau = __fmaf_rn(gm.rsq, gm.rinv, ofs[j]);
+                const tau_split ts = split_tau(tau);
+                kk[j] = ts.k;
+                tt[j] = ts.t;
+                if (j < sc) {
+                    const uint32_t k = min(ts.k, kmax_pair);
+                    const st *row = Pc + (int64_t)srow[j] * p.npad + k;
+                    float gl = 0.f, gd = 0.f;
+#pragma unroll
+                    for (int b = 0; b < BT; b++) {
+                        if (b0 + b < p.B) {
+                            const st pr = row[(int64_t)(b0 + b) * row_b];
+                            const float L = tr::tap(pr, ts.t);
+                            const float d = tr::slope(pr);
+                            gl = __fmaf_rn(g[b], L, gl);
+                            gd = __fmaf_rn(g[b], d, gd);
+                        }
+                    }
+                    gwa[j] += gl;
+                    goa[j] = __fmaf_rn(w[j], gd, goa[j]);
+                    q = __fmaf_rn(w[j], gd, q);
+                }
+            }
+            // position gradients: d r / d v = (v - c) / r
+            const float qr = q * gm.rinv;
+            const float ex = (vx - cx) * qr, ey = (vy - cy) * qr, ez = (vz - cz) * qr;
+            gpx += ex; gpy += ey; gpz += ez;
+            if (p.gsrc) {
+                float sx = -ex, sy = -ey, sz = -ez;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    sx += __shfl_xor_sync(0xffffffffu, sx, o);
+                    sy += __shfl_xor_sync(0xffffffffu, sy, o);
+                    sz += __shfl_xor_sync(0xffffffffu, sz, o);
+                }
+                if (lane == 0 && (sx != 0.f || sy != 0.f || sz != 0.f)) {
+                    atomicAdd(p.gsrc + 3 * c, sx);
+                    atomicAdd(p.gsrc + 3 * c + 1, sy);
+                    atomicAdd(p.gsrc + 3 * c + 2, sz);
+                }
+            }
+            if (!do_gx) continue;
+
+            // ---- channel-data adjoint: two-tap scatter ----
+            if constexpr (SPARSE) {
+                // event rows differ per voxel: scatter straight to global memory
+#pragma unroll
+                for (int j = 0; j < SC; j++) {
+                    if (j < sc && kk[j] < (uint32_t)(p.N - 1) && w[j] != 0.f) {
+#pragma unroll
+                        for (int b = 0; b < BT; b++) {
+                            if (b0 + b < p.B && g[b] != 0.f) {
+                                float *gr = p.gx + (((int64_t)(b0 + b) * p.C + c) * p.S + srow[j]) * p.N + kk[j];
+                                const float a = g[b] * w[j];
+                                atomicAdd(gr, a - a * tt[j]);
+                                atomicAdd(gr + 1, a * tt[j]);
+                            }
+                        }
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < SC; j++) {
+                    const bool valid = active && j < sc && kk[j] < (uint32_t)(p.N - 1);
+                    int lo = valid ? (int)kk[j] : INT_MAX;
+                    int hi = valid ? (int)kk[j] : INT_MIN;
+                    lo = __reduce_min_sync(0xffffffffu, lo);
+                    hi = __reduce_max_sync(0xffffffffu, hi);
+                    if (lane == 0 && lo != INT_MAX) {
+                        atomicMin(&kmin_s[j], lo);
+                        atomicMax(&kmax_s[j], hi);
+                    }
+                }
+                __syncthreads();
+#pragma unroll
+                for (int j = 0; j < SC; j++) {
+                    const bool valid = active && j < sc && kk[j] < (uint32_t)(p.N - 1) && w[j] != 0.f;
+                    if (!valid) continue;
+                    const int base = kmin_s[j];
+                    const bool fits = (kmax_s[j] - base + 2) <= kBwdWin;
+                    const int rel = (int)kk[j] - base;
+#pragma unroll
+                    for (int b = 0; b < BT; b++) {
+                        if (b0 + b < p.B) {
+                            const float a = g[b] * w[j];
+                            const float a1 = a * tt[j];
+                            if (fits) {
+                                atomicAdd(&win[j][b][rel], a - a1);
+                                atomicAdd(&win[j][b][rel + 1], a1);
+                            } else {
+                                float *gr = p.gx + (((int64_t)(b0 + b) * p.C + c) * p.S + (e0 + j)) * p.N + kk[j];
+                                atomicAdd(gr, a - a1);
+                                atomicAdd(gr + 1, a1);
+                            }
+                        }
+                    }
+                }
+                __syncthreads();
+                // flush the windows
+                for (int j = 0; j < sc; j++) {
+                    const int base = kmin_s[j];
+                    if (base == INT_MAX) continue;
+                    const int wlen = kmax_s[j] - base + 2;
+                    if (wlen > kBwdWin) continue;
+                    for (int i = tid; i < BT * wlen; i += kBwdThreads) {
+                        const int b = i / wlen, r = i - b * wlen;
+                        const float val = win[j][b][r];
+                        if (val != 0.f) {
+                            win[j][b][r] = 0.f;
+                            atomicAdd(p.gx + (((int64_t)(b0 + b) * p.C + c) * p.S + (e0 + j)) * p.N + base + r, val);
+                        }
+                    }
+                }
+                __syncthreads();
+                if (tid < SC) { kmin_s[tid] = INT_MAX; kmax_s[tid] = INT_MIN; }
+            }
+        }
+        if (active) {
+#pragma unroll
+            for (int j = 0; j < SC; j++) {
+                if (j < sc) {
+                    const int64_t idx = (int64_t)(e0 + j) * p.V + v;
+                    if (multi_chunk) {
+                        if (p.gw) atomicAdd(p.gw + idx, gwa[j]);
+                        if (p.goff) atomicAdd(p.goff + idx, goa[j]);
+                    } else {
+                        if (p.gw) p.gw[idx] = gwa[j];
+                        if (p.goff) p.goff[idx] = goa[j];
+                    }
+                }
+            }
+        }
+    }
+    if (active && p.gdst) {
+        if (multi_chunk) {
+            atomicAdd(p.gdst + 3 * v, gpx); atomicAdd(p.gdst + 3 * v + 1, gpy); atomicAdd(p.gdst + 3 * v + 2, gpz);
+        } else {
+            p.gdst[3 * v] = gpx; p.gdst[3 * v + 1] = gpy; p.gdst[3 * v + 2] = gpz;
+        }
+    }
+}
+
+template <int K, int BT, bool SPARSE>
+static ffdas_error_t launch_bwd_t(ffdas_context &h, const bwd_params &bp, dim3 grid) {
+    das_bwd_kernel<K, BT, 8, SPARSE><<<grid, kBwdThreads, 0, h.stream>>>(bp);
+    return ffdas_launch_check(h.stream);
+}
+
+template <int K, bool SPARSE>
+static ffdas_error_t launch_bwd_k(ffdas_context &h, const bwd_params &bp, int BT, dim3 grid) {
+    switch (BT) {
+        case 1: return launch_bwd_t<K, 1, SPARSE>(h, bp, grid);
+        case 2: return launch_bwd_t<K, 2, SPARSE>(h, bp, grid);
+        default: return launch_bwd_t<K, 4, SPARSE>(h, bp, grid);
+    }
+}
+
+// defined in das.cu
+ffdas_error_t ingest_for_backward(ffdas_context &h, const das_problem &pb, ffdas_datatype_t xt, int kind,
+                                  const void *x, int64_t npad, void *P);
+
+ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tensor_desc &gd,
+                           const void *gout, float *gx, float *goff, float *gw, float *gdst, float *gsrc) {
+    const ffdas_tensor_desc &xd = *a.x_desc;
+    if (a.srcdir != nullptr || a.wavenum != 0.f) return FFDAS_ERROR_INVALID_ARGUMENT;
+    if (gd.dtype != FFDAS_R_32F) return FFDAS_ERROR_UNSUPPORTED_TYPE;
+    const int kind = select_storage(xd.dtype, FFDAS_R_32F, a.compute_type);
+    if (kind != ST_F32 && kind != ST_F16 && kind != ST_BF16) return FFDAS_ERROR_UNSUPPORTED_TYPE;
+    if (!fits_int32_indexing(xd) || !fits_int32_indexing(gd)) return FFDAS_ERROR_INVALID_DIMS;
+    das_problem pb;
+    FFDAS_TRY(make_problem(xd, gd, pb));
+    if (a.sparse) {
+        if (a.sparse_count <= 0) return FFDAS_ERROR_INVALID_ARGUMENT;
+        if (!a.sparse_indices) return FFDAS_ERROR_NULL_POINTER;
+        pb.n_events = a.sparse_count;
+    } else {
+        pb.n_events = pb.S;
+    }
+    if (pb.N >= (1 << 22)) return FFDAS_ERROR_DIMS_TOO_LARGE;
+    if (pb.V == 0 || pb.B == 0) return FFDAS_SUCCESS;
+    if (!gout || !a.dstpos || !a.offsets || !a.weights || (pb.C > 0 && !a.srcpos)) return FFDAS_ERROR_NULL_POINTER;
+    if (!gx && !goff && !gw && !gdst && !gsrc) return FFDAS_SUCCESS;
+
+    const int64_t npad = std::max<int64_t>(2, ((int64_t)pb.N + 1) & ~int64_t(1));
+    const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
+    const size_t sb = (kind == ST_F32) ? 8 : 4;
+    workspace P(h);
+    FFDAS_TRY(P.alloc((size_t)std::max<int64_t>(rows, 1) * npad * sb));
+    FFDAS_TRY(ingest_for_backward(h, pb, xd.dtype, kind, a.x, npad, P.get<void>()));
+
+    bwd_params bp;
+    std::memset(&bp, 0, sizeof(bp));
+    bp.P = P.get<void>();
+    bp.npad = npad;
+    bp.C = pb.C; bp.S = pb.S; bp.N = pb.N; bp.n_events = pb.n_events; bp.B = pb.B; bp.V = pb.V;
+    bp.D0 = pb.D0; bp.D1 = pb.D1; bp.D2 = pb.D2;
+    if (pb.D1 <= 1) { bp.T0 = 256; bp.T1 = 1; bp.T2 = 1; }
+    else if (pb.D0 >= 16 && pb.D1 >= 16) { bp.T0 = 16; bp.T1 = 16; bp.T2 = 1; }
+    else if (pb.D0 >= 32) { bp.T0 = 32; bp.T1 = 8; bp.T2 = 1; }
+    else {
+        int t = 1;
+        while (t * 2 <= pb.D0) t *= 2;
+        bp.T0 = t; bp.T1 = 256 / t; bp.T2 = 1;
+    }
+    bp.n0 = (pb.D0 + bp.T0 - 1) / bp.T0;
+    bp.n1 = (pb.D1 + bp.T1 - 1) / bp.T1;
+    const int n2 = (pb.D2 + bp.T2 - 1) / bp.T2;
+    bp.srcpos = a.srcpos; bp.dstpos = a.dstpos; bp.offsets = a.offsets; bp.weights = a.weights;
+    bp.sparse_idx = a.sparse ? a.sparse_indices : nullptr;
+    bp.gout = static_cast<const float *>(gout);
+    bp.gout_bstride = pb.out_bstride;
+    bp.gx = gx; bp.goff = goff; bp.gw = gw; bp.gdst = gdst; bp.gsrc = gsrc;
+
+    const int BT = pb.B >= 4 ? 4 : (pb.B >= 2 ? 2 : 1);
+    const int bchunks = (pb.B + BT - 1) / BT;
+    const int64_t tiles = (int64_t)bp.n0 * bp.n1 * n2;
+    if (tiles > INT32_MAX || bchunks > 65535) return FFDAS_ERROR_DIMS_TOO_LARGE;
+    // outputs reduced with atomics must start at zero
+    const size_t ve = (size_t)pb.n_events * pb.V * sizeof(float);
+    if (bchunks > 1) {
+        if (gw) FFDAS_CUDA(cudaMemsetAsync(gw, 0, ve, h.stream));
+        if (goff) FFDAS_CUDA(cudaMemsetAsync(goff, 0, ve, h.stream));
+        if (gdst) FFDAS_CUDA(cudaMemsetAsync(gdst, 0, (size_t)pb.V * 3 * sizeof(float), h.stream));
+    }
+    if (gsrc) FFDAS_CUDA(cudaMemsetAsync(gsrc, 0, (size_t)pb.C * 3 * sizeof(float), h.stream));
+
+    dim3 grid((unsigned)tiles, (unsigned)bchunks);
+    h.last = ffdas_kernel_info_t{};
+    h.last.variant = 3;
+    h.last.tile_x = bp.T0; h.last.tile_y = bp.T1; h.last.tile_z = bp.T2;
+    h.last.batch_tile = BT; h.last.event_chunk = 8; h.last.storage = kind;
+    h.last.kernels = 2; h.last.grid = tiles * bchunks;
+    const bool sp = a.sparse;
+    ffdas_error_t err;
+    h.mark_start();
+    switch (kind) {
+        case ST_F32: err = sp ? launch_bwd_k<ST_F32, true>(h, bp, BT, grid) : launch_bwd_k<ST_F32, false>(h, bp, BT, grid); break;
+        case ST_F16: err = sp ? launch_bwd_k<ST_F16, true>(h, bp, BT, grid) : launch_bwd_k<ST_F16, false>(h, bp, BT, grid); break;
+        default: err = sp ? launch_bwd_k<ST_BF16, true>(h, bp, BT, grid) : launch_bwd_k<ST_BF16, false>(h, bp, BT, grid); break;
+    }
+    h.mark_stop();
+    return err;
+}
+
+}  // namespace ffdas
+
+using namespace ffdas;
+
+extern "C" ffdas_error_t ffdas_das_backward(
+    ffdas_handle_t handle, const float *srcpos, const float *srcdir, float wavenum,
+    ffdas_tensor_desc_t x_desc, const void *x, const float *dstpos, const float *offsets,
+    const float *weights, int sparse_count, const int *sparse_indices,
+    ffdas_tensor_desc_t grad_out_desc, const void *grad_out, float *grad_x, float *grad_offsets,
+    float *grad_weights, float *grad_dstpos, float *grad_srcpos) {
+    if (!handle) return FFDAS_ERROR_INVALID_HANDLE;
+    FFDAS_TRY(handle->check_device());
+    if (!x_desc || !grad_out_desc) return FFDAS_ERROR_NULL_POINTER;
+    das_call a;
+    a.srcpos = srcpos; a.srcdir = srcdir; a.wavenum = wavenum; a.x_desc = x_desc; a.x = x;
+    a.dstpos = dstpos; a.offsets = offsets; a.weights = weights;
+    a.sparse = sparse_indices != nullptr;
+    a.sparse_count = sparse_count; a.sparse_indices = sparse_indices;
+    a.compute_type = FFDAS_COMPUTE_DEFAULT;
+    return das_backward(*handle, a, *grad_out_desc, grad_out, grad_x, grad_offsets, grad_weights,
+                        grad_dstpos, grad_srcpos);
+}

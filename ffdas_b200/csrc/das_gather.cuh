@@ -1,0 +1,209 @@
+// das_gather.cuh -- forward delay-and-sum, L1 gather schedule.
+//
+// One thread = one voxel x BT batch items.  A CTA is a spatially compact tile
+// of voxels (tile_x x tile_y x tile_z over the output grid), so the warps of a
+// CTA read the same narrow sample window of each (channel, event) row and the
+// pair loads hit in L1.  Per (voxel, channel) the receive geometry (rsq,
+// rsqrt) is computed once and reused for every event and batch item; per
+// (voxel, channel, event) the delay is one FFMA, the floor/fraction split is
+// three FADDs, and each batch item costs one 8-byte (f32) or 4-byte (f16/bf16)
+// load, one tap FFMA and one accumulate FFMA.
+//
+// Follows the arithmetic of das_alg1_kernel (src/das/das_alg1_kernels.cuh:
+// 16-107): same tau, same floor split, same lerp and the same FFMA
+// accumulation; only the order of the sum over (channel, event) differs.
+#pragma once
+
+#include "das_pairs.cuh"
+
+namespace ffdas {
+
+struct gather_params {
+    const void *P;            // pair rows [B][C][S][Npad]
+    int64_t npad;             // pairs per row
+    int C, S;                 // channels, events in x
+    int n_events;             // S (dense) or sparse_count
+    int B;                    // batch
+    int64_t V;                // voxels
+    int D0, D1, D2;           // output grid (D0 innermost)
+    int T0, T1, T2;           // tile extents (T0*T1*T2 == blockDim.x)
+    int n0, n1;               // tiles along D0, D1
+    const float *srcpos;      // (C,3)
+    const float4 *srcdir;     // (C,4) or null
+    const float *dstpos;      // (V,3)
+    const float *offsets;     // (n_events, V)
+    const float *weights;     // (n_events, V)
+    const int *sparse_idx;    // (n_events, V) or null
+    float wavenum;
+    void *out;
+    int64_t out_bstride;      // elements between batch items of out
+    double beta_re, beta_im;
+    int beta_zero;
+};
+
+template <typename A> struct acc_ops;
+template <> struct acc_ops<float> {
+    __device__ static float zero() { return 0.f; }
+};
+template <> struct acc_ops<double> {
+    __device__ static double zero() { return 0.0; }
+};
+template <> struct acc_ops<float2> {
+    __device__ static float2 zero() { return make_float2(0.f, 0.f); }
+};
+template <> struct acc_ops<double2> {
+    __device__ static double2 zero() { return make_double2(0.0, 0.0); }
+};
+
+// cuCfmaf ordering (reference cmadd for float2, src/core/math/vector.cuh:150)
+__device__ __forceinline__ float2 cfma(float2 x, float2 y, float2 z) {
+    float re = __fmaf_rn(-x.y, y.y, __fmaf_rn(x.x, y.x, z.x));
+    float im = __fmaf_rn(x.y, y.x, __fmaf_rn(x.x, y.y, z.y));
+    return make_float2(re, im);
+}
+// reference cmadd for double2 (src/core/math/vector.cuh:156-160)
+__device__ __forceinline__ double2 cfma(double2 x, double2 y, double2 z) {
+    return make_double2(fma(x.x, y.x, z.x) - x.y * y.y, fma(x.x, y.y, z.y) + x.y * y.x);
+}
+
+// acc += w * v (real) or acc += w * exp(i wavenum tau) * v (complex)
+template <int K>
+__device__ __forceinline__ void accumulate(typename pair_traits<K>::acc &acc,
+                                           typename pair_traits<K>::value v, float w,
+                                           float wavenum, float tau) {
+    if constexpr (K == ST_F32 || K == ST_F16 || K == ST_BF16) {
+        acc = __fmaf_rn(w, v, acc);
+    } else if constexpr (K == ST_F64) {
+        acc = fma((double)w, v, acc);
+    } else if constexpr (K == ST_C32 || K == ST_C16) {
+        float sn, cs;
+        __sincosf(wavenum * tau, &sn, &cs);
+        acc = cfma(make_float2(cs * w, sn * w), v, acc);
+    } else {
+        float sn, cs;
+        __sincosf(wavenum * tau, &sn, &cs);
+        acc = cfma(make_double2((double)(cs * w), (double)(sn * w)), v, acc);
+    }
+}
+
+template <typename A> __device__ __forceinline__ void store_out(A *o, A acc, const gather_params &p);
+template <> __device__ __forceinline__ void store_out<float>(float *o, float acc, const gather_params &p) {
+    *o = p.beta_zero ? acc : __fmaf_rn((float)p.beta_re, *o, acc);
+}
+template <> __device__ __forceinline__ void store_out<double>(double *o, double acc, const gather_params &p) {
+    *o = p.beta_zero ? acc : fma(p.beta_re, *o, acc);
+}
+template <> __device__ __forceinline__ void store_out<float2>(float2 *o, float2 acc, const gather_params &p) {
+    *o = p.beta_zero ? acc : cfma(make_float2((float)p.beta_re, (float)p.beta_im), *o, acc);
+}
+template <> __device__ __forceinline__ void store_out<double2>(double2 *o, double2 acc, const gather_params &p) {
+    *o = p.beta_zero ? acc : cfma(make_double2(p.beta_re, p.beta_im), *o, acc);
+}
+
+// Output element type for a storage kind and output dtype: the kernel
+// accumulates in pair_traits<K>::acc and converts on store.
+template <int K, typename OutT, int BT, int SC, bool SPARSE>
+__global__ void __launch_bounds__(256) das_gather_kernel(const gather_params p) {
+    using tr = pair_traits<K>;
+    using st = typename tr::storage;
+    using acc_t = typename tr::acc;
+
+    const int tid = threadIdx.x;
+    const int tile = blockIdx.x;
+    const int t0 = tile % p.n0;
+    const int t1 = (tile / p.n0) % p.n1;
+    const int t2 = tile / (p.n0 * p.n1);
+    const int i0 = tid % p.T0;
+    const int i1 = (tid / p.T0) % p.T1;
+    const int i2 = tid / (p.T0 * p.T1);
+    const int g0 = t0 * p.T0 + i0, g1 = t1 * p.T1 + i1, g2 = t2 * p.T2 + i2;
+    if (g0 >= p.D0 || g1 >= p.D1 || g2 >= p.D2) return;
+    const int64_t v = ((int64_t)g2 * p.D1 + g1) * p.D0 + g0;
+    const int b0 = blockIdx.y * BT;
+
+    const float vx = __ldg(p.dstpos + 3 * v + 0);
+    const float vy = __ldg(p.dstpos + 3 * v + 1);
+    const float vz = __ldg(p.dstpos + 3 * v + 2);
+
+    const st *__restrict__ P = static_cast<const st *>(p.P);
+    const uint32_t kmax = (uint32_t)(p.npad - 1);
+    const int64_t row_stride_b = (int64_t)p.C * p.S * p.npad;  // pairs per batch item
+
+    acc_t acc[BT];
+#pragma unroll
+    for (int b = 0; b < BT; b++) acc[b] = acc_ops<acc_t>::zero();
+
+    for (int e0 = 0; e0 < p.n_events; e0 += SC) {
+        const int sc = min(SC, p.n_events - e0);
+        float ofs[SC], w[SC];
+        int srow[SC];
+#pragma unroll
+        for (int j = 0; j < SC; j++) {
+            if (j < sc) {
+                const int64_t idx = (int64_t)(e0 + j) * p.V + v;
+                ofs[j] = __ldg(p.offsets + idx);
+                w[j] = __ldg(p.weights + idx);
+                if constexpr (SPARSE) {
+                    int s = __ldg(p.sparse_idx + idx);
+                    // an out-of-range event index contributes nothing
+                    if ((unsigned)s >= (unsigned)p.S) { w[j] = 0.f; s = 0; }
+                    srow[j] = s;
+                } else {
+                    srow[j] = e0 + j;
+                }
+            } else {
+                ofs[j] = 0.f;
+                w[j] = 0.f;
+                srow[j] = 0;
+            }
+        }
+
+        for (int c = 0; c < p.C; c++) {
+            const float cx = __ldg(p.srcpos + 3 * c + 0);
+            const float cy = __ldg(p.srcpos + 3 * c + 1);
+            const float cz = __ldg(p.srcpos + 3 * c + 2);
+            recv_geom g = receive_geometry(vx, vy, vz, cx, cy, cz);
+            if (p.srcdir) apply_directivity(g, vx, vy, vz, cx, cy, cz, __ldg(p.srcdir + c));
+            const st *Pc = P + (int64_t)c * p.S * p.npad;
+
+#pragma unroll
+            for (int j = 0; j < SC; j++) {
+                if (j < sc) {
+                    if constexpr (SPARSE) {
+                        if (w[j] == 0.f) continue;  // padded entry of an uneven subset
+                    }
+                    const float tau = __fmaf_rn(g.rsq, g.rinv, ofs[j]);
+                    const tau_split ts = split_tau(tau);
+                    const uint32_t k = min(ts.k, kmax);
+                    const st *row = Pc + (int64_t)srow[j] * p.npad + k;
+#pragma unroll
+                    for (int b = 0; b < BT; b++) {
+                        if (BT == 1 || b0 + b < p.B) {
+                            const st pr = row[(int64_t)(b0 + b) * row_stride_b];
+                            accumulate<K>(acc[b], tr::tap(pr, ts.t), w[j], p.wavenum, tau);
+                        }
+                    }
+                }
+            }
+        }
+    }
+
+    OutT *out = static_cast<OutT *>(p.out);
+#pragma unroll
+    for (int b = 0; b < BT; b++) {
+        if (BT == 1 || b0 + b < p.B) {
+            OutT *o = out + (int64_t)(b0 + b) * p.out_bstride + v;
+            if constexpr (sizeof(OutT) == sizeof(acc_t)) {
+                store_out<OutT>(o, acc[b], p);
+            } else if constexpr (sizeof(OutT) == 8 && sizeof(acc_t) == 4) {
+                store_out<double>(reinterpret_cast<double *>(o), (double)acc[b], p);
+            } else {
+                // complex float accumulation stored to complex double
+                store_out<double2>(reinterpret_cast<double2 *>(o),
+                                   make_double2(acc[b].x, acc[b].y), p);
+            }
+        }
+    }
+}
+
+}  // namespace ffdas

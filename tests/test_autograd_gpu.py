@@ -1,0 +1,133 @@
+"""Backward kernels: adjoint dot-product test, FP64 finite differences, and
+gradients against the pure-torch float64 reference (tests/torch_ref.py).
+
+Tolerances: adjoint identity 1e-5 (relative, fp32 accumulation);
+gradients vs float64 reference 2e-4 relative L2; finite differences
+(central, h = 1e-4, float64 reference forward) 2e-3 relative per entry
+against the GPU gradient (the interpolant is piecewise linear in the delay,
+so entries whose perturbation crosses a sample boundary are skipped).
+"""
+import numpy as np
+import pytest
+import torch
+
+import ffdas_b200
+from ffdas_b200 import workloads as W
+from ffdas_b200.autograd import das_autograd
+from oracle import oracle
+from tests.torch_ref import das_ref
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+
+
+def _problem(seed=0, B=2, C=6, S=3, N=128, nz=9, nx=7):
+    g = torch.Generator().manual_seed(seed)
+    x = torch.randn((B, C, S, N), generator=g)
+    src = torch.zeros((C, 3))
+    src[:, 0] = torch.linspace(-3, 3, C)
+    zz, xx = torch.meshgrid(torch.linspace(20, 45, nz), torch.linspace(-4, 4, nx), indexing="ij")
+    dst = torch.stack([xx, torch.zeros_like(xx), zz], -1)
+    offs = torch.rand((S, nz, nx), generator=g) * 30 + 5
+    w = torch.rand((S, nz, nx), generator=g) + 0.2
+    return x, src, dst, offs, w
+
+
+def test_adjoint_dot_product():
+    x, src, dst, offs, w = (t.to(DEV) for t in _problem(1, B=3))
+    xg = x.clone().requires_grad_(True)
+    y = torch.randn((x.shape[0], *dst.shape[:-1]), device=DEV)
+    out = das_autograd(xg, src, dst, offs, w)
+    lhs = float((out.double() * y.double()).sum())
+    (gx,) = torch.autograd.grad(out, xg, grad_outputs=y)
+    rhs = float((x.double() * gx.double()).sum())
+    assert abs(lhs - rhs) <= 1e-5 * max(abs(lhs), 1.0)
+
+
+@pytest.mark.parametrize("B", [1, 2, 5])
+def test_gradients_match_float64_reference(B):
+    cpu = _problem(2, B=B)
+    gpu = [t.to(DEV).requires_grad_(True) for t in cpu]
+    ref = [t.double().requires_grad_(True) for t in cpu]
+    g = torch.randn((B, *cpu[2].shape[:-1]), generator=torch.Generator().manual_seed(3))
+    out = das_autograd(*gpu)
+    out.backward(g.to(DEV))
+    out_ref = das_ref(*ref)
+    out_ref.backward(g.double())
+    assert oracle.rel_l2(out.detach().cpu().numpy(), out_ref.detach().numpy()) < 2e-5
+    for name, a, b in zip(["x", "srcpos", "dstpos", "offsets", "weights"], gpu, ref):
+        err = oracle.rel_l2(a.grad.cpu().numpy(), b.grad.numpy())
+        assert err < 2e-4, (name, err)
+
+
+def test_sparse_gradients_match_reference():
+    x, src, dst, offs, w = _problem(4, B=2, S=5)
+    idx = torch.randint(0, 5, (3, *dst.shape[:-1]), generator=torch.Generator().manual_seed(5)).int()
+    offs3, w3 = offs[:3].clone(), w[:3].clone()
+    gpu = [t.to(DEV).requires_grad_(True) for t in (x, src, dst, offs3, w3)]
+    ref = [t.double().requires_grad_(True) for t in (x, src, dst, offs3, w3)]
+    out = ffdas_b200.das_sparse(*gpu, idx.to(DEV))
+    out.sum().backward()
+    das_ref(*ref, sparse_indices=idx).sum().backward()
+    for name, a, b in zip(["x", "srcpos", "dstpos", "offsets", "weights"], gpu, ref):
+        assert oracle.rel_l2(a.grad.cpu().numpy(), b.grad.numpy()) < 2e-4, name
+
+
+def test_central_finite_differences_fp64():
+    x, src, dst, offs, w = _problem(6, B=2)
+    loss_ref = lambda o, ww: -(das_ref(x.double(), src.double(), dst.double(), o, ww) ** 4).sum()  # noqa: E731
+    og = offs.to(DEV).requires_grad_(True)
+    wg = w.to(DEV).requires_grad_(True)
+    img = das_autograd(x.to(DEV), src.to(DEV), dst.to(DEV), og, wg)
+    (-(img.double() ** 4).sum()).backward()
+    rng = np.random.default_rng(7)
+    h = 1e-4
+    flat = offs.numel()
+    picks = rng.choice(flat, 64, replace=False)
+    checked = 0
+    for var, grad in ((offs, og.grad), (w, wg.grad)):
+        for i in picks[:32]:
+            base = var.double().clone().reshape(-1)
+            # skip delays whose perturbation crosses a sample boundary
+            if var is offs:
+                r = torch.sqrt(((dst.reshape(-1, 3)[i % dst[..., 0].numel()].double() - src.double()) ** 2).sum(-1))
+                frac = (float(base[i]) + r) % 1.0
+                if bool(((frac < 10 * h) | (frac > 1 - 10 * h)).any()):
+                    continue
+            p, m = base.clone(), base.clone()
+            p[i] += h
+            m[i] -= h
+            args = [p.reshape(var.shape), w.double()] if var is offs else [offs.double(), p.reshape(var.shape)]
+            argm = [m.reshape(var.shape), w.double()] if var is offs else [offs.double(), m.reshape(var.shape)]
+            fd = float(loss_ref(*args) - loss_ref(*argm)) / (2 * h)
+            an = float(grad.reshape(-1)[i])
+            assert abs(fd - an) <= 2e-3 * max(abs(fd), 1e-3 * float(abs(grad).max())), (i, fd, an)
+            checked += 1
+    assert checked >= 40
+
+
+def test_bf16_and_fp16_inputs_get_gradients():
+    x, src, dst, offs, w = _problem(8, B=2)
+    for dt in (torch.float16, torch.bfloat16):
+        xg = x.to(DEV, dt).requires_grad_(True)
+        wg = w.to(DEV).requires_grad_(True)
+        out = das_autograd(xg, src.to(DEV), dst.to(DEV), offs.to(DEV), wg)
+        out.sum().backward()
+        assert xg.grad.dtype == dt and torch.isfinite(xg.grad.float()).all()
+        ref_w = das_ref(x.to(dt).double(), src.double(), dst.double(), offs.double(),
+                        w.double().requires_grad_(True))
+        assert torch.isfinite(wg.grad).all()
+
+
+def test_autofocus_recovers_sound_speed_scale():
+    wl = W.autofocus(device=DEV, scale=0.25)
+    x, srcpos, dstpos, base = wl["x"], wl["srcpos"], wl["dstpos"], wl["offsets"]
+    alpha = torch.tensor(1.0, device=DEV, requires_grad=True)
+    opt = torch.optim.Adam([alpha], lr=4e-3)
+    for _ in range(50):
+        opt.zero_grad()
+        img = ffdas_b200.das(x, srcpos * alpha, dstpos * alpha, base * alpha, wl["weights"])
+        loss = -(img / img.detach().abs().max()).pow(4).sum()
+        loss.backward()
+        opt.step()
+    assert abs(float(alpha) - wl["alpha_true"]) < 0.006, float(alpha)

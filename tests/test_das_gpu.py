@@ -1,0 +1,251 @@
+"""GPU parity of the forward das / das_sparse against the FP64 oracle.
+
+Tolerances (relative L2 against the FP64 oracle on the same inputs):
+  fp32 pairs  2e-5   (fp32 delay rounding, as in the reference's own fp32 path)
+  fp16 pairs  2e-3   (11-bit storage of channel data)
+  bf16 pairs  8e-3   (8-bit storage of channel data)
+  fp64 pairs  1e-6   (delays are still fp32, as in the reference)
+"""
+import numpy as np
+import pytest
+import torch
+
+import ffdas_b200
+from ffdas_b200 import workloads as W
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+TOL = {torch.float32: 2e-5, torch.float16: 2e-3, torch.bfloat16: 8e-3, torch.float64: 1e-6}
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+def _oracle_of(wl, x=None, **kw):
+    x = wl["x"] if x is None else x
+    return oracle.das_f64(_np(x.float() if x.dtype in (torch.float16, torch.bfloat16) else x), _np(wl["srcpos"]),
+                          _np(wl["dstpos"]), _np(wl["offsets"]), _np(wl["weights"]),
+                          sparse_indices=_np(wl["sparse_indices"]) if "sparse_indices" in wl else None, **kw)
+
+
+def _run(wl, x=None, **kw):
+    x = wl["x"] if x is None else x
+    if "sparse_indices" in wl:
+        return ffdas_b200.das_sparse(x, wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"],
+                                     wl["sparse_indices"], **kw)
+    return ffdas_b200.das(x, wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"], **kw)
+
+
+CASES = [
+    ("plane2d", dict(scale=0.25)),
+    ("diverging3d", dict(scale=0.125)),
+    ("ensemble", dict(scale=0.1, dtype=torch.float32)),
+    ("sparse_focus", dict(scale=0.2)),
+    ("autofocus", dict(scale=0.2)),
+]
+
+
+@pytest.mark.parametrize("name,kw", CASES, ids=[c[0] for c in CASES])
+def test_forward_fp32_matches_oracle(name, kw):
+    wl = W.CONFIGS[name](device=DEV, **kw)
+    x = wl["x"].float()
+    got = _run(wl, x)
+    ref = _oracle_of(wl, x)
+    assert got.shape == ref.shape
+    assert oracle.rel_l2(_np(got), ref) < TOL[torch.float32]
+
+
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16, torch.float64])
+def test_forward_storage_dtypes(dtype):
+    wl = W.diverging3d(device=DEV, scale=0.125)
+    x = W.normalize_channels(wl["x"].double()).to(dtype)
+    got = _run(wl, x)
+    ref = _oracle_of(wl, x.double())
+    assert got.dtype == (torch.float64 if dtype == torch.float64 else torch.float32)
+    assert oracle.rel_l2(_np(got), ref) < TOL[dtype]
+
+
+@pytest.mark.parametrize("flag", ["use_fp16", "use_bf16"])
+def test_reduced_precision_from_fp32_input(flag):
+    wl = W.diverging3d(device=DEV, scale=0.125)
+    x = W.normalize_channels(wl["x"])
+    got = _run(wl, x, **{flag: True})
+    ref = _oracle_of(wl, x)
+    tol = TOL[torch.float16] if flag == "use_fp16" else TOL[torch.bfloat16]
+    assert oracle.rel_l2(_np(got), ref) < tol
+
+
+def _small(rng, B=1, C=5, S=3, N=96, V=(6, 7), complex_=False, three_d=False):
+    x = rng.standard_normal((B, C, S, N)).astype(np.float32)
+    if complex_:
+        x = (x + 1j * rng.standard_normal((B, C, S, N))).astype(np.complex64)
+    src = rng.uniform(-4, 4, (C, 3)).astype(np.float32)
+    src[:, 2] = 0
+    zz, xx = np.meshgrid(np.linspace(20, 40, V[0]), np.linspace(-3, 3, V[1]), indexing="ij")
+    dst = np.stack([xx, np.zeros_like(xx), zz], -1).astype(np.float32)   # (V0, V1, 3)
+    offs = rng.uniform(-10, 40, (S, *V)).astype(np.float32)
+    w = rng.uniform(0.1, 1, (S, *V)).astype(np.float32)
+    if three_d:
+        x = x[0]
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
+    return t(x), t(src), t(dst), t(offs), t(w)
+
+
+@pytest.mark.parametrize("B", [1, 2, 3, 5, 8, 13])
+def test_batch_sizes(rng, B):
+    x, src, dst, offs, w = _small(rng, B=B)
+    got = ffdas_b200.das(x, src, dst, offs, w)
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w))
+    assert got.shape == (B, *dst.shape[:-1])
+    assert oracle.rel_l2(_np(got), ref) < 2e-5
+
+
+def test_three_d_input_indexes_offsets_per_event(rng):
+    x, src, dst, offs, w = _small(rng, three_d=True)
+    got = ffdas_b200.das(x, src, dst, offs, w)
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w))
+    assert got.shape == tuple(dst.shape[:-1])
+    assert oracle.rel_l2(_np(got), ref) < 2e-5
+
+
+def test_complex_with_phase_rotation(rng):
+    x, src, dst, offs, w = _small(rng, B=2, complex_=True)
+    got = ffdas_b200.das(x, src, dst, offs, w, wavenum=-0.9)
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w), wavenum=-0.9)
+    assert got.dtype == torch.complex64
+    assert oracle.rel_l2(_np(got), ref) < 1e-4   # __sincosf of large phases
+
+
+def test_complex128(rng):
+    x, src, dst, offs, w = _small(rng, complex_=True)
+    x = x.to(torch.complex128)
+    got = ffdas_b200.das(x, src, dst, offs, w, wavenum=0.0)
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w))
+    assert got.dtype == torch.complex128
+    assert oracle.rel_l2(_np(got), ref) < 1e-6
+
+
+def test_directivity(rng):
+    x, src, dst, offs, w = _small(rng, B=2)
+    srcdir = torch.zeros((src.shape[0], 4), device=DEV)
+    srcdir[:, 2] = 1.0
+    srcdir[:, 3] = 0.99
+    got = ffdas_b200.das(x, src, dst, offs, w, srcdir=srcdir)
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w), srcdir=_np(srcdir))
+    assert oracle.rel_l2(_np(got), ref) < 2e-5
+    assert not np.allclose(ref, oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w)))
+
+
+def test_channels_trailing_and_strided_input(rng):
+    x, src, dst, offs, w = _small(rng, B=2)
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w))
+    xt = x.transpose(1, 2).contiguous()            # (B, S, C, N)
+    got = ffdas_b200.das(xt, src, dst, offs, w, channels_trailing=True)
+    assert oracle.rel_l2(_np(got), ref) < 2e-5
+    wide = torch.zeros((2, x.shape[1], x.shape[2], x.shape[3] + 7), device=DEV)
+    wide[..., 3:3 + x.shape[3]] = x
+    got2 = ffdas_b200.das(wide[..., 3:3 + x.shape[3]], src, dst, offs, w)  # strided rows
+    assert oracle.rel_l2(_np(got2), ref) < 2e-5
+
+
+def test_out_of_record_voxels_are_exact_zeros(rng):
+    x, src, dst, offs, w = _small(rng)
+    far = torch.full_like(offs, 1e6)
+    assert torch.count_nonzero(ffdas_b200.das(x, src, dst, far, w)).item() == 0
+    neg = torch.full_like(offs, -1e6)
+    assert torch.count_nonzero(ffdas_b200.das(x, src, dst, neg, w)).item() == 0
+
+
+@pytest.mark.parametrize("N", [1, 2, 3])
+def test_tiny_records(rng, N):
+    x, src, dst, offs, w = _small(rng, N=N)
+    offs = torch.rand_like(offs) * N - 40  # r ~ 20..40 -> tau around 0..N
+    got = ffdas_b200.das(x, src, dst, offs, w)
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w))
+    np.testing.assert_allclose(_np(got), ref, rtol=1e-4, atol=1e-5)
+
+
+def test_single_voxel_and_impulse():
+    # reference test_das.py:121
+    x = torch.zeros((1, 1, 64), device=DEV)
+    x[0, 0, 32] = 1.0
+    out = ffdas_b200.das(x, torch.zeros((1, 3), device=DEV), torch.zeros((1, 3), device=DEV),
+                         torch.full((1, 1), 32.0, device=DEV), torch.ones((1, 1), device=DEV))
+    assert abs(float(out.squeeze()) - (1 - np.sqrt(1e-7))) < 1e-6
+
+
+def test_zero_inputs(rng):
+    x, src, dst, offs, w = _small(rng)
+    assert torch.count_nonzero(ffdas_b200.das(torch.zeros_like(x), src, dst, offs, w)).item() == 0
+    assert torch.count_nonzero(ffdas_b200.das(x, src, dst, offs, torch.zeros_like(w))).item() == 0
+
+
+def test_sparse_matches_dense_and_skips_padding(rng):
+    x, src, dst, offs, w = _small(rng, B=2, S=6)
+    dense = ffdas_b200.das(x, src, dst, offs, w)
+    S = offs.shape[0]
+    idx = torch.arange(S, device=DEV, dtype=torch.int32).reshape(S, 1, 1).expand_as(offs).contiguous()
+    pad = lambda t, v: torch.cat([t, torch.full((3, *t.shape[1:]), v, device=DEV, dtype=t.dtype)])  # noqa: E731
+    sp = ffdas_b200.das_sparse(x, src, dst, pad(offs, 0.0), pad(w, 0.0), pad(idx, 0))
+    assert oracle.rel_l2(_np(sp), _np(dense)) < 1e-6
+
+
+def test_sparse_out_of_range_index_contributes_nothing(rng):
+    x, src, dst, offs, w = _small(rng, S=4)
+    idx = torch.randint(0, 4, offs.shape, device=DEV, dtype=torch.int32)
+    base = ffdas_b200.das_sparse(x, src, dst, offs, w, idx)
+    bad = idx.clone()
+    bad[0] = 99
+    w2 = w.clone()
+    w2[0] = 0
+    got = ffdas_b200.das_sparse(x, src, dst, offs, w, bad)
+    ref = ffdas_b200.das_sparse(x, src, dst, offs, w2, idx)
+    assert oracle.rel_l2(_np(got), _np(ref)) < 1e-6
+    assert not torch.allclose(base, got)
+
+
+SCHEDULES = [
+    dict(variant=1, tile_x=16, tile_y=16, batch_tile=1, event_chunk=16),
+    dict(variant=1, tile_x=32, tile_y=8, batch_tile=2, event_chunk=4),
+    dict(variant=1, tile_x=8, tile_y=8, tile_z=4, batch_tile=4, event_chunk=16),
+    dict(variant=1, tile_x=64, tile_y=4, batch_tile=8, event_chunk=4),
+]
+
+
+@pytest.mark.parametrize("cfg", SCHEDULES, ids=lambda c: "x".join(str(c.get(k, 1)) for k in
+                                                                   ("tile_x", "tile_y", "tile_z", "batch_tile",
+                                                                    "event_chunk")))
+def test_every_schedule_gives_the_same_image(rng, cfg):
+    wl = W.diverging3d(device=DEV, scale=0.125)
+    x = wl["x"].expand(3, *wl["x"].shape[1:]).contiguous()
+    h = ffdas_b200.get_library_handle(DEV)
+    ref = oracle.das_f64(_np(x), _np(wl["srcpos"]), _np(wl["dstpos"]), _np(wl["offsets"]), _np(wl["weights"]))
+    try:
+        h.set_config(cfg)
+        got = ffdas_b200.das(x, wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"])
+        info = h.last_kernel_info()
+    finally:
+        h.set_config(None)
+    assert info["tile_x"] == cfg["tile_x"] and info["batch_tile"] == cfg["batch_tile"]
+    assert oracle.rel_l2(_np(got), ref) < 2e-5
+
+
+def test_out_argument_and_no_grad_path(rng):
+    x, src, dst, offs, w = _small(rng, B=2)
+    out = torch.full((2, *dst.shape[:-1]), 7.0, device=DEV)
+    res = ffdas_b200.das(x, src, dst, offs, w, out=out)
+    assert res is out
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w))
+    assert oracle.rel_l2(_np(out), ref) < 2e-5
+
+
+def test_runs_on_current_stream(rng):
+    x, src, dst, offs, w = _small(rng, B=2)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        got = ffdas_b200.das(x, src, dst, offs, w)
+    s.synchronize()
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w))
+    assert oracle.rel_l2(_np(got), ref) < 2e-5

@@ -1,0 +1,50 @@
+"""Pure-torch float64 delay-and-sum (CPU), differentiable: the autograd checker.
+
+Same formula as the reference kernel (src/das/das_alg1_kernels.cuh:48-106):
+tau = offsets[e,v] + sqrt(max(|dst[v]-src[c]|^2, 1e-7)), k = floor(tau),
+t = tau - k, valid iff 0 <= k < N-1, out += w * (x[k] + t (x[k+1] - x[k])).
+Gradients flow through t (not through the floor), exactly the derivative the
+backward kernels implement.  Real data, no directivity.  Small sizes only.
+"""
+from __future__ import annotations
+
+import torch
+
+
+def das_ref(x, srcpos, dstpos, offsets, weights, sparse_indices=None):
+    """x ([B,] C, S, N); returns ([B,] *spatial) float64."""
+    have_batch = x.ndim == 4
+    xb = x if have_batch else x[None]
+    B, C, S, N = xb.shape
+    spatial = dstpos.shape[:-1]
+    V = dstpos[..., 0].numel()
+    dp = dstpos.reshape(V, 3).double()
+    sp = srcpos.reshape(C, 3).double()
+    offs = offsets.reshape(-1, V).double()
+    w = weights.reshape(-1, V).double()
+    E = offs.shape[0]
+    d = dp[:, None, :] - sp[None, :, :]                     # (V, C, 3)
+    rsq = (d * d).sum(-1).clamp_min(1e-7)
+    r = torch.sqrt(rsq)                                     # (V, C)
+    tau = offs[:, :, None] + r[None]                        # (E, V, C)
+    kf = torch.floor(tau.detach())
+    t = tau - kf
+    valid = (kf >= 0) & (kf < N - 1)
+    k = kf.clamp(0, max(N - 2, 0)).long()
+    if sparse_indices is None:
+        s = torch.arange(E)[:, None, None].expand(E, V, C)
+    else:
+        s = sparse_indices.reshape(E, V).long()[:, :, None].expand(E, V, C)
+        valid = valid & (s >= 0) & (s < S)
+        s = s.clamp(0, S - 1)
+    c = torch.arange(C)[None, None, :].expand(E, V, C)
+    xd = xb.double()
+    outs = []
+    for b in range(B):
+        x0 = xd[b][c, s, k]
+        x1 = xd[b][c, s, (k + 1).clamp(max=N - 1)]
+        L = x0 + t * (x1 - x0)
+        L = torch.where(valid, L, torch.zeros_like(L))
+        outs.append((w[:, :, None] * L).sum(dim=(0, 2)))
+    out = torch.stack(outs).reshape(B, *spatial)
+    return out if have_batch else out[0]
