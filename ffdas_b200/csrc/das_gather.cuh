@@ -133,28 +133,36 @@ __global__ void __launch_bounds__(256) das_gather_kernel(const gather_params p) 
 #pragma unroll
     for (int b = 0; b < BT; b++) acc[b] = acc_ops<acc_t>::zero();
 
+    // Batch items past B read batch item 0 (their results are discarded), so
+    // the unrolled loops below carry no per-item branch.
+    int64_t boff[BT];
+#pragma unroll
+    for (int b = 0; b < BT; b++) boff[b] = (b0 + b < p.B) ? (int64_t)(b0 + b) * row_stride_b : 0;
+
     for (int e0 = 0; e0 < p.n_events; e0 += SC) {
         const int sc = min(SC, p.n_events - e0);
+        // Event slots past the end, zero-weight (padding) entries and
+        // out-of-range event indices get a huge delay: their tap lands on the
+        // zero pair and their weight is 0, so every slot runs the same
+        // branch-free code.
         float ofs[SC], w[SC];
-        int srow[SC];
+        uint32_t srow[SC];  // row offset of the event within a channel, in pairs
 #pragma unroll
         for (int j = 0; j < SC; j++) {
+            ofs[j] = 1e30f;
+            w[j] = 0.f;
+            srow[j] = 0;
             if (j < sc) {
                 const int64_t idx = (int64_t)(e0 + j) * p.V + v;
-                ofs[j] = __ldg(p.offsets + idx);
-                w[j] = __ldg(p.weights + idx);
-                if constexpr (SPARSE) {
-                    int s = __ldg(p.sparse_idx + idx);
-                    // an out-of-range event index contributes nothing
-                    if ((unsigned)s >= (unsigned)p.S) { w[j] = 0.f; s = 0; }
-                    srow[j] = s;
-                } else {
-                    srow[j] = e0 + j;
+                const float o = __ldg(p.offsets + idx);
+                const float ww = __ldg(p.weights + idx);
+                int s = e0 + j;
+                if constexpr (SPARSE) s = __ldg(p.sparse_idx + idx);
+                if ((unsigned)s < (unsigned)p.S && (!SPARSE || ww != 0.f)) {
+                    ofs[j] = o;
+                    w[j] = ww;
+                    srow[j] = (uint32_t)s * (uint32_t)p.npad;
                 }
-            } else {
-                ofs[j] = 0.f;
-                w[j] = 0.f;
-                srow[j] = 0;
             }
         }
 
@@ -166,24 +174,25 @@ __global__ void __launch_bounds__(256) das_gather_kernel(const gather_params p) 
             if (p.srcdir) apply_directivity(g, vx, vy, vz, cx, cy, cz, __ldg(p.srcdir + c));
             const st *Pc = P + (int64_t)c * p.S * p.npad;
 
+            // phase 1: every tap's index and load, so all loads are in flight
+            st pr[SC][BT];
+            float tt[SC], tau[SC];
 #pragma unroll
             for (int j = 0; j < SC; j++) {
-                if (j < sc) {
-                    if constexpr (SPARSE) {
-                        if (w[j] == 0.f) continue;  // padded entry of an uneven subset
-                    }
-                    const float tau = __fmaf_rn(g.rsq, g.rinv, ofs[j]);
-                    const tau_split ts = split_tau(tau);
-                    const uint32_t k = min(ts.k, kmax);
-                    const st *row = Pc + (int64_t)srow[j] * p.npad + k;
+                tau[j] = __fmaf_rn(g.rsq, g.rinv, ofs[j]);
+                const tau_split ts = split_tau(tau[j]);
+                tt[j] = ts.t;
+                const uint32_t rowoff = SPARSE ? srow[j] : (uint32_t)(e0 + j) * (uint32_t)p.npad;
+                const st *row = Pc + (rowoff + min(ts.k, kmax));
 #pragma unroll
-                    for (int b = 0; b < BT; b++) {
-                        if (BT == 1 || b0 + b < p.B) {
-                            const st pr = row[(int64_t)(b0 + b) * row_stride_b];
-                            accumulate<K>(acc[b], tr::tap(pr, ts.t), w[j], p.wavenum, tau);
-                        }
-                    }
-                }
+                for (int b = 0; b < BT; b++) pr[j][b] = row[boff[b]];
+            }
+            // phase 2: interpolate and accumulate
+#pragma unroll
+            for (int j = 0; j < SC; j++) {
+#pragma unroll
+                for (int b = 0; b < BT; b++)
+                    accumulate<K>(acc[b], tr::tap(pr[j][b], tt[j]), w[j], p.wavenum, tau[j]);
             }
         }
     }

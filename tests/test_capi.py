@@ -147,8 +147,9 @@ def test_error_codes_match_reference():
     assert _call(h, [2, 2, 2, 16], R32, [3, 4], R32) == Error.INVALID_DIMS
     # sample stride must be 1 (das_utils.h:66)
     assert _call(h, [1, 2, 2, 16], R32, [1, 4], R32, x_strides=[64, 32, 16, 2]) == Error.INVALID_ARGUMENT
-    # int32 index guard (das_impl.cuh:34)
-    assert _call(h, [1, 2, 2, 16], R32, [1, 4], R32, x_strides=[1 << 31, 32, 16, 1]) == Error.INVALID_DIMS
+    # int32 index guard (das_impl.cuh:34); size-1 dims do not count
+    assert _call(h, [1, 2, 2, 16], R32, [1, 4], R32, x_strides=[1 << 31, 32, 16, 1]) == 0
+    assert _call(h, [2, 2, 2, 16], R32, [2, 4], R32, x_strides=[1 << 31, 32, 16, 1]) == Error.INVALID_DIMS
     # algorithms: ALG3 is not implemented; fp64 only with ALG1/DEFAULT (das_impl.cuh:37-54)
     assert _call(h, *ok, alg=3) == Error.INVALID_ARGUMENT
     assert _call(h, *ok, alg=2) == 0
