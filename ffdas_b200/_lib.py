@@ -84,10 +84,10 @@ class DasConfig(ctypes.Structure):
     """ffdas_das_config_t: schedule override (0 = planner default)."""
     _fields_ = [("variant", ctypes.c_int32), ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32),
                 ("tile_z", ctypes.c_int32), ("batch_tile", ctypes.c_int32), ("event_chunk", ctypes.c_int32),
-                ("min_blocks", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("min_blocks", ctypes.c_int32), ("window", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
-        return {f: int(getattr(self, f)) for f, _ in self._fields_ if f != "reserved"}
+        return {f: int(getattr(self, f)) for f, _ in self._fields_}
 
 
 class KernelInfo(ctypes.Structure):
@@ -133,6 +133,8 @@ SIGNATURES = {
     "ffdas_set_kernel_timing": (c_err, [c_handle, ctypes.c_int]),
     "ffdas_get_last_kernel_time": (c_err, [c_handle, ctypes.POINTER(ctypes.c_float)]),
     "ffdas_measure_fp32_peak": (c_err, [c_handle, ctypes.POINTER(ctypes.c_double)]),
+    "ffdas_get_device_status": (c_err, [c_handle, ctypes.POINTER(ctypes.c_int)]),
+    "ffdas_debug_staged_drop_stage": (None, [ctypes.c_int]),
 }
 
 _lib = None
@@ -237,6 +239,11 @@ class Handle:
         ms = ctypes.c_float()
         check(load().ffdas_get_last_kernel_time(self.h, ctypes.byref(ms)))
         return float(ms.value)
+
+    def device_status(self) -> int:
+        s = ctypes.c_int()
+        check(load().ffdas_get_device_status(self.h, ctypes.byref(s)))
+        return int(s.value)
 
     def measure_fp32_peak(self) -> float:
         tf = ctypes.c_double()

@@ -20,6 +20,16 @@ extern "C" FFDAS_API void ffdas_debug_fail_alloc_after(int n) {
     g_fail_alloc_after.store(n);
 }
 
+static std::atomic<int> g_drop_stage{0};
+
+extern "C" FFDAS_API void ffdas_debug_staged_drop_stage(int enable) {
+    g_drop_stage.store(enable ? 1 : 0);
+}
+
+int ffdas_take_debug_drop_stage() {
+    return g_drop_stage.exchange(0);
+}
+
 ffdas_error_t ffdas_launch_check(cudaStream_t stream) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return FFDAS_ERROR_CUDA_LAUNCH_FAILED;
@@ -178,9 +188,17 @@ ffdas_error_t ffdas_create(ffdas_handle_t *handle) {
     pp.location.id = h->device_id;
     if (cudaMemPoolCreate(&h->pool, &pp) != cudaSuccess) { err = FFDAS_ERROR_CUDA_RUNTIME; goto fail; }
     cudaMemPoolSetAttribute(h->pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    if (cudaMalloc(reinterpret_cast<void **>(&h->status), sizeof(int)) != cudaSuccess ||
+        cudaMemset(h->status, 0, sizeof(int)) != cudaSuccess) {
+        err = FFDAS_ERROR_ALLOCATION_FAILED;
+        goto fail;
+    }
     *handle = h;
     return FFDAS_SUCCESS;
 fail:
+    cudaGetLastError();
+    if (h->status) cudaFree(h->status);
+    if (h->pool) cudaMemPoolDestroy(h->pool);
     cudaGetLastError();
     delete h;
     return err;
@@ -201,6 +219,7 @@ ffdas_error_t ffdas_destroy(ffdas_handle_t h) {
     }
     if (h->ev_start) cudaEventDestroy(h->ev_start);
     if (h->ev_stop) cudaEventDestroy(h->ev_stop);
+    if (h->status) cudaFree(h->status);
     cudaGetLastError();
     delete h;
     return err;

@@ -35,6 +35,12 @@ struct ffdas_tensor_desc {
 // GPU fault: when > 0, the n-th following workspace allocation fails.
 extern "C" FFDAS_API void ffdas_debug_fail_alloc_after(int n);
 
+// Test hook: the next TMA-staged launch leaves its first pipeline stage
+// unfilled, so its bounded waits expire and it reports a device status of 1
+// instead of completing.  One-shot.
+extern "C" FFDAS_API void ffdas_debug_staged_drop_stage(int enable);
+int ffdas_take_debug_drop_stage();
+
 struct ffdas_context {
     int device_id = 0;
     int arch_code = 0;
@@ -45,6 +51,7 @@ struct ffdas_context {
     bool has_config = false;
     ffdas_das_config_t config{};
     ffdas_kernel_info_t last{};
+    int *status = nullptr;  // device word: bounded-wait timeouts of the staged kernels
     bool timing = false;
     bool timing_recorded = false;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;

@@ -182,7 +182,16 @@ struct schedule {
     int T0 = 16, T1 = 16, T2 = 1;
     int BT = 1;
     int SC = 16;
+    int WB = 32;   // staged kernel: pairs per window slot
 };
+
+// Events per staged pass: the smallest supported chunk covering n events.
+static int staged_event_chunk(int n) {
+    if (n <= 1) return 1;
+    if (n <= 4) return 4;
+    if (n <= 8) return 8;
+    return 16;
+}
 
 static int floor_pow2(int v) {
     int p = 1;
@@ -216,6 +225,13 @@ static schedule plan_schedule(const ffdas_context &h, const das_problem &pb, int
         }
         if (c.batch_tile) s.BT = c.batch_tile;
         if (c.event_chunk) s.SC = c.event_chunk <= 4 ? 4 : 16;
+        if (c.window) s.WB = c.window <= 32 ? 32 : 64;
+    }
+    if (s.variant == 2) {
+        // staged kernel: one batch item per CTA, event chunk from the count
+        s.BT = 1;
+        s.SC = staged_event_chunk(pb.n_events);
+        if (h.has_config && h.config.event_chunk) s.SC = staged_event_chunk(h.config.event_chunk);
     }
     if (!real && s.BT != 1) s.BT = 4;
     if (s.T0 * s.T1 * s.T2 != 256) {  // the gather kernel runs 256-thread CTAs
@@ -349,7 +365,7 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
     if (a.sparse && !a.sparse_indices) return FFDAS_ERROR_NULL_POINTER;
 
     // ---- ingest: x -> pair rows (workspace) ----
-    const int64_t npad = std::max<int64_t>(2, ((int64_t)pb.N + 1) & ~int64_t(1));
+    const int64_t npad = pair_row_length(pb.N);
     const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
     workspace P(h);
     FFDAS_TRY(P.alloc((size_t)std::max<int64_t>(rows, 1) * npad * storage_bytes(kind)));
@@ -396,6 +412,18 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
     h.last.kernels = 2;
     h.last.grid = tiles * bchunks;
 
+    const bool staged = s.variant == 2 && staged_supported(pb, kind) && od.dtype == FFDAS_R_32F;
+    if (staged) {
+        h.last.variant = 2;
+        h.last.batch_tile = 1;
+        h.last.event_chunk = s.SC;
+        h.last.grid = tiles * pb.B;
+        if (pb.B > 65535) return FFDAS_ERROR_DIMS_TOO_LARGE;
+        h.mark_start();
+        const ffdas_error_t err = launch_staged(h, pb, kind, gp, s.SC, s.WB, dim3((unsigned)tiles, (unsigned)pb.B));
+        h.mark_stop();
+        return err;
+    }
     h.mark_start();
     const ffdas_error_t err = a.sparse ? launch_gather<true>(h, kind, od.dtype, gp, s, grid)
                                        : launch_gather<false>(h, kind, od.dtype, gp, s, grid);

@@ -296,7 +296,7 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
     if (!gout || !a.dstpos || !a.offsets || !a.weights || (pb.C > 0 && !a.srcpos)) return FFDAS_ERROR_NULL_POINTER;
     if (!gx && !goff && !gw && !gdst && !gsrc) return FFDAS_SUCCESS;
 
-    const int64_t npad = std::max<int64_t>(2, ((int64_t)pb.N + 1) & ~int64_t(1));
+    const int64_t npad = pair_row_length(pb.N);
     const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
     const size_t sb = (kind == ST_F32) ? 8 : 4;
     workspace P(h);

@@ -182,7 +182,10 @@ __global__ void __launch_bounds__(256) das_gather_kernel(const gather_params p) 
                 tau[j] = __fmaf_rn(g.rsq, g.rinv, ofs[j]);
                 const tau_split ts = split_tau(tau[j]);
                 tt[j] = ts.t;
-                const uint32_t rowoff = SPARSE ? srow[j] : (uint32_t)(e0 + j) * (uint32_t)p.npad;
+                // Slots past the last event must still address a row of THIS
+                // channel (their tap is the zero pair), so clamp the event.
+                const uint32_t rowoff =
+                    SPARSE ? srow[j] : (uint32_t)min(e0 + j, p.n_events - 1) * (uint32_t)p.npad;
                 const st *row = Pc + (rowoff + min(ts.k, kmax));
 #pragma unroll
                 for (int b = 0; b < BT; b++) pr[j][b] = row[boff[b]];

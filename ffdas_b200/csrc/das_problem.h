@@ -54,4 +54,21 @@ int select_storage(ffdas_datatype_t xt, ffdas_datatype_t ot, ffdas_compute_type_
 
 ffdas_error_t das_forward(ffdas_context &h, const das_call &a);
 
+// Pairs per row, rounded so every row starts 16-byte aligned for both pair
+// sizes (the TMA tensor map needs 16-byte row strides).
+inline int64_t pair_row_length(int N) {
+    const int64_t n = (int64_t)N < 2 ? 2 : (int64_t)N;
+    return (n + 3) & ~int64_t(3);
+}
+
+}  // namespace ffdas
+
+#include "das_gather.cuh"
+
+namespace ffdas {
+
+bool staged_supported(const das_problem &pb, int kind);
+ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp, int SC,
+                            int WB, dim3 grid);
+
 }  // namespace ffdas

@@ -1,0 +1,142 @@
+"""Autotuner for the delay-and-sum schedule (kernel variant, voxel tile, window, event chunk).
+
+    cfg = autotune(x, srcpos, dstpos, offsets, weights)       # times candidates on these inputs
+    with schedule(cfg): ffdas_b200.das(...)                    # or handle.set_config(cfg)
+
+Candidates are timed with CUDA events on the caller's own inputs (the
+geometry decides which voxel tile keeps each tile's sample windows narrow).
+The winner is cached per problem signature in a JSON file
+($FFDAS_B200_TUNE_CACHE, default ~/.cache/ffdas_b200/tune.json) and reused.
+"""
+from __future__ import annotations
+
+import contextlib
+import json
+import os
+import threading
+from pathlib import Path
+
+import torch
+
+from .library import get_library_handle
+
+_lock = threading.Lock()
+
+
+def cache_path() -> Path:
+    p = os.environ.get("FFDAS_B200_TUNE_CACHE")
+    return Path(p) if p else Path.home() / ".cache" / "ffdas_b200" / "tune.json"
+
+
+def signature(x, dstpos, offsets, sparse_indices=None, use_fp16=False, use_bf16=False) -> str:
+    dev = torch.cuda.get_device_name(x.device)
+    comp = "f16" if use_fp16 else ("bf16" if use_bf16 else "default")
+    sp = "sparse" if sparse_indices is not None else "dense"
+    return f"{dev}|{tuple(x.shape)}|{x.dtype}|{tuple(dstpos.shape)}|{tuple(offsets.shape)}|{sp}|{comp}"
+
+
+def _grid_dims(dstpos) -> tuple[int, int]:
+    dims = [int(d) for d in dstpos.shape[:-1] if d != 1]
+    d0 = dims[-1] if dims else 1
+    d1 = dims[-2] if len(dims) >= 2 else 1
+    return d0, d1
+
+
+def candidates(x, dstpos, offsets, sparse_indices=None) -> list[dict]:
+    d0, d1 = _grid_dims(dstpos)
+    B = x.shape[0] if x.ndim == 4 else 1
+    real = not x.is_complex() and x.dtype != torch.float64
+    tiles = []
+    for t0 in (256, 128, 64, 32, 16, 8):
+        t1 = 256 // t0
+        if t0 <= max(d0, 8) * 2 and (t1 == 1 or t1 <= max(d1, 1) * 2):
+            tiles.append((t0, t1))
+    out = []
+    for t0, t1 in tiles:
+        for bt in sorted({1, min(4, B), min(8, B)} if real else {1}):
+            if bt & (bt - 1):
+                continue
+            out.append(dict(variant=1, tile_x=t0, tile_y=t1, batch_tile=bt))
+        if real and sparse_indices is None:
+            for wb in (32, 64):
+                for ec in (8, 16):
+                    out.append(dict(variant=2, tile_x=t0, tile_y=t1, window=wb, event_chunk=ec))
+    return out
+
+
+@contextlib.contextmanager
+def schedule(cfg: dict | None, device=None):
+    """Apply a schedule to the device's library handle for the duration of a block."""
+    h = get_library_handle(device)
+    prev = h.get_config().as_dict()
+    h.set_config(cfg)
+    try:
+        yield
+    finally:
+        h.set_config(prev if any(prev.values()) else None)
+
+
+def _time(fn, reps: int) -> float:
+    fn()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    b.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def autotune(x, srcpos, dstpos, offsets, weights, sparse_indices=None, *, use_fp16=False, use_bf16=False,
+             reps: int = 3, use_cache: bool = True, max_candidates: int | None = None) -> dict:
+    """Time the candidate schedules on these inputs; return {'config', 'ms', 'table'}."""
+    from .das import das, das_sparse
+    key = signature(x, dstpos, offsets, sparse_indices, use_fp16, use_bf16)
+    path = cache_path()
+    if use_cache and path.exists():
+        try:
+            cached = json.loads(path.read_text()).get(key)
+            if cached:
+                return cached
+        except Exception:
+            pass
+    out = torch.empty((x.shape[0], *dstpos.shape[:-1]) if x.ndim == 4 else tuple(dstpos.shape[:-1]),
+                      dtype=torch.float64 if x.dtype in (torch.float64, torch.complex128) else
+                      (torch.complex64 if x.is_complex() else torch.float32), device=x.device)
+
+    def call():
+        if sparse_indices is None:
+            das(x, srcpos, dstpos, offsets, weights, use_fp16=use_fp16, use_bf16=use_bf16, out=out)
+        else:
+            das_sparse(x, srcpos, dstpos, offsets, weights, sparse_indices, use_fp16=use_fp16, use_bf16=use_bf16,
+                       out=out)
+
+    table = []
+    cands = candidates(x, dstpos, offsets, sparse_indices)
+    if max_candidates:
+        cands = cands[:max_candidates]
+    for cfg in cands:
+        with schedule(cfg, x.device):
+            try:
+                ms = _time(call, reps)
+            except RuntimeError:
+                continue
+        table.append((ms, cfg))
+    table.sort(key=lambda t: t[0])
+    best = {"config": table[0][1], "ms": table[0][0], "table": [[m, c] for m, c in table[:8]]}
+    if use_cache:
+        with _lock:
+            path.parent.mkdir(parents=True, exist_ok=True)
+            data = {}
+            if path.exists():
+                try:
+                    data = json.loads(path.read_text())
+                except Exception:
+                    data = {}
+            data[key] = best
+            tmp = path.with_suffix(".tmp")
+            tmp.write_text(json.dumps(data, indent=1))
+            os.replace(tmp, path)
+    return best

@@ -144,7 +144,7 @@ typedef struct {
     int32_t batch_tile;   /* batch items per thread (1,2,4,8,16) */
     int32_t event_chunk;  /* events held in registers per pass (1..16) */
     int32_t min_blocks;   /* CTAs per SM hint (occupancy) */
-    int32_t reserved;
+    int32_t window;       /* TMA-staged kernel: pairs per staged window (32 or 64) */
 } ffdas_das_config_t;
 
 /* What the last das/das_sparse/backward call on a handle launched (new). */
@@ -296,6 +296,11 @@ FFDAS_API ffdas_error_t ffdas_get_last_kernel_time(ffdas_handle_t handle, float 
 /* New: measured FP32 FMA throughput of the current device (TFLOP/s), from a
  * short dependent-FMA kernel on the handle's stream (synchronous). */
 FFDAS_API ffdas_error_t ffdas_measure_fp32_peak(ffdas_handle_t handle, double *tflops);
+
+/* New: device-side status of the handle's kernels since the last query
+ * (0 = ok, 1 = a bounded wait inside a staged kernel expired and the kernel
+ * returned early).  Synchronises the handle's stream, then clears the word. */
+FFDAS_API ffdas_error_t ffdas_get_device_status(ffdas_handle_t handle, int *status);
 
 /* include/ffdas.h:290-300 */
 FFDAS_API ffdas_error_t ffdas_device_count(int *count);
