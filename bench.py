@@ -246,7 +246,10 @@ def run_ours(args, rank, world) -> dict:
     h = ffdas_b200.get_library_handle(dev)
     # schedule picked by the autotuner on these inputs (not timed)
     from ffdas_b200.tune import autotune
-    tuned = autotune(x, srcpos, dstpos, offs, w, reps=2, use_cache=False)
+    if args.schedule:
+        tuned = {"config": json.loads(args.schedule), "ms": None, "table": []}
+    else:
+        tuned = autotune(x, srcpos, dstpos, offs, w, reps=2, use_cache=False)
     h.set_config(tuned["config"])
 
     def step():
@@ -393,6 +396,8 @@ def main() -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--quick", action="store_true", help="main metric only")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--schedule", default=None,
+                    help="JSON schedule (ffdas_das_config_t fields) instead of autotuning, e.g. for profiling")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 

@@ -44,6 +44,10 @@ static ffdas_error_t launch_staged_t(ffdas_context &h, const staged_params &sp, 
     if (!attr_set) {
         FFDAS_CUDA(cudaFuncSetAttribute(das_staged_kernel<K, SC, WB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem));
+        // all of the unified L1/shared array as shared memory: several CTAs per SM
+        FFDAS_CUDA(cudaFuncSetAttribute(das_staged_kernel<K, SC, WB>,
+                                        cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared));
         attr_set = true;
     }
     das_staged_kernel<K, SC, WB><<<grid, kStThreads, smem, h.stream>>>(sp, map);

@@ -123,7 +123,14 @@ constexpr uint32_t kZeroWindow = kFloorMagicBits + 0x40000000u;
 template <int WB, int K>
 constexpr size_t staged_smem_bytes() {
     return slot_geom<WB, K>::ring_bytes + kStages * kStWin * 4 + kStages * 4 + 2 * kStages * 8 + 64 * 4 + 32 * 4 +
-           kStWarps * 16 * 2 * 4 + 128;
+           kStWarps * 16 * 2 * 4 + kStages * kStWin * 2 * 16 + 128;
+}
+
+// Interpolate one tap from a staged slot and return it (f32 accumulation).
+template <int K>
+__device__ __forceinline__ float staged_tap(const unsigned char *slot, uint32_t rel, float t) {
+    using st = typename pair_traits<K>::storage;
+    return pair_traits<K>::tap(*reinterpret_cast<const st *>(slot + rel * sizeof(st)), t);
 }
 
 template <int K, int SC, int WB>
@@ -146,6 +153,8 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
     float *ofs_hi = ofs_lo + 16;                                             // [16]
     volatile int *abort_flag = reinterpret_cast<volatile int *>(ofs_hi + 16);
     float *red = const_cast<float *>(reinterpret_cast<volatile float *>(abort_flag + 32));  // [warps][16][2]
+    float4 *chan_pos = reinterpret_cast<float4 *>(red + kStWarps * 32);                    // [kStages][kStWin]
+    float4 *chan_dir = chan_pos + kStages * kStWin;                                        // [kStages][kStWin]
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
@@ -221,6 +230,7 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
     const st *__restrict__ Pg = static_cast<const st *>(p.P);
     const uint32_t kmax_pair = (uint32_t)(p.npad - 1);
     float acc = 0.f;
+    float2 acc2 = make_float2(0.f, 0.f);  // packed partial sums (even / odd event)
     int stage = 0;
     uint32_t phase = 0;
     bool dead = false;
@@ -284,9 +294,19 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
                     const int cl = lane / SC, j = lane % SC;
                     const int c = c0 + cl;
                     uint32_t m = kZeroWindow;  // every tap index clamps to the zero pair
+                    float cx = 0.f, cy = 0.f, cz = 0.f;
+                    if (c < p.C) {
+                        cx = __ldg(p.srcpos + 3 * c);
+                        cy = __ldg(p.srcpos + 3 * c + 1);
+                        cz = __ldg(p.srcpos + 3 * c + 2);
+                    }
+                    if (j == 0) {
+                        // channel table of the stage, read by the consumers
+                        chan_pos[stage * kStWin + cl] = make_float4(cx, cy, cz, 0.f);
+                        if (p.srcdir)
+                            chan_dir[stage * kStWin + cl] = (c < p.C) ? __ldg(p.srcdir + c) : make_float4(0, 0, 0, 2.f);
+                    }
                     if (c < p.C && j < sc) {
-                        const float cx = __ldg(p.srcpos + 3 * c), cy = __ldg(p.srcpos + 3 * c + 1),
-                                    cz = __ldg(p.srcpos + 3 * c + 2);
                         const float dx = fmaxf(fmaxf(aabb[0] - cx, cx - aabb[3]), 0.f);
                         const float dy = fmaxf(fmaxf(aabb[1] - cy, cy - aabb[4]), 0.f);
                         const float dz = fmaxf(fmaxf(aabb[2] - cz, cz - aabb[5]), 0.f);
@@ -332,10 +352,10 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
                     for (int cl = 0; cl < CC; cl++) {
                         const int c = c0 + cl;
                         if (c >= p.C) break;
-                        const float cx = __ldg(p.srcpos + 3 * c), cy = __ldg(p.srcpos + 3 * c + 1),
-                                    cz = __ldg(p.srcpos + 3 * c + 2);
-                        recv_geom g = receive_geometry(vx, vy, vz, cx, cy, cz);
-                        if (p.srcdir) apply_directivity(g, vx, vy, vz, cx, cy, cz, __ldg(p.srcdir + c));
+                        const float4 cp = chan_pos[stage * kStWin + cl];
+                        recv_geom g = receive_geometry(vx, vy, vz, cp.x, cp.y, cp.z);
+                        if (p.srcdir)
+                            apply_directivity(g, vx, vy, vz, cp.x, cp.y, cp.z, chan_dir[stage * kStWin + cl]);
                         uint32_t k0p[SC];
 #pragma unroll
                         for (int j = 0; j < SC; j += 4) {
@@ -349,14 +369,35 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
                         }
                         const unsigned char *slots = stage_base + (cl * SC) * SG::bytes;
                         if (!any_ovf) {
+                            if constexpr (SC >= 2) {
+                                // Two events per packed FP32 instruction: delay, floor
+                                // split and fraction, then two taps and one packed
+                                // accumulate into the two partial sums acc2.
+                                const float2 rsq2 = make_float2(g.rsq, g.rsq);
+                                const float2 rinv2 = make_float2(g.rinv, g.rinv);
+                                const float2 magic2 = make_float2(kFloorMagic, kFloorMagic);
+                                const float2 neg1 = make_float2(-1.f, -1.f);
 #pragma unroll
-                            for (int j = 0; j < SC; j++) {
-                                const float tau = __fmaf_rn(g.rsq, g.rinv, ofs[j]);
-                                const float mm = __fadd_rd(tau, kFloorMagic);
-                                const float t = tau - (mm - kFloorMagic);
-                                const uint32_t rel = min(__float_as_uint(mm) - k0p[j], (uint32_t)WB);
-                                const st pr = *reinterpret_cast<const st *>(slots + j * SG::bytes + rel * sizeof(st));
-                                acc = __fmaf_rn(w[j], tr::tap(pr, t), acc);
+                                for (int j = 0; j < SC; j += 2) {
+                                    const float2 tau2 = __ffma2_rn(rsq2, rinv2, make_float2(ofs[j], ofs[j + 1]));
+                                    const float2 mm2 = __fadd2_rd(tau2, magic2);
+                                    const float2 nfl2 = __ffma2_rn(mm2, neg1, magic2);   // -(floor), exact
+                                    const float2 t2 = __fadd2_rn(tau2, nfl2);
+                                    const uint32_t ra = min(__float_as_uint(mm2.x) - k0p[j], (uint32_t)WB);
+                                    const uint32_t rb = min(__float_as_uint(mm2.y) - k0p[j + 1], (uint32_t)WB);
+                                    const float ta = staged_tap<K>(slots + j * SG::bytes, ra, t2.x);
+                                    const float tb = staged_tap<K>(slots + (j + 1) * SG::bytes, rb, t2.y);
+                                    acc2 = __ffma2_rn(make_float2(w[j], w[j + 1]), make_float2(ta, tb), acc2);
+                                }
+                            } else {
+#pragma unroll
+                                for (int j = 0; j < SC; j++) {
+                                    const float tau = __fmaf_rn(g.rsq, g.rinv, ofs[j]);
+                                    const float mm = __fadd_rd(tau, kFloorMagic);
+                                    const float t = tau - (mm - kFloorMagic);
+                                    const uint32_t rel = min(__float_as_uint(mm) - k0p[j], (uint32_t)WB);
+                                    acc = __fmaf_rn(w[j], staged_tap<K>(slots + j * SG::bytes, rel, t), acc);
+                                }
                             }
                         } else {
 #pragma unroll
@@ -402,6 +443,7 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
         return;
     }
     if (active && !dead) {
+        acc += acc2.x + acc2.y;
         float *o = static_cast<float *>(p.out) + (int64_t)b * p.out_bstride + v;
         *o = p.beta_zero ? acc : __fmaf_rn((float)p.beta_re, *o, acc);
     }

@@ -45,18 +45,16 @@ def test_fp32_matches_reference_das(name, kw):
     assert err < 1e-5, err
 
 
-def test_batched_ensemble_matches_reference_alg1_and_alg2():
+def test_batched_ensemble_matches_reference_alg1():
+    # ALG1 with the 16-frame register tile (FFDAS_ALG1_TILE_SIZE=16; the
+    # default tile of 32 is rejected for float output, das_alg1.cu:219-239).
+    # The reference's ALG2 is not used as a bar: on this case its image
+    # differed from its own ALG1 and from the FP64 oracle (rel-L2 ~1.0).
     wl = W.ensemble(device=DEV, scale=0.2, frames=16, dtype=torch.float32)
     x = wl["x"].contiguous()
     ours = ffdas_b200.das(x, wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"])
     ref1 = reference.das(x, wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"], alg=1, tile=16)
     assert oracle.rel_l2(ours.cpu().numpy(), ref1.cpu().numpy()) < 1e-5
-    kmin, kmax = reference.k_range(wl["srcpos"].cpu().numpy(), wl["dstpos"].cpu().numpy(),
-                                   wl["offsets"].cpu().numpy())
-    if kmin >= 0 and kmax <= x.shape[-1] - 2:
-        ref2 = reference.das(x, wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"], alg=2)
-        # ALG2 quantises the fraction to fp16 (reference das_alg2_kernels.cuh:129)
-        assert oracle.rel_l2(ours.cpu().numpy(), ref2.cpu().numpy()) < 2e-3
 
 
 def test_fp16_input_against_reference_and_oracle():

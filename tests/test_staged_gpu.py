@@ -66,12 +66,14 @@ def test_staged_16bit_pairs(dtype, tol):
     assert oracle.rel_l2(_np(out), _ref(wl, x)) < tol
 
 
-def test_staged_equals_gather_bitwise():
+def test_staged_agrees_with_gather():
+    # same taps; the staged kernel sums even and odd events in two packed
+    # partial sums, so only the summation order differs
     wl = W.diverging3d(device=DEV, scale=0.25)
     x = wl["x"].float()
     a, _ = _run(wl, x, dict(variant=2, tile_x=16, tile_y=16, window=32, event_chunk=16))
     b, _ = _run(wl, x, dict(variant=1, tile_x=16, tile_y=16, batch_tile=1, event_chunk=16))
-    assert torch.equal(a, b)
+    assert oracle.rel_l2(_np(a), _np(b)) < 1e-6
 
 
 def test_overflowing_windows_fall_back_and_stay_correct():
