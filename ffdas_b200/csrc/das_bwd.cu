@@ -326,6 +326,50 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
     bp.gout_bstride = pb.out_bstride;
     bp.gx = gx; bp.goff = goff; bp.gw = gw; bp.gdst = gdst; bp.gsrc = gsrc;
 
+    pb.sparse = a.sparse;
+    if (!a.sparse && staged_supported(pb, kind) && !(h.has_config && h.config.variant == 1)) {
+        // Dense problems: TMA-staged adjoint, one CTA per voxel tile x batch item.
+        if (h.has_config && h.config.variant == 2 && (h.config.tile_x || h.config.tile_y)) {
+            const int tx = h.config.tile_x ? h.config.tile_x : 1, ty = h.config.tile_y ? h.config.tile_y : 1,
+                      tz = h.config.tile_z ? h.config.tile_z : 1;
+            if (tx * ty * tz == 256) {
+                bp.T0 = tx; bp.T1 = ty; bp.T2 = tz;
+                bp.n0 = (pb.D0 + tx - 1) / tx;
+                bp.n1 = (pb.D1 + ty - 1) / ty;
+            }
+        }
+        const int64_t stiles = (int64_t)bp.n0 * bp.n1 * ((pb.D2 + bp.T2 - 1) / bp.T2);
+        if (stiles > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
+        const size_t ve0 = (size_t)pb.n_events * pb.V * sizeof(float);
+        if (pb.B > 1) {  // several CTAs add into the voxel-side gradients
+            if (gw) FFDAS_CUDA(cudaMemsetAsync(gw, 0, ve0, h.stream));
+            if (goff) FFDAS_CUDA(cudaMemsetAsync(goff, 0, ve0, h.stream));
+            if (gdst) FFDAS_CUDA(cudaMemsetAsync(gdst, 0, (size_t)pb.V * 3 * sizeof(float), h.stream));
+        }
+        if (gsrc) FFDAS_CUDA(cudaMemsetAsync(gsrc, 0, (size_t)pb.C * 3 * sizeof(float), h.stream));
+        gather_params gp;
+        std::memset(&gp, 0, sizeof(gp));
+        gp.P = P.get<void>();
+        gp.npad = npad;
+        gp.C = pb.C; gp.S = pb.S; gp.n_events = pb.n_events; gp.B = pb.B; gp.V = pb.V;
+        gp.D0 = pb.D0; gp.D1 = pb.D1; gp.D2 = pb.D2;
+        gp.T0 = bp.T0; gp.T1 = bp.T1; gp.T2 = bp.T2; gp.n0 = bp.n0; gp.n1 = bp.n1;
+        gp.srcpos = a.srcpos; gp.dstpos = a.dstpos; gp.offsets = a.offsets; gp.weights = a.weights;
+        gp.beta_zero = 1;
+        const staged_grads gr{static_cast<const float *>(gout), pb.out_bstride, gx, goff, gw, gdst, gsrc};
+        const int SC = pb.n_events <= 1 ? 1 : (pb.n_events <= 4 ? 4 : 8);
+        const int WB = (h.has_config && h.config.window > 32) ? 64 : 32;
+        h.last = ffdas_kernel_info_t{};
+        h.last.variant = 4;
+        h.last.tile_x = bp.T0; h.last.tile_y = bp.T1; h.last.tile_z = bp.T2;
+        h.last.batch_tile = 1; h.last.event_chunk = SC; h.last.storage = kind;
+        h.last.kernels = 2; h.last.grid = stiles * pb.B;
+        h.mark_start();
+        const ffdas_error_t err = launch_staged_bwd(h, pb, kind, gp, gr, SC, WB, dim3((unsigned)stiles, (unsigned)pb.B));
+        h.mark_stop();
+        return err;
+    }
+
     const int BT = pb.B >= 4 ? 4 : (pb.B >= 2 ? 2 : 1);
     const int bchunks = (pb.B + BT - 1) / BT;
     const int64_t tiles = (int64_t)bp.n0 * bp.n1 * n2;

@@ -71,4 +71,13 @@ bool staged_supported(const das_problem &pb, int kind);
 ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp, int SC,
                             int WB, dim3 grid);
 
+// Gradient outputs of the staged adjoint kernel (null = not computed).
+struct staged_grads {
+    const float *gout;
+    int64_t gout_bstride;
+    float *gx, *goff, *gw, *gdst, *gsrc;
+};
+ffdas_error_t launch_staged_bwd(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,
+                                const staged_grads &gr, int SC, int WB, dim3 grid);
+
 }  // namespace ffdas

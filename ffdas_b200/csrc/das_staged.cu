@@ -1,13 +1,14 @@
-// das_staged.cu -- host side of the TMA-staged forward kernel.
+// das_staged.cu -- host side of the TMA-staged forward and adjoint kernels.
 //
 // Builds the 2-D tensor map over the pair rows (inner dim = pairs of a row,
 // outer dim = rows; 8-byte or 4-byte elements; box = WB pairs x 1 row;
-// out-of-bounds elements fill with zeros) and launches das_staged_kernel with
-// one CTA per (voxel tile, batch item).  cuTensorMapEncodeTiled is fetched
-// through cudaGetDriverEntryPoint so the library has no link-time dependency
-// on libcuda.
+// out-of-bounds elements fill with zeros) and launches one CTA per (voxel
+// tile, batch item).  cuTensorMapEncodeTiled is fetched through
+// cudaGetDriverEntryPoint so the library has no link-time dependency on
+// libcuda.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <cstring>
 #include <mutex>
 
 #include "core.h"
@@ -34,58 +35,85 @@ bool staged_supported(const das_problem &pb, int kind) {
     if (pb.sparse) return false;
     if (kind != ST_F32 && kind != ST_F16 && kind != ST_BF16) return false;
     const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
-    return rows > 0 && rows < INT32_MAX && tensor_map_encoder() != nullptr;
+    return rows > 0 && rows < INT32_MAX && pb.B <= 65535 && tensor_map_encoder() != nullptr;
+}
+
+// Tensor map over the pair rows: dims {npad, rows}, box {WB, 1}, zero OOB fill.
+static ffdas_error_t pair_row_map(CUtensorMap &map, const void *P, int64_t npad, int64_t rows, int kind, int WB) {
+    auto encode = tensor_map_encoder();
+    if (!encode) return FFDAS_ERROR_CUDA_DRIVER;
+    const int pair_bytes = (kind == ST_F32) ? 8 : 4;
+    const cuuint64_t dims[2] = {(cuuint64_t)npad, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)npad * pair_bytes};
+    const cuuint32_t box[2] = {(cuuint32_t)WB, 1u};
+    const cuuint32_t estr[2] = {1u, 1u};
+    const CUresult r = encode(&map, pair_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32,
+                              2, const_cast<void *>(P), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? FFDAS_SUCCESS : FFDAS_ERROR_CUDA_DRIVER;
+}
+
+template <typename Kernel>
+static ffdas_error_t prepare_kernel(Kernel kernel, size_t smem) {
+    FFDAS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // all of the unified L1/shared array as shared memory: several CTAs per SM
+    FFDAS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared));
+    return FFDAS_SUCCESS;
 }
 
 template <int K, int SC, int WB>
-static ffdas_error_t launch_staged_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
+static ffdas_error_t launch_fwd_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
     constexpr size_t smem = staged_smem_bytes<WB, K>();
-    static bool attr_set = false;  // per instantiation; benign race (idempotent)
-    if (!attr_set) {
-        FFDAS_CUDA(cudaFuncSetAttribute(das_staged_kernel<K, SC, WB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem));
-        // all of the unified L1/shared array as shared memory: several CTAs per SM
-        FFDAS_CUDA(cudaFuncSetAttribute(das_staged_kernel<K, SC, WB>,
-                                        cudaFuncAttributePreferredSharedMemoryCarveout,
-                                        (int)cudaSharedmemCarveoutMaxShared));
-        attr_set = true;
+    static bool ready = false;  // per instantiation; idempotent
+    if (!ready) {
+        FFDAS_TRY(prepare_kernel(das_staged_kernel<K, SC, WB>, smem));
+        ready = true;
     }
     das_staged_kernel<K, SC, WB><<<grid, kStThreads, smem, h.stream>>>(sp, map);
     return ffdas_launch_check(h.stream);
 }
 
+template <int K, int SC, int WB>
+static ffdas_error_t launch_bwd_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
+    constexpr size_t smem = staged_bwd_smem_bytes<WB, K, SC>();
+    static bool ready = false;
+    if (!ready) {
+        FFDAS_TRY(prepare_kernel(das_staged_bwd_kernel<K, SC, WB>, smem));
+        ready = true;
+    }
+    das_staged_bwd_kernel<K, SC, WB><<<grid, kStThreads, smem, h.stream>>>(sp, map);
+    return ffdas_launch_check(h.stream);
+}
+
 template <int K, int WB>
-static ffdas_error_t launch_staged_sc(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, int SC,
-                                      dim3 grid) {
+static ffdas_error_t launch_fwd_sc(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, int SC,
+                                   dim3 grid) {
     switch (SC) {
-        case 1: return launch_staged_t<K, 1, WB>(h, sp, map, grid);
-        case 4: return launch_staged_t<K, 4, WB>(h, sp, map, grid);
-        case 8: return launch_staged_t<K, 8, WB>(h, sp, map, grid);
-        default: return launch_staged_t<K, 16, WB>(h, sp, map, grid);
+        case 1: return launch_fwd_t<K, 1, WB>(h, sp, map, grid);
+        case 4: return launch_fwd_t<K, 4, WB>(h, sp, map, grid);
+        case 8: return launch_fwd_t<K, 8, WB>(h, sp, map, grid);
+        default: return launch_fwd_t<K, 16, WB>(h, sp, map, grid);
     }
 }
 
-ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp, int SC,
-                            int WB, dim3 grid) {
-    auto encode = tensor_map_encoder();
-    if (!encode) return FFDAS_ERROR_CUDA_DRIVER;
-    const int pair_bytes = (kind == ST_F32) ? 8 : 4;
-    const cuuint64_t rows = (cuuint64_t)pb.B * pb.C * pb.S;
-    CUtensorMap map;
-    const cuuint64_t dims[2] = {(cuuint64_t)gp.npad, rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)gp.npad * pair_bytes};
-    const cuuint32_t box[2] = {(cuuint32_t)WB, 1u};
-    const cuuint32_t estr[2] = {1u, 1u};
-    CUresult r = encode(&map, pair_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32, 2,
-                        const_cast<void *>(gp.P), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return FFDAS_ERROR_CUDA_DRIVER;
+template <int K, int WB>
+static ffdas_error_t launch_bwd_sc(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, int SC,
+                                   dim3 grid) {
+    switch (SC) {
+        case 1: return launch_bwd_t<K, 1, WB>(h, sp, map, grid);
+        case 4: return launch_bwd_t<K, 4, WB>(h, sp, map, grid);
+        default: return launch_bwd_t<K, 8, WB>(h, sp, map, grid);
+    }
+}
 
+static staged_params base_params(ffdas_context &h, const das_problem &pb, const gather_params &gp) {
     staged_params sp;
+    std::memset(&sp, 0, sizeof(sp));
     sp.P = gp.P;
     sp.npad = gp.npad;
-    sp.C = gp.C; sp.S = gp.S; sp.n_events = gp.n_events; sp.B = gp.B; sp.V = gp.V;
+    sp.C = gp.C; sp.S = gp.S; sp.N = pb.N; sp.n_events = gp.n_events; sp.B = gp.B; sp.V = gp.V;
     sp.D0 = gp.D0; sp.D1 = gp.D1; sp.D2 = gp.D2;
     sp.T0 = gp.T0; sp.T1 = gp.T1; sp.T2 = gp.T2; sp.n0 = gp.n0; sp.n1 = gp.n1;
     sp.srcpos = gp.srcpos; sp.srcdir = gp.srcdir; sp.dstpos = gp.dstpos;
@@ -94,17 +122,40 @@ ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, c
     sp.beta_re = gp.beta_re; sp.beta_zero = gp.beta_zero;
     sp.status = h.status;
     sp.debug_drop_stage = ffdas_take_debug_drop_stage();
+    return sp;
+}
 
+ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp, int SC,
+                            int WB, dim3 grid) {
+    CUtensorMap map;
+    FFDAS_TRY(pair_row_map(map, gp.P, gp.npad, (int64_t)pb.B * pb.C * pb.S, kind, WB));
+    const staged_params sp = base_params(h, pb, gp);
     switch (kind) {
         case ST_F32:
-            return WB == 64 ? launch_staged_sc<ST_F32, 64>(h, sp, map, SC, grid)
-                            : launch_staged_sc<ST_F32, 32>(h, sp, map, SC, grid);
+            return WB == 64 ? launch_fwd_sc<ST_F32, 64>(h, sp, map, SC, grid) : launch_fwd_sc<ST_F32, 32>(h, sp, map, SC, grid);
         case ST_F16:
-            return WB == 64 ? launch_staged_sc<ST_F16, 64>(h, sp, map, SC, grid)
-                            : launch_staged_sc<ST_F16, 32>(h, sp, map, SC, grid);
+            return WB == 64 ? launch_fwd_sc<ST_F16, 64>(h, sp, map, SC, grid) : launch_fwd_sc<ST_F16, 32>(h, sp, map, SC, grid);
         default:
-            return WB == 64 ? launch_staged_sc<ST_BF16, 64>(h, sp, map, SC, grid)
-                            : launch_staged_sc<ST_BF16, 32>(h, sp, map, SC, grid);
+            return WB == 64 ? launch_fwd_sc<ST_BF16, 64>(h, sp, map, SC, grid) : launch_fwd_sc<ST_BF16, 32>(h, sp, map, SC, grid);
+    }
+}
+
+ffdas_error_t launch_staged_bwd(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,
+                                const staged_grads &gr, int SC, int WB, dim3 grid) {
+    CUtensorMap map;
+    FFDAS_TRY(pair_row_map(map, gp.P, gp.npad, (int64_t)pb.B * pb.C * pb.S, kind, WB));
+    staged_params sp = base_params(h, pb, gp);
+    sp.gout = gr.gout;
+    sp.gout_bstride = gr.gout_bstride;
+    sp.gx = gr.gx; sp.goff = gr.goff; sp.gw = gr.gw; sp.gdst = gr.gdst; sp.gsrc = gr.gsrc;
+    const int sc = SC > 8 ? 8 : SC;
+    switch (kind) {
+        case ST_F32:
+            return WB == 64 ? launch_bwd_sc<ST_F32, 64>(h, sp, map, sc, grid) : launch_bwd_sc<ST_F32, 32>(h, sp, map, sc, grid);
+        case ST_F16:
+            return WB == 64 ? launch_bwd_sc<ST_F16, 64>(h, sp, map, sc, grid) : launch_bwd_sc<ST_F16, 32>(h, sp, map, sc, grid);
+        default:
+            return WB == 64 ? launch_bwd_sc<ST_BF16, 64>(h, sp, map, sc, grid) : launch_bwd_sc<ST_BF16, 32>(h, sp, map, sc, grid);
     }
 }
 

@@ -1,4 +1,4 @@
-// das_staged.cuh -- forward delay-and-sum, TMA-staged schedule (sm_100a).
+// das_staged.cuh -- TMA-staged delay-and-sum kernels (sm_100a): forward and adjoint.
 //
 // A CTA owns a compact tile of 256 voxels (one per consumer thread) and one
 // batch item.  A ninth warp is the producer: for every (channel, event) it
@@ -7,8 +7,8 @@
 // window of interpolation pairs into shared memory with one TMA tile load
 // (cp.async.bulk.tensor, no multicast), running up to kStages chunks ahead of
 // the consumers through a full/empty mbarrier ring.  Consumers then gather
-// each tap from shared memory: per unit one FFMA for the delay, the
-// floor/fraction split, one index clamp, one 8-byte LDS and two FFMAs.
+// each tap from shared memory: per unit one packed FFMA for the delay, the
+// floor/fraction split, one index clamp, one LDS and the taps/accumulates.
 //
 // Window slot layout: WB pairs written by TMA, followed by a permanent zero
 // pair (zeroed once per CTA, never written by TMA).  A tap index is clamped to
@@ -20,8 +20,14 @@
 // global memory instead.
 //
 // Every mbarrier wait is bounded by a clock budget; on expiry the CTA records
-// FFDAS_DEVICE_STATUS_TIMEOUT in the status word, stops issuing and
-// computing, drains its own TMA copies (bounded) and exits without trapping.
+// status 1 in the handle's status word, stops issuing and computing, drains
+// its own TMA copies (bounded) and exits without trapping.
+//
+// The adjoint kernel (das_staged_bwd_kernel) runs the same producer and
+// window ring; its consumers recompute each tap and scatter the
+// channel-data adjoint g*w*(1-t), g*w*t into a per-window shared gradient
+// slot, which is flushed to global memory with one red.add per touched
+// sample after the stage.
 #pragma once
 
 #include <cuda.h>
@@ -41,7 +47,7 @@ constexpr int kStatusTimeout = 1;
 struct staged_params {
     const void *P;
     int64_t npad;
-    int C, S, n_events, B;
+    int C, S, N, n_events, B;
     int64_t V;
     int D0, D1, D2, T0, T1, T2, n0, n1;
     const float *srcpos;
@@ -53,6 +59,10 @@ struct staged_params {
     int beta_zero;
     int *status;
     int debug_drop_stage;  // test hook: the producer never fills the first stage
+    // adjoint only
+    const float *gout;
+    int64_t gout_bstride;
+    float *gx, *goff, *gw, *gdst, *gsrc;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -78,6 +88,9 @@ __device__ __forceinline__ void tma_load_row(uint32_t dst, const CUtensorMap *ma
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
         ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar) : "memory");
+}
+__device__ __forceinline__ void consumer_sync() {
+    asm volatile("bar.sync 1, %0;" ::"r"(kStConsumers) : "memory");
 }
 
 // Bounded wait: false when the CTA aborted or the clock budget ran out.
@@ -120,85 +133,110 @@ template <int WB, int K> struct slot_geom {
 // yields an index inside the slot, so every tap reads the zero pair.
 constexpr uint32_t kZeroWindow = kFloorMagicBits + 0x40000000u;
 
+constexpr size_t kStMiscBytes = kStages * kStWin * 4      // meta
+                                + kStages * 4              // overflow flags
+                                + 2 * kStages * 8          // full / empty barriers
+                                + 40 * 4                   // bounding box, per-event delay range
+                                + 32 * 4                   // abort flag (+pad)
+                                + kStWarps * 16 * 2 * 4    // reduction scratch
+                                + kStages * kStWin * 2 * 16;  // channel table (position, normal)
+
 template <int WB, int K>
 constexpr size_t staged_smem_bytes() {
-    return slot_geom<WB, K>::ring_bytes + kStages * kStWin * 4 + kStages * 4 + 2 * kStages * 8 + 64 * 4 + 32 * 4 +
-           kStWarps * 16 * 2 * 4 + kStages * kStWin * 2 * 16 + 128;
+    return slot_geom<WB, K>::ring_bytes + kStMiscBytes + 128;
 }
 
-// Interpolate one tap from a staged slot and return it (f32 accumulation).
-template <int K>
-__device__ __forceinline__ float staged_tap(const unsigned char *slot, uint32_t rel, float t) {
-    using st = typename pair_traits<K>::storage;
-    return pair_traits<K>::tap(*reinterpret_cast<const st *>(slot + rel * sizeof(st)), t);
+// Adjoint extras: gradient slots [kStages][kStWin][WB + 2] floats and the
+// per-stage channel-gradient scratch [kStWin / SC * 3][256] floats.
+template <int WB, int K, int SC>
+constexpr size_t staged_bwd_smem_bytes() {
+    return staged_smem_bytes<WB, K>() + kStages * kStWin * (WB + 2) * 4 + (kStWin / SC) * 3 * kStConsumers * 4;
 }
 
-template <int K, int SC, int WB>
-__global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_params p,
-                                                                 const __grid_constant__ CUtensorMap tmap) {
-    using tr = pair_traits<K>;
-    using st = typename tr::storage;
+// Shared-memory layout shared by the forward and adjoint kernels.
+template <int K, int WB>
+struct staged_smem {
     using SG = slot_geom<WB, K>;
-    constexpr int CC = kStWin / SC;  // channels per stage
-    static_assert(kStWin % SC == 0, "SC must divide the stage");
+    unsigned char *ring;
+    uint32_t *meta;        // [kStages][kStWin]
+    int *ovf;              // [kStages]
+    uint64_t *full, *empty;
+    float *aabb;           // [6]
+    float *ofs_lo, *ofs_hi;  // [16]
+    volatile int *abort_flag;
+    float *red;            // [warps][16][2]
+    float4 *chan_pos, *chan_dir;  // [kStages][kStWin]
+    unsigned char *extra;  // adjoint scratch
 
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char *ring = smem_raw;
-    uint32_t *meta = reinterpret_cast<uint32_t *>(ring + SG::ring_bytes);    // [kStages][kStWin]
-    int *ovf = reinterpret_cast<int *>(meta + kStages * kStWin);             // [kStages]
-    uint64_t *full = reinterpret_cast<uint64_t *>(ovf + kStages);            // [kStages]
-    uint64_t *empty = full + kStages;                                        // [kStages]
-    float *aabb = reinterpret_cast<float *>(empty + kStages);                // [6] (+pad)
-    float *ofs_lo = aabb + 8;                                                // [16]
-    float *ofs_hi = ofs_lo + 16;                                             // [16]
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(ofs_hi + 16);
-    float *red = const_cast<float *>(reinterpret_cast<volatile float *>(abort_flag + 32));  // [warps][16][2]
-    float4 *chan_pos = reinterpret_cast<float4 *>(red + kStWarps * 32);                    // [kStages][kStWin]
-    float4 *chan_dir = chan_pos + kStages * kStWin;                                        // [kStages][kStWin]
+    __device__ explicit staged_smem(unsigned char *raw) {
+        ring = raw;
+        meta = reinterpret_cast<uint32_t *>(ring + SG::ring_bytes);
+        ovf = reinterpret_cast<int *>(meta + kStages * kStWin);
+        full = reinterpret_cast<uint64_t *>(ovf + kStages);
+        empty = full + kStages;
+        aabb = reinterpret_cast<float *>(empty + kStages);
+        ofs_lo = aabb + 8;
+        ofs_hi = ofs_lo + 16;
+        abort_flag = reinterpret_cast<volatile int *>(ofs_hi + 16);
+        red = const_cast<float *>(reinterpret_cast<volatile float *>(abort_flag + 32));
+        chan_pos = reinterpret_cast<float4 *>(red + kStWarps * 32);
+        chan_dir = chan_pos + kStages * kStWin;
+        extra = reinterpret_cast<unsigned char *>(chan_dir + kStages * kStWin);
+    }
+};
 
-    const int tid = threadIdx.x;
-    const int warp = tid >> 5, lane = tid & 31;
-    const bool producer = (warp == kStWarps);
-    const int b = blockIdx.y;
+// Per-CTA state common to both kernels.
+struct staged_ctx {
+    int tid, warp, lane, b;
+    bool producer, active;
+    int64_t v;
+    float vx, vy, vz;
+};
 
-    // ---- voxel of this consumer thread ----
+// Voxel of the thread, barrier init, zero pairs, tile bounding box.
+template <int K, int WB>
+__device__ __forceinline__ staged_ctx staged_setup(const staged_params &p, staged_smem<K, WB> &sm) {
+    using SG = slot_geom<WB, K>;
+    staged_ctx cx;
+    cx.tid = threadIdx.x;
+    cx.warp = cx.tid >> 5;
+    cx.lane = cx.tid & 31;
+    cx.producer = (cx.warp == kStWarps);
+    cx.b = blockIdx.y;
+    cx.active = false;
+    cx.v = 0;
+    cx.vx = cx.vy = cx.vz = 0.f;
     const int tile = blockIdx.x;
     const int t0 = tile % p.n0, t1 = (tile / p.n0) % p.n1, t2 = tile / (p.n0 * p.n1);
-    bool active = false;
-    int64_t v = 0;
-    float vx = 0.f, vy = 0.f, vz = 0.f;
-    if (!producer) {
-        const int i0 = tid % p.T0, i1 = (tid / p.T0) % p.T1, i2 = tid / (p.T0 * p.T1);
+    if (!cx.producer) {
+        const int i0 = cx.tid % p.T0, i1 = (cx.tid / p.T0) % p.T1, i2 = cx.tid / (p.T0 * p.T1);
         const int g0 = t0 * p.T0 + i0, g1 = t1 * p.T1 + i1, g2 = t2 * p.T2 + i2;
-        active = (g0 < p.D0 && g1 < p.D1 && g2 < p.D2);
-        if (active) {
-            v = ((int64_t)g2 * p.D1 + g1) * p.D0 + g0;
-            vx = __ldg(p.dstpos + 3 * v);
-            vy = __ldg(p.dstpos + 3 * v + 1);
-            vz = __ldg(p.dstpos + 3 * v + 2);
+        cx.active = (g0 < p.D0 && g1 < p.D1 && g2 < p.D2);
+        if (cx.active) {
+            cx.v = ((int64_t)g2 * p.D1 + g1) * p.D0 + g0;
+            cx.vx = __ldg(p.dstpos + 3 * cx.v);
+            cx.vy = __ldg(p.dstpos + 3 * cx.v + 1);
+            cx.vz = __ldg(p.dstpos + 3 * cx.v + 2);
         }
     }
-
-    // ---- init: barriers, zero regions, abort flag ----
-    if (tid == 0) {
+    if (cx.tid == 0) {
         for (int i = 0; i < kStages; i++) {
-            mbar_init(smem_u32(&full[i]), 1);
-            mbar_init(smem_u32(&empty[i]), kStWarps);
+            mbar_init(smem_u32(&sm.full[i]), 1);
+            mbar_init(smem_u32(&sm.empty[i]), kStWarps);
         }
-        *abort_flag = 0;
+        *sm.abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     {
         constexpr int zwords = (SG::bytes - SG::data_bytes) / 4;
-        for (int i = tid; i < kStages * kStWin * zwords; i += kStThreads) {
+        for (int i = cx.tid; i < kStages * kStWin * zwords; i += kStThreads) {
             const int slot = i / zwords, word = i - slot * zwords;
-            reinterpret_cast<uint32_t *>(ring + slot * SG::bytes + SG::data_bytes)[word] = 0u;
+            reinterpret_cast<uint32_t *>(sm.ring + slot * SG::bytes + SG::data_bytes)[word] = 0u;
         }
     }
-    // ---- tile bounding box (consumers) ----
-    if (!producer) {
-        float mn[3] = {active ? vx : INFINITY, active ? vy : INFINITY, active ? vz : INFINITY};
-        float mx[3] = {active ? vx : -INFINITY, active ? vy : -INFINITY, active ? vz : -INFINITY};
+    if (!cx.producer) {
+        float mn[3] = {cx.active ? cx.vx : INFINITY, cx.active ? cx.vy : INFINITY, cx.active ? cx.vz : INFINITY};
+        float mx[3] = {cx.active ? cx.vx : -INFINITY, cx.active ? cx.vy : -INFINITY, cx.active ? cx.vz : -INFINITY};
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
@@ -207,25 +245,198 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
                 mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
             }
         }
-        if (lane == 0) {
+        if (cx.lane == 0) {
 #pragma unroll
             for (int a = 0; a < 3; a++) {
-                red[(warp * 16 + a) * 2] = mn[a];
-                red[(warp * 16 + a) * 2 + 1] = mx[a];
+                sm.red[(cx.warp * 16 + a) * 2] = mn[a];
+                sm.red[(cx.warp * 16 + a) * 2 + 1] = mx[a];
             }
         }
     }
     __syncthreads();
-    if (tid < 3) {
+    if (cx.tid < 3) {
         float mn = INFINITY, mx = -INFINITY;
         for (int w = 0; w < kStWarps; w++) {
-            mn = fminf(mn, red[(w * 16 + tid) * 2]);
-            mx = fmaxf(mx, red[(w * 16 + tid) * 2 + 1]);
+            mn = fminf(mn, sm.red[(w * 16 + cx.tid) * 2]);
+            mx = fmaxf(mx, sm.red[(w * 16 + cx.tid) * 2 + 1]);
         }
-        aabb[tid] = mn;
-        aabb[3 + tid] = mx;
+        sm.aabb[cx.tid] = mn;
+        sm.aabb[3 + cx.tid] = mx;
     }
     __syncthreads();
+    return cx;
+}
+
+// Consumers: load this pass's delays and weights, reduce the tile's per-event
+// delay range into ofs_lo / ofs_hi.  Ends with __syncthreads (all threads).
+template <int K, int WB, int SC>
+__device__ __forceinline__ void staged_pass_begin(const staged_params &p, staged_smem<K, WB> &sm,
+                                                  const staged_ctx &cx, int e0, int sc, float (&ofs)[SC],
+                                                  float (&w)[SC]) {
+    if (!cx.producer) {
+#pragma unroll
+        for (int j = 0; j < SC; j++) {
+            ofs[j] = 1e30f;
+            w[j] = 0.f;
+            if (cx.active && j < sc) {
+                const int64_t idx = (int64_t)(e0 + j) * p.V + cx.v;
+                ofs[j] = __ldg(p.offsets + idx);
+                w[j] = __ldg(p.weights + idx);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < SC; j++) {
+            const bool ok = cx.active && j < sc && isfinite(ofs[j]);
+            float lo = ok ? ofs[j] : INFINITY, hi = ok ? ofs[j] : -INFINITY;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+            }
+            if (cx.lane == 0) {
+                sm.red[(cx.warp * 16 + j) * 2] = lo;
+                sm.red[(cx.warp * 16 + j) * 2 + 1] = hi;
+            }
+        }
+        consumer_sync();
+        if (cx.tid < SC) {
+            float lo = INFINITY, hi = -INFINITY;
+            for (int ww = 0; ww < kStWarps; ww++) {
+                lo = fminf(lo, sm.red[(ww * 16 + cx.tid) * 2]);
+                hi = fmaxf(hi, sm.red[(ww * 16 + cx.tid) * 2 + 1]);
+            }
+            sm.ofs_lo[cx.tid] = lo;
+            sm.ofs_hi[cx.tid] = hi;
+        }
+    }
+    __syncthreads();
+}
+
+// Producer warp: stage the windows of CC channels x SC events of one chunk.
+// Publishes, with the full barrier's arrival, the window metadata, the
+// overflow flag and the channel table of the stage.
+template <int K, int WB, int SC>
+__device__ __forceinline__ void staged_produce(const staged_params &p, const CUtensorMap *tmap,
+                                               staged_smem<K, WB> &sm, const staged_ctx &cx, int stage,
+                                               uint32_t phase, int e0, int sc, int c0, bool &dead,
+                                               uint32_t &issued_mask) {
+    using SG = slot_geom<WB, K>;
+    using st = typename pair_traits<K>::storage;
+    const uint32_t full_bar = smem_u32(&sm.full[stage]);
+    const uint32_t empty_bar = smem_u32(&sm.empty[stage]);
+    unsigned char *stage_base = sm.ring + stage * SG::stage_bytes;
+    const int lane = cx.lane;
+    if (!dead && !bounded_wait(empty_bar, phase ^ 1u, sm.abort_flag, p.status)) dead = true;
+    // Test hook: leave the very first stage unfilled (no copy, no arrival) so
+    // the consumers' bounded waits must expire.
+    const bool drop = p.debug_drop_stage && e0 == 0 && c0 == 0;
+    if (drop) dead = true;
+    bool issued = false, overflow = false;
+    if (!dead) {
+        const int cl = lane / SC, j = lane % SC;
+        const int c = c0 + cl;
+        uint32_t m = kZeroWindow;  // every tap index clamps to the zero pair
+        float px = 0.f, py = 0.f, pz = 0.f;
+        if (c < p.C) {
+            px = __ldg(p.srcpos + 3 * c);
+            py = __ldg(p.srcpos + 3 * c + 1);
+            pz = __ldg(p.srcpos + 3 * c + 2);
+        }
+        if (j == 0) {
+            sm.chan_pos[stage * kStWin + cl] = make_float4(px, py, pz, 0.f);
+            if (p.srcdir)
+                sm.chan_dir[stage * kStWin + cl] = (c < p.C) ? __ldg(p.srcdir + c) : make_float4(0, 0, 0, 2.f);
+        }
+        if (c < p.C && j < sc) {
+            const float *bb = sm.aabb;
+            const float dx = fmaxf(fmaxf(bb[0] - px, px - bb[3]), 0.f);
+            const float dy = fmaxf(fmaxf(bb[1] - py, py - bb[4]), 0.f);
+            const float dz = fmaxf(fmaxf(bb[2] - pz, pz - bb[5]), 0.f);
+            const float ex = fmaxf(fabsf(px - bb[0]), fabsf(px - bb[3]));
+            const float ey = fmaxf(fabsf(py - bb[1]), fabsf(py - bb[4]));
+            const float ez = fmaxf(fabsf(pz - bb[2]), fabsf(pz - bb[5]));
+            const float rmin = sqrtf(dx * dx + dy * dy + dz * dz);
+            const float rmax = sqrtf(ex * ex + ey * ey + ez * ez);
+            const float lo = floorf(sm.ofs_lo[j] + rmin) - 2.f;
+            const float hi = floorf(sm.ofs_hi[j] + rmax) + 2.f;
+            // a window that misses the pair row entirely stays a zero window
+            if (lo == lo && hi == hi && hi >= 0.f && lo < (float)p.npad) {
+                const int k0 = ((int)fmaxf(lo, -(float)WB)) & ~(staged_traits<K>::align_pairs - 1);
+                const int k1 = (int)fminf(hi, (float)p.npad + WB);
+                if (k1 - k0 + 1 <= WB) {
+                    const int row = (cx.b * p.C + c) * p.S + (e0 + j);
+                    tma_load_row(smem_u32(stage_base + lane * SG::bytes), tmap, k0, row, full_bar);
+                    m = kFloorMagicBits + (uint32_t)k0;
+                    issued = true;
+                } else {
+                    m = kOvf;
+                    overflow = true;
+                }
+            }
+        }
+        sm.meta[stage * kStWin + lane] = m;
+    }
+    const unsigned issued_ballot = __ballot_sync(0xffffffffu, issued);
+    const unsigned ovf_ballot = __ballot_sync(0xffffffffu, overflow);
+    __syncwarp();
+    if (lane == 0 && !drop) {
+        sm.ovf[stage] = ovf_ballot != 0u;
+        // the producer's arrival also publishes meta / ovf / channel table (release)
+        mbar_arrive_expect_tx(full_bar, (uint32_t)__popc(issued_ballot) * (uint32_t)(WB * sizeof(st)));
+    }
+    if (!dead) issued_mask |= (1u << stage);
+}
+
+// After an abort the producer waits (bounded, ignoring the abort flag) until
+// every copy its CTA issued has landed, so no TMA write outlives the CTA.
+template <int K, int WB>
+__device__ __forceinline__ void staged_drain(staged_smem<K, WB> &sm, const staged_ctx &cx, int stage,
+                                             uint32_t phase, uint32_t issued_mask) {
+    if (*sm.abort_flag && cx.lane == 0) {
+        for (int i = 0; i < kStages; i++) {
+            const int s = (stage + i) % kStages;
+            if (!(issued_mask & (1u << s))) continue;
+            const uint32_t par = (s < stage) ? phase : (phase ^ 1u);
+            const long long t0 = clock64();
+            while (!mbar_try_wait(smem_u32(&sm.full[s]), par) && clock64() - t0 < kWaitCycles) __nanosleep(64);
+        }
+    }
+}
+
+// Interpolate one tap from a staged slot (f32 result).
+template <int K>
+__device__ __forceinline__ float staged_tap(const unsigned char *slot, uint32_t rel, float t) {
+    using st = typename pair_traits<K>::storage;
+    return pair_traits<K>::tap(*reinterpret_cast<const st *>(slot + rel * sizeof(st)), t);
+}
+
+// Read the SC window metadata words of channel cl of a stage.
+template <int SC>
+__device__ __forceinline__ void load_meta(const uint32_t *meta, int stage, int cl, uint32_t (&k0p)[SC]) {
+    if constexpr (SC >= 4) {
+#pragma unroll
+        for (int j = 0; j < SC; j += 4) {
+            const uint4 q = *reinterpret_cast<const uint4 *>(&meta[stage * kStWin + cl * SC + j]);
+            k0p[j] = q.x; k0p[j + 1] = q.y; k0p[j + 2] = q.z; k0p[j + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < SC; q++) k0p[q] = meta[stage * kStWin + cl * SC + q];
+    }
+}
+
+// ------------------------------------------------------------------ forward ---
+template <int K, int SC, int WB>
+__global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_params p,
+                                                                 const __grid_constant__ CUtensorMap tmap) {
+    using st = typename pair_traits<K>::storage;
+    using SG = slot_geom<WB, K>;
+    constexpr int CC = kStWin / SC;  // channels per stage
+    static_assert(kStWin % SC == 0, "SC must divide the stage");
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    staged_smem<K, WB> sm(smem_raw);
+    const staged_ctx cx = staged_setup<K, WB>(p, sm);
 
     const st *__restrict__ Pg = static_cast<const st *>(p.P);
     const uint32_t kmax_pair = (uint32_t)(p.npad - 1);
@@ -234,139 +445,32 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
     int stage = 0;
     uint32_t phase = 0;
     bool dead = false;
-    uint32_t issued_mask = 0;  // producer: stages whose copies may still be in flight
+    uint32_t issued_mask = 0;
 
     for (int e0 = 0; e0 < p.n_events; e0 += SC) {
         const int sc = min(SC, p.n_events - e0);
         float ofs[SC], w[SC];
-        // ---- per-event delay range of the tile (consumers) ----
-        if (!producer) {
-#pragma unroll
-            for (int j = 0; j < SC; j++) {
-                ofs[j] = 1e30f;
-                w[j] = 0.f;
-                if (active && j < sc) {
-                    const int64_t idx = (int64_t)(e0 + j) * p.V + v;
-                    ofs[j] = __ldg(p.offsets + idx);
-                    w[j] = __ldg(p.weights + idx);
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < SC; j++) {
-                const bool ok = active && j < sc && isfinite(ofs[j]);
-                float lo = ok ? ofs[j] : INFINITY, hi = ok ? ofs[j] : -INFINITY;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-                    hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-                }
-                if (lane == 0) {
-                    red[(warp * 16 + j) * 2] = lo;
-                    red[(warp * 16 + j) * 2 + 1] = hi;
-                }
-            }
-            asm volatile("bar.sync 1, %0;" ::"r"(kStConsumers) : "memory");
-            if (tid < SC) {
-                float lo = INFINITY, hi = -INFINITY;
-                for (int ww = 0; ww < kStWarps; ww++) {
-                    lo = fminf(lo, red[(ww * 16 + tid) * 2]);
-                    hi = fmaxf(hi, red[(ww * 16 + tid) * 2 + 1]);
-                }
-                ofs_lo[tid] = lo;
-                ofs_hi[tid] = hi;
-            }
-        }
-        __syncthreads();
+        staged_pass_begin<K, WB, SC>(p, sm, cx, e0, sc, ofs, w);
 
         for (int c0 = 0; c0 < p.C; c0 += CC) {
-            const uint32_t full_bar = smem_u32(&full[stage]);
-            const uint32_t empty_bar = smem_u32(&empty[stage]);
-            unsigned char *stage_base = ring + stage * SG::stage_bytes;
-            if (producer) {
-                // ---- stage the windows of CC channels x SC events ----
-                if (!dead && !bounded_wait(empty_bar, phase ^ 1u, abort_flag, p.status)) dead = true;
-                // Test hook: leave the very first stage unfilled (no copy, no
-                // arrival) so the consumers' bounded waits must expire.
-                const bool drop = p.debug_drop_stage && e0 == 0 && c0 == 0;
-                if (drop) dead = true;
-                bool issued = false, overflow = false;
-                if (!dead) {
-                    const int cl = lane / SC, j = lane % SC;
-                    const int c = c0 + cl;
-                    uint32_t m = kZeroWindow;  // every tap index clamps to the zero pair
-                    float cx = 0.f, cy = 0.f, cz = 0.f;
-                    if (c < p.C) {
-                        cx = __ldg(p.srcpos + 3 * c);
-                        cy = __ldg(p.srcpos + 3 * c + 1);
-                        cz = __ldg(p.srcpos + 3 * c + 2);
-                    }
-                    if (j == 0) {
-                        // channel table of the stage, read by the consumers
-                        chan_pos[stage * kStWin + cl] = make_float4(cx, cy, cz, 0.f);
-                        if (p.srcdir)
-                            chan_dir[stage * kStWin + cl] = (c < p.C) ? __ldg(p.srcdir + c) : make_float4(0, 0, 0, 2.f);
-                    }
-                    if (c < p.C && j < sc) {
-                        const float dx = fmaxf(fmaxf(aabb[0] - cx, cx - aabb[3]), 0.f);
-                        const float dy = fmaxf(fmaxf(aabb[1] - cy, cy - aabb[4]), 0.f);
-                        const float dz = fmaxf(fmaxf(aabb[2] - cz, cz - aabb[5]), 0.f);
-                        const float ex = fmaxf(fabsf(cx - aabb[0]), fabsf(cx - aabb[3]));
-                        const float ey = fmaxf(fabsf(cy - aabb[1]), fabsf(cy - aabb[4]));
-                        const float ez = fmaxf(fabsf(cz - aabb[2]), fabsf(cz - aabb[5]));
-                        const float rmin = sqrtf(dx * dx + dy * dy + dz * dz);
-                        const float rmax = sqrtf(ex * ex + ey * ey + ez * ez);
-                        const float lo = floorf(ofs_lo[j] + rmin) - 2.f;
-                        const float hi = floorf(ofs_hi[j] + rmax) + 2.f;
-                        // a window that misses the pair row entirely stays a zero window
-                        if (lo == lo && hi == hi && hi >= 0.f && lo < (float)p.npad) {
-                            const int k0 = ((int)fmaxf(lo, -(float)WB)) & ~(staged_traits<K>::align_pairs - 1);
-                            const int k1 = (int)fminf(hi, (float)p.npad + WB);
-                            if (k1 - k0 + 1 <= WB) {
-                                const int row = (b * p.C + c) * p.S + (e0 + j);
-                                const uint32_t dst = smem_u32(stage_base + lane * SG::bytes);
-                                tma_load_row(dst, &tmap, k0, row, full_bar);
-                                m = kFloorMagicBits + (uint32_t)k0;
-                                issued = true;
-                            } else {
-                                m = kOvf;
-                                overflow = true;
-                            }
-                        }
-                    }
-                    meta[stage * kStWin + lane] = m;
-                }
-                const unsigned issued_ballot = __ballot_sync(0xffffffffu, issued);
-                const unsigned ovf_ballot = __ballot_sync(0xffffffffu, overflow);
-                __syncwarp();
-                if (lane == 0 && !drop) {
-                    ovf[stage] = ovf_ballot != 0u;
-                    // the producer's arrive also publishes meta/ovf (release)
-                    mbar_arrive_expect_tx(full_bar, (uint32_t)__popc(issued_ballot) * (uint32_t)(WB * sizeof(st)));
-                }
-                if (!dead) issued_mask |= (1u << stage);
+            if (cx.producer) {
+                staged_produce<K, WB, SC>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
             } else {
-                // ---- consume: CC channels x SC events from shared memory ----
-                if (!dead && !bounded_wait(full_bar, phase, abort_flag, p.status)) dead = true;
+                const uint32_t full_bar = smem_u32(&sm.full[stage]);
+                const unsigned char *stage_base = sm.ring + stage * SG::stage_bytes;
+                if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
                 if (!dead) {
-                    const bool any_ovf = ovf[stage] != 0;
+                    const bool any_ovf = sm.ovf[stage] != 0;
                     for (int cl = 0; cl < CC; cl++) {
                         const int c = c0 + cl;
                         if (c >= p.C) break;
-                        const float4 cp = chan_pos[stage * kStWin + cl];
-                        recv_geom g = receive_geometry(vx, vy, vz, cp.x, cp.y, cp.z);
+                        const float4 cp = sm.chan_pos[stage * kStWin + cl];
+                        recv_geom g = receive_geometry(cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z);
                         if (p.srcdir)
-                            apply_directivity(g, vx, vy, vz, cp.x, cp.y, cp.z, chan_dir[stage * kStWin + cl]);
+                            apply_directivity(g, cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z,
+                                              sm.chan_dir[stage * kStWin + cl]);
                         uint32_t k0p[SC];
-#pragma unroll
-                        for (int j = 0; j < SC; j += 4) {
-                            if constexpr (SC >= 4) {
-                                const uint4 q = *reinterpret_cast<const uint4 *>(&meta[stage * kStWin + cl * SC + j]);
-                                k0p[j] = q.x; k0p[j + 1] = q.y; k0p[j + 2] = q.z; k0p[j + 3] = q.w;
-                            } else {
-#pragma unroll
-                                for (int q = 0; q < SC; q++) k0p[q] = meta[stage * kStWin + cl * SC + q];
-                            }
-                        }
+                        load_meta<SC>(sm.meta, stage, cl, k0p);
                         const unsigned char *slots = stage_base + (cl * SC) * SG::bytes;
                         if (!any_ovf) {
                             if constexpr (SC >= 2) {
@@ -406,19 +510,19 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
                                 const tau_split ts = split_tau(tau);
                                 st pr;
                                 if (k0p[j] == kOvf) {
-                                    const int64_t row = ((int64_t)b * p.C + c) * p.S + (e0 + min(j, sc - 1));
+                                    const int64_t row = ((int64_t)cx.b * p.C + c) * p.S + (e0 + min(j, sc - 1));
                                     pr = Pg[row * p.npad + min(ts.k, kmax_pair)];
                                 } else {
                                     const uint32_t rel = min(ts.k + kFloorMagicBits - k0p[j], (uint32_t)WB);
                                     pr = *reinterpret_cast<const st *>(slots + j * SG::bytes + rel * sizeof(st));
                                 }
-                                acc = __fmaf_rn(w[j], tr::tap(pr, ts.t), acc);
+                                acc = __fmaf_rn(w[j], pair_traits<K>::tap(pr, ts.t), acc);
                             }
                         }
                     }
                 }
                 __syncwarp();
-                if (lane == 0) mbar_arrive(empty_bar);
+                if (cx.lane == 0) mbar_arrive(smem_u32(&sm.empty[stage]));
             }
             if (++stage == kStages) {
                 stage = 0;
@@ -428,24 +532,198 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
         __syncthreads();
     }
 
-    if (producer) {
-        // After an abort, wait (bounded, ignoring the abort flag) until every
-        // copy this CTA issued has landed, so no TMA write outlives the CTA.
-        if (*abort_flag && lane == 0) {
-            for (int i = 0; i < kStages; i++) {
-                const int s = (stage + i) % kStages;
-                if (!(issued_mask & (1u << s))) continue;
-                const uint32_t par = (s < stage) ? phase : (phase ^ 1u);
-                const long long t0 = clock64();
-                while (!mbar_try_wait(smem_u32(&full[s]), par) && clock64() - t0 < kWaitCycles) __nanosleep(64);
-            }
-        }
+    if (cx.producer) {
+        staged_drain<K, WB>(sm, cx, stage, phase, issued_mask);
         return;
     }
-    if (active && !dead) {
+    if (cx.active && !dead) {
         acc += acc2.x + acc2.y;
-        float *o = static_cast<float *>(p.out) + (int64_t)b * p.out_bstride + v;
+        float *o = static_cast<float *>(p.out) + (int64_t)cx.b * p.out_bstride + cx.v;
         *o = p.beta_zero ? acc : __fmaf_rn((float)p.beta_re, *o, acc);
+    }
+}
+
+// ------------------------------------------------------------------ adjoint ---
+// One CTA = one voxel tile x one batch item.  Per unit (v, c, e):
+//   L = x0 + t d, d = slope;  g = dLoss/dout[b, v];  a = g w
+//   gw[e,v] += g L;  goff[e,v] += a d;  q(v,c) += a d
+//   gdst[v] += q (v - c)/r;  gsrc[c] -= q (v - c)/r
+//   gx[b,c,s,k] += a (1 - t);  gx[b,c,s,k+1] += a t      (0 <= k <= N-2)
+// The two-tap scatter goes into the window's shared gradient slot; after all
+// consumer warps finished a stage, they flush the touched entries with
+// red.global.add and zero them.  Channel-position gradients are reduced over
+// the tile in shared memory and added once per channel per CTA.
+template <int K, int SC, int WB>
+__global__ void __launch_bounds__(kStThreads) das_staged_bwd_kernel(const staged_params p,
+                                                                     const __grid_constant__ CUtensorMap tmap) {
+    using SG = slot_geom<WB, K>;
+    constexpr int CC = kStWin / SC;
+    constexpr int GS = WB + 2;  // gradient slot length (floats)
+    static_assert(kStWin % SC == 0, "SC must divide the stage");
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    staged_smem<K, WB> sm(smem_raw);
+    float *gslot = reinterpret_cast<float *>(sm.extra);                 // [kStages][kStWin][GS]
+    float *cgrad = gslot + kStages * kStWin * GS;                        // [CC * 3][256]
+    for (int i = threadIdx.x; i < kStages * kStWin * GS; i += kStThreads) gslot[i] = 0.f;
+    const staged_ctx cx = staged_setup<K, WB>(p, sm);   // ends with __syncthreads
+
+    const bool multi_b = p.B > 1;
+    const float g = (cx.active) ? __ldg(p.gout + (int64_t)cx.b * p.gout_bstride + cx.v) : 0.f;
+    const bool want_pos = p.gdst != nullptr || p.gsrc != nullptr;
+    float gpx = 0.f, gpy = 0.f, gpz = 0.f;
+    int stage = 0;
+    uint32_t phase = 0;
+    bool dead = false;
+    uint32_t issued_mask = 0;
+
+    for (int e0 = 0; e0 < p.n_events; e0 += SC) {
+        const int sc = min(SC, p.n_events - e0);
+        float ofs[SC], w[SC];
+        staged_pass_begin<K, WB, SC>(p, sm, cx, e0, sc, ofs, w);
+        float gwa[SC], goa[SC];
+#pragma unroll
+        for (int j = 0; j < SC; j++) { gwa[j] = 0.f; goa[j] = 0.f; }
+
+        for (int c0 = 0; c0 < p.C; c0 += CC) {
+            if (cx.producer) {
+                staged_produce<K, WB, SC>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
+            } else {
+                const uint32_t full_bar = smem_u32(&sm.full[stage]);
+                const unsigned char *stage_base = sm.ring + stage * SG::stage_bytes;
+                float *gstage = gslot + stage * kStWin * GS;
+                if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
+                const bool any_ovf = !dead && sm.ovf[stage] != 0;
+                if (!dead) {
+                    for (int cl = 0; cl < CC; cl++) {
+                        const int c = c0 + cl;
+                        if (c >= p.C) break;
+                        const float4 cp = sm.chan_pos[stage * kStWin + cl];
+                        const recv_geom gm = receive_geometry(cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z);
+                        uint32_t k0p[SC];
+                        load_meta<SC>(sm.meta, stage, cl, k0p);
+                        const unsigned char *slots = stage_base + (cl * SC) * SG::bytes;
+                        float q = 0.f;
+#pragma unroll
+                        for (int j = 0; j < SC; j++) {
+                            const float tau = __fmaf_rn(gm.rsq, gm.rinv, ofs[j]);
+                            const tau_split ts = split_tau(tau);
+                            typename pair_traits<K>::storage pr;
+                            const bool ovfw = any_ovf && k0p[j] == kOvf;
+                            uint32_t rel = WB;
+                            if (ovfw) {
+                                const int64_t row = ((int64_t)cx.b * p.C + c) * p.S + (e0 + min(j, sc - 1));
+                                pr = static_cast<const typename pair_traits<K>::storage *>(p.P)
+                                    [row * p.npad + min(ts.k, (uint32_t)(p.npad - 1))];
+                            } else {
+                                rel = min(ts.k + kFloorMagicBits - k0p[j], (uint32_t)WB);
+                                pr = *reinterpret_cast<const typename pair_traits<K>::storage *>(
+                                    slots + j * SG::bytes + rel * sizeof(pr));
+                            }
+                            const float L = pair_traits<K>::tap(pr, ts.t);
+                            const float d = pair_traits<K>::slope(pr);
+                            const float a = g * w[j];
+                            gwa[j] = __fmaf_rn(g, L, gwa[j]);
+                            goa[j] = __fmaf_rn(a, d, goa[j]);
+                            q = __fmaf_rn(a, d, q);
+                            // channel-data adjoint: only taps inside the record
+                            if (p.gx && a != 0.f && ts.k < (uint32_t)(p.N - 1)) {
+                                const float a1 = a * ts.t;
+                                if (!ovfw && rel < (uint32_t)WB) {
+                                    float *gs = gstage + (cl * SC + j) * GS + rel;
+                                    atomicAdd(gs, a - a1);
+                                    atomicAdd(gs + 1, a1);
+                                } else {
+                                    float *gr = p.gx + (((int64_t)cx.b * p.C + c) * p.S + (e0 + j)) * p.N + ts.k;
+                                    atomicAdd(gr, a - a1);
+                                    atomicAdd(gr + 1, a1);
+                                }
+                            }
+                        }
+                        if (want_pos) {
+                            const float qr = q * gm.rinv;
+                            const float ex = (cx.vx - cp.x) * qr, ey = (cx.vy - cp.y) * qr, ez = (cx.vz - cp.z) * qr;
+                            gpx += ex; gpy += ey; gpz += ez;
+                            if (p.gsrc) {
+                                cgrad[(cl * 3 + 0) * kStConsumers + cx.tid] = -ex;
+                                cgrad[(cl * 3 + 1) * kStConsumers + cx.tid] = -ey;
+                                cgrad[(cl * 3 + 2) * kStConsumers + cx.tid] = -ez;
+                            }
+                        }
+                    }
+                }
+                // every consumer warp finished this stage's scatter
+                consumer_sync();
+                if (!dead) {
+                    // flush the stage's gradient slots: one red.add per touched sample
+                    if (p.gx) {
+                        for (int i = cx.tid; i < kStWin * GS; i += kStConsumers) {
+                            const int win = i / GS, r = i - win * GS;
+                            const float val = gstage[i];
+                            if (val != 0.f) {
+                                gstage[i] = 0.f;
+                                const int cl = win / SC, j = win % SC;
+                                const int k = (int)(sm.meta[stage * kStWin + win] - kFloorMagicBits) + r;
+                                float *gr = p.gx + (((int64_t)cx.b * p.C + (c0 + cl)) * p.S + (e0 + j)) * p.N + k;
+                                atomicAdd(gr, val);
+                            }
+                        }
+                    }
+                    // channel-position gradients: reduce the tile, one add per channel
+                    if (p.gsrc) {
+                        for (int o = cx.warp; o < CC * 3; o += kStWarps) {
+                            const int cl = o / 3;
+                            if (c0 + cl >= p.C) continue;
+                            float s = 0.f;
+#pragma unroll
+                            for (int i = 0; i < kStConsumers / 32; i++) s += cgrad[o * kStConsumers + cx.lane + 32 * i];
+#pragma unroll
+                            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+                            if (cx.lane == 0 && s != 0.f) atomicAdd(p.gsrc + 3 * (c0 + cl) + (o % 3), s);
+                        }
+                    }
+                }
+                consumer_sync();  // scratch reused by the next stage
+                __syncwarp();
+                if (cx.lane == 0) mbar_arrive(smem_u32(&sm.empty[stage]));
+            }
+            if (++stage == kStages) {
+                stage = 0;
+                phase ^= 1u;
+            }
+        }
+        if (!cx.producer && cx.active && !dead) {
+#pragma unroll
+            for (int j = 0; j < SC; j++) {
+                if (j < sc) {
+                    const int64_t idx = (int64_t)(e0 + j) * p.V + cx.v;
+                    if (multi_b) {
+                        if (p.gw) atomicAdd(p.gw + idx, gwa[j]);
+                        if (p.goff) atomicAdd(p.goff + idx, goa[j]);
+                    } else {
+                        if (p.gw) p.gw[idx] = gwa[j];
+                        if (p.goff) p.goff[idx] = goa[j];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    if (cx.producer) {
+        staged_drain<K, WB>(sm, cx, stage, phase, issued_mask);
+        return;
+    }
+    if (cx.active && !dead && p.gdst) {
+        if (multi_b) {
+            atomicAdd(p.gdst + 3 * cx.v, gpx);
+            atomicAdd(p.gdst + 3 * cx.v + 1, gpy);
+            atomicAdd(p.gdst + 3 * cx.v + 2, gpz);
+        } else {
+            p.gdst[3 * cx.v] = gpx;
+            p.gdst[3 * cx.v + 1] = gpy;
+            p.gdst[3 * cx.v + 2] = gpz;
+        }
     }
 }
 
