@@ -50,20 +50,33 @@ template <> struct pair_traits<ST_F16> {
     }
 };
 
+// bf16 pair word: low half = bf16(x1 - x0) (the slope); high half = a bf16
+// value chosen so that the WHOLE 32-bit word, read as an f32, is as close to x0
+// as the bf16 grid allows (the low half only adds sub-bf16-ulp mantissa bits,
+// and the high half is picked to compensate).  A tap is then one shift and one
+// FFMA: fma(t, f32(word << 16), f32(word)); x0 and the slope each carry at most
+// about half a bf16 ulp of rounding, like plain bf16 storage.
 template <> struct pair_traits<ST_BF16> {
     using storage = uint32_t;
     using value = float;
     using acc = float;
     static constexpr bool complex = false;
     __device__ static storage make(float x0, float x1) {
-        __nv_bfloat162 b = __floats2bfloat162_rn(x0, x1);
-        return *reinterpret_cast<uint32_t *>(&b);
+        const __nv_bfloat16 db = __float2bfloat16_rn(x1 - x0);
+        const uint32_t lo = *reinterpret_cast<const uint16_t *>(&db);
+        const uint32_t base = __float_as_uint(x0) >> 16;
+        uint32_t best = (base << 16) | lo;
+        float err = fabsf(__uint_as_float(best) - x0);
+        for (int dlt = -1; dlt <= 1; dlt += 2) {
+            const uint32_t hi = (base + (uint32_t)dlt) & 0xFFFFu;
+            const uint32_t w = (hi << 16) | lo;
+            const float e = fabsf(__uint_as_float(w) - x0);
+            if (e < err) { err = e; best = w; }
+        }
+        return best;
     }
-    __device__ static value tap(storage p, float t) {
-        float x0 = bf16lo_to_f32(p), x1 = bf16hi_to_f32(p);
-        return __fmaf_rn(t, x1 - x0, x0);
-    }
-    __device__ static value slope(storage p) { return bf16hi_to_f32(p) - bf16lo_to_f32(p); }
+    __device__ static value tap(storage p, float t) { return __fmaf_rn(t, __uint_as_float(p << 16), __uint_as_float(p)); }
+    __device__ static value slope(storage p) { return __uint_as_float(p << 16); }
 };
 
 template <> struct pair_traits<ST_F64> {

@@ -403,6 +403,43 @@ __device__ __forceinline__ void staged_drain(staged_smem<K, WB> &sm, const stage
     }
 }
 
+// Shared-memory loads on 32-bit shared-window addresses.  Volatile keeps them
+// after the mbarrier wait that publishes the data (also volatile asm).
+__device__ __forceinline__ uint32_t lds_u32(uint32_t a) {
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ float2 lds_f2(uint32_t a) {
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ uint4 lds_u4(uint32_t a) {
+    uint4 v;
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ float4 lds_f4(uint32_t a) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
+}
+
+// Interpolate one tap from the pair at shared address `a` (f32 result).
+template <int K> __device__ __forceinline__ float tap_at(uint32_t a, float t);
+template <> __device__ __forceinline__ float tap_at<ST_F32>(uint32_t a, float t) {
+    const float2 p = lds_f2(a);
+    return __fmaf_rn(t, p.y, p.x);
+}
+template <> __device__ __forceinline__ float tap_at<ST_F16>(uint32_t a, float t) {
+    const uint32_t u = lds_u32(a);
+    return pair_traits<ST_F16>::tap(*reinterpret_cast<const __half2 *>(&u), t);
+}
+template <> __device__ __forceinline__ float tap_at<ST_BF16>(uint32_t a, float t) {
+    return pair_traits<ST_BF16>::tap(lds_u32(a), t);
+}
+
 // Interpolate one tap from a staged slot (f32 result).
 template <int K>
 __device__ __forceinline__ float staged_tap(const unsigned char *slot, uint32_t rel, float t) {
@@ -413,15 +450,16 @@ __device__ __forceinline__ float staged_tap(const unsigned char *slot, uint32_t 
 // Read the SC window metadata words of channel cl of a stage.
 template <int SC>
 __device__ __forceinline__ void load_meta(const uint32_t *meta, int stage, int cl, uint32_t (&k0p)[SC]) {
+    const uint32_t base = smem_u32(meta + stage * kStWin + cl * SC);
     if constexpr (SC >= 4) {
 #pragma unroll
         for (int j = 0; j < SC; j += 4) {
-            const uint4 q = *reinterpret_cast<const uint4 *>(&meta[stage * kStWin + cl * SC + j]);
+            const uint4 q = lds_u4(base + 4 * j);
             k0p[j] = q.x; k0p[j + 1] = q.y; k0p[j + 2] = q.z; k0p[j + 3] = q.w;
         }
     } else {
 #pragma unroll
-        for (int q = 0; q < SC; q++) k0p[q] = meta[stage * kStWin + cl * SC + q];
+        for (int q = 0; q < SC; q++) k0p[q] = lds_u32(base + 4 * q);
     }
 }
 
@@ -447,10 +485,20 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
     bool dead = false;
     uint32_t issued_mask = 0;
 
+    const uint32_t ring_u32 = smem_u32(sm.ring);
+    const uint32_t chan_u32 = smem_u32(sm.chan_pos);
+
     for (int e0 = 0; e0 < p.n_events; e0 += SC) {
         const int sc = min(SC, p.n_events - e0);
         float ofs[SC], w[SC];
         staged_pass_begin<K, WB, SC>(p, sm, cx, e0, sc, ofs, w);
+        // delays and weights as event pairs for the packed FP32 loop
+        float2 ofs2[(SC + 1) / 2], w2[(SC + 1) / 2];
+#pragma unroll
+        for (int j = 0; j + 1 < SC; j += 2) {
+            ofs2[j / 2] = make_float2(ofs[j], ofs[j + 1]);
+            w2[j / 2] = make_float2(w[j], w[j + 1]);
+        }
 
         for (int c0 = 0; c0 < p.C; c0 += CC) {
             if (cx.producer) {
@@ -461,16 +509,18 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
                 if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
                 if (!dead) {
                     const bool any_ovf = sm.ovf[stage] != 0;
+                    const uint32_t stage_u32 = ring_u32 + stage * SG::stage_bytes;
                     for (int cl = 0; cl < CC; cl++) {
                         const int c = c0 + cl;
                         if (c >= p.C) break;
-                        const float4 cp = sm.chan_pos[stage * kStWin + cl];
+                        const float4 cp = lds_f4(chan_u32 + (stage * kStWin + cl) * 16);
                         recv_geom g = receive_geometry(cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z);
                         if (p.srcdir)
                             apply_directivity(g, cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z,
                                               sm.chan_dir[stage * kStWin + cl]);
                         uint32_t k0p[SC];
                         load_meta<SC>(sm.meta, stage, cl, k0p);
+                        const uint32_t slots_u32 = stage_u32 + (cl * SC) * SG::bytes;
                         const unsigned char *slots = stage_base + (cl * SC) * SG::bytes;
                         if (!any_ovf) {
                             if constexpr (SC >= 2) {
@@ -483,15 +533,16 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
                                 const float2 neg1 = make_float2(-1.f, -1.f);
 #pragma unroll
                                 for (int j = 0; j < SC; j += 2) {
-                                    const float2 tau2 = __ffma2_rn(rsq2, rinv2, make_float2(ofs[j], ofs[j + 1]));
+                                    const float2 tau2 = __ffma2_rn(rsq2, rinv2, ofs2[j / 2]);
                                     const float2 mm2 = __fadd2_rd(tau2, magic2);
                                     const float2 nfl2 = __ffma2_rn(mm2, neg1, magic2);   // -(floor), exact
                                     const float2 t2 = __fadd2_rn(tau2, nfl2);
                                     const uint32_t ra = min(__float_as_uint(mm2.x) - k0p[j], (uint32_t)WB);
                                     const uint32_t rb = min(__float_as_uint(mm2.y) - k0p[j + 1], (uint32_t)WB);
-                                    const float ta = staged_tap<K>(slots + j * SG::bytes, ra, t2.x);
-                                    const float tb = staged_tap<K>(slots + (j + 1) * SG::bytes, rb, t2.y);
-                                    acc2 = __ffma2_rn(make_float2(w[j], w[j + 1]), make_float2(ta, tb), acc2);
+                                    const float ta = tap_at<K>(slots_u32 + j * SG::bytes + ra * sizeof(st), t2.x);
+                                    const float tb =
+                                        tap_at<K>(slots_u32 + (j + 1) * SG::bytes + rb * sizeof(st), t2.y);
+                                    acc2 = __ffma2_rn(w2[j / 2], make_float2(ta, tb), acc2);
                                 }
                             } else {
 #pragma unroll
@@ -500,7 +551,8 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
                                     const float mm = __fadd_rd(tau, kFloorMagic);
                                     const float t = tau - (mm - kFloorMagic);
                                     const uint32_t rel = min(__float_as_uint(mm) - k0p[j], (uint32_t)WB);
-                                    acc = __fmaf_rn(w[j], staged_tap<K>(slots + j * SG::bytes, rel, t), acc);
+                                    acc = __fmaf_rn(w[j], tap_at<K>(slots_u32 + j * SG::bytes + rel * sizeof(st), t),
+                                                    acc);
                                 }
                             }
                         } else {

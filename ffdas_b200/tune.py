@@ -58,8 +58,10 @@ def candidates(x, dstpos, offsets, sparse_indices=None) -> list[dict]:
                 continue
             out.append(dict(variant=1, tile_x=t0, tile_y=t1, batch_tile=bt))
         if real and sparse_indices is None:
+            n_ev = offsets.shape[0]
+            chunks = sorted({min(c, max(n_ev, 1)) for c in (4, 8, 16)})
             for wb in (32, 64):
-                for ec in (8, 16):
+                for ec in chunks:
                     out.append(dict(variant=2, tile_x=t0, tile_y=t1, window=wb, event_chunk=ec))
     return out
 
