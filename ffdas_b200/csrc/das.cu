@@ -9,6 +9,7 @@
 // forward kernel chosen by the planner or the handle's config.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "core.h"
 #include "das_problem.h"
@@ -473,3 +474,108 @@ ffdas_error_t ffdas_das_sparse(ffdas_handle_t handle, const float *srcpos, const
 }
 
 }  // extern "C"
+
+// ------------------------------------------------- allocation-free variant ---
+// ffdas_das_static: the forward delay-and-sum for callers that cannot allocate
+// device memory -- a real-time thread or an embedded host that forbids
+// cudaMalloc, a memory budget that is fixed before the first frame, or a caller
+// with no ffdas handle (creating one allocates its workspace pool).  Instead of
+// workspace from a pool, the interpolation-pair rows live in the file-scope
+// array below, which every GPU that loads this library holds until exit.  The
+// entry point calls no cudaMalloc/cudaFree and no allocating library routine.
+namespace {
+
+constexpr size_t kStaticPairBytes = size_t(16) << 20;   // 16 MiB per GPU
+constexpr int kStaticMaxDevices = 64;
+static __device__ __align__(256) unsigned char g_static_pairs[kStaticPairBytes];
+
+std::mutex g_static_mu;
+void *g_static_addr[kStaticMaxDevices] = {};
+
+// Device address of g_static_pairs on the current device, looked up once per
+// device (host code may not use the symbol itself: its host-side name is a
+// stand-in, not a device address).
+ffdas_error_t static_pairs_address(void **ptr) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return FFDAS_ERROR_CUDA_RUNTIME;
+    if (dev < 0 || dev >= kStaticMaxDevices) return FFDAS_ERROR_INVALID_DEVICE;
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_static_pairs) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return FFDAS_ERROR_CUDA_RUNTIME;
+        }
+        g_static_addr[dev] = p;
+    }
+    *ptr = g_static_addr[dev];
+    return FFDAS_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" ffdas_error_t ffdas_das_static(uintptr_t stream, const float *srcpos, const float *srcdir,
+                                          float wavenum, ffdas_tensor_desc_t x_desc, const void *x,
+                                          const float *dstpos, const float *offsets, const float *weights,
+                                          const void *beta, ffdas_tensor_desc_t out_desc, void *out,
+                                          ffdas_compute_type_t compute_type, ffdas_alg_t alg) {
+    if (!x_desc || !out_desc) return FFDAS_ERROR_NULL_POINTER;
+    const ffdas_tensor_desc &xd = *x_desc;
+    const ffdas_tensor_desc &od = *out_desc;
+    const bool combo_ok = (xd.dtype == FFDAS_R_16F || xd.dtype == FFDAS_R_16BF || xd.dtype == FFDAS_R_32F) &&
+                          od.dtype == FFDAS_R_32F;
+    if (!combo_ok) return FFDAS_ERROR_UNSUPPORTED_TYPE;   // real channel data, float output
+    if (!fits_int32_indexing(xd) || !fits_int32_indexing(od)) return FFDAS_ERROR_INVALID_DIMS;
+    if (alg != FFDAS_ALG_DEFAULT && alg != FFDAS_ALG1 && alg != FFDAS_ALG2 && alg != FFDAS_ALG4)
+        return FFDAS_ERROR_INVALID_ARGUMENT;
+    das_problem pb;
+    FFDAS_TRY(make_problem(xd, od, pb));
+    pb.n_events = pb.S;
+    const int kind = select_storage(xd.dtype, od.dtype, compute_type);
+    if (kind < 0) return FFDAS_ERROR_UNSUPPORTED_TYPE;
+    if (pb.N >= (1 << 22)) return FFDAS_ERROR_DIMS_TOO_LARGE;
+    if (pb.V == 0 || pb.B == 0) return FFDAS_SUCCESS;
+    if (!out || !dstpos || !offsets || !weights) return FFDAS_ERROR_NULL_POINTER;
+    if (pb.C > 0 && !srcpos) return FFDAS_ERROR_NULL_POINTER;
+    if ((int64_t)pb.B * pb.C * pb.S * pb.N > 0 && !x) return FFDAS_ERROR_NULL_POINTER;
+
+    // the pair rows must fit the static array; larger problems use ffdas_das
+    const int64_t npad = pair_row_length(pb.N);
+    const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
+    const size_t bytes = (size_t)std::max<int64_t>(rows, 1) * npad * storage_bytes(kind);
+    if (bytes > kStaticPairBytes) return FFDAS_ERROR_DIMS_TOO_LARGE;
+    void *P = nullptr;
+    FFDAS_TRY(static_pairs_address(&P));
+
+    // A handle-shaped view of the caller's stream: no pool, no status word, no
+    // events; the launch helpers below only read its stream.
+    ffdas_context ctx;
+    ctx.stream = reinterpret_cast<cudaStream_t>(stream);
+    cudaGetDevice(&ctx.device_id);
+    // Every pair of every row is rewritten by the ingest pass, so nothing left
+    // in the array by an earlier call needs clearing.
+    FFDAS_TRY(launch_ingest(ctx, pb, xd.dtype, kind, x, npad, P));
+
+    const schedule s = plan_schedule(ctx, pb, kind);
+    gather_params gp;
+    std::memset(&gp, 0, sizeof(gp));
+    gp.P = P;
+    gp.npad = npad;
+    gp.C = pb.C; gp.S = pb.S; gp.n_events = pb.n_events; gp.B = pb.B; gp.V = pb.V;
+    gp.D0 = pb.D0; gp.D1 = pb.D1; gp.D2 = pb.D2;
+    gp.T0 = s.T0; gp.T1 = s.T1; gp.T2 = s.T2;
+    gp.n0 = (pb.D0 + s.T0 - 1) / s.T0;
+    gp.n1 = (pb.D1 + s.T1 - 1) / s.T1;
+    const int n2 = (pb.D2 + s.T2 - 1) / s.T2;
+    gp.srcpos = srcpos;
+    gp.srcdir = reinterpret_cast<const float4 *>(srcdir);
+    gp.dstpos = dstpos; gp.offsets = offsets; gp.weights = weights;
+    gp.wavenum = wavenum;
+    gp.out = out;
+    gp.out_bstride = pb.out_bstride;
+    read_beta(od.dtype, beta, gp.beta_re, gp.beta_im, gp.beta_zero);
+    const int64_t tiles = (int64_t)gp.n0 * gp.n1 * n2;
+    const int bchunks = (pb.B + s.BT - 1) / s.BT;
+    if (tiles > INT32_MAX || bchunks > 65535) return FFDAS_ERROR_DIMS_TOO_LARGE;
+    return launch_gather<false>(ctx, kind, od.dtype, gp, s, dim3((unsigned)tiles, (unsigned)bchunks));
+}

@@ -276,6 +276,37 @@ FFDAS_API ffdas_error_t ffdas_das_backward(
     float *grad_srcpos
 );
 
+/* New, no counterpart in the reference: the forward delay-and-sum for callers
+ * that cannot allocate device memory (a real-time or embedded host where
+ * cudaMalloc is forbidden, a memory budget fixed before the first frame, or a
+ * caller without an ffdas handle, whose creation allocates a workspace pool).
+ * Same arguments as ffdas_das, except that it takes the CUDA stream directly
+ * instead of a handle.  It allocates nothing: the interpolation-pair workspace
+ * is a 16 MiB array in the library's device image (every GPU that loads the
+ * library holds it until exit), so B * C * S * roundup(N, 4) * 8 bytes (4 for
+ * 16-bit channel data) must not exceed 16 MiB, else FFDAS_ERROR_DIMS_TOO_LARGE.
+ * Real channel data (float32, float16, bfloat16) with float32 output only.
+ * The first call on a device looks up the array's device address (once per
+ * device); make that first call before any stream capture.  All calls share
+ * the one array: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller. */
+FFDAS_API ffdas_error_t ffdas_das_static(
+    uintptr_t stream,
+    const float *srcpos,
+    const float *srcdir,
+    float wavenum,
+    ffdas_tensor_desc_t x_desc,
+    const void* x,
+    const float *dstpos,
+    const float *offsets,
+    const float *weights,
+    const void *beta,
+    ffdas_tensor_desc_t out_desc,
+    void* out,
+    ffdas_compute_type_t compute_type,
+    ffdas_alg_t alg
+);
+
 /* New: schedule override for the following calls on this handle
  * (NULL restores the planner default). */
 FFDAS_API ffdas_error_t ffdas_das_set_config(ffdas_handle_t handle,
