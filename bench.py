@@ -20,10 +20,13 @@ against the FP32 FMA peak measured on this GPU; the HBM figure beside it),
 all host threads), `e2e` (through the public Python API with the channel data
 copied from pinned host memory and the image read back each step), `bf16` /
 `fp16` (reduced-precision pair storage: throughput, speed-up over FP32 and
-error against the FP64 oracle), `bwd_fwd` (backward / forward time on the
-differentiable 128-channel, 8-plane-wave, batch-4 workload) and `reference_gpu`
-parity.  `--impl reference` times the reference implementation (its CUDA das,
-built from its sources into oracle/_ref) on the same workload and GPU.
+error against this library's FP64-pair pipeline), `bwd_fwd` (backward /
+forward time on the differentiable 128-channel, 8-plane-wave, batch-4
+workload, with the kernels that ran) and `configs` (the 2-D plane-wave frame
+under graph replay, the 200-frame FP16 ensemble and uneven das_sparse).
+`--impl reference` times the reference implementation (its CUDA das, built
+from its sources into oracle/_ref) on the same workloads and GPU.
+`--section bwd|configs` runs one part alone (for profiling).
 """
 from __future__ import annotations
 
@@ -229,6 +232,8 @@ def run_reference(args, rank, world) -> dict:
             "clocks": ck}
     if cpu:
         line["cpu_baseline"] = cpu
+    if not args.quick:
+        line.update(config_extras(args, "reference"))
     return line
 
 
@@ -311,27 +316,42 @@ def run_ours(args, rank, world) -> dict:
 
     if rank == 0 and world == 1 and not args.quick:
         line.update(extras(args, wl, ms, h))
+        line.update(bwd_extras(args, h))
+        line.update(config_extras(args, "ours"))
         if args.cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(wl)
     return line
 
 
+def error_report(img: np.ndarray, ref: np.ndarray) -> dict:
+    d = img.astype(np.float64) - ref
+    peak = float(np.abs(ref).max()) or 1.0
+    rel = float(np.linalg.norm(d) / max(np.linalg.norm(ref), 1e-300))
+    pa = float(np.abs(d).max())
+    return {"rel_l2": rel, "peak_abs": pa, "peak_db_below_max": float(20 * np.log10(max(pa, 1e-300) / peak))}
+
+
 def extras(args, wl, ms_fp32, h) -> dict:
-    """Reduced-precision storage, errors against the FP64 oracle, backward/forward."""
+    """Reduced-precision pair storage: throughput and error.
+
+    The error reference is this library's own FP64 pipeline (FP64 pairs and
+    accumulation, the same FP32 delays) on six depth planes spread over the
+    volume, so the figure isolates what the 16-bit storage costs; the test
+    suite holds the same claim against the FP64 CPU oracle.
+    """
     import ffdas_b200
     from ffdas_b200 import workloads as W
-    from oracle import oracle
     dev = wl["x"].device
     srcpos, dstpos, offs, w = wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"]
     units = wl["units"]
     xn = W.normalize_channels(wl["x"])          # per-channel peak 1
     stream = torch.cuda.current_stream(dev)
     res = {}
-    # FP64 oracle on depth planes spread over the volume
     nz = dstpos.shape[0]
-    sel = np.linspace(0, nz - 1, 6).astype(int)
-    ref = oracle.das_f64(xn.cpu().numpy(), srcpos.cpu().numpy(), dstpos[sel].cpu().numpy(),
-                         offs[:, sel].cpu().numpy(), w[:, sel].cpu().numpy())
+    sel = torch.from_numpy(np.linspace(0, nz - 1, 6).astype(np.int64)).to(dev)
+    h.set_config(None)
+    ref = ffdas_b200.das(xn.double(), srcpos, dstpos[sel].contiguous(), offs[:, sel].contiguous(),
+                         w[:, sel].contiguous()).cpu().numpy()
 
     from ffdas_b200.tune import autotune
 
@@ -342,27 +362,44 @@ def extras(args, wl, ms_fp32, h) -> dict:
         ms = timed(lambda: ffdas_b200.das(x, srcpos, dstpos, offs, w, out=out, **kw), args.steps, args.warmup,
                    stream, 1)
         img = out[:, sel].cpu().numpy()
-        return ms, oracle.error_report(img, ref)
+        return ms, error_report(img, ref), cfg
 
-    ms32, err32 = measure(xn)
-    res["fp32_error_vs_fp64_oracle"] = err32
+    ms32, err32, _ = measure(xn)
+    res["fp32_error_vs_fp64_pairs"] = err32
     for name, x in (("bf16", xn.to(torch.bfloat16)), ("fp16", xn.to(torch.float16))):
-        msr, err = measure(x)
+        msr, err, cfg = measure(x)
         res[name] = {"value": units / (msr * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": msr,
-                     "speedup_vs_fp32": ms32 / msr, "error_vs_fp64_oracle": err,
+                     "speedup_vs_fp32": ms32 / msr, "error_vs_fp64_pairs": err, "schedule": cfg,
                      "input": f"channel data stored as {name} (per-channel peak 1), FP32 geometry and accumulation"}
-    # backward / forward on the differentiable workload
+    h.set_config(None)
+    return res
+
+
+def bwd_extras(args, h) -> dict:
+    """Backward / forward time on the differentiable workload (autofocus).
+
+    The forward is autotuned; the backward is timed under its planner default
+    and a few staged-adjoint tiles plus the gather adjoint, and the fastest is
+    reported together with the kernel that ran.
+    """
+    import ffdas_b200
+    from ffdas_b200 import workloads as W, _lib
+    from ffdas_b200._lib import DataType
+    from ffdas_b200.tune import autotune
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream(dev)
     af = W.autofocus(device=dev)
     xa = af["x"]
     args_f = (af["srcpos"], af["dstpos"], af["offsets"], af["weights"])
     gout = torch.randn((xa.shape[0], *af["dstpos"].shape[:-1]), device=dev)
-    from ffdas_b200 import _lib
-    from ffdas_b200._lib import DataType
-
-    h.set_config(autotune(xa, *args_f, reps=2, use_cache=False)["config"])
+    fcfg = autotune(xa, *args_f, reps=2, use_cache=False)["config"]
+    h.set_config(fcfg)
 
     def fwd():
         ffdas_b200.das(xa, *args_f)
+
+    msf = timed(fwd, args.steps, args.warmup, stream, 1)
+    finfo = h.last_kernel_info()
 
     gx = torch.zeros(xa.shape, device=dev)
     go = torch.empty_like(af["offsets"])
@@ -372,20 +409,90 @@ def extras(args, wl, ms_fp32, h) -> dict:
     xdsc = _lib.TensorDesc(list(xa.shape), list(xa.stride()), DataType.R_32F)
     gdsc = _lib.TensorDesc(list(gout.shape), None, DataType.R_32F)
     L = _lib.load()
-    hh = ffdas_b200.get_library_handle(dev)
 
     def bwd():
-        hh.set_stream(torch.cuda.current_stream(dev).cuda_stream)
-        _lib.check(L.ffdas_das_backward(hh.h, af["srcpos"].data_ptr(), None, 0.0, xdsc.desc, xa.data_ptr(),
+        h.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+        _lib.check(L.ffdas_das_backward(h.h, af["srcpos"].data_ptr(), None, 0.0, xdsc.desc, xa.data_ptr(),
                                         af["dstpos"].data_ptr(), af["offsets"].data_ptr(), af["weights"].data_ptr(),
                                         0, None, gdsc.desc, gout.data_ptr(), gx.data_ptr(), go.data_ptr(),
                                         gw.data_ptr(), gd.data_ptr(), gs.data_ptr()))
-    msf = timed(fwd, args.steps, args.warmup, stream, 1)
-    msb = timed(bwd, args.steps, args.warmup, stream, 1)
-    res["bwd_fwd"] = {"ratio": msb / msf, "fwd_ms": msf, "bwd_ms": msb,
-                      "workload": "autofocus: 128 ch, 8 plane waves, batch 4, 2048 samples, 256x256 voxels; "
-                                  "backward = grads of x, offsets, weights, voxel and channel positions"}
-    return res
+
+    table = []
+    bcands = [None] + [dict(variant=2, tile_x=tx, tile_y=256 // tx, window=wb)
+                       for tx in (16, 32, 64) for wb in (32, 64)] + [dict(variant=3)]
+    if args.schedule_bwd:
+        bcands = [json.loads(args.schedule_bwd)]
+    for cfg in bcands:
+        h.set_config(cfg)
+        ms = timed(bwd, args.steps, args.warmup, stream, 1)
+        table.append((ms, cfg, h.last_kernel_info()))
+    table.sort(key=lambda t: t[0])
+    msb, bcfg, binfo = table[0]
+    h.set_config(None)
+    return {"bwd_fwd": {"ratio": msb / msf, "fwd_ms": msf, "bwd_ms": msb,
+                        "fwd_schedule": finfo, "bwd_schedule": binfo, "bwd_config": bcfg,
+                        "bwd_table": [[m, c, i["variant"]] for m, c, i in table],
+                        "workload": "autofocus: 128 ch, 8 plane waves, batch 4, 2048 samples, 256x256 voxels; "
+                                    "backward = grads of x, offsets, weights, voxel and channel positions"}}
+
+
+
+def config_extras(args, impl: str) -> dict:
+    """The other benchmark configurations, one entry each, for either arm.
+
+    plane2d: 128-element linear array, 1 plane wave, 2048 samples, 256x128
+      pixels, FP32; ours replays a captured CUDA graph (DASRunner), the
+      reference is called through its API; time per call in microseconds.
+    ensemble: 200-frame FP16 ensemble, 128 ch, 11 plane waves, 1536 samples,
+      400x256 pixels (frames batched in one call).
+    sparse_focus: das_sparse, 64 focused transmits, 1..32 events per pixel
+      (padding repeats an index with zero weight); units count real events.
+    Parity of the two arms on these inputs is held by the test suite.
+    """
+    from ffdas_b200 import workloads as W
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    steps, warm = max(args.steps, 5), args.warmup
+    for name in ("plane2d", "ensemble", "sparse_focus"):
+        wl = W.CONFIGS[name](device=dev)
+        geo = (wl["x"], wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"])
+        idx = wl.get("sparse_indices")
+        units = wl.get("real_units", wl["units"])
+        reps = 50 if name == "plane2d" else 1
+        if impl == "reference":
+            from oracle import reference
+            if not reference.available():
+                out[name] = {"unavailable": "oracle/_ref/libffdas_ref.so not built"}
+                continue
+            B = wl["x"].shape[0]
+            # the reference's default ALG1 batch tile for B >= 32 FP32 has no kernel; 16 is its largest
+            call = reference.Prepared(*geo, sparse_indices=idx, alg=1, tile=16 if B >= 32 else None)
+
+            def fn():
+                for _ in range(reps):
+                    call()
+            ms = timed(fn, steps, warm, stream, 1) / reps
+            call.close()
+            kind = "reference ALG1 through ffdas_das" + ("_sparse" if idx is not None else "")
+        else:
+            from ffdas_b200.runner import DASRunner
+            run = DASRunner(*geo, sparse_indices=idx)
+
+            def fn():
+                for _ in range(reps):
+                    run.replay()
+            ms = timed(fn, steps, warm, stream, 1) / reps
+            kind = f"ffdas_b200 CUDA graph replay, schedule {run.config}"
+            del run
+        e = {"value": units / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_call": ms, "units_per_call": units,
+             "x_dtype": str(wl["x"].dtype).replace("torch.", ""), "impl": kind}
+        if name == "plane2d":
+            e["us_per_call"] = ms * 1e3
+        out[name] = e
+        del wl, geo
+        torch.cuda.empty_cache()
+    return {"configs": out}
 
 
 def main() -> int:
@@ -398,6 +505,10 @@ def main() -> int:
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--schedule", default=None,
                     help="JSON schedule (ffdas_das_config_t fields) instead of autotuning, e.g. for profiling")
+    ap.add_argument("--schedule-bwd", dest="schedule_bwd", default=None,
+                    help="JSON schedule for the backward instead of trying several")
+    ap.add_argument("--section", choices=["all", "bwd", "configs"], default="all",
+                    help="bwd / configs: only that part, printed as its own JSON object (for profiling)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -408,6 +519,16 @@ def main() -> int:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     try:
+        if args.section != "all":
+            if world > 1 or (args.impl == "reference" and args.section == "bwd"):
+                return 0
+            import ffdas_b200
+            if args.section == "bwd":
+                part = bwd_extras(args, ffdas_b200.get_library_handle(torch.device("cuda", 0)))
+            else:
+                part = config_extras(args, args.impl)
+            print(json.dumps({"section": args.section, "impl": args.impl, **part}), flush=True)
+            return 0
         if args.impl == "reference":
             if rank != 0:
                 line = None

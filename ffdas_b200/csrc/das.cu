@@ -218,7 +218,7 @@ static schedule plan_schedule(const ffdas_context &h, const das_problem &pb, int
     }
     if (h.has_config) {
         const ffdas_das_config_t &c = h.config;
-        if (c.variant) s.variant = c.variant;
+        if (c.variant == 1 || c.variant == 2) s.variant = c.variant;   // 3 selects a backward kernel only
         if (c.tile_x || c.tile_y || c.tile_z) {
             s.T0 = c.tile_x ? c.tile_x : 1;
             s.T1 = c.tile_y ? c.tile_y : 1;

@@ -327,7 +327,9 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
     bp.gx = gx; bp.goff = goff; bp.gw = gw; bp.gdst = gdst; bp.gsrc = gsrc;
 
     pb.sparse = a.sparse;
-    if (!a.sparse && staged_supported(pb, kind) && !(h.has_config && h.config.variant == 1)) {
+    // The backward kernel does not follow a forward schedule choice: only
+    // variant 3 asks for the gather adjoint on dense problems.
+    if (!a.sparse && staged_supported(pb, kind) && !(h.has_config && h.config.variant == 3)) {
         // Dense problems: TMA-staged adjoint, one CTA per voxel tile x batch item.
         if (h.has_config && h.config.variant == 2 && (h.config.tile_x || h.config.tile_y)) {
             const int tx = h.config.tile_x ? h.config.tile_x : 1, ty = h.config.tile_y ? h.config.tile_y : 1,

@@ -137,7 +137,8 @@ typedef struct ffdas_tensor_desc* ffdas_tensor_desc_t;
 /* Kernel schedule for the delay-and-sum kernels (new).  Zero in a field
  * means "planner default".  The autotuner sweeps these. */
 typedef struct {
-    int32_t variant;      /* 0 auto, 1 L1 gather kernel, 2 TMA-staged kernel */
+    int32_t variant;      /* 0 auto, 1 L1 gather kernel, 2 TMA-staged kernel (forward and adjoint),
+                             3 gather adjoint in ffdas_das_backward (forward as 0) */
     int32_t tile_x;       /* voxels per CTA along the innermost spatial dim */
     int32_t tile_y;       /* ... along the middle spatial dim */
     int32_t tile_z;       /* ... along the outermost spatial dim */

@@ -142,3 +142,21 @@ def test_autofocus_recovers_sound_speed_scale():
         opt.step()
         sched.step()
     assert abs(float(alpha) - wl["alpha_true"]) < 0.004, float(alpha)
+
+
+def test_staged_and_gather_adjoints_agree():
+    # dense problems take the staged adjoint unless the schedule asks for the
+    # gather adjoint (variant 3); a forward schedule choice does not switch it
+    from ffdas_b200.tune import schedule
+    x, src, dst, offs, w = (t.to(DEV) for t in _problem(9, B=3, nz=40, nx=36))
+    h = ffdas_b200.get_library_handle(DEV)
+    grads, kinds = [], []
+    for cfg in (None, dict(variant=1, batch_tile=2), dict(variant=3)):
+        leaves = [t.clone().requires_grad_(True) for t in (x, src, dst, offs, w)]
+        with schedule(cfg, DEV):
+            das_autograd(*leaves).square().sum().backward()
+            kinds.append(h.last_kernel_info()["variant"])
+        grads.append([t.grad for t in leaves])
+    assert kinds == [4, 4, 3]
+    for a, b in zip(grads[0], grads[2]):
+        assert oracle.rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-5

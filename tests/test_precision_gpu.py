@@ -1,0 +1,42 @@
+"""Storage precision on the full 3-D diverging-wave volume against the FP64
+CPU oracle: FP32 pairs, and 16-bit channel data (FP16 and BF16 pairs, FP32
+geometry and accumulation) within 1e-3 relative L2.
+
+The volume is the benchmark's (1024 channels, 16 transmits, 4096 samples,
+128^3 voxels) with every channel scaled to peak 1; four depth planes spread
+over the volume are beamformed and compared, so the oracle finishes in
+seconds.  The FP32 figure is dominated by FP32 delay rounding (the reference
+computes delays in FP32 too).
+"""
+import numpy as np
+import pytest
+import torch
+
+import ffdas_b200
+from ffdas_b200 import workloads as W
+from ffdas_b200.tune import schedule
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+
+
+@pytest.fixture(scope="module")
+def volume():
+    wl = W.diverging3d(device=DEV)
+    xn = W.normalize_channels(wl["x"])
+    sel = torch.tensor(np.linspace(0, wl["dstpos"].shape[0] - 1, 4).astype(np.int64), device=DEV)
+    geo = (wl["srcpos"], wl["dstpos"][sel].contiguous(), wl["offsets"][:, sel].contiguous(),
+           wl["weights"][:, sel].contiguous())
+    ref = oracle.das_f64(xn.cpu().numpy(), *(t.cpu().numpy() for t in geo))
+    return xn, geo, ref
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.float32, 1e-4), (torch.float16, 1e-3), (torch.bfloat16, 1e-3)])
+@pytest.mark.parametrize("cfg", [None, dict(variant=2, tile_x=16, tile_y=16, window=32),
+                                 dict(variant=1, tile_x=16, tile_y=16)], ids=["auto", "staged", "gather"])
+def test_storage_precision_vs_fp64_oracle(volume, dtype, tol, cfg):
+    xn, geo, ref = volume
+    with schedule(cfg, DEV):
+        img = ffdas_b200.das(xn.to(dtype), *geo)
+    assert oracle.rel_l2(img.cpu().numpy(), ref) < tol
