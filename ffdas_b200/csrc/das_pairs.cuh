@@ -12,8 +12,8 @@ namespace ffdas {
 
 enum storage_kind : int {
     ST_F32 = 0,   // float2 (x0, x1 - x0)
-    ST_F16 = 1,   // half2  (x0, x1)
-    ST_BF16 = 2,  // bf162  (x0, x1)
+    ST_F16 = 1,   // half2  (x0, x1 - x0)
+    ST_BF16 = 2,  // u32    bf16 x0 (high half), bf16 (x1 - x0) (low half)
     ST_F64 = 3,   // double2 (x0, x1 - x0)
     ST_C32 = 4,   // float4 (x0.re, x0.im, d.re, d.im)
     ST_C16 = 5,   // uint2 = half2 x0, half2 x1
@@ -34,48 +34,45 @@ template <> struct pair_traits<ST_F32> {
     __device__ static value slope(storage p) { return p.y; }
 };
 
+// 16-bit pairs hold the sample and the slope, (x0, x1 - x0), each rounded to
+// the storage type once: a tap is two conversions and one FFMA.  x0 stays the
+// stored sample itself (exact for 16-bit channel data); only the slope takes a
+// rounding, which enters the tap scaled by t < 1.
 template <> struct pair_traits<ST_F16> {
     using storage = __half2;
     using value = float;
     using acc = float;
     static constexpr bool complex = false;
-    __device__ static storage make(float x0, float x1) { return __floats2half2_rn(x0, x1); }
+    __device__ static storage make(float x0, float x1) {
+        const float a = __half2float(__float2half_rn(x0)), b = __half2float(__float2half_rn(x1));
+        return __floats2half2_rn(a, b - a);
+    }
     __device__ static value tap(storage p, float t) {
-        float2 f = __half22float2(p);
-        return __fmaf_rn(t, f.y - f.x, f.x);
+        const float2 f = __half22float2(p);
+        return __fmaf_rn(t, f.y, f.x);
     }
-    __device__ static value slope(storage p) {
-        float2 f = __half22float2(p);
-        return f.y - f.x;
-    }
+    __device__ static value slope(storage p) { return __high2float(p); }
 };
 
-// bf16 pair word: low half = bf16(x1 - x0) (the slope); high half = a bf16
-// value chosen so that the WHOLE 32-bit word, read as an f32, is as close to x0
-// as the bf16 grid allows (the low half only adds sub-bf16-ulp mantissa bits,
-// and the high half is picked to compensate).  A tap is then one shift and one
-// FFMA: fma(t, f32(word << 16), f32(word)); x0 and the slope each carry at most
-// about half a bf16 ulp of rounding, like plain bf16 storage.
+// bf16 pair word: high half = bf16(x0), low half = bf16(x1 - x0).  Both
+// halves widen to f32 with one integer op each (mask, shift).
 template <> struct pair_traits<ST_BF16> {
     using storage = uint32_t;
     using value = float;
     using acc = float;
     static constexpr bool complex = false;
-    __device__ static storage make(float x0, float x1) {
-        const __nv_bfloat16 db = __float2bfloat16_rn(x1 - x0);
-        const uint32_t lo = *reinterpret_cast<const uint16_t *>(&db);
-        const uint32_t base = __float_as_uint(x0) >> 16;
-        uint32_t best = (base << 16) | lo;
-        float err = fabsf(__uint_as_float(best) - x0);
-        for (int dlt = -1; dlt <= 1; dlt += 2) {
-            const uint32_t hi = (base + (uint32_t)dlt) & 0xFFFFu;
-            const uint32_t w = (hi << 16) | lo;
-            const float e = fabsf(__uint_as_float(w) - x0);
-            if (e < err) { err = e; best = w; }
-        }
-        return best;
+    __device__ static uint32_t bits(float v) {
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        return *reinterpret_cast<const uint16_t *>(&h);
     }
-    __device__ static value tap(storage p, float t) { return __fmaf_rn(t, __uint_as_float(p << 16), __uint_as_float(p)); }
+    __device__ static storage make(float x0, float x1) {
+        const uint32_t hi = bits(x0);
+        const float a = __uint_as_float(hi << 16), b = __uint_as_float(bits(x1) << 16);
+        return (hi << 16) | bits(b - a);
+    }
+    __device__ static value tap(storage p, float t) {
+        return __fmaf_rn(t, __uint_as_float(p << 16), __uint_as_float(p & 0xFFFF0000u));
+    }
     __device__ static value slope(storage p) { return __uint_as_float(p << 16); }
 };
 

@@ -93,21 +93,30 @@ __device__ __forceinline__ void consumer_sync() {
     asm volatile("bar.sync 1, %0;" ::"r"(kStConsumers) : "memory");
 }
 
+// try_wait with a suspend-time hint: the thread sleeps in the barrier until
+// the phase completes or about `ns` nanoseconds pass, issuing nothing.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint32_t bar, uint32_t parity, uint32_t ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok) : "r"(bar), "r"(parity), "r"(ns) : "memory");
+    return ok != 0;
+}
+
 // Bounded wait: false when the CTA aborted or the clock budget ran out.
+// Waiting threads sleep in the barrier (suspend hint) rather than spin, so a
+// warp that waits takes no issue slots from the warps that compute.
 __device__ __forceinline__ bool bounded_wait(uint32_t bar, uint32_t parity, volatile int *abort, int *status) {
     if (*abort) return false;
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
-    for (uint32_t i = 1;; i++) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((i & 31) == 0) {
-            if (*abort) return false;
-            if (clock64() - t0 > kWaitCycles) {
-                *abort = 1;
-                atomicExch(status, kStatusTimeout);
-                return false;
-            }
-            __nanosleep(64);
+    for (;;) {
+        if (mbar_try_wait_sleep(bar, parity, 20000u)) return true;
+        if (*abort) return false;
+        if (clock64() - t0 > kWaitCycles) {
+            *abort = 1;
+            atomicExch(status, kStatusTimeout);
+            return false;
         }
     }
 }
@@ -440,6 +449,28 @@ template <> __device__ __forceinline__ float tap_at<ST_BF16>(uint32_t a, float t
     return pair_traits<ST_BF16>::tap(lds_u32(a), t);
 }
 
+// Warp-wide segmented sum by key.  Lanes holding the same key in consecutive
+// lanes form one segment; the last lane of each segment returns the segment's
+// sums of v0 and v1 and true, every other lane false.  Neighbouring voxels of
+// a warp hit the same or adjacent samples, so a window's scatter collapses to
+// a few adds per warp instead of 32 contended shared-memory atomics.  All 32
+// lanes must call it together.
+__device__ __forceinline__ bool warp_segment_sum(uint32_t key, float &v0, float &v1, int lane) {
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
+    const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));  // this lane's segment head
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const float u0 = __shfl_up_sync(0xffffffffu, v0, d);
+        const float u1 = __shfl_up_sync(0xffffffffu, v1, d);
+        if (lane - d >= start) {
+            v0 += u0;
+            v1 += u1;
+        }
+    }
+    return lane == 31 || ((heads >> lane) >> 1) & 1u;
+}
+
 // Interpolate one tap from a staged slot (f32 result).
 template <int K>
 __device__ __forceinline__ float staged_tap(const unsigned char *slot, uint32_t rel, float t) {
@@ -510,9 +541,11 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
                 if (!dead) {
                     const bool any_ovf = sm.ovf[stage] != 0;
                     const uint32_t stage_u32 = ring_u32 + stage * SG::stage_bytes;
+                    // channels past C carry a zero window and a zero position: their
+                    // taps read the zero pair, so the loop needs no bound check
+#pragma unroll
                     for (int cl = 0; cl < CC; cl++) {
                         const int c = c0 + cl;
-                        if (c >= p.C) break;
                         const float4 cp = lds_f4(chan_u32 + (stage * kStWin + cl) * 16);
                         recv_geom g = receive_geometry(cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z);
                         if (p.srcdir)
@@ -606,7 +639,7 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
 // red.global.add and zero them.  Channel-position gradients are reduced over
 // the tile in shared memory and added once per channel per CTA.
 template <int K, int SC, int WB>
-__global__ void __launch_bounds__(kStThreads) das_staged_bwd_kernel(const staged_params p,
+__global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const staged_params p,
                                                                      const __grid_constant__ CUtensorMap tmap) {
     using SG = slot_geom<WB, K>;
     constexpr int CC = kStWin / SC;
@@ -645,11 +678,12 @@ __global__ void __launch_bounds__(kStThreads) das_staged_bwd_kernel(const staged
                 const unsigned char *stage_base = sm.ring + stage * SG::stage_bytes;
                 float *gstage = gslot + stage * kStWin * GS;
                 if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
+                dead = __any_sync(0xffffffffu, dead);   // warp-uniform: the scatter below is warp-wide
                 const bool any_ovf = !dead && sm.ovf[stage] != 0;
                 if (!dead) {
                     for (int cl = 0; cl < CC; cl++) {
                         const int c = c0 + cl;
-                        if (c >= p.C) break;
+                        if (c >= p.C) break;   // a phantom channel's taps would scatter outside gx
                         const float4 cp = sm.chan_pos[stage * kStWin + cl];
                         const recv_geom gm = receive_geometry(cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z);
                         uint32_t k0p[SC];
@@ -679,16 +713,25 @@ __global__ void __launch_bounds__(kStThreads) das_staged_bwd_kernel(const staged
                             goa[j] = __fmaf_rn(a, d, goa[j]);
                             q = __fmaf_rn(a, d, q);
                             // channel-data adjoint: only taps inside the record
-                            if (p.gx && a != 0.f && ts.k < (uint32_t)(p.N - 1)) {
-                                const float a1 = a * ts.t;
-                                if (!ovfw && rel < (uint32_t)WB) {
-                                    float *gs = gstage + (cl * SC + j) * GS + rel;
-                                    atomicAdd(gs, a - a1);
-                                    atomicAdd(gs + 1, a1);
-                                } else {
-                                    float *gr = p.gx + (((int64_t)cx.b * p.C + c) * p.S + (e0 + j)) * p.N + ts.k;
-                                    atomicAdd(gr, a - a1);
-                                    atomicAdd(gr + 1, a1);
+                            if (p.gx) {
+                                uint32_t key = 0xffffffffu;   // no in-window contribution
+                                float v0 = 0.f, v1 = 0.f;
+                                if (a != 0.f && ts.k < (uint32_t)(p.N - 1)) {
+                                    const float a1 = a * ts.t;
+                                    if (!ovfw && rel < (uint32_t)WB) {
+                                        key = rel;
+                                        v0 = a - a1;
+                                        v1 = a1;
+                                    } else {
+                                        float *gr = p.gx + (((int64_t)cx.b * p.C + c) * p.S + (e0 + j)) * p.N + ts.k;
+                                        atomicAdd(gr, a - a1);
+                                        atomicAdd(gr + 1, a1);
+                                    }
+                                }
+                                if (warp_segment_sum(key, v0, v1, cx.lane) && key < (uint32_t)WB) {
+                                    float *gs = gstage + (cl * SC + j) * GS + key;
+                                    atomicAdd(gs, v0);
+                                    atomicAdd(gs + 1, v1);
                                 }
                             }
                         }

@@ -61,7 +61,7 @@ def test_staged_matches_oracle(name, kw, cfg):
     assert ffdas_b200.get_library_handle(DEV).device_status() == 0
 
 
-@pytest.mark.parametrize("dtype,tol", [(torch.float16, 2e-3), (torch.bfloat16, 8e-3)])
+@pytest.mark.parametrize("dtype,tol", [(torch.float16, 1e-3), (torch.bfloat16, 1e-3)])
 def test_staged_16bit_pairs(dtype, tol):
     wl = W.diverging3d(device=DEV, scale=0.25)
     x = W.normalize_channels(wl["x"]).to(dtype)
