@@ -359,7 +359,7 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
         gp.srcpos = a.srcpos; gp.dstpos = a.dstpos; gp.offsets = a.offsets; gp.weights = a.weights;
         gp.beta_zero = 1;
         const staged_grads gr{static_cast<const float *>(gout), pb.out_bstride, gx, goff, gw, gdst, gsrc};
-        const int SC = pb.n_events <= 1 ? 1 : (pb.n_events <= 4 ? 4 : 8);
+        const int SC = pb.n_events <= 1 ? 1 : 4;
         const int WB = (h.has_config && h.config.window > 32) ? 64 : 32;
         h.last = ffdas_kernel_info_t{};
         h.last.variant = 4;

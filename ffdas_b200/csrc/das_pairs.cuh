@@ -13,7 +13,7 @@ namespace ffdas {
 enum storage_kind : int {
     ST_F32 = 0,   // float2 (x0, x1 - x0)
     ST_F16 = 1,   // half2  (x0, x1 - x0)
-    ST_BF16 = 2,  // u32    bf16 x0 (high half), bf16 (x1 - x0) (low half)
+    ST_BF16 = 2,  // u32    bf16 x0 (low half), bf16 x1 (high half)
     ST_F64 = 3,   // double2 (x0, x1 - x0)
     ST_C32 = 4,   // float4 (x0.re, x0.im, d.re, d.im)
     ST_C16 = 5,   // uint2 = half2 x0, half2 x1
@@ -34,10 +34,10 @@ template <> struct pair_traits<ST_F32> {
     __device__ static value slope(storage p) { return p.y; }
 };
 
-// 16-bit pairs hold the sample and the slope, (x0, x1 - x0), each rounded to
-// the storage type once: a tap is two conversions and one FFMA.  x0 stays the
-// stored sample itself (exact for 16-bit channel data); only the slope takes a
-// rounding, which enters the tap scaled by t < 1.
+// f16 pairs hold the sample and the slope, (x0, x1 - x0): a tap is two
+// conversions and one FFMA.  x0 stays the stored sample itself (exact for
+// f16 channel data); the slope takes one f16 rounding (11-bit mantissa),
+// which enters the tap scaled by t < 1.
 template <> struct pair_traits<ST_F16> {
     using storage = __half2;
     using value = float;
@@ -54,8 +54,11 @@ template <> struct pair_traits<ST_F16> {
     __device__ static value slope(storage p) { return __high2float(p); }
 };
 
-// bf16 pair word: high half = bf16(x0), low half = bf16(x1 - x0).  Both
-// halves widen to f32 with one integer op each (mask, shift).
+// bf16 pair word: low half = bf16(x0), high half = bf16(x1).  Both samples
+// are kept as stored, so a tap interpolates the bf16 data exactly (in f32);
+// a bf16 slope would add its own rounding, which on 1024-channel volumes
+// doubled the image error of bf16 channel data.  Each half widens to f32
+// with one integer op (shift, mask).
 template <> struct pair_traits<ST_BF16> {
     using storage = uint32_t;
     using value = float;
@@ -65,15 +68,12 @@ template <> struct pair_traits<ST_BF16> {
         const __nv_bfloat16 h = __float2bfloat16_rn(v);
         return *reinterpret_cast<const uint16_t *>(&h);
     }
-    __device__ static storage make(float x0, float x1) {
-        const uint32_t hi = bits(x0);
-        const float a = __uint_as_float(hi << 16), b = __uint_as_float(bits(x1) << 16);
-        return (hi << 16) | bits(b - a);
-    }
+    __device__ static storage make(float x0, float x1) { return (bits(x1) << 16) | bits(x0); }
     __device__ static value tap(storage p, float t) {
-        return __fmaf_rn(t, __uint_as_float(p << 16), __uint_as_float(p & 0xFFFF0000u));
+        const float a = __uint_as_float(p << 16), b = __uint_as_float(p & 0xFFFF0000u);
+        return __fmaf_rn(t, b - a, a);
     }
-    __device__ static value slope(storage p) { return __uint_as_float(p << 16); }
+    __device__ static value slope(storage p) { return __uint_as_float(p & 0xFFFF0000u) - __uint_as_float(p << 16); }
 };
 
 template <> struct pair_traits<ST_F64> {

@@ -101,11 +101,8 @@ static ffdas_error_t launch_fwd_sc(ffdas_context &h, const staged_params &sp, co
 template <int K, int WB>
 static ffdas_error_t launch_bwd_sc(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, int SC,
                                    dim3 grid) {
-    switch (SC) {
-        case 1: return launch_bwd_t<K, 1, WB>(h, sp, map, grid);
-        case 4: return launch_bwd_t<K, 4, WB>(h, sp, map, grid);
-        default: return launch_bwd_t<K, 8, WB>(h, sp, map, grid);
-    }
+    // event chunks of 1 or 4: eight events per pass would spill registers
+    return SC == 1 ? launch_bwd_t<K, 1, WB>(h, sp, map, grid) : launch_bwd_t<K, 4, WB>(h, sp, map, grid);
 }
 
 static staged_params base_params(ffdas_context &h, const das_problem &pb, const gather_params &gp) {

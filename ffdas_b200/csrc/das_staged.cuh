@@ -155,11 +155,27 @@ constexpr size_t staged_smem_bytes() {
     return slot_geom<WB, K>::ring_bytes + kStMiscBytes + 128;
 }
 
-// Adjoint extras: gradient slots [kStages][kStWin][WB + 2] floats and the
-// per-stage channel-gradient scratch [kStWin / SC * 3][256] floats.
+// Adjoint extras: fixed-point gradient slots [kStages][kStWin][WB + 2] int32,
+// the per-stage channel-gradient scratch [kStWin / SC * 3][256] floats and a
+// per-warp reduction scratch.
 template <int WB, int K, int SC>
 constexpr size_t staged_bwd_smem_bytes() {
-    return staged_smem_bytes<WB, K>() + kStages * kStWin * (WB + 2) * 4 + (kStWin / SC) * 3 * kStConsumers * 4;
+    return staged_smem_bytes<WB, K>() + kStages * kStWin * (WB + 2) * 4 + (kStWin / SC) * 3 * kStConsumers * 4 +
+           kStWarps * 4;
+}
+
+__device__ __forceinline__ void red_shared_add(uint32_t addr, int v) {
+    asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
+// Fixed point for the adjoint's shared gradient slots: a value |v| <= 2^22
+// rounds to the nearest integer as bits(v + 1.5 * 2^23) - bits(1.5 * 2^23).
+constexpr float kFixRange = 4194000.0f;   // a little under 2^22
+__device__ __forceinline__ int fix_round(float v) {
+    return __float_as_int(v + kFloorMagic) - (int)kFloorMagicBits;
+}
+__device__ __forceinline__ int fix_round_fma(float a, float b) {   // round(a * b), one rounding
+    return __float_as_int(__fmaf_rn(a, b, kFloorMagic)) - (int)kFloorMagicBits;
 }
 
 // Shared-memory layout shared by the forward and adjoint kernels.
@@ -203,8 +219,12 @@ struct staged_ctx {
 };
 
 // Voxel of the thread, barrier init, zero pairs, tile bounding box.
+// With spread, lane l of warp w takes the tile's voxel l * 8 + w, so a warp's
+// voxels sit across the whole tile and rarely hit the same sample of a window
+// (the adjoint's scatter then meets few same-address atomics).
 template <int K, int WB>
-__device__ __forceinline__ staged_ctx staged_setup(const staged_params &p, staged_smem<K, WB> &sm) {
+__device__ __forceinline__ staged_ctx staged_setup(const staged_params &p, staged_smem<K, WB> &sm,
+                                                   bool spread = false) {
     using SG = slot_geom<WB, K>;
     staged_ctx cx;
     cx.tid = threadIdx.x;
@@ -218,7 +238,8 @@ __device__ __forceinline__ staged_ctx staged_setup(const staged_params &p, stage
     const int tile = blockIdx.x;
     const int t0 = tile % p.n0, t1 = (tile / p.n0) % p.n1, t2 = tile / (p.n0 * p.n1);
     if (!cx.producer) {
-        const int i0 = cx.tid % p.T0, i1 = (cx.tid / p.T0) % p.T1, i2 = cx.tid / (p.T0 * p.T1);
+        const int lt = spread ? (cx.lane * kStWarps + cx.warp) : cx.tid;
+        const int i0 = lt % p.T0, i1 = (lt / p.T0) % p.T1, i2 = lt / (p.T0 * p.T1);
         const int g0 = t0 * p.T0 + i0, g1 = t1 * p.T1 + i1, g2 = t2 * p.T2 + i2;
         cx.active = (g0 < p.D0 && g1 < p.D1 && g2 < p.D2);
         if (cx.active) {
@@ -449,28 +470,6 @@ template <> __device__ __forceinline__ float tap_at<ST_BF16>(uint32_t a, float t
     return pair_traits<ST_BF16>::tap(lds_u32(a), t);
 }
 
-// Warp-wide segmented sum by key.  Lanes holding the same key in consecutive
-// lanes form one segment; the last lane of each segment returns the segment's
-// sums of v0 and v1 and true, every other lane false.  Neighbouring voxels of
-// a warp hit the same or adjacent samples, so a window's scatter collapses to
-// a few adds per warp instead of 32 contended shared-memory atomics.  All 32
-// lanes must call it together.
-__device__ __forceinline__ bool warp_segment_sum(uint32_t key, float &v0, float &v1, int lane) {
-    const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
-    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
-    const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));  // this lane's segment head
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const float u0 = __shfl_up_sync(0xffffffffu, v0, d);
-        const float u1 = __shfl_up_sync(0xffffffffu, v1, d);
-        if (lane - d >= start) {
-            v0 += u0;
-            v1 += u1;
-        }
-    }
-    return lane == 31 || ((heads >> lane) >> 1) & 1u;
-}
-
 // Interpolate one tap from a staged slot (f32 result).
 template <int K>
 __device__ __forceinline__ float staged_tap(const unsigned char *slot, uint32_t rel, float t) {
@@ -634,24 +633,36 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
 //   gw[e,v] += g L;  goff[e,v] += a d;  q(v,c) += a d
 //   gdst[v] += q (v - c)/r;  gsrc[c] -= q (v - c)/r
 //   gx[b,c,s,k] += a (1 - t);  gx[b,c,s,k+1] += a t      (0 <= k <= N-2)
-// The two-tap scatter goes into the window's shared gradient slot; after all
-// consumer warps finished a stage, they flush the touched entries with
-// red.global.add and zero them.  Channel-position gradients are reduced over
-// the tile in shared memory and added once per channel per CTA.
+// The two-tap scatter goes into the window's shared gradient slot as fixed
+// point: per event pass the CTA takes amax = max |g w| over its tile, scales
+// every contribution by 2^22 / amax and adds round(a s t) and
+// round(a s) - round(a s t) with native shared-memory integer adds (float adds
+// to shared memory would be compare-and-swap loops).  A slot entry collects at
+// most 2 x 256 contributions per stage, so it stays within 2^31; the rounding
+// error per contribution is 2^-23 amax.  After all consumer warps finished a
+// stage, they flush the touched entries to gx (red.global.add.f32) and zero
+// them.  Taps outside a staged window (overflowing windows) and passes whose
+// amax is not a positive finite number scatter with global float atomics.
+// Channel-position gradients are reduced over the tile in shared memory and
+// added once per channel per CTA.  Voxels are spread over the warps
+// (staged_setup's spread mapping) so a warp's lanes rarely share a sample.
 template <int K, int SC, int WB>
 __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const staged_params p,
                                                                      const __grid_constant__ CUtensorMap tmap) {
     using SG = slot_geom<WB, K>;
+    using st = typename pair_traits<K>::storage;
     constexpr int CC = kStWin / SC;
-    constexpr int GS = WB + 2;  // gradient slot length (floats)
+    constexpr int GS = WB + 2;  // gradient slot length (int32 entries)
     static_assert(kStWin % SC == 0, "SC must divide the stage");
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     staged_smem<K, WB> sm(smem_raw);
-    float *gslot = reinterpret_cast<float *>(sm.extra);                 // [kStages][kStWin][GS]
-    float *cgrad = gslot + kStages * kStWin * GS;                        // [CC * 3][256]
-    for (int i = threadIdx.x; i < kStages * kStWin * GS; i += kStThreads) gslot[i] = 0.f;
-    const staged_ctx cx = staged_setup<K, WB>(p, sm);   // ends with __syncthreads
+    int *gslot = reinterpret_cast<int *>(sm.extra);                      // [kStages][kStWin][GS]
+    float *cgrad = reinterpret_cast<float *>(gslot + kStages * kStWin * GS);  // [CC * 3][256]
+    float *wmax = cgrad + CC * 3 * kStConsumers;                          // [kStWarps]
+    for (int i = threadIdx.x; i < kStages * kStWin * GS; i += kStThreads) gslot[i] = 0;
+    const staged_ctx cx = staged_setup<K, WB>(p, sm, true);   // ends with __syncthreads
+    const uint32_t gslot_u32 = smem_u32(gslot);
 
     const bool multi_b = p.B > 1;
     const float g = (cx.active) ? __ldg(p.gout + (int64_t)cx.b * p.gout_bstride + cx.v) : 0.f;
@@ -669,6 +680,38 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
         float gwa[SC], goa[SC];
 #pragma unroll
         for (int j = 0; j < SC; j++) { gwa[j] = 0.f; goa[j] = 0.f; }
+        // fixed-point scale of this pass: amax = max |g w| over the tile
+        float fscale = 0.f, finv = 0.f;
+        bool fixed = false;
+        if (!cx.producer) {
+            float m = 0.f;
+            bool bad = false;   // a non-finite g w (NaN fails the comparison)
+#pragma unroll
+            for (int j = 0; j < SC; j++) {
+                const float aw = fabsf(g * w[j]);
+                m = fmaxf(m, aw);
+                bad |= !(aw <= 3.0e38f);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            bad = __any_sync(0xffffffffu, bad);
+            if (cx.lane == 0) wmax[cx.warp] = bad ? -1.f : m;
+            consumer_sync();
+            float amax = 0.f;
+            bool any_bad = false;
+#pragma unroll
+            for (int i = 0; i < kStWarps; i++) {
+                const float v = wmax[i];
+                any_bad |= v < 0.f;
+                amax = fmaxf(amax, v);
+            }
+            fixed = !any_bad && amax > 0.f && amax <= 3.0e38f;
+            if (fixed) {
+                fscale = kFixRange / amax;
+                finv = amax / kFixRange;
+            }
+            consumer_sync();   // wmax is rewritten by the next pass
+        }
 
         for (int c0 = 0; c0 < p.C; c0 += CC) {
             if (cx.producer) {
@@ -676,9 +719,9 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
             } else {
                 const uint32_t full_bar = smem_u32(&sm.full[stage]);
                 const unsigned char *stage_base = sm.ring + stage * SG::stage_bytes;
-                float *gstage = gslot + stage * kStWin * GS;
+                int *gstage = gslot + stage * kStWin * GS;
+                const uint32_t gstage_u32 = gslot_u32 + stage * kStWin * GS * 4;
                 if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
-                dead = __any_sync(0xffffffffu, dead);   // warp-uniform: the scatter below is warp-wide
                 const bool any_ovf = !dead && sm.ovf[stage] != 0;
                 if (!dead) {
                     for (int cl = 0; cl < CC; cl++) {
@@ -694,17 +737,15 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
                         for (int j = 0; j < SC; j++) {
                             const float tau = __fmaf_rn(gm.rsq, gm.rinv, ofs[j]);
                             const tau_split ts = split_tau(tau);
-                            typename pair_traits<K>::storage pr;
+                            st pr;
                             const bool ovfw = any_ovf && k0p[j] == kOvf;
                             uint32_t rel = WB;
                             if (ovfw) {
                                 const int64_t row = ((int64_t)cx.b * p.C + c) * p.S + (e0 + min(j, sc - 1));
-                                pr = static_cast<const typename pair_traits<K>::storage *>(p.P)
-                                    [row * p.npad + min(ts.k, (uint32_t)(p.npad - 1))];
+                                pr = static_cast<const st *>(p.P)[row * p.npad + min(ts.k, (uint32_t)(p.npad - 1))];
                             } else {
                                 rel = min(ts.k + kFloorMagicBits - k0p[j], (uint32_t)WB);
-                                pr = *reinterpret_cast<const typename pair_traits<K>::storage *>(
-                                    slots + j * SG::bytes + rel * sizeof(pr));
+                                pr = *reinterpret_cast<const st *>(slots + j * SG::bytes + rel * sizeof(st));
                             }
                             const float L = pair_traits<K>::tap(pr, ts.t);
                             const float d = pair_traits<K>::slope(pr);
@@ -713,25 +754,19 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
                             goa[j] = __fmaf_rn(a, d, goa[j]);
                             q = __fmaf_rn(a, d, q);
                             // channel-data adjoint: only taps inside the record
-                            if (p.gx) {
-                                uint32_t key = 0xffffffffu;   // no in-window contribution
-                                float v0 = 0.f, v1 = 0.f;
-                                if (a != 0.f && ts.k < (uint32_t)(p.N - 1)) {
+                            if (p.gx && a != 0.f && ts.k < (uint32_t)(p.N - 1)) {
+                                if (fixed && !ovfw && rel < (uint32_t)WB) {
+                                    const float as = a * fscale;
+                                    const int it = fix_round(as);
+                                    const int i1 = fix_round_fma(as, ts.t);
+                                    const uint32_t ga = gstage_u32 + ((cl * SC + j) * GS + rel) * 4;
+                                    red_shared_add(ga, it - i1);
+                                    red_shared_add(ga + 4, i1);
+                                } else {
                                     const float a1 = a * ts.t;
-                                    if (!ovfw && rel < (uint32_t)WB) {
-                                        key = rel;
-                                        v0 = a - a1;
-                                        v1 = a1;
-                                    } else {
-                                        float *gr = p.gx + (((int64_t)cx.b * p.C + c) * p.S + (e0 + j)) * p.N + ts.k;
-                                        atomicAdd(gr, a - a1);
-                                        atomicAdd(gr + 1, a1);
-                                    }
-                                }
-                                if (warp_segment_sum(key, v0, v1, cx.lane) && key < (uint32_t)WB) {
-                                    float *gs = gstage + (cl * SC + j) * GS + key;
-                                    atomicAdd(gs, v0);
-                                    atomicAdd(gs + 1, v1);
+                                    float *gr = p.gx + (((int64_t)cx.b * p.C + c) * p.S + (e0 + j)) * p.N + ts.k;
+                                    atomicAdd(gr, a - a1);
+                                    atomicAdd(gr + 1, a1);
                                 }
                             }
                         }
@@ -751,16 +786,16 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
                 consumer_sync();
                 if (!dead) {
                     // flush the stage's gradient slots: one red.add per touched sample
-                    if (p.gx) {
+                    if (p.gx && fixed) {
                         for (int i = cx.tid; i < kStWin * GS; i += kStConsumers) {
-                            const int win = i / GS, r = i - win * GS;
-                            const float val = gstage[i];
-                            if (val != 0.f) {
-                                gstage[i] = 0.f;
+                            const int val = gstage[i];
+                            if (val != 0) {
+                                gstage[i] = 0;
+                                const int win = i / GS, r = i - win * GS;
                                 const int cl = win / SC, j = win % SC;
                                 const int k = (int)(sm.meta[stage * kStWin + win] - kFloorMagicBits) + r;
                                 float *gr = p.gx + (((int64_t)cx.b * p.C + (c0 + cl)) * p.S + (e0 + j)) * p.N + k;
-                                atomicAdd(gr, val);
+                                atomicAdd(gr, (float)val * finv);
                             }
                         }
                     }
