@@ -84,7 +84,7 @@ class DasConfig(ctypes.Structure):
     """ffdas_das_config_t: schedule override (0 = planner default)."""
     _fields_ = [("variant", ctypes.c_int32), ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32),
                 ("tile_z", ctypes.c_int32), ("batch_tile", ctypes.c_int32), ("event_chunk", ctypes.c_int32),
-                ("min_blocks", ctypes.c_int32), ("window", ctypes.c_int32)]
+                ("min_blocks", ctypes.c_int32), ("window", ctypes.c_int32), ("copy_engine", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
@@ -94,7 +94,8 @@ class KernelInfo(ctypes.Structure):
     """ffdas_kernel_info_t: what the last call launched."""
     _fields_ = [("variant", ctypes.c_int32), ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32),
                 ("tile_z", ctypes.c_int32), ("batch_tile", ctypes.c_int32), ("event_chunk", ctypes.c_int32),
-                ("storage", ctypes.c_int32), ("kernels", ctypes.c_int32), ("grid", ctypes.c_int64)]
+                ("storage", ctypes.c_int32), ("kernels", ctypes.c_int32), ("grid", ctypes.c_int64),
+                ("copy_engine", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: int(getattr(self, f)) for f, _ in self._fields_}

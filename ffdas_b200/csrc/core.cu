@@ -253,6 +253,7 @@ ffdas_error_t ffdas_das_set_config(ffdas_handle_t h, const ffdas_das_config_t *c
     if (!pow2_or_zero(c.batch_tile, 16)) return FFDAS_ERROR_INVALID_ARGUMENT;
     if (c.event_chunk < 0 || c.event_chunk > 16) return FFDAS_ERROR_INVALID_ARGUMENT;
     if (c.min_blocks < 0 || c.min_blocks > 32) return FFDAS_ERROR_INVALID_ARGUMENT;
+    if (c.copy_engine < 0 || c.copy_engine > 2) return FFDAS_ERROR_INVALID_ARGUMENT;
     int tx = c.tile_x ? c.tile_x : 1, ty = c.tile_y ? c.tile_y : 1, tz = c.tile_z ? c.tile_z : 1;
     if ((c.tile_x || c.tile_y || c.tile_z) && (tx * ty * tz < 32 || tx * ty * tz > 1024))
         return FFDAS_ERROR_INVALID_ARGUMENT;

@@ -184,6 +184,7 @@ struct schedule {
     int BT = 1;
     int SC = 16;
     int WB = 32;   // staged kernel: pairs per window slot
+    int copy = 0;  // staged kernel: copy engine (0 default)
 };
 
 // Events per staged pass: the smallest supported chunk covering n events.
@@ -227,6 +228,7 @@ static schedule plan_schedule(const ffdas_context &h, const das_problem &pb, int
         if (c.batch_tile) s.BT = c.batch_tile;
         if (c.event_chunk) s.SC = c.event_chunk <= 4 ? 4 : 16;
         if (c.window) s.WB = c.window <= 32 ? 32 : 64;
+        s.copy = c.copy_engine;
     }
     if (s.variant == 2) {
         // staged kernel: one batch item per CTA, event chunk from the count
@@ -421,7 +423,8 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
         h.last.grid = tiles * pb.B;
         if (pb.B > 65535) return FFDAS_ERROR_DIMS_TOO_LARGE;
         h.mark_start();
-        const ffdas_error_t err = launch_staged(h, pb, kind, gp, s.SC, s.WB, dim3((unsigned)tiles, (unsigned)pb.B));
+        const ffdas_error_t err =
+            launch_staged(h, pb, kind, gp, s.SC, s.WB, s.copy, dim3((unsigned)tiles, (unsigned)pb.B));
         h.mark_stop();
         return err;
     }

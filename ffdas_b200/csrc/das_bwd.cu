@@ -367,7 +367,9 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
         h.last.batch_tile = 1; h.last.event_chunk = SC; h.last.storage = kind;
         h.last.kernels = 2; h.last.grid = stiles * pb.B;
         h.mark_start();
-        const ffdas_error_t err = launch_staged_bwd(h, pb, kind, gp, gr, SC, WB, dim3((unsigned)stiles, (unsigned)pb.B));
+        const int copy = h.has_config ? h.config.copy_engine : 0;
+        const ffdas_error_t err =
+            launch_staged_bwd(h, pb, kind, gp, gr, SC, WB, copy, dim3((unsigned)stiles, (unsigned)pb.B));
         h.mark_stop();
         return err;
     }

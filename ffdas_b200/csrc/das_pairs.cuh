@@ -12,7 +12,7 @@ namespace ffdas {
 
 enum storage_kind : int {
     ST_F32 = 0,   // float2 (x0, x1 - x0)
-    ST_F16 = 1,   // half2  (x0, x1 - x0)
+    ST_F16 = 1,   // half2  (x0, x1)
     ST_BF16 = 2,  // u32    bf16 x0 (low half), bf16 x1 (high half)
     ST_F64 = 3,   // double2 (x0, x1 - x0)
     ST_C32 = 4,   // float4 (x0.re, x0.im, d.re, d.im)
@@ -34,24 +34,23 @@ template <> struct pair_traits<ST_F32> {
     __device__ static value slope(storage p) { return p.y; }
 };
 
-// f16 pairs hold the sample and the slope, (x0, x1 - x0): a tap is two
-// conversions and one FFMA.  x0 stays the stored sample itself (exact for
-// f16 channel data); the slope takes one f16 rounding (11-bit mantissa),
-// which enters the tap scaled by t < 1.
+// f16 pairs hold both samples, (x0, x1): a tap interpolates the stored f16
+// values exactly (in f32) -- two conversions, one FADD, one FFMA.  Storing
+// the slope instead would save the FADD but add an f16 rounding of x1 - x0.
 template <> struct pair_traits<ST_F16> {
     using storage = __half2;
     using value = float;
     using acc = float;
     static constexpr bool complex = false;
-    __device__ static storage make(float x0, float x1) {
-        const float a = __half2float(__float2half_rn(x0)), b = __half2float(__float2half_rn(x1));
-        return __floats2half2_rn(a, b - a);
-    }
+    __device__ static storage make(float x0, float x1) { return __floats2half2_rn(x0, x1); }
     __device__ static value tap(storage p, float t) {
         const float2 f = __half22float2(p);
-        return __fmaf_rn(t, f.y, f.x);
+        return __fmaf_rn(t, f.y - f.x, f.x);
     }
-    __device__ static value slope(storage p) { return __high2float(p); }
+    __device__ static value slope(storage p) {
+        const float2 f = __half22float2(p);
+        return f.y - f.x;
+    }
 };
 
 // bf16 pair word: low half = bf16(x0), high half = bf16(x1).  Both samples

@@ -68,8 +68,10 @@ inline int64_t pair_row_length(int N) {
 namespace ffdas {
 
 bool staged_supported(const das_problem &pb, int kind);
+// copy: 0 default, 1 TMA tile loads, 2 per-thread cp.async (also used when the
+// driver's tensor-map encoder is unavailable).  Records it in h.last.
 ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp, int SC,
-                            int WB, dim3 grid);
+                            int WB, int copy, dim3 grid);
 
 // Gradient outputs of the staged adjoint kernel (null = not computed).
 struct staged_grads {
@@ -78,6 +80,6 @@ struct staged_grads {
     float *gx, *goff, *gw, *gdst, *gsrc;
 };
 ffdas_error_t launch_staged_bwd(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,
-                                const staged_grads &gr, int SC, int WB, dim3 grid);
+                                const staged_grads &gr, int SC, int WB, int copy, dim3 grid);
 
 }  // namespace ffdas

@@ -17,6 +17,8 @@
 
 namespace ffdas {
 
+constexpr int kDefaultCopy = 1;   // TMA tile loads
+
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static std::once_flag once;
@@ -35,7 +37,14 @@ bool staged_supported(const das_problem &pb, int kind) {
     if (pb.sparse) return false;
     if (kind != ST_F32 && kind != ST_F16 && kind != ST_BF16) return false;
     const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
-    return rows > 0 && rows < INT32_MAX && pb.B <= 65535 && tensor_map_encoder() != nullptr;
+    return rows > 0 && rows < INT32_MAX && pb.B <= 65535;
+}
+
+// Copy engine actually used: TMA needs the driver's tensor-map encoder.
+static int resolve_copy(int copy) {
+    if (copy == 0) copy = kDefaultCopy;
+    if (copy == 1 && tensor_map_encoder() == nullptr) copy = 2;
+    return copy;
 }
 
 // Tensor map over the pair rows: dims {npad, rows}, box {WB, 1}, zero OOB fill.
@@ -123,10 +132,14 @@ static staged_params base_params(ffdas_context &h, const das_problem &pb, const 
 }
 
 ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp, int SC,
-                            int WB, dim3 grid) {
+                            int WB, int copy, dim3 grid) {
+    copy = resolve_copy(copy);
     CUtensorMap map;
-    FFDAS_TRY(pair_row_map(map, gp.P, gp.npad, (int64_t)pb.B * pb.C * pb.S, kind, WB));
-    const staged_params sp = base_params(h, pb, gp);
+    std::memset(&map, 0, sizeof(map));
+    if (copy == 1) FFDAS_TRY(pair_row_map(map, gp.P, gp.npad, (int64_t)pb.B * pb.C * pb.S, kind, WB));
+    staged_params sp = base_params(h, pb, gp);
+    sp.copy_async = copy == 2;
+    h.last.copy_engine = copy;
     switch (kind) {
         case ST_F32:
             return WB == 64 ? launch_fwd_sc<ST_F32, 64>(h, sp, map, SC, grid) : launch_fwd_sc<ST_F32, 32>(h, sp, map, SC, grid);
@@ -138,10 +151,14 @@ ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, c
 }
 
 ffdas_error_t launch_staged_bwd(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,
-                                const staged_grads &gr, int SC, int WB, dim3 grid) {
+                                const staged_grads &gr, int SC, int WB, int copy, dim3 grid) {
+    copy = resolve_copy(copy);
     CUtensorMap map;
-    FFDAS_TRY(pair_row_map(map, gp.P, gp.npad, (int64_t)pb.B * pb.C * pb.S, kind, WB));
+    std::memset(&map, 0, sizeof(map));
+    if (copy == 1) FFDAS_TRY(pair_row_map(map, gp.P, gp.npad, (int64_t)pb.B * pb.C * pb.S, kind, WB));
     staged_params sp = base_params(h, pb, gp);
+    sp.copy_async = copy == 2;
+    h.last.copy_engine = copy;
     sp.gout = gr.gout;
     sp.gout_bstride = gr.gout_bstride;
     sp.gx = gr.gx; sp.goff = gr.goff; sp.gw = gr.gw; sp.gdst = gr.gdst; sp.gsrc = gr.gsrc;

@@ -59,6 +59,7 @@ struct staged_params {
     int beta_zero;
     int *status;
     int debug_drop_stage;  // test hook: the producer never fills the first stage
+    int copy_async;        // 1: windows staged by per-lane cp.async copies instead of TMA tile loads
     // adjoint only
     const float *gout;
     int64_t gout_bstride;
@@ -89,6 +90,16 @@ __device__ __forceinline__ void tma_load_row(uint32_t dst, const CUtensorMap *ma
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
         ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar) : "memory");
 }
+// 16-byte global->shared async copy; src_bytes 0 writes 16 zero bytes.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+// The mbarrier receives one arrival when all of this thread's earlier
+// cp.async copies have landed (its expected count includes that arrival).
+__device__ __forceinline__ void cp_async_arrive(uint32_t bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 __device__ __forceinline__ void consumer_sync() {
     asm volatile("bar.sync 1, %0;" ::"r"(kStConsumers) : "memory");
 }
@@ -251,7 +262,9 @@ __device__ __forceinline__ staged_ctx staged_setup(const staged_params &p, stage
     }
     if (cx.tid == 0) {
         for (int i = 0; i < kStages; i++) {
-            mbar_init(smem_u32(&sm.full[i]), 1);
+            // TMA: one arrival (expect_tx) by producer lane 0.  cp.async: lane 0's
+            // arrival plus one completion arrival per producer lane.
+            mbar_init(smem_u32(&sm.full[i]), p.copy_async ? 33u : 1u);
             mbar_init(smem_u32(&sm.empty[i]), kStWarps);
         }
         *sm.abort_flag = 0;
@@ -362,6 +375,7 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
     const bool drop = p.debug_drop_stage && e0 == 0 && c0 == 0;
     if (drop) dead = true;
     bool issued = false, overflow = false;
+    int k0w = 0;
     if (!dead) {
         const int cl = lane / SC, j = lane % SC;
         const int c = c0 + cl;
@@ -394,8 +408,11 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
                 const int k0 = ((int)fmaxf(lo, -(float)WB)) & ~(staged_traits<K>::align_pairs - 1);
                 const int k1 = (int)fminf(hi, (float)p.npad + WB);
                 if (k1 - k0 + 1 <= WB) {
-                    const int row = (cx.b * p.C + c) * p.S + (e0 + j);
-                    tma_load_row(smem_u32(stage_base + lane * SG::bytes), tmap, k0, row, full_bar);
+                    if (!p.copy_async) {
+                        const int row = (cx.b * p.C + c) * p.S + (e0 + j);
+                        tma_load_row(smem_u32(stage_base + lane * SG::bytes), tmap, k0, row, full_bar);
+                    }
+                    k0w = k0;
                     m = kFloorMagicBits + (uint32_t)k0;
                     issued = true;
                 } else {
@@ -408,11 +425,43 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
     }
     const unsigned issued_ballot = __ballot_sync(0xffffffffu, issued);
     const unsigned ovf_ballot = __ballot_sync(0xffffffffu, overflow);
+    if (p.copy_async && !drop) {
+        // The warp copies the issued windows together, 16 bytes per lane per
+        // copy: CPW lanes per window, 32 / CPW windows per round, coalesced
+        // within each window.  Chunks outside the pair row are zero-filled
+        // (the window start is 16-byte aligned and the row length a multiple
+        // of 16 bytes, so a chunk lies wholly inside or outside the row).
+        constexpr int PB = (int)sizeof(st);
+        constexpr int CPW = WB * PB / 16;          // 16-byte chunks per window
+        constexpr int WPR = 32 / CPW;              // windows per round
+        constexpr int PPC = 16 / PB;               // pairs per chunk
+        static_assert(CPW >= 1 && CPW <= 32 && 32 % CPW == 0, "window must split into lane chunks");
+        const uint32_t stage_u32 = smem_u32(stage_base);
+        const char *Pb = static_cast<const char *>(p.P);
+        const int q = lane % CPW;
+        const int64_t brow = (int64_t)(cx.b * p.C + c0) * p.S + e0;   // pair row of window 0
+#pragma unroll 1
+        for (int it = 0; it < CPW; it++) {
+            const int w = it * WPR + lane / CPW;
+            const int kw = __shfl_sync(0xffffffffu, k0w, w);
+            if ((issued_ballot >> w) & 1u) {
+                const int64_t row = brow + (int64_t)(w / SC) * p.S + (w % SC);
+                const int kp = kw + q * PPC;
+                const bool in_row = kp >= 0 && (int64_t)kp < p.npad;
+                const char *src = Pb + (row * p.npad + (in_row ? kp : 0)) * PB;
+                cp_async16(stage_u32 + w * SG::bytes + q * 16, src, in_row ? 16u : 0u);
+            }
+        }
+        cp_async_arrive(full_bar);
+    }
     __syncwarp();
     if (lane == 0 && !drop) {
         sm.ovf[stage] = ovf_ballot != 0u;
         // the producer's arrival also publishes meta / ovf / channel table (release)
-        mbar_arrive_expect_tx(full_bar, (uint32_t)__popc(issued_ballot) * (uint32_t)(WB * sizeof(st)));
+        if (p.copy_async)
+            mbar_arrive(full_bar);
+        else
+            mbar_arrive_expect_tx(full_bar, (uint32_t)__popc(issued_ballot) * (uint32_t)(WB * sizeof(st)));
     }
     if (!dead) issued_mask |= (1u << stage);
 }
@@ -422,6 +471,7 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
 template <int K, int WB>
 __device__ __forceinline__ void staged_drain(staged_smem<K, WB> &sm, const staged_ctx &cx, int stage,
                                              uint32_t phase, uint32_t issued_mask) {
+    cp_async_wait_all();   // no cp.async of this thread outlives the CTA (none in TMA mode)
     if (*sm.abort_flag && cx.lane == 0) {
         for (int i = 0; i < kStages; i++) {
             const int s = (stage + i) % kStages;

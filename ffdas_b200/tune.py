@@ -62,7 +62,8 @@ def candidates(x, dstpos, offsets, sparse_indices=None) -> list[dict]:
             chunks = sorted({min(c, max(n_ev, 1)) for c in (4, 8, 16)})
             for wb in (32, 64):
                 for ec in chunks:
-                    out.append(dict(variant=2, tile_x=t0, tile_y=t1, window=wb, event_chunk=ec))
+                    for ce in (1, 2):   # TMA tile loads / per-thread cp.async copies
+                        out.append(dict(variant=2, tile_x=t0, tile_y=t1, window=wb, event_chunk=ec, copy_engine=ce))
     return out
 
 

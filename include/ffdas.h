@@ -146,6 +146,7 @@ typedef struct {
     int32_t event_chunk;  /* events held in registers per pass (1..16) */
     int32_t min_blocks;   /* CTAs per SM hint (occupancy) */
     int32_t window;       /* TMA-staged kernel: pairs per staged window (32 or 64) */
+    int32_t copy_engine;  /* staged kernels: 0 auto, 1 TMA tile loads, 2 per-thread cp.async copies */
 } ffdas_das_config_t;
 
 /* What the last das/das_sparse/backward call on a handle launched (new). */
@@ -157,6 +158,7 @@ typedef struct {
     int32_t storage;      /* pair storage: 0 f32, 1 f16, 2 bf16, 3 f64, 4 c32, 5 c16, 6 c64 */
     int32_t kernels;      /* kernels launched by the call */
     int64_t grid;         /* CTAs of the main kernel */
+    int32_t copy_engine;  /* staged kernels: 1 TMA, 2 cp.async; 0 otherwise */
 } ffdas_kernel_info_t;
 
 #if defined(__cplusplus)

@@ -151,12 +151,13 @@ def test_staged_and_gather_adjoints_agree():
     x, src, dst, offs, w = (t.to(DEV) for t in _problem(9, B=3, nz=40, nx=36))
     h = ffdas_b200.get_library_handle(DEV)
     grads, kinds = [], []
-    for cfg in (None, dict(variant=1, batch_tile=2), dict(variant=3)):
+    for cfg in (None, dict(variant=1, batch_tile=2), dict(variant=2, copy_engine=2), dict(variant=3)):
         leaves = [t.clone().requires_grad_(True) for t in (x, src, dst, offs, w)]
         with schedule(cfg, DEV):
             das_autograd(*leaves).square().sum().backward()
             kinds.append(h.last_kernel_info()["variant"])
         grads.append([t.grad for t in leaves])
-    assert kinds == [4, 4, 3]
-    for a, b in zip(grads[0], grads[2]):
-        assert oracle.rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-5
+    assert kinds == [4, 4, 4, 3]
+    for staged in grads[:3]:
+        for a, b in zip(staged, grads[3]):
+            assert oracle.rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-5

@@ -49,14 +49,15 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("copy", [1, 2], ids=["tma", "cp_async"])
 @pytest.mark.parametrize("name,kw,cfg", CASES, ids=[f"{c[0]}-{c[2]['tile_x']}x{c[2]['tile_y']}" for c in CASES])
-def test_staged_matches_oracle(name, kw, cfg):
+def test_staged_matches_oracle(name, kw, cfg, copy):
     wl = W.CONFIGS[name](device=DEV, **kw)
     x = wl["x"].float()
-    cfg = dict(cfg)
+    cfg = dict(cfg, copy_engine=copy)
     tol = cfg.pop("tol", 2e-5)
     out, info = _run(wl, x, cfg)
-    assert info["variant"] == 2
+    assert info["variant"] == 2 and info["copy_engine"] == copy
     assert oracle.rel_l2(_np(out), _ref(wl, x)) < tol
     assert ffdas_b200.get_library_handle(DEV).device_status() == 0
 
@@ -78,6 +79,21 @@ def test_staged_agrees_with_gather():
     a, _ = _run(wl, x, dict(variant=2, tile_x=16, tile_y=16, window=32, event_chunk=16))
     b, _ = _run(wl, x, dict(variant=1, tile_x=16, tile_y=16, batch_tile=1, event_chunk=16))
     assert oracle.rel_l2(_np(a), _np(b)) < 1e-6
+
+
+def test_copy_engines_stage_identical_windows():
+    # TMA tile loads and cp.async copies fill the same slots: bitwise equal images
+    wl = W.diverging3d(device=DEV, scale=0.25)
+    x = wl["x"].float()
+    for wb in (32, 64):
+        a, _ = _run(wl, x, dict(variant=2, tile_x=32, tile_y=8, window=wb, copy_engine=1))
+        b, _ = _run(wl, x, dict(variant=2, tile_x=32, tile_y=8, window=wb, copy_engine=2))
+        assert torch.equal(a, b)
+    for dt in (torch.float16, torch.bfloat16):
+        xs = W.normalize_channels(x).to(dt)
+        a, _ = _run(wl, xs, dict(variant=2, tile_x=16, tile_y=16, window=64, copy_engine=1))
+        b, _ = _run(wl, xs, dict(variant=2, tile_x=16, tile_y=16, window=64, copy_engine=2))
+        assert torch.equal(a, b)
 
 
 def test_overflowing_windows_fall_back_and_stay_correct():
@@ -105,14 +121,15 @@ def test_directivity_and_beta_through_staged(rng):
     assert oracle.rel_l2(_np(out), ref) < 2e-5
 
 
-def test_bounded_wait_expires_into_a_status_not_a_hang():
+@pytest.mark.parametrize("copy", [1, 2], ids=["tma", "cp_async"])
+def test_bounded_wait_expires_into_a_status_not_a_hang(copy):
     wl = W.diverging3d(device=DEV, scale=0.125)
     x = wl["x"].float()
     h = ffdas_b200.get_library_handle(DEV)
     assert h.device_status() == 0
     sentinel = torch.full((1, *wl["dstpos"].shape[:-1]), 123.0, device=DEV)
     _lib.load().ffdas_debug_staged_drop_stage(1)
-    with schedule(dict(variant=2, tile_x=16, tile_y=16, window=32), DEV):
+    with schedule(dict(variant=2, tile_x=16, tile_y=16, window=32, copy_engine=copy), DEV):
         ffdas_b200.das(x, wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"], out=sentinel)
     torch.cuda.synchronize()
     assert h.device_status() == 1              # the kernel gave up and said so
