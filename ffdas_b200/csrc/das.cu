@@ -201,7 +201,9 @@ static int floor_pow2(int v) {
     return p;
 }
 
-static schedule plan_schedule(const ffdas_context &h, const das_problem &pb, int kind) {
+// staged_ok: the staged kernel can run this problem; without it a staged
+// request falls back to the gather kernel.
+static schedule plan_schedule(const ffdas_context &h, const das_problem &pb, int kind, bool staged_ok = false) {
     schedule s;
     const bool real = (kind == ST_F32 || kind == ST_F16 || kind == ST_BF16);
     // batch tile: amortise geometry over batch items, bounded by registers
@@ -237,7 +239,10 @@ static schedule plan_schedule(const ffdas_context &h, const das_problem &pb, int
         if (h.has_config && h.config.event_chunk) s.SC = staged_event_chunk(h.config.event_chunk);
     }
     if (!real && s.BT != 1) s.BT = 4;
-    if (s.T0 * s.T1 * s.T2 != 256) {  // the gather kernel runs 256-thread CTAs
+    if (s.variant == 2 && !staged_ok) s.variant = 1;
+    const int tile_voxels = s.T0 * s.T1 * s.T2;
+    // the gather kernel runs 256-voxel tiles; the staged kernel 256 or 512
+    if (tile_voxels != 256 && !(s.variant == 2 && tile_voxels == 512)) {
         s.T0 = 16; s.T1 = 16; s.T2 = 1;
         if (pb.D1 <= 1) { s.T0 = 256; s.T1 = 1; }
     }
@@ -375,7 +380,8 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
     FFDAS_TRY(launch_ingest(h, pb, xd.dtype, kind, a.x, npad, P.get<void>()));
 
     // ---- forward kernel ----
-    const schedule s = plan_schedule(h, pb, kind);
+    const bool staged_ok = staged_supported(pb, kind) && od.dtype == FFDAS_R_32F;
+    const schedule s = plan_schedule(h, pb, kind, staged_ok);
     gather_params gp;
     std::memset(&gp, 0, sizeof(gp));
     gp.P = P.get<void>();
@@ -415,7 +421,7 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
     h.last.kernels = 2;
     h.last.grid = tiles * bchunks;
 
-    const bool staged = s.variant == 2 && staged_supported(pb, kind) && od.dtype == FFDAS_R_32F;
+    const bool staged = s.variant == 2;
     if (staged) {
         h.last.variant = 2;
         h.last.batch_tile = 1;

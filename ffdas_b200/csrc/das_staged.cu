@@ -85,6 +85,18 @@ static ffdas_error_t launch_fwd_t(ffdas_context &h, const staged_params &sp, con
 }
 
 template <int K, int SC, int WB>
+static ffdas_error_t launch_fwd2_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
+    constexpr size_t smem = staged_smem_bytes<WB, K>();
+    static bool ready = false;
+    if (!ready) {
+        FFDAS_TRY(prepare_kernel(das_staged2_kernel<K, SC, WB>, smem));
+        ready = true;
+    }
+    das_staged2_kernel<K, SC, WB><<<grid, kStThreads, smem, h.stream>>>(sp, map);
+    return ffdas_launch_check(h.stream);
+}
+
+template <int K, int SC, int WB>
 static ffdas_error_t launch_bwd_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
     constexpr size_t smem = staged_bwd_smem_bytes<WB, K, SC>();
     static bool ready = false;
@@ -99,6 +111,10 @@ static ffdas_error_t launch_bwd_t(ffdas_context &h, const staged_params &sp, con
 template <int K, int WB>
 static ffdas_error_t launch_fwd_sc(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, int SC,
                                    dim3 grid) {
+    if (sp.T0 * sp.T1 * sp.T2 == 2 * kStConsumers) {   // 512-voxel tiles: two voxels per thread
+        // event chunks of 1 or 4 (eight events would spill at three CTAs per SM)
+        return SC == 1 ? launch_fwd2_t<K, 1, WB>(h, sp, map, grid) : launch_fwd2_t<K, 4, WB>(h, sp, map, grid);
+    }
     switch (SC) {
         case 1: return launch_fwd_t<K, 1, WB>(h, sp, map, grid);
         case 4: return launch_fwd_t<K, 4, WB>(h, sp, map, grid);

@@ -227,15 +227,21 @@ struct staged_ctx {
     bool producer, active;
     int64_t v;
     float vx, vy, vz;
+    // second voxel of the thread in 512-voxel tiles (tile index + 256)
+    bool active2;
+    int64_t v2;
+    float vx2, vy2, vz2;
 };
 
 // Voxel of the thread, barrier init, zero pairs, tile bounding box.
 // With spread, lane l of warp w takes the tile's voxel l * 8 + w, so a warp's
 // voxels sit across the whole tile and rarely hit the same sample of a window
 // (the adjoint's scatter then meets few same-address atomics).
+// With vt == 2 the tile holds 512 voxels and each consumer thread also owns
+// the voxel 256 places further in the tile's linear order.
 template <int K, int WB>
 __device__ __forceinline__ staged_ctx staged_setup(const staged_params &p, staged_smem<K, WB> &sm,
-                                                   bool spread = false) {
+                                                   bool spread = false, int vt = 1) {
     using SG = slot_geom<WB, K>;
     staged_ctx cx;
     cx.tid = threadIdx.x;
@@ -246,6 +252,9 @@ __device__ __forceinline__ staged_ctx staged_setup(const staged_params &p, stage
     cx.active = false;
     cx.v = 0;
     cx.vx = cx.vy = cx.vz = 0.f;
+    cx.active2 = false;
+    cx.v2 = 0;
+    cx.vx2 = cx.vy2 = cx.vz2 = 0.f;
     const int tile = blockIdx.x;
     const int t0 = tile % p.n0, t1 = (tile / p.n0) % p.n1, t2 = tile / (p.n0 * p.n1);
     if (!cx.producer) {
@@ -258,6 +267,18 @@ __device__ __forceinline__ staged_ctx staged_setup(const staged_params &p, stage
             cx.vx = __ldg(p.dstpos + 3 * cx.v);
             cx.vy = __ldg(p.dstpos + 3 * cx.v + 1);
             cx.vz = __ldg(p.dstpos + 3 * cx.v + 2);
+        }
+        if (vt == 2) {
+            const int lt2 = lt + kStConsumers;
+            const int j0 = lt2 % p.T0, j1 = (lt2 / p.T0) % p.T1, j2 = lt2 / (p.T0 * p.T1);
+            const int h0 = t0 * p.T0 + j0, h1 = t1 * p.T1 + j1, h2 = t2 * p.T2 + j2;
+            cx.active2 = (h0 < p.D0 && h1 < p.D1 && h2 < p.D2);
+            if (cx.active2) {
+                cx.v2 = ((int64_t)h2 * p.D1 + h1) * p.D0 + h0;
+                cx.vx2 = __ldg(p.dstpos + 3 * cx.v2);
+                cx.vy2 = __ldg(p.dstpos + 3 * cx.v2 + 1);
+                cx.vz2 = __ldg(p.dstpos + 3 * cx.v2 + 2);
+            }
         }
     }
     if (cx.tid == 0) {
@@ -280,6 +301,10 @@ __device__ __forceinline__ staged_ctx staged_setup(const staged_params &p, stage
     if (!cx.producer) {
         float mn[3] = {cx.active ? cx.vx : INFINITY, cx.active ? cx.vy : INFINITY, cx.active ? cx.vz : INFINITY};
         float mx[3] = {cx.active ? cx.vx : -INFINITY, cx.active ? cx.vy : -INFINITY, cx.active ? cx.vz : -INFINITY};
+        if (cx.active2) {
+            mn[0] = fminf(mn[0], cx.vx2); mn[1] = fminf(mn[1], cx.vy2); mn[2] = fminf(mn[2], cx.vz2);
+            mx[0] = fmaxf(mx[0], cx.vx2); mx[1] = fmaxf(mx[1], cx.vy2); mx[2] = fmaxf(mx[2], cx.vz2);
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
@@ -331,6 +356,59 @@ __device__ __forceinline__ void staged_pass_begin(const staged_params &p, staged
         for (int j = 0; j < SC; j++) {
             const bool ok = cx.active && j < sc && isfinite(ofs[j]);
             float lo = ok ? ofs[j] : INFINITY, hi = ok ? ofs[j] : -INFINITY;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+            }
+            if (cx.lane == 0) {
+                sm.red[(cx.warp * 16 + j) * 2] = lo;
+                sm.red[(cx.warp * 16 + j) * 2 + 1] = hi;
+            }
+        }
+        consumer_sync();
+        if (cx.tid < SC) {
+            float lo = INFINITY, hi = -INFINITY;
+            for (int ww = 0; ww < kStWarps; ww++) {
+                lo = fminf(lo, sm.red[(ww * 16 + cx.tid) * 2]);
+                hi = fmaxf(hi, sm.red[(ww * 16 + cx.tid) * 2 + 1]);
+            }
+            sm.ofs_lo[cx.tid] = lo;
+            sm.ofs_hi[cx.tid] = hi;
+        }
+    }
+    __syncthreads();
+}
+
+// staged_pass_begin for two voxels per thread: delays and weights as
+// (voxel 1, voxel 2) pairs; the per-event delay range covers both.
+template <int K, int WB, int SC>
+__device__ __forceinline__ void staged_pass_begin2(const staged_params &p, staged_smem<K, WB> &sm,
+                                                   const staged_ctx &cx, int e0, int sc, float2 (&ofs2)[SC],
+                                                   float2 (&w2)[SC]) {
+    if (!cx.producer) {
+#pragma unroll
+        for (int j = 0; j < SC; j++) {
+            ofs2[j] = make_float2(1e30f, 1e30f);
+            w2[j] = make_float2(0.f, 0.f);
+            if (j < sc) {
+                const int64_t base = (int64_t)(e0 + j) * p.V;
+                if (cx.active) {
+                    ofs2[j].x = __ldg(p.offsets + base + cx.v);
+                    w2[j].x = __ldg(p.weights + base + cx.v);
+                }
+                if (cx.active2) {
+                    ofs2[j].y = __ldg(p.offsets + base + cx.v2);
+                    w2[j].y = __ldg(p.weights + base + cx.v2);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < SC; j++) {
+            const bool oka = cx.active && j < sc && isfinite(ofs2[j].x);
+            const bool okb = cx.active2 && j < sc && isfinite(ofs2[j].y);
+            float lo = fminf(oka ? ofs2[j].x : INFINITY, okb ? ofs2[j].y : INFINITY);
+            float hi = fmaxf(oka ? ofs2[j].x : -INFINITY, okb ? ofs2[j].y : -INFINITY);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
@@ -675,6 +753,142 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
         float *o = static_cast<float *>(p.out) + (int64_t)cx.b * p.out_bstride + cx.v;
         *o = p.beta_zero ? acc : __fmaf_rn((float)p.beta_re, *o, acc);
     }
+}
+
+// ------------------------------------------------- forward, 512-voxel tiles ---
+// Same producer, ring and windows as das_staged_kernel, but each consumer
+// thread owns two voxels of a 512-voxel tile (tile positions t and t + 256).
+// A staged window then serves twice the units, which halves the producer's
+// work, the channel-table and window-metadata loads and the barrier waits per
+// unit.  The packed FP32 lanes carry the two voxels (not two events): the
+// delay, floor split and fraction of one event for both voxels are one
+// instruction each, and both taps read the same window.
+template <int K, int SC, int WB>
+__global__ void __launch_bounds__(kStThreads, 3) das_staged2_kernel(const staged_params p,
+                                                                  const __grid_constant__ CUtensorMap tmap) {
+    using st = typename pair_traits<K>::storage;
+    using SG = slot_geom<WB, K>;
+    constexpr int CC = kStWin / SC;  // channels per stage
+    static_assert(kStWin % SC == 0, "SC must divide the stage");
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    staged_smem<K, WB> sm(smem_raw);
+    const staged_ctx cx = staged_setup<K, WB>(p, sm, false, 2);
+
+    const st *__restrict__ Pg = static_cast<const st *>(p.P);
+    const uint32_t kmax_pair = (uint32_t)(p.npad - 1);
+    float2 acc2 = make_float2(0.f, 0.f);  // (voxel 1, voxel 2)
+    int stage = 0;
+    uint32_t phase = 0;
+    bool dead = false;
+    uint32_t issued_mask = 0;
+
+    const uint32_t ring_u32 = smem_u32(sm.ring);
+    const uint32_t chan_u32 = smem_u32(sm.chan_pos);
+    const float2 vx2 = make_float2(cx.vx, cx.vx2), vy2 = make_float2(cx.vy, cx.vy2), vz2 = make_float2(cx.vz, cx.vz2);
+    const float2 magic2 = make_float2(kFloorMagic, kFloorMagic);
+    const float2 neg1 = make_float2(-1.f, -1.f);
+
+    for (int e0 = 0; e0 < p.n_events; e0 += SC) {
+        const int sc = min(SC, p.n_events - e0);
+        float2 ofs2[SC], w2[SC];
+        staged_pass_begin2<K, WB, SC>(p, sm, cx, e0, sc, ofs2, w2);
+
+        for (int c0 = 0; c0 < p.C; c0 += CC) {
+            if (cx.producer) {
+                staged_produce<K, WB, SC>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
+            } else {
+                const uint32_t full_bar = smem_u32(&sm.full[stage]);
+                if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
+                if (!dead) {
+                    const bool any_ovf = sm.ovf[stage] != 0;
+                    const uint32_t stage_u32 = ring_u32 + stage * SG::stage_bytes;
+                    // channels past C carry a zero window and a zero position: their
+                    // taps read the zero pair, so the loop needs no bound check
+#pragma unroll
+                    for (int cl = 0; cl < CC; cl++) {
+                        const int c = c0 + cl;
+                        const float4 cp = lds_f4(chan_u32 + (stage * kStWin + cl) * 16);
+                        // receive geometry of both voxels, packed; the same operation
+                        // sequence per lane as receive_geometry
+                        const float2 cx2 = make_float2(-cp.x, -cp.x), cy2 = make_float2(-cp.y, -cp.y),
+                                     cz2 = make_float2(-cp.z, -cp.z);
+                        const float2 dx = __fadd2_rn(vx2, cx2), dy = __fadd2_rn(vy2, cy2), dz = __fadd2_rn(vz2, cz2);
+                        float2 r2 = __fmul2_rn(dx, dx);
+                        r2 = __ffma2_rn(dy, dy, r2);
+                        r2 = __ffma2_rn(dz, dz, r2);
+                        recv_geom ga, gb;
+                        ga.rsq = fmaxf(r2.x, 1e-7f);
+                        gb.rsq = fmaxf(r2.y, 1e-7f);
+                        ga.rinv = rsqrtf(ga.rsq);
+                        gb.rinv = rsqrtf(gb.rsq);
+                        if (p.srcdir) {
+                            const float4 dir = sm.chan_dir[stage * kStWin + cl];
+                            apply_directivity(ga, cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z, dir);
+                            apply_directivity(gb, cx.vx2, cx.vy2, cx.vz2, cp.x, cp.y, cp.z, dir);
+                        }
+                        const float2 rsq2 = make_float2(ga.rsq, gb.rsq), rinv2 = make_float2(ga.rinv, gb.rinv);
+                        uint32_t k0p[SC];
+                        load_meta<SC>(sm.meta, stage, cl, k0p);
+                        const uint32_t slots_u32 = stage_u32 + (cl * SC) * SG::bytes;
+                        if (!any_ovf) {
+#pragma unroll
+                            for (int j = 0; j < SC; j++) {
+                                const float2 tau2 = __ffma2_rn(rsq2, rinv2, ofs2[j]);
+                                const float2 mm2 = __fadd2_rd(tau2, magic2);
+                                const float2 nfl2 = __ffma2_rn(mm2, neg1, magic2);   // -(floor), exact
+                                const float2 t2 = __fadd2_rn(tau2, nfl2);
+                                const uint32_t ra = min(__float_as_uint(mm2.x) - k0p[j], (uint32_t)WB);
+                                const uint32_t rb = min(__float_as_uint(mm2.y) - k0p[j], (uint32_t)WB);
+                                const uint32_t slot = slots_u32 + j * SG::bytes;
+                                const float ta = tap_at<K>(slot + ra * sizeof(st), t2.x);
+                                const float tb = tap_at<K>(slot + rb * sizeof(st), t2.y);
+                                acc2 = __ffma2_rn(w2[j], make_float2(ta, tb), acc2);
+                            }
+                        } else {
+                            const unsigned char *slots = sm.ring + stage * SG::stage_bytes + (cl * SC) * SG::bytes;
+#pragma unroll
+                            for (int j = 0; j < SC; j++) {
+                                float tv[2];
+#pragma unroll
+                                for (int h = 0; h < 2; h++) {
+                                    const recv_geom &g = h ? gb : ga;
+                                    const float tau = __fmaf_rn(g.rsq, g.rinv, h ? ofs2[j].y : ofs2[j].x);
+                                    const tau_split ts = split_tau(tau);
+                                    st pr;
+                                    if (k0p[j] == kOvf) {
+                                        const int64_t row = ((int64_t)cx.b * p.C + c) * p.S + (e0 + min(j, sc - 1));
+                                        pr = Pg[row * p.npad + min(ts.k, kmax_pair)];
+                                    } else {
+                                        const uint32_t rel = min(ts.k + kFloorMagicBits - k0p[j], (uint32_t)WB);
+                                        pr = *reinterpret_cast<const st *>(slots + j * SG::bytes + rel * sizeof(st));
+                                    }
+                                    tv[h] = pair_traits<K>::tap(pr, ts.t);
+                                }
+                                acc2 = __ffma2_rn(w2[j], make_float2(tv[0], tv[1]), acc2);
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+                if (cx.lane == 0) mbar_arrive(smem_u32(&sm.empty[stage]));
+            }
+            if (++stage == kStages) {
+                stage = 0;
+                phase ^= 1u;
+            }
+        }
+        __syncthreads();
+    }
+
+    if (cx.producer) {
+        staged_drain<K, WB>(sm, cx, stage, phase, issued_mask);
+        return;
+    }
+    if (dead) return;
+    float *o = static_cast<float *>(p.out) + (int64_t)cx.b * p.out_bstride;
+    if (cx.active) o[cx.v] = p.beta_zero ? acc2.x : __fmaf_rn((float)p.beta_re, o[cx.v], acc2.x);
+    if (cx.active2) o[cx.v2] = p.beta_zero ? acc2.y : __fmaf_rn((float)p.beta_re, o[cx.v2], acc2.y);
 }
 
 // ------------------------------------------------------------------ adjoint ---

@@ -64,6 +64,16 @@ def candidates(x, dstpos, offsets, sparse_indices=None) -> list[dict]:
                 for ec in chunks:
                     for ce in (1, 2):   # TMA tile loads / per-thread cp.async copies
                         out.append(dict(variant=2, tile_x=t0, tile_y=t1, window=wb, event_chunk=ec, copy_engine=ce))
+    if real and sparse_indices is None:
+        # staged kernel with 512-voxel tiles (two voxels per thread)
+        n_ev = offsets.shape[0]
+        chunks = sorted({min(4, max(n_ev, 1))})
+        for t0 in (128, 64, 32, 16, 8):
+            t1 = 512 // t0
+            if t0 <= max(d0, 8) * 2 and t1 <= max(d1, 1) * 2:
+                for wb in (32, 64):
+                    for ec in chunks:
+                        out.append(dict(variant=2, tile_x=t0, tile_y=t1, window=wb, event_chunk=ec, copy_engine=1))
     return out
 
 

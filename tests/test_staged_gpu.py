@@ -46,11 +46,18 @@ CASES = [
     ("plane2d", dict(scale=1.0), dict(variant=2, tile_x=128, tile_y=2, window=64, tol=5e-5)),
     ("ensemble", dict(scale=0.1, dtype=torch.float32), dict(variant=2, tile_x=64, tile_y=4, window=64)),
     ("autofocus", dict(scale=0.25), dict(variant=2, tile_x=32, tile_y=8, window=32)),
+    # 512-voxel tiles: two voxels per consumer thread
+    ("diverging3d", dict(scale=0.25), dict(variant=2, tile_x=32, tile_y=16, window=32)),
+    ("diverging3d", dict(scale=0.25), dict(variant=2, tile_x=16, tile_y=32, window=64, event_chunk=1)),
+    ("plane2d", dict(scale=1.0), dict(variant=2, tile_x=128, tile_y=4, window=64, tol=5e-5)),
+    ("ensemble", dict(scale=0.1, dtype=torch.float32), dict(variant=2, tile_x=64, tile_y=8, window=64)),
+    ("autofocus", dict(scale=0.25), dict(variant=2, tile_x=32, tile_y=16, window=32)),
 ]
 
 
 @pytest.mark.parametrize("copy", [1, 2], ids=["tma", "cp_async"])
-@pytest.mark.parametrize("name,kw,cfg", CASES, ids=[f"{c[0]}-{c[2]['tile_x']}x{c[2]['tile_y']}" for c in CASES])
+@pytest.mark.parametrize("name,kw,cfg", CASES,
+                         ids=[f"{c[0]}-{c[2]['tile_x']}x{c[2]['tile_y']}-w{c[2]['window']}" for c in CASES])
 def test_staged_matches_oracle(name, kw, cfg, copy):
     wl = W.CONFIGS[name](device=DEV, **kw)
     x = wl["x"].float()
@@ -58,15 +65,17 @@ def test_staged_matches_oracle(name, kw, cfg, copy):
     tol = cfg.pop("tol", 2e-5)
     out, info = _run(wl, x, cfg)
     assert info["variant"] == 2 and info["copy_engine"] == copy
+    assert info["tile_x"] * info["tile_y"] == cfg["tile_x"] * cfg["tile_y"]
     assert oracle.rel_l2(_np(out), _ref(wl, x)) < tol
     assert ffdas_b200.get_library_handle(DEV).device_status() == 0
 
 
+@pytest.mark.parametrize("tile", [(16, 16), (32, 16)], ids=["256", "512"])
 @pytest.mark.parametrize("dtype,tol", [(torch.float16, 1e-3), (torch.bfloat16, 1e-3)])
-def test_staged_16bit_pairs(dtype, tol):
+def test_staged_16bit_pairs(dtype, tol, tile):
     wl = W.diverging3d(device=DEV, scale=0.25)
     x = W.normalize_channels(wl["x"]).to(dtype)
-    out, info = _run(wl, x, dict(variant=2, tile_x=16, tile_y=16, window=32))
+    out, info = _run(wl, x, dict(variant=2, tile_x=tile[0], tile_y=tile[1], window=32))
     assert info["variant"] == 2 and info["storage"] in (1, 2)
     assert oracle.rel_l2(_np(out), _ref(wl, x)) < tol
 
@@ -78,7 +87,9 @@ def test_staged_agrees_with_gather():
     x = wl["x"].float()
     a, _ = _run(wl, x, dict(variant=2, tile_x=16, tile_y=16, window=32, event_chunk=16))
     b, _ = _run(wl, x, dict(variant=1, tile_x=16, tile_y=16, batch_tile=1, event_chunk=16))
+    c, _ = _run(wl, x, dict(variant=2, tile_x=32, tile_y=16, window=32, event_chunk=4))
     assert oracle.rel_l2(_np(a), _np(b)) < 1e-6
+    assert oracle.rel_l2(_np(c), _np(b)) < 1e-6
 
 
 def test_copy_engines_stage_identical_windows():
@@ -103,9 +114,12 @@ def test_overflowing_windows_fall_back_and_stay_correct():
     out, info = _run(wl, x, dict(variant=2, tile_x=16, tile_y=16, window=32))
     assert info["variant"] == 2
     assert oracle.rel_l2(_np(out), _ref(wl, x)) < 2e-5
+    out, info = _run(wl, x, dict(variant=2, tile_x=32, tile_y=16, window=32))
+    assert oracle.rel_l2(_np(out), _ref(wl, x)) < 2e-5
 
 
-def test_directivity_and_beta_through_staged(rng):
+@pytest.mark.parametrize("tile", [(32, 8), (32, 16)], ids=["256", "512"])
+def test_directivity_through_staged(rng, tile):
     wl = W.autofocus(device=DEV, scale=0.25)
     x = wl["x"].float()
     srcdir = torch.zeros((x.shape[-3], 4), device=DEV)
@@ -114,7 +128,7 @@ def test_directivity_and_beta_through_staged(rng):
     # on: at exactly 0.8 the 3-4-5 triangles of the grid make FP32 and FP64
     # disagree about which channels are inside
     srcdir[:, 3] = 0.8137
-    out, info = _run(wl, x, dict(variant=2, tile_x=32, tile_y=8, window=32), srcdir=srcdir)
+    out, info = _run(wl, x, dict(variant=2, tile_x=tile[0], tile_y=tile[1], window=32), srcdir=srcdir)
     ref = oracle.das_f64(_np(x), _np(wl["srcpos"]), _np(wl["dstpos"]), _np(wl["offsets"]), _np(wl["weights"]),
                          srcdir=_np(srcdir))
     assert info["variant"] == 2
@@ -149,3 +163,29 @@ def test_autotune_picks_a_correct_schedule(tmp_path, monkeypatch):
     assert oracle.rel_l2(_np(out), _ref(wl, x)) < 2e-5
     again = autotune(x, wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"], reps=1)
     assert again["config"] == best["config"]
+
+
+@pytest.mark.parametrize("cfg", [dict(variant=1, tile_x=32, tile_y=8), dict(variant=2, tile_x=32, tile_y=8, window=32),
+                                 dict(variant=2, tile_x=32, tile_y=16, window=32)], ids=["gather", "staged256", "staged512"])
+def test_beta_accumulates_into_out(cfg):
+    # out = beta * out + das(...), through the C-ABI (the Python API has no beta)
+    import ctypes
+    from ffdas_b200._lib import DataType
+    wl = W.autofocus(device=DEV, scale=0.25)
+    x = wl["x"].float().contiguous()
+    h = ffdas_b200.get_library_handle(DEV)
+    L = _lib.load()
+    prev = torch.randn((x.shape[0], *wl["dstpos"].shape[:-1]), device=DEV)
+    out = prev.clone()
+    xd = _lib.TensorDesc(list(x.shape), None, DataType.R_32F)
+    od = _lib.TensorDesc(list(out.shape), None, DataType.R_32F)
+    beta = (ctypes.c_float * 2)(0.75, 0.0)
+    with schedule(cfg, DEV):
+        h.set_stream(torch.cuda.current_stream().cuda_stream)
+        _lib.check(L.ffdas_das(h.h, wl["srcpos"].data_ptr(), None, 0.0, xd.desc, x.data_ptr(),
+                               wl["dstpos"].data_ptr(), wl["offsets"].data_ptr(), wl["weights"].data_ptr(),
+                               ctypes.cast(beta, ctypes.c_void_p), od.desc, out.data_ptr(), 0, 0))
+        assert h.last_kernel_info()["variant"] == cfg["variant"]
+    torch.cuda.synchronize()
+    ref = 0.75 * _np(prev) + _ref(wl, x)
+    assert oracle.rel_l2(_np(out), ref) < 2e-5
