@@ -100,6 +100,54 @@ template <> __device__ __forceinline__ void store_out<double2>(double2 *o, doubl
     *o = p.beta_zero ? acc : cfma(make_double2(p.beta_re, p.beta_im), *o, acc);
 }
 
+// Sparse load balance.  A voxel's event list may end in padding (entries
+// with zero weight or an out-of-range index, as the reference's callers pad
+// uneven lists to sparse_count).  Each thread of a sparse CTA measures, for
+// its tile position, L = 1 + the last real entry; the CTA then orders its
+// voxels by L (a 64-bucket counting sort in shared memory) so that each warp
+// holds voxels of similar L, and each warp runs the event loop only up to the
+// largest L among its lanes.  Work then follows the real event count instead
+// of sparse_count.  Returns the tile position this thread takes; L_out is the
+// L of the thread's original position (the caller exchanges them through
+// shared memory).
+__device__ __forceinline__ int sparse_balance(const gather_params &p, int tid, int t0, int t1, int t2,
+                                              int &L_out) {
+    __shared__ int hist[64], base[64];
+    __shared__ short order[256];
+    const int i0 = tid % p.T0, i1 = (tid / p.T0) % p.T1, i2 = tid / (p.T0 * p.T1);
+    const int g0 = t0 * p.T0 + i0, g1 = t1 * p.T1 + i1, g2 = t2 * p.T2 + i2;
+    int L = 0;
+    if (g0 < p.D0 && g1 < p.D1 && g2 < p.D2) {
+        const int64_t v = ((int64_t)g2 * p.D1 + g1) * p.D0 + g0;
+        for (int e = 0; e < p.n_events; e++) {
+            const int64_t idx = (int64_t)e * p.V + v;
+            const int s = __ldg(p.sparse_idx + idx);
+            if ((unsigned)s < (unsigned)p.S && __ldg(p.weights + idx) != 0.f) L = e + 1;
+        }
+    }
+    if (tid < 64) hist[tid] = 0;
+    __syncthreads();
+    const int bucket = (int)(((int64_t)L * 63) / max(p.n_events, 1));   // 0..63, monotone in L
+    const int pos = atomicAdd(&hist[bucket], 1);
+    __syncthreads();
+    if (tid < 32) {   // exclusive prefix over the 64 buckets, two per lane
+        const int a = hist[2 * tid], b = hist[2 * tid + 1];
+        int incl = a + b;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (tid >= o) incl += y;
+        }
+        base[2 * tid] = incl - a - b;
+        base[2 * tid + 1] = incl - b;
+    }
+    __syncthreads();
+    order[base[bucket] + pos] = (short)tid;
+    __syncthreads();
+    L_out = L;          // L of this thread's own tile position
+    return order[tid];  // the tile position this thread takes over
+}
+
 // Output element type for a storage kind and output dtype: the kernel
 // accumulates in pair_traits<K>::acc and converts on store.
 template <int K, typename OutT, int BT, int SC, bool SPARSE>
@@ -108,11 +156,22 @@ __global__ void __launch_bounds__(256) das_gather_kernel(const gather_params p) 
     using st = typename tr::storage;
     using acc_t = typename tr::acc;
 
-    const int tid = threadIdx.x;
+    int tid = threadIdx.x;
     const int tile = blockIdx.x;
     const int t0 = tile % p.n0;
     const int t1 = (tile / p.n0) % p.n1;
     const int t2 = tile / (p.n0 * p.n1);
+    int n_ev = p.n_events;
+    if constexpr (SPARSE) {
+        __shared__ int Ls[256];
+        int L;
+        const int me = sparse_balance(p, tid, t0, t1, t2, L);
+        Ls[tid] = L;
+        __syncthreads();
+        tid = me;                      // the tile position this thread now owns
+        L = Ls[me];
+        n_ev = __reduce_max_sync(0xffffffffu, (unsigned)L);   // the warp's longest list
+    }
     const int i0 = tid % p.T0;
     const int i1 = (tid / p.T0) % p.T1;
     const int i2 = tid / (p.T0 * p.T1);
@@ -139,8 +198,8 @@ __global__ void __launch_bounds__(256) das_gather_kernel(const gather_params p) 
 #pragma unroll
     for (int b = 0; b < BT; b++) boff[b] = (b0 + b < p.B) ? (int64_t)(b0 + b) * row_stride_b : 0;
 
-    for (int e0 = 0; e0 < p.n_events; e0 += SC) {
-        const int sc = min(SC, p.n_events - e0);
+    for (int e0 = 0; e0 < n_ev; e0 += SC) {
+        const int sc = min(SC, n_ev - e0);
         // Event slots past the end, zero-weight (padding) entries and
         // out-of-range event indices get a huge delay: their tap lands on the
         // zero pair and their weight is 0, so every slot runs the same

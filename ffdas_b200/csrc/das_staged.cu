@@ -112,8 +112,12 @@ template <int K, int WB>
 static ffdas_error_t launch_fwd_sc(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, int SC,
                                    dim3 grid) {
     if (sp.T0 * sp.T1 * sp.T2 == 2 * kStConsumers) {   // 512-voxel tiles: two voxels per thread
-        // event chunks of 1 or 4 (eight events would spill at three CTAs per SM)
-        return SC == 1 ? launch_fwd2_t<K, 1, WB>(h, sp, map, grid) : launch_fwd2_t<K, 4, WB>(h, sp, map, grid);
+        // event chunks of 1, 4 (three CTAs per SM) or 8 (two CTAs per SM)
+        switch (SC) {
+            case 1: return launch_fwd2_t<K, 1, WB>(h, sp, map, grid);
+            case 4: return launch_fwd2_t<K, 4, WB>(h, sp, map, grid);
+            default: return launch_fwd2_t<K, 8, WB>(h, sp, map, grid);
+        }
     }
     switch (SC) {
         case 1: return launch_fwd_t<K, 1, WB>(h, sp, map, grid);

@@ -159,7 +159,8 @@ constexpr size_t kStMiscBytes = kStages * kStWin * 4      // meta
                                 + 40 * 4                   // bounding box, per-event delay range
                                 + 32 * 4                   // abort flag (+pad)
                                 + kStWarps * 16 * 2 * 4    // reduction scratch
-                                + kStages * kStWin * 2 * 16;  // channel table (position, normal)
+                                + kStages * kStWin * 2 * 16   // channel table (position, normal)
+                                + kStages * kStWin * 2 * 16;  // channel positions as pairs (x,x,y,y), (z,z,0,0)
 
 template <int WB, int K>
 constexpr size_t staged_smem_bytes() {
@@ -202,6 +203,7 @@ struct staged_smem {
     volatile int *abort_flag;
     float *red;            // [warps][16][2]
     float4 *chan_pos, *chan_dir;  // [kStages][kStWin]
+    float4 *chan_pair;            // [kStages][kStWin][2]: (x, x, y, y), (z, z, 0, 0)
     unsigned char *extra;  // adjoint scratch
 
     __device__ explicit staged_smem(unsigned char *raw) {
@@ -217,7 +219,8 @@ struct staged_smem {
         red = const_cast<float *>(reinterpret_cast<volatile float *>(abort_flag + 32));
         chan_pos = reinterpret_cast<float4 *>(red + kStWarps * 32);
         chan_dir = chan_pos + kStages * kStWin;
-        extra = reinterpret_cast<unsigned char *>(chan_dir + kStages * kStWin);
+        chan_pair = chan_dir + kStages * kStWin;
+        extra = reinterpret_cast<unsigned char *>(chan_pair + kStages * kStWin * 2);
     }
 };
 
@@ -466,6 +469,8 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
         }
         if (j == 0) {
             sm.chan_pos[stage * kStWin + cl] = make_float4(px, py, pz, 0.f);
+            sm.chan_pair[(stage * kStWin + cl) * 2] = make_float4(px, px, py, py);
+            sm.chan_pair[(stage * kStWin + cl) * 2 + 1] = make_float4(pz, pz, 0.f, 0.f);
             if (p.srcdir)
                 sm.chan_dir[stage * kStWin + cl] = (c < p.C) ? __ldg(p.srcdir + c) : make_float4(0, 0, 0, 2.f);
         }
@@ -764,7 +769,7 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
 // delay, floor split and fraction of one event for both voxels are one
 // instruction each, and both taps read the same window.
 template <int K, int SC, int WB>
-__global__ void __launch_bounds__(kStThreads, 3) das_staged2_kernel(const staged_params p,
+__global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kernel(const staged_params p,
                                                                   const __grid_constant__ CUtensorMap tmap) {
     using st = typename pair_traits<K>::storage;
     using SG = slot_geom<WB, K>;
@@ -786,6 +791,9 @@ __global__ void __launch_bounds__(kStThreads, 3) das_staged2_kernel(const staged
     const uint32_t ring_u32 = smem_u32(sm.ring);
     const uint32_t chan_u32 = smem_u32(sm.chan_pos);
     const float2 vx2 = make_float2(cx.vx, cx.vx2), vy2 = make_float2(cx.vy, cx.vy2), vz2 = make_float2(cx.vz, cx.vz2);
+    const float2 nvx2 = make_float2(-cx.vx, -cx.vx2), nvy2 = make_float2(-cx.vy, -cx.vy2),
+                 nvz2 = make_float2(-cx.vz, -cx.vz2);
+    const uint32_t pair_u32 = smem_u32(sm.chan_pair);
     const float2 magic2 = make_float2(kFloorMagic, kFloorMagic);
     const float2 neg1 = make_float2(-1.f, -1.f);
 
@@ -803,9 +811,43 @@ __global__ void __launch_bounds__(kStThreads, 3) das_staged2_kernel(const staged
                 if (!dead) {
                     const bool any_ovf = sm.ovf[stage] != 0;
                     const uint32_t stage_u32 = ring_u32 + stage * SG::stage_bytes;
-                    // channels past C carry a zero window and a zero position: their
-                    // taps read the zero pair, so the loop needs no bound check
+                    if (!any_ovf && !p.srcdir) {
+                        // Common case, no per-channel branch.  The channel table's
+                        // (x, x, y, y), (z, z, 0, 0) rows feed the packed geometry
+                        // directly: d = c - v, the exact negative of v - c, so rsq is
+                        // the same as receive_geometry's.  Channels past C carry a
+                        // zero window: their taps read the zero pair.
 #pragma unroll
+                        for (int cl = 0; cl < CC; cl++) {
+                            const float4 qa = lds_f4(pair_u32 + (stage * kStWin + cl) * 32);
+                            const float4 qb = lds_f4(pair_u32 + (stage * kStWin + cl) * 32 + 16);
+                            const float2 dx = __fadd2_rn(make_float2(qa.x, qa.y), nvx2);
+                            const float2 dy = __fadd2_rn(make_float2(qa.z, qa.w), nvy2);
+                            const float2 dz = __fadd2_rn(make_float2(qb.x, qb.y), nvz2);
+                            float2 r2 = __fmul2_rn(dx, dx);
+                            r2 = __ffma2_rn(dy, dy, r2);
+                            r2 = __ffma2_rn(dz, dz, r2);
+                            const float2 rsq2 = make_float2(fmaxf(r2.x, 1e-7f), fmaxf(r2.y, 1e-7f));
+                            const float2 rinv2 = make_float2(rsqrtf(rsq2.x), rsqrtf(rsq2.y));
+                            uint32_t k0p[SC];
+                            load_meta<SC>(sm.meta, stage, cl, k0p);
+                            const uint32_t slots_u32 = stage_u32 + (cl * SC) * SG::bytes;
+#pragma unroll
+                            for (int j = 0; j < SC; j++) {
+                                const float2 tau2 = __ffma2_rn(rsq2, rinv2, ofs2[j]);
+                                const float2 mm2 = __fadd2_rd(tau2, magic2);
+                                const float2 nfl2 = __ffma2_rn(mm2, neg1, magic2);   // -(floor), exact
+                                const float2 t2 = __fadd2_rn(tau2, nfl2);
+                                const uint32_t ra = min(__float_as_uint(mm2.x) - k0p[j], (uint32_t)WB);
+                                const uint32_t rb = min(__float_as_uint(mm2.y) - k0p[j], (uint32_t)WB);
+                                const uint32_t slot = slots_u32 + j * SG::bytes;
+                                const float ta = tap_at<K>(slot + ra * sizeof(st), t2.x);
+                                const float tb = tap_at<K>(slot + rb * sizeof(st), t2.y);
+                                acc2 = __ffma2_rn(w2[j], make_float2(ta, tb), acc2);
+                            }
+                        }
+                    } else {
+#pragma unroll 1
                     for (int cl = 0; cl < CC; cl++) {
                         const int c = c0 + cl;
                         const float4 cp = lds_f4(chan_u32 + (stage * kStWin + cl) * 16);
@@ -868,6 +910,7 @@ __global__ void __launch_bounds__(kStThreads, 3) das_staged2_kernel(const staged
                                 acc2 = __ffma2_rn(w2[j], make_float2(tv[0], tv[1]), acc2);
                             }
                         }
+                    }
                     }
                 }
                 __syncwarp();

@@ -67,7 +67,7 @@ def candidates(x, dstpos, offsets, sparse_indices=None) -> list[dict]:
     if real and sparse_indices is None:
         # staged kernel with 512-voxel tiles (two voxels per thread)
         n_ev = offsets.shape[0]
-        chunks = sorted({min(4, max(n_ev, 1))})
+        chunks = sorted({min(c, max(n_ev, 1)) for c in (4, 8)})
         for t0 in (128, 64, 32, 16, 8):
             t1 = 512 // t0
             if t0 <= max(d0, 8) * 2 and t1 <= max(d1, 1) * 2:

@@ -207,6 +207,28 @@ def test_sparse_out_of_range_index_contributes_nothing(rng):
     assert not torch.allclose(base, got)
 
 
+@pytest.mark.parametrize("B", [1, 3])
+def test_sparse_uneven_lists_with_holes(rng, B):
+    # per-voxel list lengths 0..n, trailing padding, zero-weight holes and
+    # out-of-range indices inside the lists: every kind of padding the
+    # load-balanced sparse schedule must skip or neutralise
+    x, src, dst, offs, w = _small(rng, B=B, S=7, V=(23, 19))
+    n = 20
+    V = dst.shape[:-1]
+    g = torch.Generator().manual_seed(11)
+    idx = torch.randint(0, 7, (n, *V), generator=g).int()
+    length = torch.randint(0, n + 1, V, generator=g)
+    ofs_s = (torch.rand((n, *V), generator=g) * 50 - 10).float()
+    w_s = (torch.rand((n, *V), generator=g) + 0.1).float()
+    w_s[torch.arange(n)[:, None, None] >= length[None]] = 0.0          # trailing padding
+    w_s[torch.rand((n, *V), generator=g) < 0.1] = 0.0                    # holes
+    idx[torch.rand((n, *V), generator=g) < 0.05] = 1000                  # out-of-range entries
+    idx, ofs_s, w_s = idx.to(DEV), ofs_s.to(DEV), w_s.to(DEV)
+    got = ffdas_b200.das_sparse(x, src, dst, ofs_s, w_s, idx)
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(ofs_s), _np(w_s), sparse_indices=_np(idx))
+    assert oracle.rel_l2(_np(got), ref) < 2e-5
+
+
 SCHEDULES = [
     dict(variant=1, tile_x=16, tile_y=16, batch_tile=1, event_chunk=16),
     dict(variant=1, tile_x=32, tile_y=8, batch_tile=2, event_chunk=4),
