@@ -279,8 +279,13 @@ def run_ours(args, rank, world) -> dict:
     pk = peaks()
     achieved_tf = FLOP_PER_UNIT * units / (kernel_ms * 1e-3) / 1e12
     bytes_alg = algorithmic_bytes(wl, 4)
-    kname = "das_staged_kernel<f32 pairs>" if info["variant"] == 2 else "das_gather_kernel<f32 pairs>"
-    pname = "das_staged_diverging3d" if info["variant"] == 2 else "das_gather_diverging3d"
+    tile_voxels = info["tile_x"] * info["tile_y"] * info["tile_z"]
+    if info["variant"] == 2 and tile_voxels == 512:
+        kname, pname = "das_staged2_kernel<f32 pairs>", "das_staged2_diverging3d"
+    elif info["variant"] == 2:
+        kname, pname = "das_staged_kernel<f32 pairs>", "das_staged_diverging3d"
+    else:
+        kname, pname = "das_gather_kernel<f32 pairs>", "das_gather_diverging3d"
     roofline = {"bound": "fp32", "achieved": achieved_tf, "peak": fp32_peak, "unit": "TFLOP/s",
                 "frac": achieved_tf / fp32_peak, "traffic": profile_traffic(pname),
                 "kernel": kname, "kernel_ms": kernel_ms,
