@@ -219,6 +219,18 @@ static schedule plan_schedule(const ffdas_context &h, const das_problem &pb, int
     } else {
         s.T0 = std::max(1, floor_pow2(pb.D0)); s.T1 = 256 / s.T0; s.T2 = 1;
     }
+    // Default: the staged kernel for every dense real problem of a few
+    // thousand voxels or more -- 512-voxel tiles for one batch item, batch
+    // tiles of up to 4 items otherwise; the gather kernel for the rest.
+    bool staged_default = false;
+    if (staged_ok && pb.V >= 4096) {
+        staged_default = true;
+        s.variant = 2;
+        if (pb.B == 1) {
+            if (pb.D1 <= 1) { s.T0 = 512; s.T1 = 1; s.T2 = 1; }
+            else { s.T0 = std::min(32, std::max(1, floor_pow2(pb.D0))); s.T1 = 512 / s.T0; s.T2 = 1; }
+        }
+    }
     if (h.has_config) {
         const ffdas_das_config_t &c = h.config;
         if (c.variant == 1 || c.variant == 2) s.variant = c.variant;   // 3 selects a backward kernel only
@@ -233,10 +245,21 @@ static schedule plan_schedule(const ffdas_context &h, const das_problem &pb, int
         s.copy = c.copy_engine;
     }
     if (s.variant == 2) {
-        // staged kernel: one batch item per CTA, event chunk from the count
-        s.BT = 1;
+        // staged kernel: event chunk from the count; batch tile from the
+        // config, else up to 4 items (512-voxel tiles take one item)
         s.SC = staged_event_chunk(pb.n_events);
         if (h.has_config && h.config.event_chunk) s.SC = staged_event_chunk(h.config.event_chunk);
+        int bt = (h.has_config && h.config.batch_tile) ? h.config.batch_tile
+                                                        : std::min(4, floor_pow2(std::max(1, pb.B)));
+        if (!staged_default && !(h.has_config && h.config.batch_tile)) bt = 1;
+        if (s.T0 * s.T1 * s.T2 == 512) bt = 1;
+        bt = std::min(bt, 8);
+        if (bt > 1) {
+            // batch tiles pair events: chunks of 4 or 8, at most 32 windows per stage
+            s.SC = s.SC <= 4 ? 4 : 8;
+            if (s.SC * bt > 32) s.SC = 32 / bt;
+        }
+        s.BT = bt;
     }
     if (!real && s.BT != 1) s.BT = 4;
     if (s.variant == 2 && !staged_ok) s.variant = 1;
@@ -423,14 +446,15 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
 
     const bool staged = s.variant == 2;
     if (staged) {
+        const int bchunks_st = (pb.B + s.BT - 1) / s.BT;
         h.last.variant = 2;
-        h.last.batch_tile = 1;
+        h.last.batch_tile = s.BT;
         h.last.event_chunk = s.SC;
-        h.last.grid = tiles * pb.B;
-        if (pb.B > 65535) return FFDAS_ERROR_DIMS_TOO_LARGE;
+        h.last.grid = tiles * bchunks_st;
+        if (bchunks_st > 65535) return FFDAS_ERROR_DIMS_TOO_LARGE;
         h.mark_start();
-        const ffdas_error_t err =
-            launch_staged(h, pb, kind, gp, s.SC, s.WB, s.copy, dim3((unsigned)tiles, (unsigned)pb.B));
+        const ffdas_error_t err = launch_staged(h, pb, kind, gp, s.SC, s.WB, s.BT, s.copy,
+                                                dim3((unsigned)tiles, (unsigned)bchunks_st));
         h.mark_stop();
         return err;
     }

@@ -70,8 +70,9 @@ namespace ffdas {
 bool staged_supported(const das_problem &pb, int kind);
 // copy: 0 default, 1 TMA tile loads, 2 per-thread cp.async (also used when the
 // driver's tensor-map encoder is unavailable).  Records it in h.last.
+// BT > 1: batch tiles of BT items per CTA (256-voxel tiles, SC * BT <= 32).
 ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp, int SC,
-                            int WB, int copy, dim3 grid);
+                            int WB, int BT, int copy, dim3 grid);
 
 // Gradient outputs of the staged adjoint kernel (null = not computed).
 struct staged_grads {

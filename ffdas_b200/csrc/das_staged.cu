@@ -37,7 +37,8 @@ bool staged_supported(const das_problem &pb, int kind) {
     if (pb.sparse) return false;
     if (kind != ST_F32 && kind != ST_F16 && kind != ST_BF16) return false;
     const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
-    return rows > 0 && rows < INT32_MAX && pb.B <= 65535;
+    // pair rows at least as long as the widest window (64 pairs)
+    return rows > 0 && rows < INT32_MAX && pb.B <= 65535 && pair_row_length(pb.N) >= 64;
 }
 
 // Copy engine actually used: TMA needs the driver's tensor-map encoder.
@@ -96,6 +97,26 @@ static ffdas_error_t launch_fwd2_t(ffdas_context &h, const staged_params &sp, co
     return ffdas_launch_check(h.stream);
 }
 
+template <int K, int SC, int WB, int BT>
+static ffdas_error_t launch_fwdb_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
+    constexpr size_t smem = staged_smem_bytes<WB, K>();
+    static bool ready = false;
+    if (!ready) {
+        FFDAS_TRY(prepare_kernel(das_staged_batch_kernel<K, SC, WB, BT>, smem));
+        ready = true;
+    }
+    das_staged_batch_kernel<K, SC, WB, BT><<<grid, kStThreads, smem, h.stream>>>(sp, map);
+    return ffdas_launch_check(h.stream);
+}
+
+template <int K, int WB>
+static ffdas_error_t launch_fwd_batch(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, int SC,
+                                      int BT, dim3 grid) {
+    if (BT == 2) return SC <= 4 ? launch_fwdb_t<K, 4, WB, 2>(h, sp, map, grid) : launch_fwdb_t<K, 8, WB, 2>(h, sp, map, grid);
+    if (BT == 4) return SC <= 4 ? launch_fwdb_t<K, 4, WB, 4>(h, sp, map, grid) : launch_fwdb_t<K, 8, WB, 4>(h, sp, map, grid);
+    return launch_fwdb_t<K, 4, WB, 8>(h, sp, map, grid);
+}
+
 template <int K, int SC, int WB>
 static ffdas_error_t launch_bwd_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
     constexpr size_t smem = staged_bwd_smem_bytes<WB, K, SC>();
@@ -152,7 +173,7 @@ static staged_params base_params(ffdas_context &h, const das_problem &pb, const 
 }
 
 ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp, int SC,
-                            int WB, int copy, dim3 grid) {
+                            int WB, int BT, int copy, dim3 grid) {
     copy = resolve_copy(copy);
     CUtensorMap map;
     std::memset(&map, 0, sizeof(map));
@@ -160,6 +181,19 @@ ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, c
     staged_params sp = base_params(h, pb, gp);
     sp.copy_async = copy == 2;
     h.last.copy_engine = copy;
+    if (BT > 1) {
+        switch (kind) {
+            case ST_F32:
+                return WB == 64 ? launch_fwd_batch<ST_F32, 64>(h, sp, map, SC, BT, grid)
+                                : launch_fwd_batch<ST_F32, 32>(h, sp, map, SC, BT, grid);
+            case ST_F16:
+                return WB == 64 ? launch_fwd_batch<ST_F16, 64>(h, sp, map, SC, BT, grid)
+                                : launch_fwd_batch<ST_F16, 32>(h, sp, map, SC, BT, grid);
+            default:
+                return WB == 64 ? launch_fwd_batch<ST_BF16, 64>(h, sp, map, SC, BT, grid)
+                                : launch_fwd_batch<ST_BF16, 32>(h, sp, map, SC, BT, grid);
+        }
+    }
     switch (kind) {
         case ST_F32:
             return WB == 64 ? launch_fwd_sc<ST_F32, 64>(h, sp, map, SC, grid) : launch_fwd_sc<ST_F32, 32>(h, sp, map, SC, grid);

@@ -439,7 +439,12 @@ __device__ __forceinline__ void staged_pass_begin2(const staged_params &p, stage
 // Producer warp: stage the windows of CC channels x SC events of one chunk.
 // Publishes, with the full barrier's arrival, the window metadata, the
 // overflow flag and the channel table of the stage.
-template <int K, int WB, int SC>
+//
+// With BT > 1 (batch tiles) the CTA serves batch items blockIdx.y * BT ...
+// + BT - 1: lane = (cl * SC + j) * BT + bi stages the window of batch item bi;
+// the BT windows of one (channel, event) have the same bounds, because the
+// delays do not depend on the batch item.  Items past B get zero windows.
+template <int K, int WB, int SC, int BT = 1>
 __device__ __forceinline__ void staged_produce(const staged_params &p, const CUtensorMap *tmap,
                                                staged_smem<K, WB> &sm, const staged_ctx &cx, int stage,
                                                uint32_t phase, int e0, int sc, int c0, bool &dead,
@@ -458,8 +463,9 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
     bool issued = false, overflow = false;
     int k0w = 0;
     if (!dead) {
-        const int cl = lane / SC, j = lane % SC;
+        const int cl = lane / (SC * BT), j = (lane / BT) % SC, bi = lane % BT;
         const int c = c0 + cl;
+        const int bb = cx.b * BT + bi;   // batch item of this window
         uint32_t m = kZeroWindow;  // every tap index clamps to the zero pair
         float px = 0.f, py = 0.f, pz = 0.f;
         if (c < p.C) {
@@ -467,21 +473,21 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
             py = __ldg(p.srcpos + 3 * c + 1);
             pz = __ldg(p.srcpos + 3 * c + 2);
         }
-        if (j == 0) {
+        if (j == 0 && bi == 0) {
             sm.chan_pos[stage * kStWin + cl] = make_float4(px, py, pz, 0.f);
             sm.chan_pair[(stage * kStWin + cl) * 2] = make_float4(px, px, py, py);
             sm.chan_pair[(stage * kStWin + cl) * 2 + 1] = make_float4(pz, pz, 0.f, 0.f);
             if (p.srcdir)
                 sm.chan_dir[stage * kStWin + cl] = (c < p.C) ? __ldg(p.srcdir + c) : make_float4(0, 0, 0, 2.f);
         }
-        if (c < p.C && j < sc) {
-            const float *bb = sm.aabb;
-            const float dx = fmaxf(fmaxf(bb[0] - px, px - bb[3]), 0.f);
-            const float dy = fmaxf(fmaxf(bb[1] - py, py - bb[4]), 0.f);
-            const float dz = fmaxf(fmaxf(bb[2] - pz, pz - bb[5]), 0.f);
-            const float ex = fmaxf(fabsf(px - bb[0]), fabsf(px - bb[3]));
-            const float ey = fmaxf(fabsf(py - bb[1]), fabsf(py - bb[4]));
-            const float ez = fmaxf(fabsf(pz - bb[2]), fabsf(pz - bb[5]));
+        if (c < p.C && j < sc && bb < p.B) {
+            const float *ab = sm.aabb;
+            const float dx = fmaxf(fmaxf(ab[0] - px, px - ab[3]), 0.f);
+            const float dy = fmaxf(fmaxf(ab[1] - py, py - ab[4]), 0.f);
+            const float dz = fmaxf(fmaxf(ab[2] - pz, pz - ab[5]), 0.f);
+            const float ex = fmaxf(fabsf(px - ab[0]), fabsf(px - ab[3]));
+            const float ey = fmaxf(fabsf(py - ab[1]), fabsf(py - ab[4]));
+            const float ez = fmaxf(fabsf(pz - ab[2]), fabsf(pz - ab[5]));
             const float rmin = sqrtf(dx * dx + dy * dy + dz * dz);
             const float rmax = sqrtf(ex * ex + ey * ey + ez * ez);
             const float lo = floorf(sm.ofs_lo[j] + rmin) - 2.f;
@@ -492,7 +498,7 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
                 const int k1 = (int)fminf(hi, (float)p.npad + WB);
                 if (k1 - k0 + 1 <= WB) {
                     if (!p.copy_async) {
-                        const int row = (cx.b * p.C + c) * p.S + (e0 + j);
+                        const int row = (bb * p.C + c) * p.S + (e0 + j);
                         tma_load_row(smem_u32(stage_base + lane * SG::bytes), tmap, k0, row, full_bar);
                     }
                     k0w = k0;
@@ -522,13 +528,13 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
         const uint32_t stage_u32 = smem_u32(stage_base);
         const char *Pb = static_cast<const char *>(p.P);
         const int q = lane % CPW;
-        const int64_t brow = (int64_t)(cx.b * p.C + c0) * p.S + e0;   // pair row of window 0
 #pragma unroll 1
         for (int it = 0; it < CPW; it++) {
             const int w = it * WPR + lane / CPW;
             const int kw = __shfl_sync(0xffffffffu, k0w, w);
             if ((issued_ballot >> w) & 1u) {
-                const int64_t row = brow + (int64_t)(w / SC) * p.S + (w % SC);
+                const int wc = w / (SC * BT), wj = (w / BT) % SC, wb = w % BT;
+                const int64_t row = ((int64_t)(cx.b * BT + wb) * p.C + c0 + wc) * p.S + e0 + wj;
                 const int kp = kw + q * PPC;
                 const bool in_row = kp >= 0 && (int64_t)kp < p.npad;
                 const char *src = Pb + (row * p.npad + (in_row ? kp : 0)) * PB;
@@ -932,6 +938,149 @@ __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kerne
     float *o = static_cast<float *>(p.out) + (int64_t)cx.b * p.out_bstride;
     if (cx.active) o[cx.v] = p.beta_zero ? acc2.x : __fmaf_rn((float)p.beta_re, o[cx.v], acc2.x);
     if (cx.active2) o[cx.v2] = p.beta_zero ? acc2.y : __fmaf_rn((float)p.beta_re, o[cx.v2], acc2.y);
+}
+
+// ------------------------------------------------- forward, batch tiles ---
+// One CTA = one 256-voxel tile x BT batch items (frame ensembles, batched
+// acquisitions).  The delays do not depend on the batch item, so per (voxel,
+// channel, event) the delay, floor split, fraction and window index are
+// computed once and reused for BT taps: a unit then costs one shared load,
+// one tap FFMA and half a packed accumulate, plus 4/BT for the shared
+// arithmetic.  Slot (cl * SC + j) * BT + bi of a stage holds batch item bi's
+// window of channel cl, event j; all BT slots of a window share its bounds.
+template <int K, int SC, int WB, int BT>
+__global__ void __launch_bounds__(kStThreads) das_staged_batch_kernel(const staged_params p,
+                                                                       const __grid_constant__ CUtensorMap tmap) {
+    using st = typename pair_traits<K>::storage;
+    using SG = slot_geom<WB, K>;
+    constexpr int CC = kStWin / (SC * BT);  // channels per stage
+    static_assert(SC % 2 == 0 && kStWin % (SC * BT) == 0, "SC * BT must divide the stage");
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    staged_smem<K, WB> sm(smem_raw);
+    const staged_ctx cx = staged_setup<K, WB>(p, sm);
+
+    const st *__restrict__ Pg = static_cast<const st *>(p.P);
+    const uint32_t kmax_pair = (uint32_t)(p.npad - 1);
+    float2 acc2[BT];   // per batch item: (even events, odd events)
+#pragma unroll
+    for (int bi = 0; bi < BT; bi++) acc2[bi] = make_float2(0.f, 0.f);
+    int stage = 0;
+    uint32_t phase = 0;
+    bool dead = false;
+    uint32_t issued_mask = 0;
+
+    const uint32_t ring_u32 = smem_u32(sm.ring);
+    const uint32_t chan_u32 = smem_u32(sm.chan_pos);
+    const uint32_t meta_u32 = smem_u32(sm.meta);
+    const float2 magic2 = make_float2(kFloorMagic, kFloorMagic);
+    const float2 neg1 = make_float2(-1.f, -1.f);
+
+    for (int e0 = 0; e0 < p.n_events; e0 += SC) {
+        const int sc = min(SC, p.n_events - e0);
+        float ofs[SC], w[SC];
+        staged_pass_begin<K, WB, SC>(p, sm, cx, e0, sc, ofs, w);
+        float2 ofs2[SC / 2], w2[SC / 2];
+#pragma unroll
+        for (int j = 0; j < SC; j += 2) {
+            ofs2[j / 2] = make_float2(ofs[j], ofs[j + 1]);
+            w2[j / 2] = make_float2(w[j], w[j + 1]);
+        }
+
+        for (int c0 = 0; c0 < p.C; c0 += CC) {
+            if (cx.producer) {
+                staged_produce<K, WB, SC, BT>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
+            } else {
+                const uint32_t full_bar = smem_u32(&sm.full[stage]);
+                if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
+                if (!dead) {
+                    const bool any_ovf = sm.ovf[stage] != 0;
+                    const uint32_t stage_u32 = ring_u32 + stage * SG::stage_bytes;
+#pragma unroll 1
+                    for (int cl = 0; cl < CC; cl++) {
+                        const int c = c0 + cl;
+                        const float4 cp = lds_f4(chan_u32 + (stage * kStWin + cl) * 16);
+                        recv_geom g = receive_geometry(cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z);
+                        if (p.srcdir)
+                            apply_directivity(g, cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z,
+                                              sm.chan_dir[stage * kStWin + cl]);
+                        // window start of each event: the bi = 0 slot's metadata word
+                        uint32_t k0p[SC];
+#pragma unroll
+                        for (int j = 0; j < SC; j++)
+                            k0p[j] = lds_u32(meta_u32 + (stage * kStWin + (cl * SC + j) * BT) * 4);
+                        const uint32_t slots_u32 = stage_u32 + (cl * SC * BT) * SG::bytes;
+                        if (!any_ovf) {
+                            const float2 rsq2 = make_float2(g.rsq, g.rsq);
+                            const float2 rinv2 = make_float2(g.rinv, g.rinv);
+#pragma unroll
+                            for (int j = 0; j < SC; j += 2) {
+                                const float2 tau2 = __ffma2_rn(rsq2, rinv2, ofs2[j / 2]);
+                                const float2 mm2 = __fadd2_rd(tau2, magic2);
+                                const float2 nfl2 = __ffma2_rn(mm2, neg1, magic2);   // -(floor), exact
+                                const float2 t2 = __fadd2_rn(tau2, nfl2);
+                                const uint32_t ra = min(__float_as_uint(mm2.x) - k0p[j], (uint32_t)WB);
+                                const uint32_t rb = min(__float_as_uint(mm2.y) - k0p[j + 1], (uint32_t)WB);
+                                const uint32_t aa = slots_u32 + (j * BT) * SG::bytes + ra * sizeof(st);
+                                const uint32_t ab = slots_u32 + ((j + 1) * BT) * SG::bytes + rb * sizeof(st);
+#pragma unroll
+                                for (int bi = 0; bi < BT; bi++) {
+                                    const float ta = tap_at<K>(aa + bi * SG::bytes, t2.x);
+                                    const float tb = tap_at<K>(ab + bi * SG::bytes, t2.y);
+                                    acc2[bi] = __ffma2_rn(w2[j / 2], make_float2(ta, tb), acc2[bi]);
+                                }
+                            }
+                        } else {
+                            const unsigned char *slots = sm.ring + stage * SG::stage_bytes + (cl * SC * BT) * SG::bytes;
+#pragma unroll
+                            for (int j = 0; j < SC; j++) {
+                                const float tau = __fmaf_rn(g.rsq, g.rinv, ofs[j]);
+                                const tau_split ts = split_tau(tau);
+#pragma unroll
+                                for (int bi = 0; bi < BT; bi++) {
+                                    st pr;
+                                    if (k0p[j] == kOvf) {
+                                        const int bb = min(cx.b * BT + bi, p.B - 1);
+                                        const int64_t row = ((int64_t)bb * p.C + c) * p.S + (e0 + min(j, sc - 1));
+                                        pr = Pg[row * p.npad + min(ts.k, kmax_pair)];
+                                    } else {
+                                        const uint32_t rel = min(ts.k + kFloorMagicBits - k0p[j], (uint32_t)WB);
+                                        pr = *reinterpret_cast<const st *>(slots + (j * BT + bi) * SG::bytes +
+                                                                           rel * sizeof(st));
+                                    }
+                                    const float tv = pair_traits<K>::tap(pr, ts.t);
+                                    if (j & 1) acc2[bi].y = __fmaf_rn(w[j], tv, acc2[bi].y);
+                                    else acc2[bi].x = __fmaf_rn(w[j], tv, acc2[bi].x);
+                                }
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+                if (cx.lane == 0) mbar_arrive(smem_u32(&sm.empty[stage]));
+            }
+            if (++stage == kStages) {
+                stage = 0;
+                phase ^= 1u;
+            }
+        }
+        __syncthreads();
+    }
+
+    if (cx.producer) {
+        staged_drain<K, WB>(sm, cx, stage, phase, issued_mask);
+        return;
+    }
+    if (!cx.active || dead) return;
+#pragma unroll
+    for (int bi = 0; bi < BT; bi++) {
+        const int bb = cx.b * BT + bi;
+        if (bb < p.B) {
+            float *o = static_cast<float *>(p.out) + (int64_t)bb * p.out_bstride + cx.v;
+            const float acc = acc2[bi].x + acc2[bi].y;
+            *o = p.beta_zero ? acc : __fmaf_rn((float)p.beta_re, *o, acc);
+        }
+    }
 }
 
 // ------------------------------------------------------------------ adjoint ---

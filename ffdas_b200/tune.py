@@ -63,7 +63,15 @@ def candidates(x, dstpos, offsets, sparse_indices=None) -> list[dict]:
             for wb in (32, 64):
                 for ec in chunks:
                     for ce in (1, 2):   # TMA tile loads / per-thread cp.async copies
-                        out.append(dict(variant=2, tile_x=t0, tile_y=t1, window=wb, event_chunk=ec, copy_engine=ce))
+                        out.append(dict(variant=2, tile_x=t0, tile_y=t1, window=wb, event_chunk=ec, copy_engine=ce,
+                                        batch_tile=1))
+                # batch tiles: BT items per CTA share each window's delays
+                for bt in (2, 4, 8):
+                    if bt > B:
+                        continue
+                    for ec in sorted({4, 8} if bt <= 4 else {4}):
+                        out.append(dict(variant=2, tile_x=t0, tile_y=t1, window=wb, event_chunk=ec, copy_engine=1,
+                                        batch_tile=bt))
     if real and sparse_indices is None:
         # staged kernel with 512-voxel tiles (two voxels per thread)
         n_ev = offsets.shape[0]
@@ -73,7 +81,8 @@ def candidates(x, dstpos, offsets, sparse_indices=None) -> list[dict]:
             if t0 <= max(d0, 8) * 2 and t1 <= max(d1, 1) * 2:
                 for wb in (32, 64):
                     for ec in chunks:
-                        out.append(dict(variant=2, tile_x=t0, tile_y=t1, window=wb, event_chunk=ec, copy_engine=1))
+                        out.append(dict(variant=2, tile_x=t0, tile_y=t1, window=wb, event_chunk=ec, copy_engine=1,
+                                        batch_tile=1))
     return out
 
 

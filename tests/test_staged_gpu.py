@@ -189,3 +189,39 @@ def test_beta_accumulates_into_out(cfg):
     torch.cuda.synchronize()
     ref = 0.75 * _np(prev) + _ref(wl, x)
     assert oracle.rel_l2(_np(out), ref) < 2e-5
+
+
+@pytest.mark.parametrize("B,bt,ec,wb", [(4, 2, 8, 32), (4, 4, 4, 32), (5, 4, 8, 64), (11, 8, 4, 64), (3, 2, 4, 64)],
+                         ids=lambda v: str(v))
+def test_batch_tiles_match_oracle(B, bt, ec, wb):
+    # several batch items per CTA share each window's delays; B not a multiple
+    # of the batch tile leaves items past B with zero windows
+    wl = W.ensemble(device=DEV, scale=0.1, frames=B, dtype=torch.float32)
+    x = wl["x"]
+    out, info = _run(wl, x, dict(variant=2, tile_x=32, tile_y=8, window=wb, event_chunk=ec, batch_tile=bt))
+    assert info["variant"] == 2 and info["batch_tile"] == bt
+    assert oracle.rel_l2(_np(out), _ref(wl, x)) < 2e-5
+
+
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+def test_batch_tiles_16bit(dtype):
+    wl = W.ensemble(device=DEV, scale=0.1, frames=6, dtype=dtype)
+    x = wl["x"]
+    out, info = _run(wl, x, dict(variant=2, tile_x=64, tile_y=4, window=64, batch_tile=4))
+    assert info["batch_tile"] == 4 and info["storage"] in (1, 2)
+    assert oracle.rel_l2(_np(out), _ref(wl, x)) < 2e-4
+
+
+def test_default_planner_picks_staged_for_dense_volumes():
+    h = ffdas_b200.get_library_handle(DEV)
+    h.set_config(None)
+    wl = W.diverging3d(device=DEV, scale=0.25)
+    out = ffdas_b200.das(wl["x"], wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"])
+    info = h.last_kernel_info()
+    assert info["variant"] == 2 and info["tile_x"] * info["tile_y"] * info["tile_z"] == 512
+    assert oracle.rel_l2(_np(out), _ref(wl, wl["x"])) < 2e-5
+    af = W.autofocus(device=DEV, scale=0.25)
+    out = ffdas_b200.das(af["x"], af["srcpos"], af["dstpos"], af["offsets"], af["weights"])
+    info = h.last_kernel_info()
+    assert info["variant"] == 2 and info["batch_tile"] == 4
+    assert oracle.rel_l2(_np(out), _ref(af, af["x"])) < 2e-5
