@@ -609,6 +609,25 @@ template <> __device__ __forceinline__ float tap_at<ST_BF16>(uint32_t a, float t
     return pair_traits<ST_BF16>::tap(lds_u32(a), t);
 }
 
+// Sample x0 and slope d of the pair at shared address `a` (tap = x0 + t d).
+template <int K> __device__ __forceinline__ void pair_x0_d(uint32_t a, float &x0, float &d);
+template <> __device__ __forceinline__ void pair_x0_d<ST_F32>(uint32_t a, float &x0, float &d) {
+    const float2 p = lds_f2(a);
+    x0 = p.x;
+    d = p.y;
+}
+template <> __device__ __forceinline__ void pair_x0_d<ST_F16>(uint32_t a, float &x0, float &d) {
+    const uint32_t u = lds_u32(a);
+    const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&u));
+    x0 = f.x;
+    d = f.y - f.x;
+}
+template <> __device__ __forceinline__ void pair_x0_d<ST_BF16>(uint32_t a, float &x0, float &d) {
+    const uint32_t u = lds_u32(a);
+    x0 = __uint_as_float(u << 16);
+    d = __uint_as_float(u & 0xFFFF0000u) - x0;
+}
+
 // Interpolate one tap from a staged slot (f32 result).
 template <int K>
 __device__ __forceinline__ float staged_tap(const unsigned char *slot, uint32_t rel, float t) {
@@ -1133,9 +1152,11 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
         const int sc = min(SC, p.n_events - e0);
         float ofs[SC], w[SC];
         staged_pass_begin<K, WB, SC>(p, sm, cx, e0, sc, ofs, w);
-        float gwa[SC], goa[SC];
+        // Per event: sums over channels of x0, d and t*d of the taps (L = x0 + t d),
+        // so gw = g (sx0 + std) and goff = g w sd at the end of the pass.
+        float sx0[SC], sd[SC], std_[SC];
 #pragma unroll
-        for (int j = 0; j < SC; j++) { gwa[j] = 0.f; goa[j] = 0.f; }
+        for (int j = 0; j < SC; j++) { sx0[j] = 0.f; sd[j] = 0.f; std_[j] = 0.f; }
         // fixed-point scale of this pass: amax = max |g w| over the tile
         float fscale = 0.f, finv = 0.f;
         bool fixed = false;
@@ -1168,6 +1189,14 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
             }
             consumer_sync();   // wmax is rewritten by the next pass
         }
+        float aw[SC], asw[SC];   // g w and its fixed-point scaling, per event
+#pragma unroll
+        for (int j = 0; j < SC; j++) {
+            aw[j] = g * w[j];
+            asw[j] = aw[j] * fscale;
+        }
+        const float2 magic2 = make_float2(kFloorMagic, kFloorMagic);
+        const float2 neg1 = make_float2(-1.f, -1.f);
 
         for (int c0 = 0; c0 < p.C; c0 += CC) {
             if (cx.producer) {
@@ -1179,7 +1208,65 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
                 const uint32_t gstage_u32 = gslot_u32 + stage * kStWin * GS * 4;
                 if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
                 const bool any_ovf = !dead && sm.ovf[stage] != 0;
-                if (!dead) {
+                if (!dead && !any_ovf && (fixed || !p.gx)) {
+                    // Common case, branch-free per unit: every tap lies in its window
+                    // (out-of-window taps are out of the record and read the zero
+                    // pair), and a tap outside the record scatters a zero.
+                    const uint32_t stage_u32 = smem_u32(stage_base);
+                    const uint32_t nlast = (uint32_t)(p.N - 1);
+                    for (int cl = 0; cl < CC; cl++) {
+                        const int c = c0 + cl;
+                        if (c >= p.C) break;   // a phantom channel's taps would scatter outside gx
+                        const float4 cp = sm.chan_pos[stage * kStWin + cl];
+                        const recv_geom gm = receive_geometry(cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z);
+                        uint32_t k0p[SC];
+                        load_meta<SC>(sm.meta, stage, cl, k0p);
+                        const uint32_t slots_u32 = stage_u32 + (cl * SC) * SG::bytes;
+                        const uint32_t gwin_u32 = gstage_u32 + (cl * SC) * GS * 4;
+                        const float2 rsq2 = make_float2(gm.rsq, gm.rsq), rinv2 = make_float2(gm.rinv, gm.rinv);
+                        float q = 0.f;
+#pragma unroll
+                        for (int j = 0; j < SC; j += 2) {
+                            const float o1 = (j + 1 < SC) ? ofs[j + 1] : 1e30f;
+                            const float2 tau2 = __ffma2_rn(rsq2, rinv2, make_float2(ofs[j], o1));
+                            const float2 mm2 = __fadd2_rd(tau2, magic2);
+                            const float2 nfl2 = __ffma2_rn(mm2, neg1, magic2);   // -(floor), exact
+                            const float2 t2 = __fadd2_rn(tau2, nfl2);
+#pragma unroll
+                            for (int h = 0; h < 2; h++) {
+                                const int jj = j + h;
+                                if (jj >= SC) break;
+                                const uint32_t mb = __float_as_uint(h ? mm2.y : mm2.x);
+                                const float t = h ? t2.y : t2.x;
+                                const uint32_t rel = min(mb - k0p[jj], (uint32_t)WB);
+                                float x0, d;
+                                pair_x0_d<K>(slots_u32 + jj * SG::bytes + rel * sizeof(st), x0, d);
+                                sx0[jj] += x0;
+                                sd[jj] += d;
+                                std_[jj] = __fmaf_rn(t, d, std_[jj]);
+                                q = __fmaf_rn(aw[jj], d, q);
+                                if (p.gx) {
+                                    const float as = (mb - kFloorMagicBits < nlast) ? asw[jj] : 0.f;
+                                    const int it = fix_round(as);
+                                    const int i1 = fix_round_fma(as, t);
+                                    const uint32_t ga = gwin_u32 + (jj * GS + rel) * 4;
+                                    red_shared_add(ga, it - i1);
+                                    red_shared_add(ga + 4, i1);
+                                }
+                            }
+                        }
+                        if (want_pos) {
+                            const float qr = q * gm.rinv;
+                            const float ex = (cx.vx - cp.x) * qr, ey = (cx.vy - cp.y) * qr, ez = (cx.vz - cp.z) * qr;
+                            gpx += ex; gpy += ey; gpz += ez;
+                            if (p.gsrc) {
+                                cgrad[(cl * 3 + 0) * kStConsumers + cx.tid] = -ex;
+                                cgrad[(cl * 3 + 1) * kStConsumers + cx.tid] = -ey;
+                                cgrad[(cl * 3 + 2) * kStConsumers + cx.tid] = -ez;
+                            }
+                        }
+                    }
+                } else if (!dead) {
                     for (int cl = 0; cl < CC; cl++) {
                         const int c = c0 + cl;
                         if (c >= p.C) break;   // a phantom channel's taps would scatter outside gx
@@ -1203,16 +1290,17 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
                                 rel = min(ts.k + kFloorMagicBits - k0p[j], (uint32_t)WB);
                                 pr = *reinterpret_cast<const st *>(slots + j * SG::bytes + rel * sizeof(st));
                             }
-                            const float L = pair_traits<K>::tap(pr, ts.t);
                             const float d = pair_traits<K>::slope(pr);
-                            const float a = g * w[j];
-                            gwa[j] = __fmaf_rn(g, L, gwa[j]);
-                            goa[j] = __fmaf_rn(a, d, goa[j]);
+                            const float x0 = pair_traits<K>::tap(pr, 0.f);
+                            const float a = aw[j];
+                            sx0[j] += x0;
+                            sd[j] += d;
+                            std_[j] = __fmaf_rn(ts.t, d, std_[j]);
                             q = __fmaf_rn(a, d, q);
                             // channel-data adjoint: only taps inside the record
                             if (p.gx && a != 0.f && ts.k < (uint32_t)(p.N - 1)) {
                                 if (fixed && !ovfw && rel < (uint32_t)WB) {
-                                    const float as = a * fscale;
+                                    const float as = asw[j];
                                     const int it = fix_round(as);
                                     const int i1 = fix_round_fma(as, ts.t);
                                     const uint32_t ga = gstage_u32 + ((cl * SC + j) * GS + rel) * 4;
@@ -1283,12 +1371,14 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
             for (int j = 0; j < SC; j++) {
                 if (j < sc) {
                     const int64_t idx = (int64_t)(e0 + j) * p.V + cx.v;
+                    const float gwv = g * (sx0[j] + std_[j]);   // g * sum over channels of the taps
+                    const float gov = aw[j] * sd[j];            // g w * sum of the slopes
                     if (multi_b) {
-                        if (p.gw) atomicAdd(p.gw + idx, gwa[j]);
-                        if (p.goff) atomicAdd(p.goff + idx, goa[j]);
+                        if (p.gw) atomicAdd(p.gw + idx, gwv);
+                        if (p.goff) atomicAdd(p.goff + idx, gov);
                     } else {
-                        if (p.gw) p.gw[idx] = gwa[j];
-                        if (p.goff) p.goff[idx] = goa[j];
+                        if (p.gw) p.gw[idx] = gwv;
+                        if (p.goff) p.goff[idx] = gov;
                     }
                 }
             }
