@@ -252,6 +252,7 @@ static schedule plan_schedule(const ffdas_context &h, const das_problem &pb, int
         int bt = (h.has_config && h.config.batch_tile) ? h.config.batch_tile
                                                         : std::min(4, floor_pow2(std::max(1, pb.B)));
         if (!staged_default && !(h.has_config && h.config.batch_tile)) bt = 1;
+        if (!staged_batch_supported()) bt = 1;
         if (s.T0 * s.T1 * s.T2 == 512) bt = 1;
         bt = std::min(bt, 8);
         if (bt > 1) {

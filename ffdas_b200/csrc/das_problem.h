@@ -70,6 +70,8 @@ namespace ffdas {
 bool staged_supported(const das_problem &pb, int kind);
 // copy: 0 default, 1 TMA tile loads, 2 per-thread cp.async (also used when the
 // driver's tensor-map encoder is unavailable).  Records it in h.last.
+// Batch tiles need the TMA tensor-map encoder (3-D boxes).
+bool staged_batch_supported();
 // BT > 1: batch tiles of BT items per CTA (256-voxel tiles, SC * BT <= 32).
 ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp, int SC,
                             int WB, int BT, int copy, dim3 grid);

@@ -64,6 +64,26 @@ static ffdas_error_t pair_row_map(CUtensorMap &map, const void *P, int64_t npad,
     return r == CUDA_SUCCESS ? FFDAS_SUCCESS : FFDAS_ERROR_CUDA_DRIVER;
 }
 
+// 3-D map over the same rows for batch tiles: dims {npad, C*S, B}, box
+// {WB, 1, BT}; batch items past B read as zeros.
+static ffdas_error_t pair_batch_map(CUtensorMap &map, const void *P, int64_t npad, int64_t cs, int64_t B, int kind,
+                                    int WB, int BT) {
+    auto encode = tensor_map_encoder();
+    if (!encode) return FFDAS_ERROR_CUDA_DRIVER;
+    const int pair_bytes = (kind == ST_F32) ? 8 : 4;
+    const cuuint64_t dims[3] = {(cuuint64_t)npad, (cuuint64_t)cs, (cuuint64_t)B};
+    const cuuint64_t strides[2] = {(cuuint64_t)npad * pair_bytes, (cuuint64_t)(cs * npad * pair_bytes)};
+    const cuuint32_t box[3] = {(cuuint32_t)WB, 1u, (cuuint32_t)BT};
+    const cuuint32_t estr[3] = {1u, 1u, 1u};
+    const CUresult r = encode(&map, pair_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32,
+                              3, const_cast<void *>(P), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? FFDAS_SUCCESS : FFDAS_ERROR_CUDA_DRIVER;
+}
+
+bool staged_batch_supported() { return tensor_map_encoder() != nullptr; }
+
 template <typename Kernel>
 static ffdas_error_t prepare_kernel(Kernel kernel, size_t smem) {
     FFDAS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -99,7 +119,7 @@ static ffdas_error_t launch_fwd2_t(ffdas_context &h, const staged_params &sp, co
 
 template <int K, int SC, int WB, int BT>
 static ffdas_error_t launch_fwdb_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
-    constexpr size_t smem = staged_smem_bytes<WB, K>();
+    constexpr size_t smem = staged_batch_smem_bytes<WB, K, BT>();
     static bool ready = false;
     if (!ready) {
         FFDAS_TRY(prepare_kernel(das_staged_batch_kernel<K, SC, WB, BT>, smem));
@@ -174,10 +194,15 @@ static staged_params base_params(ffdas_context &h, const das_problem &pb, const 
 
 ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp, int SC,
                             int WB, int BT, int copy, dim3 grid) {
+    if (BT > 1) copy = 1;   // batch tiles stage their windows with 3-D TMA boxes
     copy = resolve_copy(copy);
+    if (BT > 1 && copy != 1) return FFDAS_ERROR_CUDA_DRIVER;
     CUtensorMap map;
     std::memset(&map, 0, sizeof(map));
-    if (copy == 1) FFDAS_TRY(pair_row_map(map, gp.P, gp.npad, (int64_t)pb.B * pb.C * pb.S, kind, WB));
+    if (copy == 1 && BT > 1)
+        FFDAS_TRY(pair_batch_map(map, gp.P, gp.npad, (int64_t)pb.C * pb.S, pb.B, kind, WB, BT));
+    else if (copy == 1)
+        FFDAS_TRY(pair_row_map(map, gp.P, gp.npad, (int64_t)pb.B * pb.C * pb.S, kind, WB));
     staged_params sp = base_params(h, pb, gp);
     sp.copy_async = copy == 2;
     h.last.copy_engine = copy;

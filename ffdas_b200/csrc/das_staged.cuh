@@ -100,6 +100,13 @@ __device__ __forceinline__ void cp_async_arrive(uint32_t bar) {
     asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// Box {WB pairs, 1 row, BT batch items} of the 3-D pair-row map.
+__device__ __forceinline__ void tma_load_box3(uint32_t dst, const CUtensorMap *map, int x, int y, int z,
+                                              uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar) : "memory");
+}
 __device__ __forceinline__ void consumer_sync() {
     asm volatile("bar.sync 1, %0;" ::"r"(kStConsumers) : "memory");
 }
@@ -146,6 +153,19 @@ template <int WB, int K> struct slot_geom {
     static constexpr int bytes = ((data_bytes + 16 + 127) / 128) * 128;
     static constexpr int stage_bytes = bytes * kStWin;
     static constexpr int ring_bytes = stage_bytes * kStages;
+};
+
+// Batch-tile window groups: the BT windows of one (channel, event) lie back to
+// back ([BT][WB] pairs, one TMA box), groups 128-byte aligned; a stage holds
+// kStWin / BT groups, so the ring is no larger than the single-item ring.
+template <int WB, int K, int BT> struct group_geom {
+    static constexpr int pair_bytes = staged_traits<K>::bytes;
+    static constexpr int item_bytes = WB * pair_bytes;
+    static constexpr int data_bytes = BT * item_bytes;
+    static constexpr int bytes = ((data_bytes + 127) / 128) * 128;
+    static constexpr int groups = kStWin / BT;
+    static constexpr int stage_bytes = bytes * groups;
+    static_assert(stage_bytes <= slot_geom<WB, K>::stage_bytes, "batch stage must fit the ring");
 };
 
 // Meta value of a window that holds no data: with it, no tap whose delay is
@@ -439,12 +459,7 @@ __device__ __forceinline__ void staged_pass_begin2(const staged_params &p, stage
 // Producer warp: stage the windows of CC channels x SC events of one chunk.
 // Publishes, with the full barrier's arrival, the window metadata, the
 // overflow flag and the channel table of the stage.
-//
-// With BT > 1 (batch tiles) the CTA serves batch items blockIdx.y * BT ...
-// + BT - 1: lane = (cl * SC + j) * BT + bi stages the window of batch item bi;
-// the BT windows of one (channel, event) have the same bounds, because the
-// delays do not depend on the batch item.  Items past B get zero windows.
-template <int K, int WB, int SC, int BT = 1>
+template <int K, int WB, int SC>
 __device__ __forceinline__ void staged_produce(const staged_params &p, const CUtensorMap *tmap,
                                                staged_smem<K, WB> &sm, const staged_ctx &cx, int stage,
                                                uint32_t phase, int e0, int sc, int c0, bool &dead,
@@ -463,9 +478,9 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
     bool issued = false, overflow = false;
     int k0w = 0;
     if (!dead) {
-        const int cl = lane / (SC * BT), j = (lane / BT) % SC, bi = lane % BT;
+        const int cl = lane / SC, j = lane % SC;
         const int c = c0 + cl;
-        const int bb = cx.b * BT + bi;   // batch item of this window
+        const int bb = cx.b;   // batch item of the CTA
         uint32_t m = kZeroWindow;  // every tap index clamps to the zero pair
         float px = 0.f, py = 0.f, pz = 0.f;
         if (c < p.C) {
@@ -473,14 +488,14 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
             py = __ldg(p.srcpos + 3 * c + 1);
             pz = __ldg(p.srcpos + 3 * c + 2);
         }
-        if (j == 0 && bi == 0) {
+        if (j == 0) {
             sm.chan_pos[stage * kStWin + cl] = make_float4(px, py, pz, 0.f);
             sm.chan_pair[(stage * kStWin + cl) * 2] = make_float4(px, px, py, py);
             sm.chan_pair[(stage * kStWin + cl) * 2 + 1] = make_float4(pz, pz, 0.f, 0.f);
             if (p.srcdir)
                 sm.chan_dir[stage * kStWin + cl] = (c < p.C) ? __ldg(p.srcdir + c) : make_float4(0, 0, 0, 2.f);
         }
-        if (c < p.C && j < sc && bb < p.B) {
+        if (c < p.C && j < sc) {
             const float *ab = sm.aabb;
             const float dx = fmaxf(fmaxf(ab[0] - px, px - ab[3]), 0.f);
             const float dy = fmaxf(fmaxf(ab[1] - py, py - ab[4]), 0.f);
@@ -533,8 +548,7 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
             const int w = it * WPR + lane / CPW;
             const int kw = __shfl_sync(0xffffffffu, k0w, w);
             if ((issued_ballot >> w) & 1u) {
-                const int wc = w / (SC * BT), wj = (w / BT) % SC, wb = w % BT;
-                const int64_t row = ((int64_t)(cx.b * BT + wb) * p.C + c0 + wc) * p.S + e0 + wj;
+                const int64_t row = ((int64_t)cx.b * p.C + c0 + w / SC) * p.S + e0 + w % SC;
                 const int kp = kw + q * PPC;
                 const bool in_row = kp >= 0 && (int64_t)kp < p.npad;
                 const char *src = Pb + (row * p.npad + (in_row ? kp : 0)) * PB;
@@ -961,23 +975,101 @@ __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kerne
 
 // ------------------------------------------------- forward, batch tiles ---
 // One CTA = one 256-voxel tile x BT batch items (frame ensembles, batched
-// acquisitions).  The delays do not depend on the batch item, so per (voxel,
-// channel, event) the delay, floor split, fraction and window index are
-// computed once and reused for BT taps: a unit then costs one shared load,
-// one tap FFMA and half a packed accumulate, plus 4/BT for the shared
-// arithmetic.  Slot (cl * SC + j) * BT + bi of a stage holds batch item bi's
-// window of channel cl, event j; all BT slots of a window share its bounds.
+// acquisitions).  The delays do not depend on the batch item, so the BT
+// windows of one (channel, event) have the same bounds: the producer stages
+// them with ONE 3-D TMA box {WB pairs, 1 row, BT items} (a stage holds
+// kStWin / BT such groups, so copies per unit drop by BT), and per (voxel,
+// channel, event) the consumers compute the delay, floor split, fraction and
+// window index once for BT taps.  Groups are dense ([BT][WB] pairs, no zero
+// pair between items): a tap outside its window (outside the record, an
+// excluded channel, an unused slot) is redirected to a zeroed group instead.
+template <int K, int WB, int SC, int BT>
+__device__ __forceinline__ void staged_produce_batch(const staged_params &p, const CUtensorMap *tmap,
+                                                     staged_smem<K, WB> &sm, const staged_ctx &cx, int stage,
+                                                     uint32_t phase, int e0, int sc, int c0, bool &dead,
+                                                     uint32_t &issued_mask) {
+    using SG = slot_geom<WB, K>;
+    using GG = group_geom<WB, K, BT>;
+    const uint32_t full_bar = smem_u32(&sm.full[stage]);
+    const uint32_t empty_bar = smem_u32(&sm.empty[stage]);
+    const uint32_t stage_u32 = smem_u32(sm.ring + stage * SG::stage_bytes);
+    const int lane = cx.lane;
+    if (!dead && !bounded_wait(empty_bar, phase ^ 1u, sm.abort_flag, p.status)) dead = true;
+    const bool drop = p.debug_drop_stage && e0 == 0 && c0 == 0;   // test hook, as in staged_produce
+    if (drop) dead = true;
+    bool issued = false, overflow = false;
+    const bool own = lane < GG::groups;
+    if (!dead && own) {
+        const int cl = lane / SC, j = lane % SC;
+        const int c = c0 + cl;
+        uint32_t m = kZeroWindow;
+        float px = 0.f, py = 0.f, pz = 0.f;
+        if (c < p.C) {
+            px = __ldg(p.srcpos + 3 * c);
+            py = __ldg(p.srcpos + 3 * c + 1);
+            pz = __ldg(p.srcpos + 3 * c + 2);
+        }
+        if (j == 0) {
+            sm.chan_pos[stage * kStWin + cl] = make_float4(px, py, pz, 0.f);
+            if (p.srcdir)
+                sm.chan_dir[stage * kStWin + cl] = (c < p.C) ? __ldg(p.srcdir + c) : make_float4(0, 0, 0, 2.f);
+        }
+        if (c < p.C && j < sc) {
+            const float *ab = sm.aabb;
+            const float dx = fmaxf(fmaxf(ab[0] - px, px - ab[3]), 0.f);
+            const float dy = fmaxf(fmaxf(ab[1] - py, py - ab[4]), 0.f);
+            const float dz = fmaxf(fmaxf(ab[2] - pz, pz - ab[5]), 0.f);
+            const float ex = fmaxf(fabsf(px - ab[0]), fabsf(px - ab[3]));
+            const float ey = fmaxf(fabsf(py - ab[1]), fabsf(py - ab[4]));
+            const float ez = fmaxf(fabsf(pz - ab[2]), fabsf(pz - ab[5]));
+            const float rmin = sqrtf(dx * dx + dy * dy + dz * dz);
+            const float rmax = sqrtf(ex * ex + ey * ey + ez * ez);
+            const float lo = floorf(sm.ofs_lo[j] + rmin) - 2.f;
+            const float hi = floorf(sm.ofs_hi[j] + rmax) + 2.f;
+            if (lo == lo && hi == hi && hi >= 0.f && lo < (float)p.npad) {
+                const int k0 = ((int)fmaxf(lo, -(float)WB)) & ~(staged_traits<K>::align_pairs - 1);
+                const int k1 = (int)fminf(hi, (float)p.npad + WB);
+                if (k1 - k0 + 1 <= WB) {
+                    tma_load_box3(stage_u32 + lane * GG::bytes, tmap, k0, c * p.S + e0 + j, cx.b * BT, full_bar);
+                    m = kFloorMagicBits + (uint32_t)k0;
+                    issued = true;
+                } else {
+                    m = kOvf;
+                    overflow = true;
+                }
+            }
+        }
+        sm.meta[stage * kStWin + lane] = m;
+    }
+    const unsigned issued_ballot = __ballot_sync(0xffffffffu, issued);
+    const unsigned ovf_ballot = __ballot_sync(0xffffffffu, overflow);
+    __syncwarp();
+    if (lane == 0 && !drop) {
+        sm.ovf[stage] = ovf_ballot != 0u;
+        mbar_arrive_expect_tx(full_bar, (uint32_t)__popc(issued_ballot) * (uint32_t)GG::data_bytes);
+    }
+    if (!dead) issued_mask |= (1u << stage);
+}
+
+template <int WB, int K, int BT>
+constexpr size_t staged_batch_smem_bytes() {
+    return staged_smem_bytes<WB, K>() + group_geom<WB, K, BT>::data_bytes;   // + the zero group
+}
+
 template <int K, int SC, int WB, int BT>
 __global__ void __launch_bounds__(kStThreads) das_staged_batch_kernel(const staged_params p,
                                                                        const __grid_constant__ CUtensorMap tmap) {
     using st = typename pair_traits<K>::storage;
     using SG = slot_geom<WB, K>;
-    constexpr int CC = kStWin / (SC * BT);  // channels per stage
-    static_assert(SC % 2 == 0 && kStWin % (SC * BT) == 0, "SC * BT must divide the stage");
+    using GG = group_geom<WB, K, BT>;
+    constexpr int CC = GG::groups / SC;  // channels per stage
+    static_assert(SC % 2 == 0 && GG::groups % SC == 0, "SC * BT must divide the stage");
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     staged_smem<K, WB> sm(smem_raw);
-    const staged_ctx cx = staged_setup<K, WB>(p, sm);
+    unsigned char *zero_group = sm.extra;
+    for (int i = threadIdx.x; i < GG::data_bytes / 4; i += kStThreads) reinterpret_cast<uint32_t *>(zero_group)[i] = 0u;
+    const staged_ctx cx = staged_setup<K, WB>(p, sm);   // ends with __syncthreads
 
     const st *__restrict__ Pg = static_cast<const st *>(p.P);
     const uint32_t kmax_pair = (uint32_t)(p.npad - 1);
@@ -991,7 +1083,7 @@ __global__ void __launch_bounds__(kStThreads) das_staged_batch_kernel(const stag
 
     const uint32_t ring_u32 = smem_u32(sm.ring);
     const uint32_t chan_u32 = smem_u32(sm.chan_pos);
-    const uint32_t meta_u32 = smem_u32(sm.meta);
+    const uint32_t zero_u32 = smem_u32(zero_group);
     const float2 magic2 = make_float2(kFloorMagic, kFloorMagic);
     const float2 neg1 = make_float2(-1.f, -1.f);
 
@@ -1008,7 +1100,7 @@ __global__ void __launch_bounds__(kStThreads) das_staged_batch_kernel(const stag
 
         for (int c0 = 0; c0 < p.C; c0 += CC) {
             if (cx.producer) {
-                staged_produce<K, WB, SC, BT>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
+                staged_produce_batch<K, WB, SC, BT>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
             } else {
                 const uint32_t full_bar = smem_u32(&sm.full[stage]);
                 if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
@@ -1023,12 +1115,9 @@ __global__ void __launch_bounds__(kStThreads) das_staged_batch_kernel(const stag
                         if (p.srcdir)
                             apply_directivity(g, cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z,
                                               sm.chan_dir[stage * kStWin + cl]);
-                        // window start of each event: the bi = 0 slot's metadata word
                         uint32_t k0p[SC];
-#pragma unroll
-                        for (int j = 0; j < SC; j++)
-                            k0p[j] = lds_u32(meta_u32 + (stage * kStWin + (cl * SC + j) * BT) * 4);
-                        const uint32_t slots_u32 = stage_u32 + (cl * SC * BT) * SG::bytes;
+                        load_meta<SC>(sm.meta, stage, cl, k0p);
+                        const uint32_t groups_u32 = stage_u32 + (cl * SC) * GG::bytes;
                         if (!any_ovf) {
                             const float2 rsq2 = make_float2(g.rsq, g.rsq);
                             const float2 rinv2 = make_float2(g.rinv, g.rinv);
@@ -1038,23 +1127,27 @@ __global__ void __launch_bounds__(kStThreads) das_staged_batch_kernel(const stag
                                 const float2 mm2 = __fadd2_rd(tau2, magic2);
                                 const float2 nfl2 = __ffma2_rn(mm2, neg1, magic2);   // -(floor), exact
                                 const float2 t2 = __fadd2_rn(tau2, nfl2);
-                                const uint32_t ra = min(__float_as_uint(mm2.x) - k0p[j], (uint32_t)WB);
-                                const uint32_t rb = min(__float_as_uint(mm2.y) - k0p[j + 1], (uint32_t)WB);
-                                const uint32_t aa = slots_u32 + (j * BT) * SG::bytes + ra * sizeof(st);
-                                const uint32_t ab = slots_u32 + ((j + 1) * BT) * SG::bytes + rb * sizeof(st);
+                                const uint32_t ra = __float_as_uint(mm2.x) - k0p[j];
+                                const uint32_t rb = __float_as_uint(mm2.y) - k0p[j + 1];
+                                const uint32_t aa = ra < (uint32_t)WB ? groups_u32 + j * GG::bytes + ra * sizeof(st)
+                                                                      : zero_u32;
+                                const uint32_t ab = rb < (uint32_t)WB
+                                                        ? groups_u32 + (j + 1) * GG::bytes + rb * sizeof(st)
+                                                        : zero_u32;
 #pragma unroll
                                 for (int bi = 0; bi < BT; bi++) {
-                                    const float ta = tap_at<K>(aa + bi * SG::bytes, t2.x);
-                                    const float tb = tap_at<K>(ab + bi * SG::bytes, t2.y);
+                                    const float ta = tap_at<K>(aa + bi * GG::item_bytes, t2.x);
+                                    const float tb = tap_at<K>(ab + bi * GG::item_bytes, t2.y);
                                     acc2[bi] = __ffma2_rn(w2[j / 2], make_float2(ta, tb), acc2[bi]);
                                 }
                             }
                         } else {
-                            const unsigned char *slots = sm.ring + stage * SG::stage_bytes + (cl * SC * BT) * SG::bytes;
+                            const unsigned char *groups = sm.ring + stage * SG::stage_bytes + (cl * SC) * GG::bytes;
 #pragma unroll
                             for (int j = 0; j < SC; j++) {
                                 const float tau = __fmaf_rn(g.rsq, g.rinv, ofs[j]);
                                 const tau_split ts = split_tau(tau);
+                                const uint32_t rr = ts.k + kFloorMagicBits - k0p[j];
 #pragma unroll
                                 for (int bi = 0; bi < BT; bi++) {
                                     st pr;
@@ -1062,10 +1155,11 @@ __global__ void __launch_bounds__(kStThreads) das_staged_batch_kernel(const stag
                                         const int bb = min(cx.b * BT + bi, p.B - 1);
                                         const int64_t row = ((int64_t)bb * p.C + c) * p.S + (e0 + min(j, sc - 1));
                                         pr = Pg[row * p.npad + min(ts.k, kmax_pair)];
+                                    } else if (rr < (uint32_t)WB) {
+                                        pr = *reinterpret_cast<const st *>(groups + j * GG::bytes + bi * GG::item_bytes +
+                                                                           rr * sizeof(st));
                                     } else {
-                                        const uint32_t rel = min(ts.k + kFloorMagicBits - k0p[j], (uint32_t)WB);
-                                        pr = *reinterpret_cast<const st *>(slots + (j * BT + bi) * SG::bytes +
-                                                                           rel * sizeof(st));
+                                        pr = *reinterpret_cast<const st *>(zero_group);
                                     }
                                     const float tv = pair_traits<K>::tap(pr, ts.t);
                                     if (j & 1) acc2[bi].y = __fmaf_rn(w[j], tv, acc2[bi].y);
