@@ -250,9 +250,12 @@ static schedule plan_schedule(const ffdas_context &h, const das_problem &pb, int
         s.SC = staged_event_chunk(pb.n_events);
         if (h.has_config && h.config.event_chunk) s.SC = staged_event_chunk(h.config.event_chunk);
         int bt = (h.has_config && h.config.batch_tile) ? h.config.batch_tile
-                                                        : std::min(4, floor_pow2(std::max(1, pb.B)));
+                                                        : std::min(8, floor_pow2(std::max(1, pb.B)));
         if (!staged_default && !(h.has_config && h.config.batch_tile)) bt = 1;
-        if (!staged_batch_supported()) bt = 1;
+        // batch tiles use TMA boxes: not with an explicit cp.async request or without the encoder
+        if (!staged_batch_supported() || (h.has_config && h.config.copy_engine == 2)) bt = 1;
+        // batch groups of delays widen windows (frame ensembles): default 64-pair windows
+        if (bt > 1 && !(h.has_config && h.config.window)) s.WB = 64;
         if (s.T0 * s.T1 * s.T2 == 512) bt = 1;
         bt = std::min(bt, 8);
         if (bt > 1) {
