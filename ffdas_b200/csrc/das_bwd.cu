@@ -359,17 +359,23 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
         gp.srcpos = a.srcpos; gp.dstpos = a.dstpos; gp.offsets = a.offsets; gp.weights = a.weights;
         gp.beta_zero = 1;
         const staged_grads gr{static_cast<const float *>(gout), pb.out_bstride, gx, goff, gw, gdst, gsrc};
-        const int SC = pb.n_events <= 1 ? 1 : 4;
         const int WB = (h.has_config && h.config.window > 32) ? 64 : 32;
+        const int copy = h.has_config ? h.config.copy_engine : 0;
+        // batch tiles: up to 8 items per CTA share each window's delays
+        int BT = 1;
+        while (BT * 2 <= std::min(pb.B, 8)) BT *= 2;
+        if (h.has_config && h.config.variant == 2 && h.config.batch_tile) BT = std::min(h.config.batch_tile, 8);
+        if (copy == 2 || !staged_batch_supported()) BT = 1;
+        const int SC = BT > 1 ? 4 : (pb.n_events <= 1 ? 1 : 4);
+        const int bchunks_st = (pb.B + BT - 1) / BT;
         h.last = ffdas_kernel_info_t{};
         h.last.variant = 4;
         h.last.tile_x = bp.T0; h.last.tile_y = bp.T1; h.last.tile_z = bp.T2;
-        h.last.batch_tile = 1; h.last.event_chunk = SC; h.last.storage = kind;
-        h.last.kernels = 2; h.last.grid = stiles * pb.B;
+        h.last.batch_tile = BT; h.last.event_chunk = SC; h.last.storage = kind;
+        h.last.kernels = 2; h.last.grid = stiles * bchunks_st;
         h.mark_start();
-        const int copy = h.has_config ? h.config.copy_engine : 0;
-        const ffdas_error_t err =
-            launch_staged_bwd(h, pb, kind, gp, gr, SC, WB, copy, dim3((unsigned)stiles, (unsigned)pb.B));
+        const ffdas_error_t err = launch_staged_bwd(h, pb, kind, gp, gr, SC, WB, BT, copy,
+                                                    dim3((unsigned)stiles, (unsigned)bchunks_st));
         h.mark_stop();
         return err;
     }

@@ -83,6 +83,6 @@ struct staged_grads {
     float *gx, *goff, *gw, *gdst, *gsrc;
 };
 ffdas_error_t launch_staged_bwd(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,
-                                const staged_grads &gr, int SC, int WB, int copy, dim3 grid);
+                                const staged_grads &gr, int SC, int WB, int BT, int copy, dim3 grid);
 
 }  // namespace ffdas

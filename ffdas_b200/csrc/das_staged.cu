@@ -168,6 +168,27 @@ static ffdas_error_t launch_fwd_sc(ffdas_context &h, const staged_params &sp, co
     }
 }
 
+template <int K, int WB, int BT>
+static ffdas_error_t launch_bwdb_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
+    constexpr size_t smem = staged_bwd_batch_smem_bytes<WB, K, 4, BT>();
+    static bool ready = false;
+    if (!ready) {
+        FFDAS_TRY(prepare_kernel(das_staged_bwd_batch_kernel<K, 4, WB, BT>, smem));
+        ready = true;
+    }
+    das_staged_bwd_batch_kernel<K, 4, WB, BT><<<grid, kStThreads, smem, h.stream>>>(sp, map);
+    return ffdas_launch_check(h.stream);
+}
+
+// Batch tiles of 2, 4 or 8 items, event chunk 4.
+template <int K, int WB>
+static ffdas_error_t launch_bwd_batch(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, int BT,
+                                      dim3 grid) {
+    if (BT == 2) return launch_bwdb_t<K, WB, 2>(h, sp, map, grid);
+    if (BT == 4) return launch_bwdb_t<K, WB, 4>(h, sp, map, grid);
+    return launch_bwdb_t<K, WB, 8>(h, sp, map, grid);
+}
+
 template <int K, int WB>
 static ffdas_error_t launch_bwd_sc(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, int SC,
                                    dim3 grid) {
@@ -230,17 +251,35 @@ ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, c
 }
 
 ffdas_error_t launch_staged_bwd(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,
-                                const staged_grads &gr, int SC, int WB, int copy, dim3 grid) {
+                                const staged_grads &gr, int SC, int WB, int BT, int copy, dim3 grid) {
+    if (BT > 1) copy = 1;   // batch tiles stage their windows with 3-D TMA boxes
     copy = resolve_copy(copy);
+    if (BT > 1 && copy != 1) return FFDAS_ERROR_CUDA_DRIVER;
     CUtensorMap map;
     std::memset(&map, 0, sizeof(map));
-    if (copy == 1) FFDAS_TRY(pair_row_map(map, gp.P, gp.npad, (int64_t)pb.B * pb.C * pb.S, kind, WB));
+    if (copy == 1 && BT > 1)
+        FFDAS_TRY(pair_batch_map(map, gp.P, gp.npad, (int64_t)pb.C * pb.S, pb.B, kind, WB, BT));
+    else if (copy == 1)
+        FFDAS_TRY(pair_row_map(map, gp.P, gp.npad, (int64_t)pb.B * pb.C * pb.S, kind, WB));
     staged_params sp = base_params(h, pb, gp);
     sp.copy_async = copy == 2;
     h.last.copy_engine = copy;
     sp.gout = gr.gout;
     sp.gout_bstride = gr.gout_bstride;
     sp.gx = gr.gx; sp.goff = gr.goff; sp.gw = gr.gw; sp.gdst = gr.gdst; sp.gsrc = gr.gsrc;
+    if (BT > 1) {
+        switch (kind) {
+            case ST_F32:
+                return WB == 64 ? launch_bwd_batch<ST_F32, 64>(h, sp, map, BT, grid)
+                                : launch_bwd_batch<ST_F32, 32>(h, sp, map, BT, grid);
+            case ST_F16:
+                return WB == 64 ? launch_bwd_batch<ST_F16, 64>(h, sp, map, BT, grid)
+                                : launch_bwd_batch<ST_F16, 32>(h, sp, map, BT, grid);
+            default:
+                return WB == 64 ? launch_bwd_batch<ST_BF16, 64>(h, sp, map, BT, grid)
+                                : launch_bwd_batch<ST_BF16, 32>(h, sp, map, BT, grid);
+        }
+    }
     const int sc = SC > 8 ? 8 : SC;
     switch (kind) {
         case ST_F32:

@@ -1497,4 +1497,303 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
     }
 }
 
+// ------------------------------------------------------- adjoint, batch tiles ---
+// The adjoint for BT batch items per CTA: windows staged as in
+// das_staged_batch_kernel (one 3-D TMA box per channel and event), delays,
+// split and window index computed once per (voxel, channel, event), then per
+// item: the tap's sample and slope, g_b-weighted sums for the weight, offset
+// and position gradients, and the fixed-point scatter of g_b w (1 - t), g_b w t
+// into the item's gradient slot.  amax = max_b |g_b| * max_j |w_j| over the tile.
+template <int WB, int K, int SC, int BT>
+constexpr size_t staged_bwd_batch_smem_bytes() {
+    return staged_bwd_smem_bytes<WB, K, SC>() + 16 + group_geom<WB, K, BT>::data_bytes;
+}
+
+template <int K, int SC, int WB, int BT>
+__global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(const staged_params p,
+                                                                            const __grid_constant__ CUtensorMap tmap) {
+    using SG = slot_geom<WB, K>;
+    using GG = group_geom<WB, K, BT>;
+    using st = typename pair_traits<K>::storage;
+    constexpr int CC = GG::groups / SC;
+    constexpr int GS = WB + 2;  // gradient slot length (int32 entries)
+    static_assert(SC % 2 == 0 && GG::groups % SC == 0, "SC * BT must divide the stage");
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    staged_smem<K, WB> sm(smem_raw);
+    int *gslot = reinterpret_cast<int *>(sm.extra);                      // [kStages][kStWin][GS], window = group * BT + item
+    float *cgrad = reinterpret_cast<float *>(gslot + kStages * kStWin * GS);  // [CC * 3][256]
+    float *wmax = cgrad + CC * 3 * kStConsumers;                          // [kStWarps]
+    unsigned char *zero_group = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(wmax + kStWarps) + 15) & ~uintptr_t(15));
+    for (int i = threadIdx.x; i < kStages * kStWin * GS; i += kStThreads) gslot[i] = 0;
+    for (int i = threadIdx.x; i < GG::data_bytes / 4; i += kStThreads) reinterpret_cast<uint32_t *>(zero_group)[i] = 0u;
+    const staged_ctx cx = staged_setup<K, WB>(p, sm, true);   // ends with __syncthreads
+    const uint32_t gslot_u32 = smem_u32(gslot);
+    const uint32_t zero_u32 = smem_u32(zero_group);
+
+    const int b0 = cx.b * BT;
+    const bool multi = gridDim.y > 1;   // several CTAs add into the voxel-side gradients
+    float g[BT];
+    float gmax = 0.f;
+#pragma unroll
+    for (int bi = 0; bi < BT; bi++) {
+        g[bi] = (cx.active && b0 + bi < p.B) ? __ldg(p.gout + (int64_t)(b0 + bi) * p.gout_bstride + cx.v) : 0.f;
+        gmax = fmaxf(gmax, fabsf(g[bi]));
+    }
+    bool gbad = false;
+#pragma unroll
+    for (int bi = 0; bi < BT; bi++) gbad |= !(fabsf(g[bi]) <= 3.0e38f);
+    const bool want_pos = p.gdst != nullptr || p.gsrc != nullptr;
+    float gpx = 0.f, gpy = 0.f, gpz = 0.f;
+    int stage = 0;
+    uint32_t phase = 0;
+    bool dead = false;
+    uint32_t issued_mask = 0;
+    const float2 magic2 = make_float2(kFloorMagic, kFloorMagic);
+    const float2 neg1 = make_float2(-1.f, -1.f);
+
+    for (int e0 = 0; e0 < p.n_events; e0 += SC) {
+        const int sc = min(SC, p.n_events - e0);
+        float ofs[SC], w[SC];
+        staged_pass_begin<K, WB, SC>(p, sm, cx, e0, sc, ofs, w);
+        // per event: sum of g_b x0, of g_b d and of t g_b d over channels and items
+        float sx[SC], sd[SC], std_[SC];
+#pragma unroll
+        for (int j = 0; j < SC; j++) { sx[j] = 0.f; sd[j] = 0.f; std_[j] = 0.f; }
+        float fscale = 0.f, finv = 0.f;
+        bool fixed = false;
+        if (!cx.producer) {
+            float wm = 0.f;
+            bool bad = gbad;
+#pragma unroll
+            for (int j = 0; j < SC; j++) {
+                wm = fmaxf(wm, fabsf(w[j]));
+                bad |= !(fabsf(w[j]) <= 3.0e38f);
+            }
+            float m = gmax * wm;
+            bad |= !(m <= 3.0e38f);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            bad = __any_sync(0xffffffffu, bad);
+            if (cx.lane == 0) wmax[cx.warp] = bad ? -1.f : m;
+            consumer_sync();
+            float amax = 0.f;
+            bool any_bad = false;
+#pragma unroll
+            for (int i = 0; i < kStWarps; i++) {
+                const float v = wmax[i];
+                any_bad |= v < 0.f;
+                amax = fmaxf(amax, v);
+            }
+            fixed = !any_bad && amax > 0.f && amax <= 3.0e38f;
+            if (fixed) {
+                fscale = kFixRange / amax;
+                finv = amax / kFixRange;
+            }
+            consumer_sync();   // wmax is rewritten by the next pass
+        }
+        float gsw[SC];   // w scaled to fixed point; a contribution is g_b * gsw
+#pragma unroll
+        for (int j = 0; j < SC; j++) gsw[j] = w[j] * fscale;
+
+        for (int c0 = 0; c0 < p.C; c0 += CC) {
+            if (cx.producer) {
+                staged_produce_batch<K, WB, SC, BT>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
+            } else {
+                const uint32_t full_bar = smem_u32(&sm.full[stage]);
+                const uint32_t stage_u32 = smem_u32(sm.ring + stage * SG::stage_bytes);
+                int *gstage = gslot + stage * kStWin * GS;
+                const uint32_t gstage_u32 = gslot_u32 + stage * kStWin * GS * 4;
+                if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
+                const bool any_ovf = !dead && sm.ovf[stage] != 0;
+                if (!dead) {
+                    const uint32_t nlast = (uint32_t)(p.N - 1);
+                    for (int cl = 0; cl < CC; cl++) {
+                        const int c = c0 + cl;
+                        if (c >= p.C) break;   // a phantom channel's taps would scatter outside gx
+                        const float4 cp = sm.chan_pos[stage * kStWin + cl];
+                        const recv_geom gm = receive_geometry(cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z);
+                        uint32_t k0p[SC];
+                        load_meta<SC>(sm.meta, stage, cl, k0p);
+                        const uint32_t groups_u32 = stage_u32 + (cl * SC) * GG::bytes;
+                        const uint32_t gwin_u32 = gstage_u32 + (cl * SC * BT) * GS * 4;
+                        float q = 0.f;
+                        if (!any_ovf && (fixed || !p.gx)) {
+                            // common case: every in-record tap is in its window
+                            const float2 rsq2 = make_float2(gm.rsq, gm.rsq), rinv2 = make_float2(gm.rinv, gm.rinv);
+#pragma unroll
+                            for (int j = 0; j < SC; j += 2) {
+                                const float2 tau2 = __ffma2_rn(rsq2, rinv2, make_float2(ofs[j], ofs[j + 1]));
+                                const float2 mm2 = __fadd2_rd(tau2, magic2);
+                                const float2 nfl2 = __ffma2_rn(mm2, neg1, magic2);   // -(floor), exact
+                                const float2 t2 = __fadd2_rn(tau2, nfl2);
+#pragma unroll
+                                for (int h = 0; h < 2; h++) {
+                                    const int jj = j + h;
+                                    const uint32_t mb = __float_as_uint(h ? mm2.y : mm2.x);
+                                    const float t = h ? t2.y : t2.x;
+                                    const uint32_t rr = mb - k0p[jj];
+                                    const uint32_t base =
+                                        rr < (uint32_t)WB ? groups_u32 + jj * GG::bytes + rr * sizeof(st) : zero_u32;
+                                    const uint32_t relc = min(rr, (uint32_t)WB);
+                                    const bool kin = mb - kFloorMagicBits < nlast;
+                                    float gd = 0.f;
+#pragma unroll
+                                    for (int bi = 0; bi < BT; bi++) {
+                                        float x0, d;
+                                        pair_x0_d<K>(base + bi * GG::item_bytes, x0, d);
+                                        sx[jj] = __fmaf_rn(g[bi], x0, sx[jj]);
+                                        gd = __fmaf_rn(g[bi], d, gd);
+                                        if (p.gx) {
+                                            const float as = kin ? g[bi] * gsw[jj] : 0.f;
+                                            const int it = fix_round(as);
+                                            const int i1 = fix_round_fma(as, t);
+                                            const uint32_t ga = gwin_u32 + ((jj * BT + bi) * GS + relc) * 4;
+                                            red_shared_add(ga, it - i1);
+                                            red_shared_add(ga + 4, i1);
+                                        }
+                                    }
+                                    sd[jj] += gd;
+                                    std_[jj] = __fmaf_rn(t, gd, std_[jj]);
+                                    q = __fmaf_rn(w[jj], gd, q);
+                                }
+                            }
+                        } else {
+                            const unsigned char *groups = sm.ring + stage * SG::stage_bytes + (cl * SC) * GG::bytes;
+#pragma unroll 1
+                            for (int j = 0; j < SC; j++) {
+                                const float tau = __fmaf_rn(gm.rsq, gm.rinv, ofs[j]);
+                                const tau_split ts = split_tau(tau);
+                                const bool ovfw = k0p[j] == kOvf;
+                                const uint32_t rr = ts.k + kFloorMagicBits - k0p[j];
+                                float gd = 0.f;
+                                for (int bi = 0; bi < BT; bi++) {
+                                    st pr;
+                                    if (ovfw) {
+                                        const int bb = min(b0 + bi, p.B - 1);
+                                        const int64_t row = ((int64_t)bb * p.C + c) * p.S + (e0 + min(j, sc - 1));
+                                        pr = static_cast<const st *>(p.P)[row * p.npad + min(ts.k, (uint32_t)(p.npad - 1))];
+                                    } else if (rr < (uint32_t)WB) {
+                                        pr = *reinterpret_cast<const st *>(groups + j * GG::bytes + bi * GG::item_bytes +
+                                                                           rr * sizeof(st));
+                                    } else {
+                                        pr = *reinterpret_cast<const st *>(zero_group);
+                                    }
+                                    const float d = pair_traits<K>::slope(pr);
+                                    const float x0 = pair_traits<K>::tap(pr, 0.f);
+                                    sx[j] = __fmaf_rn(g[bi], x0, sx[j]);
+                                    gd = __fmaf_rn(g[bi], d, gd);
+                                    const float a = g[bi] * w[j];
+                                    if (p.gx && a != 0.f && ts.k < nlast && b0 + bi < p.B) {
+                                        if (fixed && !ovfw && rr < (uint32_t)WB) {
+                                            const float as = g[bi] * gsw[j];
+                                            const int it = fix_round(as);
+                                            const int i1 = fix_round_fma(as, ts.t);
+                                            const uint32_t ga = gwin_u32 + ((j * BT + bi) * GS + rr) * 4;
+                                            red_shared_add(ga, it - i1);
+                                            red_shared_add(ga + 4, i1);
+                                        } else {
+                                            const float a1 = a * ts.t;
+                                            float *gr = p.gx + (((int64_t)(b0 + bi) * p.C + c) * p.S + (e0 + j)) * p.N + ts.k;
+                                            atomicAdd(gr, a - a1);
+                                            atomicAdd(gr + 1, a1);
+                                        }
+                                    }
+                                }
+                                sd[j] += gd;
+                                std_[j] = __fmaf_rn(ts.t, gd, std_[j]);
+                                q = __fmaf_rn(w[j], gd, q);
+                            }
+                        }
+                        if (want_pos) {
+                            const float qr = q * gm.rinv;
+                            const float ex = (cx.vx - cp.x) * qr, ey = (cx.vy - cp.y) * qr, ez = (cx.vz - cp.z) * qr;
+                            gpx += ex; gpy += ey; gpz += ez;
+                            if (p.gsrc) {
+                                cgrad[(cl * 3 + 0) * kStConsumers + cx.tid] = -ex;
+                                cgrad[(cl * 3 + 1) * kStConsumers + cx.tid] = -ey;
+                                cgrad[(cl * 3 + 2) * kStConsumers + cx.tid] = -ez;
+                            }
+                        }
+                    }
+                }
+                // every consumer warp finished this stage's scatter
+                consumer_sync();
+                if (!dead) {
+                    if (p.gx && fixed) {
+                        for (int i = cx.tid; i < kStWin * GS; i += kStConsumers) {
+                            const int val = gstage[i];
+                            if (val != 0) {
+                                gstage[i] = 0;
+                                const int win = i / GS, r = i - win * GS;
+                                const int grp = win / BT, bi = win % BT;
+                                const int cl = grp / SC, j = grp % SC;
+                                const int k = (int)(sm.meta[stage * kStWin + grp] - kFloorMagicBits) + r;
+                                if (b0 + bi < p.B && k >= 0 && k < p.N) {
+                                    float *gr = p.gx + (((int64_t)(b0 + bi) * p.C + (c0 + cl)) * p.S + (e0 + j)) * p.N + k;
+                                    atomicAdd(gr, (float)val * finv);
+                                }
+                            }
+                        }
+                    }
+                    if (p.gsrc) {
+                        for (int o = cx.warp; o < CC * 3; o += kStWarps) {
+                            const int cl = o / 3;
+                            if (c0 + cl >= p.C) continue;
+                            float s = 0.f;
+#pragma unroll
+                            for (int i = 0; i < kStConsumers / 32; i++) s += cgrad[o * kStConsumers + cx.lane + 32 * i];
+#pragma unroll
+                            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+                            if (cx.lane == 0 && s != 0.f) atomicAdd(p.gsrc + 3 * (c0 + cl) + (o % 3), s);
+                        }
+                    }
+                }
+                consumer_sync();  // scratch reused by the next stage
+                __syncwarp();
+                if (cx.lane == 0) mbar_arrive(smem_u32(&sm.empty[stage]));
+            }
+            if (++stage == kStages) {
+                stage = 0;
+                phase ^= 1u;
+            }
+        }
+        if (!cx.producer && cx.active && !dead) {
+#pragma unroll
+            for (int j = 0; j < SC; j++) {
+                if (j < sc) {
+                    const int64_t idx = (int64_t)(e0 + j) * p.V + cx.v;
+                    const float gwv = sx[j] + std_[j];   // sum over items and channels of g_b L
+                    const float gov = w[j] * sd[j];      // w * sum of g_b d
+                    if (multi) {
+                        if (p.gw) atomicAdd(p.gw + idx, gwv);
+                        if (p.goff) atomicAdd(p.goff + idx, gov);
+                    } else {
+                        if (p.gw) p.gw[idx] = gwv;
+                        if (p.goff) p.goff[idx] = gov;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    if (cx.producer) {
+        staged_drain<K, WB>(sm, cx, stage, phase, issued_mask);
+        return;
+    }
+    if (cx.active && !dead && p.gdst) {
+        if (multi) {
+            atomicAdd(p.gdst + 3 * cx.v, gpx);
+            atomicAdd(p.gdst + 3 * cx.v + 1, gpy);
+            atomicAdd(p.gdst + 3 * cx.v + 2, gpz);
+        } else {
+            p.gdst[3 * cx.v] = gpx;
+            p.gdst[3 * cx.v + 1] = gpy;
+            p.gdst[3 * cx.v + 2] = gpz;
+        }
+    }
+}
+
 }  // namespace ffdas
