@@ -71,16 +71,21 @@ ffdas_error_t make_problem(const ffdas_tensor_desc &x, const ffdas_tensor_desc &
 
 int select_storage(ffdas_datatype_t xt, ffdas_datatype_t ot, ffdas_compute_type_t ct) {
     switch (xt) {
+        // 16-bit channel data is widened to FP32 pairs unless a 16-bit compute
+        // type asks for 16-bit pairs: the widening is exact, and the kernels
+        // are bound by instruction issue, not by the pair bytes, so FP32 pairs
+        // interpolate the 16-bit samples exactly and run the fewest
+        // instructions per tap (16-bit pairs halve the workspace instead).
         case FFDAS_R_16F:
             if (ot != FFDAS_R_32F) return -1;
             // reference: a half-precision compute request on half input is
             // rejected (das_alg1.cu:172-178)
             if (ct == FFDAS_COMPUTE_16F) return -1;
-            return ct == FFDAS_COMPUTE_16BF ? ST_BF16 : ST_F16;
+            return ct == FFDAS_COMPUTE_16BF ? ST_BF16 : ST_F32;
         case FFDAS_R_16BF:
             if (ot != FFDAS_R_32F) return -1;
             if (ct == FFDAS_COMPUTE_16F) return ST_F16;
-            return ST_BF16;
+            return ct == FFDAS_COMPUTE_16BF ? ST_BF16 : ST_F32;
         case FFDAS_R_32F:
             if (ot != FFDAS_R_32F) return -1;
             if (ct == FFDAS_COMPUTE_16F) return ST_F16;
@@ -144,10 +149,12 @@ static ffdas_error_t launch_ingest(ffdas_context &h, const das_problem &pb, ffda
             if (kind == ST_BF16) return launch_ingest_t<float, ST_BF16>(h, pb, x, npad, P);
             break;
         case FFDAS_R_16F:
+            if (kind == ST_F32) return launch_ingest_t<__half, ST_F32>(h, pb, x, npad, P);
             if (kind == ST_F16) return launch_ingest_t<__half, ST_F16>(h, pb, x, npad, P);
             if (kind == ST_BF16) return launch_ingest_t<__half, ST_BF16>(h, pb, x, npad, P);
             break;
         case FFDAS_R_16BF:
+            if (kind == ST_F32) return launch_ingest_t<__nv_bfloat16, ST_F32>(h, pb, x, npad, P);
             if (kind == ST_BF16) return launch_ingest_t<__nv_bfloat16, ST_BF16>(h, pb, x, npad, P);
             if (kind == ST_F16) return launch_ingest_t<__nv_bfloat16, ST_F16>(h, pb, x, npad, P);
             break;

@@ -1661,13 +1661,14 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                             }
                         } else {
                             const unsigned char *groups = sm.ring + stage * SG::stage_bytes + (cl * SC) * GG::bytes;
-#pragma unroll 1
+#pragma unroll
                             for (int j = 0; j < SC; j++) {
                                 const float tau = __fmaf_rn(gm.rsq, gm.rinv, ofs[j]);
                                 const tau_split ts = split_tau(tau);
                                 const bool ovfw = k0p[j] == kOvf;
                                 const uint32_t rr = ts.k + kFloorMagicBits - k0p[j];
                                 float gd = 0.f;
+#pragma unroll
                                 for (int bi = 0; bi < BT; bi++) {
                                     st pr;
                                     if (ovfw) {

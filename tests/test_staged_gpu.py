@@ -71,13 +71,24 @@ def test_staged_matches_oracle(name, kw, cfg, copy):
 
 
 @pytest.mark.parametrize("tile", [(16, 16), (32, 16)], ids=["256", "512"])
-@pytest.mark.parametrize("dtype,tol", [(torch.float16, 1e-3), (torch.bfloat16, 1e-3)])
-def test_staged_16bit_pairs(dtype, tol, tile):
+@pytest.mark.parametrize("dtype,flag", [(torch.float16, "use_fp16"), (torch.bfloat16, "use_bf16")])
+def test_staged_16bit_pairs(dtype, flag, tile):
+    # FP32 data stored as 16-bit pairs (the fp16 / bf16 compute types): the
+    # image interpolates the rounded samples exactly
+    wl = W.diverging3d(device=DEV, scale=0.25)
+    x = W.normalize_channels(wl["x"])
+    out, info = _run(wl, x, dict(variant=2, tile_x=tile[0], tile_y=tile[1], window=32), **{flag: True})
+    assert info["variant"] == 2 and info["storage"] == (1 if dtype == torch.float16 else 2)
+    assert oracle.rel_l2(_np(out), _ref(wl, x.to(dtype))) < 2e-5
+
+
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+def test_16bit_input_widens_to_fp32_pairs(dtype):
     wl = W.diverging3d(device=DEV, scale=0.25)
     x = W.normalize_channels(wl["x"]).to(dtype)
-    out, info = _run(wl, x, dict(variant=2, tile_x=tile[0], tile_y=tile[1], window=32))
-    assert info["variant"] == 2 and info["storage"] in (1, 2)
-    assert oracle.rel_l2(_np(out), _ref(wl, x)) < tol
+    out, info = _run(wl, x, dict(variant=2, tile_x=32, tile_y=16, window=32))
+    assert info["storage"] == 0
+    assert oracle.rel_l2(_np(out), _ref(wl, x)) < 2e-5
 
 
 def test_staged_agrees_with_gather():
@@ -203,13 +214,17 @@ def test_batch_tiles_match_oracle(B, bt, ec, wb):
     assert oracle.rel_l2(_np(out), _ref(wl, x)) < 2e-5
 
 
-@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
-def test_batch_tiles_16bit(dtype):
-    wl = W.ensemble(device=DEV, scale=0.1, frames=6, dtype=dtype)
+@pytest.mark.parametrize("dtype,flag", [(torch.float16, "use_fp16"), (torch.bfloat16, "use_bf16")])
+def test_batch_tiles_16bit(dtype, flag):
+    wl = W.ensemble(device=DEV, scale=0.1, frames=6, dtype=torch.float32)
     x = wl["x"]
-    out, info = _run(wl, x, dict(variant=2, tile_x=64, tile_y=4, window=64, batch_tile=4))
+    out, info = _run(wl, x, dict(variant=2, tile_x=64, tile_y=4, window=64, batch_tile=4), **{flag: True})
     assert info["batch_tile"] == 4 and info["storage"] in (1, 2)
-    assert oracle.rel_l2(_np(out), _ref(wl, x)) < 2e-4
+    assert oracle.rel_l2(_np(out), _ref(wl, x.to(dtype))) < 2e-5
+    x16 = x.to(dtype)   # 16-bit data, default compute: FP32 pairs
+    out, info = _run(wl, x16, dict(variant=2, tile_x=64, tile_y=4, window=64, batch_tile=4))
+    assert info["storage"] == 0
+    assert oracle.rel_l2(_np(out), _ref(wl, x16)) < 2e-5
 
 
 def test_default_planner_picks_staged_for_dense_volumes():
