@@ -363,8 +363,8 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
         const int copy = h.has_config ? h.config.copy_engine : 0;
         // batch tiles: up to 8 items per CTA share each window's delays
         int BT = 1;
-        while (BT * 2 <= std::min(pb.B, 8)) BT *= 2;
-        if (h.has_config && h.config.variant == 2 && h.config.batch_tile) BT = std::min(h.config.batch_tile, 8);
+        while (BT * 2 <= std::min(pb.B, 4)) BT *= 2;
+        if (h.has_config && h.config.variant == 2 && h.config.batch_tile) BT = std::min(h.config.batch_tile, 4);
         if (copy == 2 || !staged_batch_supported()) BT = 1;
         const int SC = BT > 1 ? 4 : (pb.n_events <= 1 ? 1 : 4);
         const int bchunks_st = (pb.B + BT - 1) / BT;

@@ -180,13 +180,12 @@ static ffdas_error_t launch_bwdb_t(ffdas_context &h, const staged_params &sp, co
     return ffdas_launch_check(h.stream);
 }
 
-// Batch tiles of 2, 4 or 8 items, event chunk 4.
+// Batch tiles of 2 or 4 items (eight would spill), event chunk 4.
 template <int K, int WB>
 static ffdas_error_t launch_bwd_batch(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, int BT,
                                       dim3 grid) {
     if (BT == 2) return launch_bwdb_t<K, WB, 2>(h, sp, map, grid);
-    if (BT == 4) return launch_bwdb_t<K, WB, 4>(h, sp, map, grid);
-    return launch_bwdb_t<K, WB, 8>(h, sp, map, grid);
+    return launch_bwdb_t<K, WB, 4>(h, sp, map, grid);
 }
 
 template <int K, int WB>

@@ -1504,9 +1504,18 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
 // item: the tap's sample and slope, g_b-weighted sums for the weight, offset
 // and position gradients, and the fixed-point scatter of g_b w (1 - t), g_b w t
 // into the item's gradient slot.  amax = max_b |g_b| * max_j |w_j| over the tile.
+//
+// The slot of a window holds two fixed-point bin arrays per sample k of the
+// window: A[k] += g_b w and T[k] += g_b w t for a tap at k, so that the flush
+// adds A[k] - T[k] to gx[k] and T[k] to gx[k+1] -- for 0 <= k <= N-2 only.
+// A tap outside the record therefore needs no test in the loop (its bins are
+// dropped at the flush), and a tap outside its window (always outside the
+// record) lands in the bin past the window, which the flush never reads.
 template <int WB, int K, int SC, int BT>
 constexpr size_t staged_bwd_batch_smem_bytes() {
-    return staged_bwd_smem_bytes<WB, K, SC>() + 16 + group_geom<WB, K, BT>::data_bytes;
+    return staged_smem_bytes<WB, K>() + kStages * kStWin * 2 * (WB + 1) * 4 +
+           (group_geom<WB, K, BT>::groups / SC) * 3 * kStConsumers * 4 + kStWarps * 4 + 16 +
+           group_geom<WB, K, BT>::data_bytes;
 }
 
 template <int K, int SC, int WB, int BT>
@@ -1516,17 +1525,18 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
     using GG = group_geom<WB, K, BT>;
     using st = typename pair_traits<K>::storage;
     constexpr int CC = GG::groups / SC;
-    constexpr int GS = WB + 2;  // gradient slot length (int32 entries)
+    constexpr int GS = WB + 1;  // bins per window and array (the last one collects out-of-window taps)
+    constexpr int GW = 2 * GS;  // A bins then T bins
     static_assert(SC % 2 == 0 && GG::groups % SC == 0, "SC * BT must divide the stage");
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     staged_smem<K, WB> sm(smem_raw);
-    int *gslot = reinterpret_cast<int *>(sm.extra);                      // [kStages][kStWin][GS], window = group * BT + item
-    float *cgrad = reinterpret_cast<float *>(gslot + kStages * kStWin * GS);  // [CC * 3][256]
+    int *gslot = reinterpret_cast<int *>(sm.extra);                      // [kStages][kStWin][2][GS], window = group * BT + item
+    float *cgrad = reinterpret_cast<float *>(gslot + kStages * kStWin * GW);  // [CC * 3][256]
     float *wmax = cgrad + CC * 3 * kStConsumers;                          // [kStWarps]
     unsigned char *zero_group = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(wmax + kStWarps) + 15) & ~uintptr_t(15));
-    for (int i = threadIdx.x; i < kStages * kStWin * GS; i += kStThreads) gslot[i] = 0;
+    for (int i = threadIdx.x; i < kStages * kStWin * GW; i += kStThreads) gslot[i] = 0;
     for (int i = threadIdx.x; i < GG::data_bytes / 4; i += kStThreads) reinterpret_cast<uint32_t *>(zero_group)[i] = 0u;
     const staged_ctx cx = staged_setup<K, WB>(p, sm, true);   // ends with __syncthreads
     const uint32_t gslot_u32 = smem_u32(gslot);
@@ -1603,8 +1613,8 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
             } else {
                 const uint32_t full_bar = smem_u32(&sm.full[stage]);
                 const uint32_t stage_u32 = smem_u32(sm.ring + stage * SG::stage_bytes);
-                int *gstage = gslot + stage * kStWin * GS;
-                const uint32_t gstage_u32 = gslot_u32 + stage * kStWin * GS * 4;
+                int *gstage = gslot + stage * kStWin * GW;
+                const uint32_t gstage_u32 = gslot_u32 + stage * kStWin * GW * 4;
                 if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
                 const bool any_ovf = !dead && sm.ovf[stage] != 0;
                 if (!dead) {
@@ -1617,7 +1627,7 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                         uint32_t k0p[SC];
                         load_meta<SC>(sm.meta, stage, cl, k0p);
                         const uint32_t groups_u32 = stage_u32 + (cl * SC) * GG::bytes;
-                        const uint32_t gwin_u32 = gstage_u32 + (cl * SC * BT) * GS * 4;
+                        const uint32_t gwin_u32 = gstage_u32 + (cl * SC * BT) * GW * 4;
                         float q = 0.f;
                         if (!any_ovf && (fixed || !p.gx)) {
                             // common case: every in-record tap is in its window
@@ -1637,23 +1647,21 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                                     const uint32_t base =
                                         rr < (uint32_t)WB ? groups_u32 + jj * GG::bytes + rr * sizeof(st) : zero_u32;
                                     const uint32_t relc = min(rr, (uint32_t)WB);
-                                    const bool kin = mb - kFloorMagicBits < nlast;
-                                    float gd = 0.f;
+                                    const uint32_t gb = gwin_u32 + ((jj * BT) * GW + relc) * 4;
+                                    float2 sg = make_float2(sx[jj], 0.f);   // (sum g_b x0, sum g_b d)
 #pragma unroll
                                     for (int bi = 0; bi < BT; bi++) {
                                         float x0, d;
                                         pair_x0_d<K>(base + bi * GG::item_bytes, x0, d);
-                                        sx[jj] = __fmaf_rn(g[bi], x0, sx[jj]);
-                                        gd = __fmaf_rn(g[bi], d, gd);
+                                        sg = __ffma2_rn(make_float2(g[bi], g[bi]), make_float2(x0, d), sg);
                                         if (p.gx) {
-                                            const float as = kin ? g[bi] * gsw[jj] : 0.f;
-                                            const int it = fix_round(as);
-                                            const int i1 = fix_round_fma(as, t);
-                                            const uint32_t ga = gwin_u32 + ((jj * BT + bi) * GS + relc) * 4;
-                                            red_shared_add(ga, it - i1);
-                                            red_shared_add(ga + 4, i1);
+                                            const float as = g[bi] * gsw[jj];
+                                            red_shared_add(gb + bi * GW * 4, fix_round(as));
+                                            red_shared_add(gb + (bi * GW + GS) * 4, fix_round_fma(as, t));
                                         }
                                     }
+                                    sx[jj] = sg.x;
+                                    const float gd = sg.y;
                                     sd[jj] += gd;
                                     std_[jj] = __fmaf_rn(t, gd, std_[jj]);
                                     q = __fmaf_rn(w[jj], gd, q);
@@ -1689,11 +1697,9 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                                     if (p.gx && a != 0.f && ts.k < nlast && b0 + bi < p.B) {
                                         if (fixed && !ovfw && rr < (uint32_t)WB) {
                                             const float as = g[bi] * gsw[j];
-                                            const int it = fix_round(as);
-                                            const int i1 = fix_round_fma(as, ts.t);
-                                            const uint32_t ga = gwin_u32 + ((j * BT + bi) * GS + rr) * 4;
-                                            red_shared_add(ga, it - i1);
-                                            red_shared_add(ga + 4, i1);
+                                            const uint32_t ga = gwin_u32 + ((j * BT + bi) * GW + rr) * 4;
+                                            red_shared_add(ga, fix_round(as));
+                                            red_shared_add(ga + GS * 4, fix_round_fma(as, ts.t));
                                         } else {
                                             const float a1 = a * ts.t;
                                             float *gr = p.gx + (((int64_t)(b0 + bi) * p.C + c) * p.S + (e0 + j)) * p.N + ts.k;
@@ -1723,17 +1729,23 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                 consumer_sync();
                 if (!dead) {
                     if (p.gx && fixed) {
+                        // bins 0..WB-1 of each window: gx[k] += A - T, gx[k+1] += T for 0 <= k <= N-2;
+                        // every bin (the out-of-window one too) is cleared for the stage's next use
                         for (int i = cx.tid; i < kStWin * GS; i += kStConsumers) {
-                            const int val = gstage[i];
-                            if (val != 0) {
-                                gstage[i] = 0;
-                                const int win = i / GS, r = i - win * GS;
+                            const int win = i / GS, r = i - win * GS;
+                            int *bin = gstage + win * GW + r;
+                            const int va = bin[0], vt = bin[GS];
+                            if ((va | vt) != 0) {
+                                bin[0] = 0;
+                                bin[GS] = 0;
                                 const int grp = win / BT, bi = win % BT;
                                 const int cl = grp / SC, j = grp % SC;
                                 const int k = (int)(sm.meta[stage * kStWin + grp] - kFloorMagicBits) + r;
-                                if (b0 + bi < p.B && k >= 0 && k < p.N) {
+                                if (r < WB && b0 + bi < p.B && k >= 0 && k <= p.N - 2) {
                                     float *gr = p.gx + (((int64_t)(b0 + bi) * p.C + (c0 + cl)) * p.S + (e0 + j)) * p.N + k;
-                                    atomicAdd(gr, (float)val * finv);
+                                    const float a1 = (float)vt * finv;
+                                    atomicAdd(gr, (float)(va - vt) * finv);
+                                    atomicAdd(gr + 1, a1);
                                 }
                             }
                         }
