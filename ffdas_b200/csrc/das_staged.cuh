@@ -642,6 +642,19 @@ template <> __device__ __forceinline__ void pair_x0_d<ST_BF16>(uint32_t a, float
     d = __uint_as_float(u & 0xFFFF0000u) - x0;
 }
 
+// pair_x0_d on a shared-memory pointer (lets constant offsets fold).
+template <int K> __device__ __forceinline__ void pair_x0_d_ptr(const typename pair_traits<K>::storage *q, float &x0,
+                                                               float &d) {
+    const typename pair_traits<K>::storage pr = *q;
+    if constexpr (K == ST_F32) {
+        x0 = pr.x;
+        d = pr.y;
+    } else {
+        d = pair_traits<K>::slope(pr);
+        x0 = pair_traits<K>::tap(pr, 0.f);
+    }
+}
+
 // Interpolate one tap from a staged slot (f32 result).
 template <int K>
 __device__ __forceinline__ float staged_tap(const unsigned char *slot, uint32_t rel, float t) {
@@ -1117,7 +1130,7 @@ __global__ void __launch_bounds__(kStThreads) das_staged_batch_kernel(const stag
                                               sm.chan_dir[stage * kStWin + cl]);
                         uint32_t k0p[SC];
                         load_meta<SC>(sm.meta, stage, cl, k0p);
-                        const uint32_t groups_u32 = stage_u32 + (cl * SC) * GG::bytes;
+                        const unsigned char *groups = sm.ring + stage * SG::stage_bytes + (cl * SC) * GG::bytes;
                         if (!any_ovf) {
                             const float2 rsq2 = make_float2(g.rsq, g.rsq);
                             const float2 rinv2 = make_float2(g.rinv, g.rinv);
@@ -1129,20 +1142,23 @@ __global__ void __launch_bounds__(kStThreads) das_staged_batch_kernel(const stag
                                 const float2 t2 = __fadd2_rn(tau2, nfl2);
                                 const uint32_t ra = __float_as_uint(mm2.x) - k0p[j];
                                 const uint32_t rb = __float_as_uint(mm2.y) - k0p[j + 1];
-                                const uint32_t aa = ra < (uint32_t)WB ? groups_u32 + j * GG::bytes + ra * sizeof(st)
-                                                                      : zero_u32;
-                                const uint32_t ab = rb < (uint32_t)WB
-                                                        ? groups_u32 + (j + 1) * GG::bytes + rb * sizeof(st)
-                                                        : zero_u32;
+                                // plain shared-memory pointers: the per-item offsets fold into
+                                // the loads as immediates
+                                const st *pa = ra < (uint32_t)WB
+                                                   ? reinterpret_cast<const st *>(groups + j * GG::bytes) + ra
+                                                   : reinterpret_cast<const st *>(zero_group);
+                                const st *pb = rb < (uint32_t)WB
+                                                   ? reinterpret_cast<const st *>(groups + (j + 1) * GG::bytes) + rb
+                                                   : reinterpret_cast<const st *>(zero_group);
 #pragma unroll
                                 for (int bi = 0; bi < BT; bi++) {
-                                    const float ta = tap_at<K>(aa + bi * GG::item_bytes, t2.x);
-                                    const float tb = tap_at<K>(ab + bi * GG::item_bytes, t2.y);
+                                    constexpr int IE = GG::item_bytes / (int)sizeof(st);
+                                    const float ta = pair_traits<K>::tap(pa[bi * IE], t2.x);
+                                    const float tb = pair_traits<K>::tap(pb[bi * IE], t2.y);
                                     acc2[bi] = __ffma2_rn(w2[j / 2], make_float2(ta, tb), acc2[bi]);
                                 }
                             }
                         } else {
-                            const unsigned char *groups = sm.ring + stage * SG::stage_bytes + (cl * SC) * GG::bytes;
 #pragma unroll
                             for (int j = 0; j < SC; j++) {
                                 const float tau = __fmaf_rn(g.rsq, g.rinv, ofs[j]);
@@ -1630,6 +1646,7 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                         const uint32_t gwin_u32 = gstage_u32 + (cl * SC * BT) * GW * 4;
                         float q = 0.f;
                         if (!any_ovf && (fixed || !p.gx)) {
+                            const unsigned char *groups = sm.ring + stage * SG::stage_bytes + (cl * SC) * GG::bytes;
                             // common case: every in-record tap is in its window
                             const float2 rsq2 = make_float2(gm.rsq, gm.rsq), rinv2 = make_float2(gm.rinv, gm.rinv);
 #pragma unroll
@@ -1644,20 +1661,22 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                                     const uint32_t mb = __float_as_uint(h ? mm2.y : mm2.x);
                                     const float t = h ? t2.y : t2.x;
                                     const uint32_t rr = mb - k0p[jj];
-                                    const uint32_t base =
-                                        rr < (uint32_t)WB ? groups_u32 + jj * GG::bytes + rr * sizeof(st) : zero_u32;
-                                    const uint32_t relc = min(rr, (uint32_t)WB);
-                                    const uint32_t gb = gwin_u32 + ((jj * BT) * GW + relc) * 4;
+                                    // plain shared-memory pointers: the per-item offsets fold
+                                    // into the load / atomic instructions as immediates
+                                    const st *tp = rr < (uint32_t)WB
+                                                       ? reinterpret_cast<const st *>(groups + jj * GG::bytes) + rr
+                                                       : reinterpret_cast<const st *>(zero_group);
+                                    int *gbp = gstage + (cl * SC * BT + jj * BT) * GW + min(rr, (uint32_t)WB);
                                     float2 sg = make_float2(sx[jj], 0.f);   // (sum g_b x0, sum g_b d)
 #pragma unroll
                                     for (int bi = 0; bi < BT; bi++) {
                                         float x0, d;
-                                        pair_x0_d<K>(base + bi * GG::item_bytes, x0, d);
+                                        pair_x0_d_ptr<K>(tp + bi * (GG::item_bytes / (int)sizeof(st)), x0, d);
                                         sg = __ffma2_rn(make_float2(g[bi], g[bi]), make_float2(x0, d), sg);
                                         if (p.gx) {
                                             const float as = g[bi] * gsw[jj];
-                                            red_shared_add(gb + bi * GW * 4, fix_round(as));
-                                            red_shared_add(gb + (bi * GW + GS) * 4, fix_round_fma(as, t));
+                                            atomicAdd(gbp + bi * GW, fix_round(as));
+                                            atomicAdd(gbp + bi * GW + GS, fix_round_fma(as, t));
                                         }
                                     }
                                     sx[jj] = sg.x;
