@@ -69,23 +69,26 @@ ffdas_error_t make_problem(const ffdas_tensor_desc &x, const ffdas_tensor_desc &
     return FFDAS_SUCCESS;
 }
 
-int select_storage(ffdas_datatype_t xt, ffdas_datatype_t ot, ffdas_compute_type_t ct) {
+int select_storage(ffdas_datatype_t xt, ffdas_datatype_t ot, ffdas_compute_type_t ct, int batch) {
     switch (xt) {
-        // 16-bit channel data is widened to FP32 pairs unless a 16-bit compute
-        // type asks for 16-bit pairs: the widening is exact, and the kernels
-        // are bound by instruction issue, not by the pair bytes, so FP32 pairs
-        // interpolate the 16-bit samples exactly and run the fewest
-        // instructions per tap (16-bit pairs halve the workspace instead).
+        // 16-bit channel data: both pair formats interpolate the 16-bit
+        // samples exactly (in FP32), so the choice is speed.  For one to a few
+        // items the kernels are bound by instruction issue and FP32 pairs need
+        // the fewest instructions per tap; for large batches (8 items or more
+        // per CTA) the per-tap arithmetic is shared and the pair bytes start
+        // to count, so the data keeps its 16-bit pairs.
         case FFDAS_R_16F:
             if (ot != FFDAS_R_32F) return -1;
             // reference: a half-precision compute request on half input is
             // rejected (das_alg1.cu:172-178)
             if (ct == FFDAS_COMPUTE_16F) return -1;
-            return ct == FFDAS_COMPUTE_16BF ? ST_BF16 : ST_F32;
+            if (ct == FFDAS_COMPUTE_16BF) return ST_BF16;
+            return (ct == FFDAS_COMPUTE_DEFAULT && batch >= 8) ? ST_F16 : ST_F32;
         case FFDAS_R_16BF:
             if (ot != FFDAS_R_32F) return -1;
             if (ct == FFDAS_COMPUTE_16F) return ST_F16;
-            return ct == FFDAS_COMPUTE_16BF ? ST_BF16 : ST_F32;
+            if (ct == FFDAS_COMPUTE_16BF) return ST_BF16;
+            return (ct == FFDAS_COMPUTE_DEFAULT && batch >= 8) ? ST_BF16 : ST_F32;
         case FFDAS_R_32F:
             if (ot != FFDAS_R_32F) return -1;
             if (ct == FFDAS_COMPUTE_16F) return ST_F16;
@@ -364,7 +367,7 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
     const ffdas_tensor_desc &xd = *a.x_desc;
     const ffdas_tensor_desc &od = *a.out_desc;
 
-    const int kind = select_storage(xd.dtype, od.dtype, a.compute_type);
+    const int kind = select_storage(xd.dtype, od.dtype, a.compute_type, xd.ndim == 4 ? (int)xd.dims[0] : 1);
     // dtype combination first (reference das.cu:40-82); compute-type
     // rejections are reported at the same code, after the dims checks below.
     const bool combo_ok =
@@ -575,7 +578,7 @@ extern "C" ffdas_error_t ffdas_das_static(uintptr_t stream, const float *srcpos,
     das_problem pb;
     FFDAS_TRY(make_problem(xd, od, pb));
     pb.n_events = pb.S;
-    const int kind = select_storage(xd.dtype, od.dtype, compute_type);
+    const int kind = select_storage(xd.dtype, od.dtype, compute_type, pb.B);
     if (kind < 0) return FFDAS_ERROR_UNSUPPORTED_TYPE;
     if (pb.N >= (1 << 22)) return FFDAS_ERROR_DIMS_TOO_LARGE;
     if (pb.V == 0 || pb.B == 0) return FFDAS_SUCCESS;

@@ -50,7 +50,8 @@ ffdas_error_t make_problem(const ffdas_tensor_desc &x, const ffdas_tensor_desc &
 
 // Storage kind for a (x dtype, out dtype, compute type), or -1 if the
 // combination is unsupported (FFDAS_ERROR_UNSUPPORTED_TYPE).
-int select_storage(ffdas_datatype_t xt, ffdas_datatype_t ot, ffdas_compute_type_t ct);
+// batch: items in x (dims[0] of 4-D x, else 1); it picks the 16-bit data layout.
+int select_storage(ffdas_datatype_t xt, ffdas_datatype_t ot, ffdas_compute_type_t ct, int batch);
 
 ffdas_error_t das_forward(ffdas_context &h, const das_call &a);
 

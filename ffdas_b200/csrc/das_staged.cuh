@@ -1550,8 +1550,10 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
     int *gslot = reinterpret_cast<int *>(sm.extra);                      // [kStages][kStWin][2][GS], window = group * BT + item
     float *cgrad = reinterpret_cast<float *>(gslot + kStages * kStWin * GW);  // [CC * 3][256]
     float *wmax = cgrad + CC * 3 * kStConsumers;                          // [kStWarps]
-    unsigned char *zero_group = reinterpret_cast<unsigned char *>(
-        (reinterpret_cast<uintptr_t>(wmax + kStWarps) + 15) & ~uintptr_t(15));
+    // zero group after the scratch, 16-byte aligned (offset arithmetic on the
+    // shared pointer keeps its address space visible to the compiler)
+    constexpr int kZeroOff = ((kStages * kStWin * GW + CC * 3 * kStConsumers + kStWarps) * 4 + 15) & ~15;
+    unsigned char *zero_group = sm.extra + kZeroOff;
     for (int i = threadIdx.x; i < kStages * kStWin * GW; i += kStThreads) gslot[i] = 0;
     for (int i = threadIdx.x; i < GG::data_bytes / 4; i += kStThreads) reinterpret_cast<uint32_t *>(zero_group)[i] = 0u;
     const staged_ctx cx = staged_setup<K, WB>(p, sm, true);   // ends with __syncthreads

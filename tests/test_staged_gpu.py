@@ -240,3 +240,14 @@ def test_default_planner_picks_staged_for_dense_volumes():
     info = h.last_kernel_info()
     assert info["variant"] == 2 and info["batch_tile"] == 4
     assert oracle.rel_l2(_np(out), _ref(af, af["x"])) < 2e-5
+
+
+@pytest.mark.parametrize("dtype,kind", [(torch.float16, 1), (torch.bfloat16, 2)])
+def test_large_16bit_batches_keep_16bit_pairs(dtype, kind):
+    # eight or more items: the 16-bit data stays in 16-bit pairs (bytes count
+    # once the per-tap arithmetic is shared); the image is the same
+    wl = W.ensemble(device=DEV, scale=0.1, frames=9, dtype=dtype)
+    x = wl["x"]
+    out, info = _run(wl, x, dict(variant=2, tile_x=32, tile_y=8, window=64, batch_tile=8))
+    assert info["storage"] == kind and info["batch_tile"] == 8
+    assert oracle.rel_l2(_np(out), _ref(wl, x)) < 2e-5
