@@ -83,12 +83,12 @@ int select_storage(ffdas_datatype_t xt, ffdas_datatype_t ot, ffdas_compute_type_
             // rejected (das_alg1.cu:172-178)
             if (ct == FFDAS_COMPUTE_16F) return -1;
             if (ct == FFDAS_COMPUTE_16BF) return ST_BF16;
-            return (ct == FFDAS_COMPUTE_DEFAULT && batch >= 8) ? ST_F16 : ST_F32;
+            return batch >= 8 ? ST_F16 : ST_F32;   // default or FP32 compute: both formats compute in FP32
         case FFDAS_R_16BF:
             if (ot != FFDAS_R_32F) return -1;
             if (ct == FFDAS_COMPUTE_16F) return ST_F16;
             if (ct == FFDAS_COMPUTE_16BF) return ST_BF16;
-            return (ct == FFDAS_COMPUTE_DEFAULT && batch >= 8) ? ST_BF16 : ST_F32;
+            return batch >= 8 ? ST_BF16 : ST_F32;
         case FFDAS_R_32F:
             if (ot != FFDAS_R_32F) return -1;
             if (ct == FFDAS_COMPUTE_16F) return ST_F16;

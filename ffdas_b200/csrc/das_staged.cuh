@@ -1441,15 +1441,19 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
                 if (!dead) {
                     // flush the stage's gradient slots: one red.add per touched sample
                     if (p.gx && fixed) {
-                        for (int i = cx.tid; i < kStWin * GS; i += kStConsumers) {
-                            const int val = gstage[i];
+                        // eight threads per window, bins r0, r0 + 8, ...: no division in the loop
+                        static_assert(kStConsumers == kStWin * 8, "flush layout: eight threads per window");
+                        const int win = cx.tid >> 3, r0 = cx.tid & 7;
+                        const int cl = win / SC, j = win % SC;
+                        const int kw = (int)(sm.meta[stage * kStWin + win] - kFloorMagicBits);
+                        float *grow = p.gx + (((int64_t)cx.b * p.C + (c0 + cl)) * p.S + (e0 + j)) * p.N;
+                        int *bins = gstage + win * GS;
+#pragma unroll
+                        for (int r = r0; r < GS; r += 8) {
+                            const int val = bins[r];
                             if (val != 0) {
-                                gstage[i] = 0;
-                                const int win = i / GS, r = i - win * GS;
-                                const int cl = win / SC, j = win % SC;
-                                const int k = (int)(sm.meta[stage * kStWin + win] - kFloorMagicBits) + r;
-                                float *gr = p.gx + (((int64_t)cx.b * p.C + (c0 + cl)) * p.S + (e0 + j)) * p.N + k;
-                                atomicAdd(gr, (float)val * finv);
+                                bins[r] = 0;
+                                atomicAdd(grow + kw + r, (float)val * finv);
                             }
                         }
                     }
@@ -1570,8 +1574,12 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
         gmax = fmaxf(gmax, fabsf(g[bi]));
     }
     bool gbad = false;
+    float2 g2[BT];   // (g_b, g_b) for the packed sample / slope sums
 #pragma unroll
-    for (int bi = 0; bi < BT; bi++) gbad |= !(fabsf(g[bi]) <= 3.0e38f);
+    for (int bi = 0; bi < BT; bi++) {
+        gbad |= !(fabsf(g[bi]) <= 3.0e38f);
+        g2[bi] = make_float2(g[bi], g[bi]);
+    }
     const bool want_pos = p.gdst != nullptr || p.gsrc != nullptr;
     float gpx = 0.f, gpy = 0.f, gpz = 0.f;
     int stage = 0;
@@ -1670,15 +1678,22 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                                                        : reinterpret_cast<const st *>(zero_group);
                                     int *gbp = gstage + (cl * SC * BT + jj * BT) * GW + min(rr, (uint32_t)WB);
                                     float2 sg = make_float2(sx[jj], 0.f);   // (sum g_b x0, sum g_b d)
+                                    if (p.gx) {
 #pragma unroll
-                                    for (int bi = 0; bi < BT; bi++) {
-                                        float x0, d;
-                                        pair_x0_d_ptr<K>(tp + bi * (GG::item_bytes / (int)sizeof(st)), x0, d);
-                                        sg = __ffma2_rn(make_float2(g[bi], g[bi]), make_float2(x0, d), sg);
-                                        if (p.gx) {
+                                        for (int bi = 0; bi < BT; bi++) {
+                                            float x0, d;
+                                            pair_x0_d_ptr<K>(tp + bi * (GG::item_bytes / (int)sizeof(st)), x0, d);
+                                            sg = __ffma2_rn(g2[bi], make_float2(x0, d), sg);
                                             const float as = g[bi] * gsw[jj];
                                             atomicAdd(gbp + bi * GW, fix_round(as));
                                             atomicAdd(gbp + bi * GW + GS, fix_round_fma(as, t));
+                                        }
+                                    } else {
+#pragma unroll
+                                        for (int bi = 0; bi < BT; bi++) {
+                                            float x0, d;
+                                            pair_x0_d_ptr<K>(tp + bi * (GG::item_bytes / (int)sizeof(st)), x0, d);
+                                            sg = __ffma2_rn(g2[bi], make_float2(x0, d), sg);
                                         }
                                     }
                                     sx[jj] = sg.x;
@@ -1751,22 +1766,26 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                 if (!dead) {
                     if (p.gx && fixed) {
                         // bins 0..WB-1 of each window: gx[k] += A - T, gx[k+1] += T for 0 <= k <= N-2;
-                        // every bin (the out-of-window one too) is cleared for the stage's next use
-                        for (int i = cx.tid; i < kStWin * GS; i += kStConsumers) {
-                            const int win = i / GS, r = i - win * GS;
-                            int *bin = gstage + win * GW + r;
-                            const int va = bin[0], vt = bin[GS];
+                        // every bin (the out-of-window one too) is cleared for the stage's next use.
+                        // Eight threads per window, bins r0, r0 + 8, ...: no division in the loop.
+                        static_assert(kStConsumers == kStWin * 8, "flush layout: eight threads per window");
+                        const int win = cx.tid >> 3, r0 = cx.tid & 7;
+                        const int grp = win / BT, bi = win % BT;
+                        const int cl = grp / SC, j = grp % SC;
+                        const int kw = (int)(sm.meta[stage * kStWin + grp] - kFloorMagicBits);
+                        const bool live = b0 + bi < p.B;
+                        float *grow = p.gx + (((int64_t)(b0 + bi) * p.C + (c0 + cl)) * p.S + (e0 + j)) * p.N;
+                        int *bins = gstage + win * GW;
+#pragma unroll
+                        for (int r = r0; r < GS; r += 8) {
+                            const int va = bins[r], vt = bins[GS + r];
                             if ((va | vt) != 0) {
-                                bin[0] = 0;
-                                bin[GS] = 0;
-                                const int grp = win / BT, bi = win % BT;
-                                const int cl = grp / SC, j = grp % SC;
-                                const int k = (int)(sm.meta[stage * kStWin + grp] - kFloorMagicBits) + r;
-                                if (r < WB && b0 + bi < p.B && k >= 0 && k <= p.N - 2) {
-                                    float *gr = p.gx + (((int64_t)(b0 + bi) * p.C + (c0 + cl)) * p.S + (e0 + j)) * p.N + k;
-                                    const float a1 = (float)vt * finv;
-                                    atomicAdd(gr, (float)(va - vt) * finv);
-                                    atomicAdd(gr + 1, a1);
+                                bins[r] = 0;
+                                bins[GS + r] = 0;
+                                const int k = kw + r;
+                                if (r < WB && live && k >= 0 && k <= p.N - 2) {
+                                    atomicAdd(grow + k, (float)(va - vt) * finv);
+                                    atomicAdd(grow + k + 1, (float)vt * finv);
                                 }
                             }
                         }
