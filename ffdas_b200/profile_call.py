@@ -1,0 +1,55 @@
+"""Run one delay-and-sum workload under a fixed schedule, for profilers.
+
+    python -m ffdas_b200.profile_call ensemble --frames 50 --calls 4 \\
+        --schedule '{"variant": 2, "tile_x": 32, "tile_y": 8, "window": 64, "batch_tile": 8}'
+
+Builds the named synthetic workload (ffdas_b200.workloads.CONFIGS), applies the
+schedule to the device's library handle, calls das / das_sparse `--calls`
+times (the first calls warm the kernel attributes and the memory pool), and
+prints the last call's kernel info.  `--backward` runs ffdas_das_backward
+instead (random output gradient).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import torch
+
+from . import workloads as W
+from .das import das, das_sparse
+from .library import get_library_handle
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("workload", choices=sorted(W.CONFIGS))
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--frames", type=int, default=None, help="ensemble: number of frames")
+    ap.add_argument("--calls", type=int, default=4)
+    ap.add_argument("--schedule", default=None, help="JSON ffdas_das_config_t fields")
+    ap.add_argument("--backward", action="store_true")
+    args = ap.parse_args()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    kw = {"frames": args.frames} if args.frames is not None else {}
+    wl = W.CONFIGS[args.workload](device=dev, scale=args.scale, **kw)
+    h = get_library_handle(dev)
+    h.set_config(json.loads(args.schedule) if args.schedule else None)
+    geo = (wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"])
+    x = wl["x"]
+    for _ in range(args.calls):
+        if args.backward:
+            xg = x.float().requires_grad_(True)
+            out = das(xg, *geo)
+            out.backward(torch.ones_like(out))
+        elif "sparse_indices" in wl:
+            das_sparse(x, *geo, wl["sparse_indices"])
+        else:
+            das(x, *geo)
+    torch.cuda.synchronize()
+    print(json.dumps(h.last_kernel_info()))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
