@@ -461,14 +461,30 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
     const bool staged = s.variant == 2;
     if (staged) {
         const int bchunks_st = (pb.B + s.BT - 1) / s.BT;
+        // Small problems (fewer CTAs than the target of min_blocks, default 3,
+        // per SM): split each tile's channels over blockIdx.z slices of 32+
+        // channels that add into the image, so every SM has work.
+        int csplit = 1;
+        {
+            const int per_sm = (h.has_config && h.config.min_blocks) ? h.config.min_blocks : 3;
+            const int64_t ctas = tiles * bchunks_st;
+            const int64_t want = (int64_t)std::max(h.sm_count, 1) * per_sm;
+            while (ctas * csplit * 2 <= want && pb.C >= 64 * csplit && csplit < 64) csplit *= 2;
+        }
+        if (csplit > 1) {
+            const int chunk = ((pb.C + csplit - 1) / csplit + 31) / 32 * 32;   // whole stages of channels
+            csplit = (pb.C + chunk - 1) / chunk;
+            gp.cchunk = csplit > 1 ? chunk : 0;
+        }
         h.last.variant = 2;
         h.last.batch_tile = s.BT;
         h.last.event_chunk = s.SC;
-        h.last.grid = tiles * bchunks_st;
+        h.last.grid = tiles * bchunks_st * csplit;
+        h.last.kernels = csplit > 1 ? 3 : 2;   // ingest, (image preparation,) delay-and-sum
         if (bchunks_st > 65535) return FFDAS_ERROR_DIMS_TOO_LARGE;
         h.mark_start();
         const ffdas_error_t err = launch_staged(h, pb, kind, gp, s.SC, s.WB, s.BT, s.copy,
-                                                dim3((unsigned)tiles, (unsigned)bchunks_st));
+                                                dim3((unsigned)tiles, (unsigned)bchunks_st, (unsigned)csplit));
         h.mark_stop();
         return err;
     }

@@ -39,6 +39,7 @@ struct gather_params {
     int64_t out_bstride;      // elements between batch items of out
     double beta_re, beta_im;
     int beta_zero;
+    int cchunk;               // staged forward: channels per blockIdx.z slice (0: no split)
 };
 
 template <typename A> struct acc_ops;

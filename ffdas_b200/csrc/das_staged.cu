@@ -8,6 +8,7 @@
 // libcuda.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 
@@ -209,11 +210,19 @@ static staged_params base_params(ffdas_context &h, const das_problem &pb, const 
     sp.beta_re = gp.beta_re; sp.beta_zero = gp.beta_zero;
     sp.status = h.status;
     sp.debug_drop_stage = ffdas_take_debug_drop_stage();
+    sp.cchunk = gp.cchunk;
     return sp;
 }
 
 ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp, int SC,
                             int WB, int BT, int copy, dim3 grid) {
+    if (gp.cchunk) {   // channel slices add into the image: prepare it (beta * out, or 0)
+        if (grid.z < 2) return FFDAS_ERROR_INTERNAL;
+        dim3 sg((unsigned)((pb.V + 255) / 256), (unsigned)std::min(pb.B, 65535));
+        scale_image_kernel<<<sg, 256, 0, h.stream>>>(static_cast<float *>(gp.out), pb.out_bstride, pb.V, pb.B,
+                                                     (float)gp.beta_re, gp.beta_zero);
+        FFDAS_TRY(ffdas_launch_check(h.stream));
+    }
     if (BT > 1) copy = 1;   // batch tiles stage their windows with 3-D TMA boxes
     copy = resolve_copy(copy);
     if (BT > 1 && copy != 1) return FFDAS_ERROR_CUDA_DRIVER;

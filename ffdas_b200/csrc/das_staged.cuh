@@ -60,6 +60,7 @@ struct staged_params {
     int *status;
     int debug_drop_stage;  // test hook: the producer never fills the first stage
     int copy_async;        // 1: windows staged by per-lane cp.async copies instead of TMA tile loads
+    int cchunk;            // forward: channels per blockIdx.z slice (0: all channels in one CTA)
     // adjoint only
     const float *gout;
     int64_t gout_bstride;
@@ -243,6 +244,13 @@ struct staged_smem {
         extra = reinterpret_cast<unsigned char *>(chan_pair + kStages * kStWin * 2);
     }
 };
+
+// Channel range of this CTA: the forward kernels may split the channels of a
+// tile over blockIdx.z (small problems), each slice adding into the image.
+__device__ __forceinline__ int chan_begin(const staged_params &p) { return p.cchunk ? (int)blockIdx.z * p.cchunk : 0; }
+__device__ __forceinline__ int chan_end(const staged_params &p) {
+    return p.cchunk ? min(p.C, ((int)blockIdx.z + 1) * p.cchunk) : p.C;
+}
 
 // Per-CTA state common to both kernels.
 struct staged_ctx {
@@ -466,6 +474,7 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
                                                uint32_t &issued_mask) {
     using SG = slot_geom<WB, K>;
     using st = typename pair_traits<K>::storage;
+    const int cend = chan_end(p);
     const uint32_t full_bar = smem_u32(&sm.full[stage]);
     const uint32_t empty_bar = smem_u32(&sm.empty[stage]);
     unsigned char *stage_base = sm.ring + stage * SG::stage_bytes;
@@ -483,7 +492,7 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
         const int bb = cx.b;   // batch item of the CTA
         uint32_t m = kZeroWindow;  // every tap index clamps to the zero pair
         float px = 0.f, py = 0.f, pz = 0.f;
-        if (c < p.C) {
+        if (c < cend) {
             px = __ldg(p.srcpos + 3 * c);
             py = __ldg(p.srcpos + 3 * c + 1);
             pz = __ldg(p.srcpos + 3 * c + 2);
@@ -493,9 +502,9 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
             sm.chan_pair[(stage * kStWin + cl) * 2] = make_float4(px, px, py, py);
             sm.chan_pair[(stage * kStWin + cl) * 2 + 1] = make_float4(pz, pz, 0.f, 0.f);
             if (p.srcdir)
-                sm.chan_dir[stage * kStWin + cl] = (c < p.C) ? __ldg(p.srcdir + c) : make_float4(0, 0, 0, 2.f);
+                sm.chan_dir[stage * kStWin + cl] = (c < cend) ? __ldg(p.srcdir + c) : make_float4(0, 0, 0, 2.f);
         }
-        if (c < p.C && j < sc) {
+        if (c < cend && j < sc) {
             const float *ab = sm.aabb;
             const float dx = fmaxf(fmaxf(ab[0] - px, px - ab[3]), 0.f);
             const float dy = fmaxf(fmaxf(ab[1] - py, py - ab[4]), 0.f);
@@ -715,7 +724,7 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
             w2[j / 2] = make_float2(w[j], w[j + 1]);
         }
 
-        for (int c0 = 0; c0 < p.C; c0 += CC) {
+        for (int c0 = chan_begin(p); c0 < chan_end(p); c0 += CC) {
             if (cx.producer) {
                 staged_produce<K, WB, SC>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
             } else {
@@ -808,7 +817,8 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
     if (cx.active && !dead) {
         acc += acc2.x + acc2.y;
         float *o = static_cast<float *>(p.out) + (int64_t)cx.b * p.out_bstride + cx.v;
-        *o = p.beta_zero ? acc : __fmaf_rn((float)p.beta_re, *o, acc);
+        if (p.cchunk) atomicAdd(o, acc);   // channel slices add into the prepared image
+        else *o = p.beta_zero ? acc : __fmaf_rn((float)p.beta_re, *o, acc);
     }
 }
 
@@ -854,7 +864,7 @@ __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kerne
         float2 ofs2[SC], w2[SC];
         staged_pass_begin2<K, WB, SC>(p, sm, cx, e0, sc, ofs2, w2);
 
-        for (int c0 = 0; c0 < p.C; c0 += CC) {
+        for (int c0 = chan_begin(p); c0 < chan_end(p); c0 += CC) {
             if (cx.producer) {
                 staged_produce<K, WB, SC>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
             } else {
@@ -982,8 +992,13 @@ __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kerne
     }
     if (dead) return;
     float *o = static_cast<float *>(p.out) + (int64_t)cx.b * p.out_bstride;
-    if (cx.active) o[cx.v] = p.beta_zero ? acc2.x : __fmaf_rn((float)p.beta_re, o[cx.v], acc2.x);
-    if (cx.active2) o[cx.v2] = p.beta_zero ? acc2.y : __fmaf_rn((float)p.beta_re, o[cx.v2], acc2.y);
+    if (p.cchunk) {   // channel slices add into the prepared image
+        if (cx.active) atomicAdd(o + cx.v, acc2.x);
+        if (cx.active2) atomicAdd(o + cx.v2, acc2.y);
+    } else {
+        if (cx.active) o[cx.v] = p.beta_zero ? acc2.x : __fmaf_rn((float)p.beta_re, o[cx.v], acc2.x);
+        if (cx.active2) o[cx.v2] = p.beta_zero ? acc2.y : __fmaf_rn((float)p.beta_re, o[cx.v2], acc2.y);
+    }
 }
 
 // ------------------------------------------------- forward, batch tiles ---
@@ -1003,6 +1018,7 @@ __device__ __forceinline__ void staged_produce_batch(const staged_params &p, con
                                                      uint32_t &issued_mask) {
     using SG = slot_geom<WB, K>;
     using GG = group_geom<WB, K, BT>;
+    const int cend = chan_end(p);
     const uint32_t full_bar = smem_u32(&sm.full[stage]);
     const uint32_t empty_bar = smem_u32(&sm.empty[stage]);
     const uint32_t stage_u32 = smem_u32(sm.ring + stage * SG::stage_bytes);
@@ -1017,7 +1033,7 @@ __device__ __forceinline__ void staged_produce_batch(const staged_params &p, con
         const int c = c0 + cl;
         uint32_t m = kZeroWindow;
         float px = 0.f, py = 0.f, pz = 0.f;
-        if (c < p.C) {
+        if (c < cend) {
             px = __ldg(p.srcpos + 3 * c);
             py = __ldg(p.srcpos + 3 * c + 1);
             pz = __ldg(p.srcpos + 3 * c + 2);
@@ -1025,9 +1041,9 @@ __device__ __forceinline__ void staged_produce_batch(const staged_params &p, con
         if (j == 0) {
             sm.chan_pos[stage * kStWin + cl] = make_float4(px, py, pz, 0.f);
             if (p.srcdir)
-                sm.chan_dir[stage * kStWin + cl] = (c < p.C) ? __ldg(p.srcdir + c) : make_float4(0, 0, 0, 2.f);
+                sm.chan_dir[stage * kStWin + cl] = (c < cend) ? __ldg(p.srcdir + c) : make_float4(0, 0, 0, 2.f);
         }
-        if (c < p.C && j < sc) {
+        if (c < cend && j < sc) {
             const float *ab = sm.aabb;
             const float dx = fmaxf(fmaxf(ab[0] - px, px - ab[3]), 0.f);
             const float dy = fmaxf(fmaxf(ab[1] - py, py - ab[4]), 0.f);
@@ -1111,7 +1127,7 @@ __global__ void __launch_bounds__(kStThreads) das_staged_batch_kernel(const stag
             w2[j / 2] = make_float2(w[j], w[j + 1]);
         }
 
-        for (int c0 = 0; c0 < p.C; c0 += CC) {
+        for (int c0 = chan_begin(p); c0 < chan_end(p); c0 += CC) {
             if (cx.producer) {
                 staged_produce_batch<K, WB, SC, BT>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
             } else {
@@ -1207,7 +1223,8 @@ __global__ void __launch_bounds__(kStThreads) das_staged_batch_kernel(const stag
         if (bb < p.B) {
             float *o = static_cast<float *>(p.out) + (int64_t)bb * p.out_bstride + cx.v;
             const float acc = acc2[bi].x + acc2[bi].y;
-            *o = p.beta_zero ? acc : __fmaf_rn((float)p.beta_re, *o, acc);
+            if (p.cchunk) atomicAdd(o, acc);   // channel slices add into the prepared image
+            else *o = p.beta_zero ? acc : __fmaf_rn((float)p.beta_re, *o, acc);
         }
     }
 }
@@ -1846,6 +1863,18 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
             p.gdst[3 * cx.v + 1] = gpy;
             p.gdst[3 * cx.v + 2] = gpz;
         }
+    }
+}
+
+// Prepares the image for channel slices that add into it: out = beta * out
+// (or 0) for every batch item and voxel.
+__global__ void __launch_bounds__(256) scale_image_kernel(float *out, int64_t bstride, int64_t V, int B,
+                                                          float beta, int beta_zero) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V) return;
+    for (int b = blockIdx.y; b < B; b += gridDim.y) {
+        float *o = out + (int64_t)b * bstride + i;
+        *o = beta_zero ? 0.f : beta * *o;
     }
 }
 

@@ -144,7 +144,8 @@ typedef struct {
     int32_t tile_z;       /* ... along the outermost spatial dim */
     int32_t batch_tile;   /* batch items per thread (1,2,4,8,16) */
     int32_t event_chunk;  /* events held in registers per pass (1..16) */
-    int32_t min_blocks;   /* CTAs per SM hint (occupancy) */
+    int32_t min_blocks;   /* staged forward: target CTAs per SM; problems with fewer tiles split
+                             each tile's channels over CTAs that add into the image (default 3) */
     int32_t window;       /* TMA-staged kernel: pairs per staged window (32 or 64) */
     int32_t copy_engine;  /* staged kernels: 0 auto, 1 TMA tile loads, 2 per-thread cp.async copies */
 } ffdas_das_config_t;
