@@ -70,3 +70,95 @@ class DASRunner:
             self.x.copy_(x, non_blocking=True)
         out = self.replay()
         return out.clone() if clone else out
+
+
+class DASStream:
+    """Pipelined delay-and-sum over a sequence of frames from host memory.
+
+        stream = DASStream(x_example, srcpos, dstpos, offsets, weights)     # tunes once
+        images = stream.run(frames)                # frames: pinned host tensors
+        stream.run(frames, outputs=images)         # or write into pinned host outputs
+
+    Per frame: host-to-device copy of the channel data, das / das_sparse, and
+    device-to-host copy of the image.  Copies run on a copy stream and the
+    beamformer on a compute stream, with `depth` (default 2) device buffers in
+    rotation, so frame i+1's upload and frame i-1's download overlap frame
+    i's delay-and-sum; the call returns when every image is in host memory.
+    Geometry is fixed for the stream's lifetime, as for DASRunner.
+    """
+
+    def __init__(self, x, srcpos, dstpos, offsets, weights, sparse_indices=None, *, depth: int = 2,
+                 srcdir=None, wavenum: float = 0.0, use_fp16: bool = False, use_bf16: bool = False,
+                 tune: bool = True, config: dict | None = None):
+        if not x.is_cuda:
+            raise ValueError("DASStream needs an example of the channel data on the GPU")
+        if depth < 1:
+            raise ValueError("depth must be >= 1")
+        self.device = x.device
+        self.depth = depth
+        self._geom = dict(srcpos=srcpos.contiguous(), dstpos=dstpos.contiguous(), offsets=offsets.contiguous(),
+                          weights=weights.contiguous())
+        self._idx = sparse_indices.contiguous() if sparse_indices is not None else None
+        self._kw = dict(srcdir=srcdir, wavenum=wavenum, use_fp16=use_fp16, use_bf16=use_bf16)
+        if config is None and tune:
+            config = autotune(x.contiguous(), *self._geom.values(), sparse_indices=self._idx, use_fp16=use_fp16,
+                              use_bf16=use_bf16)["config"]
+        self.config = config
+        self.handle = get_library_handle(self.device)
+        self.copy_stream = torch.cuda.Stream(self.device)
+        self.compute_stream = torch.cuda.Stream(self.device)
+        self.x_dev = [torch.empty_like(x, memory_format=torch.contiguous_format) for _ in range(depth)]
+        self.out_dev = [None] * depth
+        self.ev_in = [torch.cuda.Event() for _ in range(depth)]     # upload of the slot's frame done
+        self.ev_done = [torch.cuda.Event() for _ in range(depth)]   # its delay-and-sum done
+        self.ev_out = [torch.cuda.Event() for _ in range(depth)]    # its image downloaded
+        self._used = [False] * depth
+
+    def _beamform(self, xd, out):
+        g = self._geom
+        with torch.no_grad():
+            if self._idx is None:
+                return das(xd, g["srcpos"], g["dstpos"], g["offsets"], g["weights"], out=out, **self._kw)
+            return das_sparse(xd, g["srcpos"], g["dstpos"], g["offsets"], g["weights"], self._idx, out=out,
+                              **self._kw)
+
+    def run(self, frames, outputs=None) -> list:
+        """Beamform `frames` (host tensors, pinned for asynchronous copies).
+
+        Writes image i into outputs[i] (pinned host tensors of the image's shape)
+        or into newly allocated pinned tensors, and returns the list."""
+        frames = list(frames)
+        if outputs is not None and len(outputs) != len(frames):
+            raise ValueError("need one output per frame")
+        outs = list(outputs) if outputs is not None else [None] * len(frames)
+        cs, ks = self.copy_stream, self.compute_stream
+        # the caller's prior work on the current stream comes first
+        cur = torch.cuda.current_stream(self.device)
+        cs.wait_stream(cur)
+        ks.wait_stream(cur)
+        for i, xh in enumerate(frames):
+            s = i % self.depth
+            if self._used[s]:
+                # the slot's previous frame has been read by its compute and its
+                # image has left out_dev[s] before either is overwritten
+                cs.wait_event(self.ev_done[s])
+                ks.wait_event(self.ev_out[s])
+            with torch.cuda.stream(cs):
+                self.x_dev[s].copy_(xh, non_blocking=True)
+                self.ev_in[s].record(cs)
+            ks.wait_event(self.ev_in[s])
+            with torch.cuda.stream(ks):
+                self.handle.set_config(self.config)
+                self.out_dev[s] = self._beamform(self.x_dev[s], self.out_dev[s])
+                self.ev_done[s].record(ks)
+            if outs[i] is None:
+                outs[i] = torch.empty(self.out_dev[s].shape, dtype=self.out_dev[s].dtype, pin_memory=True)
+            cs.wait_event(self.ev_done[s])
+            with torch.cuda.stream(cs):
+                outs[i].copy_(self.out_dev[s], non_blocking=True)
+                self.ev_out[s].record(cs)
+            self._used[s] = True
+        for s in range(self.depth):
+            if self._used[s]:
+                self.ev_out[s].synchronize()
+        return outs
