@@ -320,7 +320,7 @@ def run_ours(args, rank, world) -> dict:
     eb = torch.cuda.Event(enable_timing=True)
     ea.record(stream)
     pipe.run([xh] * args.steps, outs[:args.steps])
-    stream.wait_stream(pipe.copy_stream)
+    stream.wait_stream(pipe.download_stream)
     eb.record(stream)
     torch.cuda.synchronize()
     ms_e2e = ea.elapsed_time(eb) / args.steps

@@ -80,10 +80,10 @@ class DASStream:
         stream.run(frames, outputs=images)         # or write into pinned host outputs
 
     Per frame: host-to-device copy of the channel data, das / das_sparse, and
-    device-to-host copy of the image.  Copies run on a copy stream and the
-    beamformer on a compute stream, with `depth` (default 2) device buffers in
-    rotation, so frame i+1's upload and frame i-1's download overlap frame
-    i's delay-and-sum; the call returns when every image is in host memory.
+    device-to-host copy of the image.  Uploads, the beamformer and downloads
+    run on three streams, with `depth` (default 2) device buffers in rotation,
+    so frame i+1's upload and frame i-1's download overlap frame i's
+    delay-and-sum; the call returns when every image is in host memory.
     Geometry is fixed for the stream's lifetime, as for DASRunner.
     """
 
@@ -105,8 +105,9 @@ class DASStream:
                               use_bf16=use_bf16)["config"]
         self.config = config
         self.handle = get_library_handle(self.device)
-        self.copy_stream = torch.cuda.Stream(self.device)
+        self.upload_stream = torch.cuda.Stream(self.device)
         self.compute_stream = torch.cuda.Stream(self.device)
+        self.download_stream = torch.cuda.Stream(self.device)
         self.x_dev = [torch.empty_like(x, memory_format=torch.contiguous_format) for _ in range(depth)]
         self.out_dev = [None] * depth
         self.ev_in = [torch.cuda.Event() for _ in range(depth)]     # upload of the slot's frame done
@@ -131,21 +132,21 @@ class DASStream:
         if outputs is not None and len(outputs) != len(frames):
             raise ValueError("need one output per frame")
         outs = list(outputs) if outputs is not None else [None] * len(frames)
-        cs, ks = self.copy_stream, self.compute_stream
+        us, ks, ds = self.upload_stream, self.compute_stream, self.download_stream
         # the caller's prior work on the current stream comes first
         cur = torch.cuda.current_stream(self.device)
-        cs.wait_stream(cur)
-        ks.wait_stream(cur)
+        for st in (us, ks, ds):
+            st.wait_stream(cur)
         for i, xh in enumerate(frames):
             s = i % self.depth
             if self._used[s]:
                 # the slot's previous frame has been read by its compute and its
                 # image has left out_dev[s] before either is overwritten
-                cs.wait_event(self.ev_done[s])
+                us.wait_event(self.ev_done[s])
                 ks.wait_event(self.ev_out[s])
-            with torch.cuda.stream(cs):
+            with torch.cuda.stream(us):
                 self.x_dev[s].copy_(xh, non_blocking=True)
-                self.ev_in[s].record(cs)
+                self.ev_in[s].record(us)
             ks.wait_event(self.ev_in[s])
             with torch.cuda.stream(ks):
                 self.handle.set_config(self.config)
@@ -153,10 +154,10 @@ class DASStream:
                 self.ev_done[s].record(ks)
             if outs[i] is None:
                 outs[i] = torch.empty(self.out_dev[s].shape, dtype=self.out_dev[s].dtype, pin_memory=True)
-            cs.wait_event(self.ev_done[s])
-            with torch.cuda.stream(cs):
+            ds.wait_event(self.ev_done[s])
+            with torch.cuda.stream(ds):
                 outs[i].copy_(self.out_dev[s], non_blocking=True)
-                self.ev_out[s].record(cs)
+                self.ev_out[s].record(ds)
             self._used[s] = True
         for s in range(self.depth):
             if self._used[s]:
