@@ -31,6 +31,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <type_traits>
 #include "das_gather.cuh"
 
 namespace ffdas {
@@ -199,6 +200,21 @@ constexpr size_t staged_bwd_smem_bytes() {
 
 __device__ __forceinline__ void red_shared_add(uint32_t addr, int v) {
     asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+// red.shared.add.s32 at addr + OFF bytes (OFF an immediate): no result
+// register, and the offset folds into the instruction.
+template <int OFF>
+__device__ __forceinline__ void red_shared_add_at(uint32_t addr, int v) {
+    asm volatile("red.shared.add.s32 [%0+%2], %1;" ::"r"(addr), "r"(v), "n"(OFF) : "memory");
+}
+
+// Calls f(std::integral_constant<int, I>) for I = 0 .. N-1 (compile-time loop).
+template <int I, int N, class F>
+__device__ __forceinline__ void static_for(F &&f) {
+    if constexpr (I < N) {
+        f(std::integral_constant<int, I>{});
+        static_for<I + 1, N>(f);
+    }
 }
 
 // Fixed point for the adjoint's shared gradient slots: a value |v| <= 2^22
@@ -1693,18 +1709,18 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                                     const st *tp = rr < (uint32_t)WB
                                                        ? reinterpret_cast<const st *>(groups + jj * GG::bytes) + rr
                                                        : reinterpret_cast<const st *>(zero_group);
-                                    int *gbp = gstage + (cl * SC * BT + jj * BT) * GW + min(rr, (uint32_t)WB);
+                                    const uint32_t gb = gwin_u32 + ((jj * BT) * GW + min(rr, (uint32_t)WB)) * 4;
                                     float2 sg = make_float2(sx[jj], 0.f);   // (sum g_b x0, sum g_b d)
                                     if (p.gx) {
-#pragma unroll
-                                        for (int bi = 0; bi < BT; bi++) {
+                                        static_for<0, BT>([&](auto bic) {
+                                            constexpr int bi = decltype(bic)::value;
                                             float x0, d;
                                             pair_x0_d_ptr<K>(tp + bi * (GG::item_bytes / (int)sizeof(st)), x0, d);
                                             sg = __ffma2_rn(g2[bi], make_float2(x0, d), sg);
                                             const float as = g[bi] * gsw[jj];
-                                            atomicAdd(gbp + bi * GW, fix_round(as));
-                                            atomicAdd(gbp + bi * GW + GS, fix_round_fma(as, t));
-                                        }
+                                            red_shared_add_at<bi * GW * 4>(gb, fix_round(as));
+                                            red_shared_add_at<(bi * GW + GS) * 4>(gb, fix_round_fma(as, t));
+                                        });
                                     } else {
 #pragma unroll
                                         for (int bi = 0; bi < BT; bi++) {
