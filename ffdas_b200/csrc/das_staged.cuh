@@ -208,20 +208,6 @@ __device__ __forceinline__ void red_shared_add_at(uint32_t addr, int v) {
     asm volatile("red.shared.add.s32 [%0+%2], %1;" ::"r"(addr), "r"(v), "n"(OFF) : "memory");
 }
 
-// 64-bit shared reduction at addr + OFF bytes: adds (a << 32) + t, i.e. the
-// pair (a, t) of a fixed-point bin in one instruction; the 64-bit sum is
-// exact, and the flush recovers t from the low word (sign-extended) and a
-// from the rest, while |sum a|, |sum t| < 2^31.
-template <int OFF>
-__device__ __forceinline__ void red_shared_add_pair_at(uint32_t addr, int a, int t) {
-    const long long v = ((long long)a << 32) + (long long)t;
-    asm volatile("red.shared.add.u64 [%0+%2], %1;" ::"r"(addr), "l"(v), "n"(OFF) : "memory");
-}
-__device__ __forceinline__ void red_shared_add_pair(uint32_t addr, int a, int t) {
-    const long long v = ((long long)a << 32) + (long long)t;
-    asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(addr), "l"(v) : "memory");
-}
-
 // Calls f(std::integral_constant<int, I>) for I = 0 .. N-1 (compile-time loop).
 template <int I, int N, class F>
 __device__ __forceinline__ void static_for(F &&f) {
@@ -1572,10 +1558,9 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
 // and position gradients, and the fixed-point scatter of g_b w (1 - t), g_b w t
 // into the item's gradient slot.  amax = max_b |g_b| * max_j |w_j| over the tile.
 //
-// The slot of a window holds one 64-bit fixed-point bin per sample k of the
-// window carrying a pair: A[k] += g_b w and T[k] += g_b w t for a tap at k
-// (one red.shared.add.u64 of (A << 32) + T), so that the flush adds
-// A[k] - T[k] to gx[k] and T[k] to gx[k+1] -- for 0 <= k <= N-2 only.
+// The slot of a window holds two fixed-point bin arrays per sample k of the
+// window: A[k] += g_b w and T[k] += g_b w t for a tap at k, so that the flush
+// adds A[k] - T[k] to gx[k] and T[k] to gx[k+1] -- for 0 <= k <= N-2 only.
 // A tap outside the record therefore needs no test in the loop (its bins are
 // dropped at the flush), and a tap outside its window (always outside the
 // record) lands in the bin past the window, which the flush never reads.
@@ -1594,7 +1579,7 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
     using st = typename pair_traits<K>::storage;
     constexpr int CC = GG::groups / SC;
     constexpr int GS = WB + 1;  // bins per window and array (the last one collects out-of-window taps)
-    constexpr int GW = 2 * GS;  // int32 words per window: GS 64-bit (A, T) bins
+    constexpr int GW = 2 * GS;  // A bins then T bins
     static_assert(SC % 2 == 0 && GG::groups % SC == 0, "SC * BT must divide the stage");
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1724,7 +1709,7 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                                     const st *tp = rr < (uint32_t)WB
                                                        ? reinterpret_cast<const st *>(groups + jj * GG::bytes) + rr
                                                        : reinterpret_cast<const st *>(zero_group);
-                                    const uint32_t gb = gwin_u32 + (jj * BT) * GW * 4 + min(rr, (uint32_t)WB) * 8;
+                                    const uint32_t gb = gwin_u32 + ((jj * BT) * GW + min(rr, (uint32_t)WB)) * 4;
                                     float2 sg = make_float2(sx[jj], 0.f);   // (sum g_b x0, sum g_b d)
                                     if (p.gx) {
                                         static_for<0, BT>([&](auto bic) {
@@ -1733,7 +1718,8 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                                             pair_x0_d_ptr<K>(tp + bi * (GG::item_bytes / (int)sizeof(st)), x0, d);
                                             sg = __ffma2_rn(g2[bi], make_float2(x0, d), sg);
                                             const float as = g[bi] * gsw[jj];
-                                            red_shared_add_pair_at<bi * GW * 4>(gb, fix_round(as), fix_round_fma(as, t));
+                                            red_shared_add_at<bi * GW * 4>(gb, fix_round(as));
+                                            red_shared_add_at<(bi * GW + GS) * 4>(gb, fix_round_fma(as, t));
                                         });
                                     } else {
 #pragma unroll
@@ -1780,8 +1766,9 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                                     if (p.gx && a != 0.f && ts.k < nlast && b0 + bi < p.B) {
                                         if (fixed && !ovfw && rr < (uint32_t)WB) {
                                             const float as = g[bi] * gsw[j];
-                                            const uint32_t ga = gwin_u32 + (j * BT + bi) * GW * 4 + rr * 8;
-                                            red_shared_add_pair(ga, fix_round(as), fix_round_fma(as, ts.t));
+                                            const uint32_t ga = gwin_u32 + ((j * BT + bi) * GW + rr) * 4;
+                                            red_shared_add(ga, fix_round(as));
+                                            red_shared_add(ga + GS * 4, fix_round_fma(as, ts.t));
                                         } else {
                                             const float a1 = a * ts.t;
                                             float *gr = p.gx + (((int64_t)(b0 + bi) * p.C + c) * p.S + (e0 + j)) * p.N + ts.k;
@@ -1821,14 +1808,13 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                         const int kw = (int)(sm.meta[stage * kStWin + grp] - kFloorMagicBits);
                         const bool live = b0 + bi < p.B;
                         float *grow = p.gx + (((int64_t)(b0 + bi) * p.C + (c0 + cl)) * p.S + (e0 + j)) * p.N;
-                        long long *bins = reinterpret_cast<long long *>(gstage + win * GW);
+                        int *bins = gstage + win * GW;
 #pragma unroll
                         for (int r = r0; r < GS; r += 8) {
-                            const long long sum = bins[r];
-                            if (sum != 0) {
+                            const int va = bins[r], vt = bins[GS + r];
+                            if ((va | vt) != 0) {
                                 bins[r] = 0;
-                                const int vt = (int)(unsigned)(sum & 0xffffffffll);   // low word, sign-extended
-                                const int va = (int)((sum - (long long)vt) >> 32);
+                                bins[GS + r] = 0;
                                 const int k = kw + r;
                                 if (r < WB && live && k >= 0 && k <= p.N - 2) {
                                     atomicAdd(grow + k, (float)(va - vt) * finv);
