@@ -150,6 +150,25 @@ def timed(fn, steps: int, warmup: int, stream, world: int):
     return ms
 
 
+def in_record_fraction(wl, every: int = 8) -> float:
+    """Share of units whose tap lies inside the record (0 <= floor(tau) < N-1),
+    from every `every`-th voxel (all channels, events): the metric counts all
+    units, like the reference, and this says how many of them are real taps."""
+    x, dst, src, offs = wl["x"], wl["dstpos"], wl["srcpos"], wl["offsets"]
+    N = x.shape[-1]
+    d = dst.reshape(-1, 3)[::every].float()
+    o = offs.reshape(offs.shape[0], -1)[:, ::every].float()
+    inside = 0
+    total = 0
+    for c0 in range(0, src.shape[0], 64):
+        r = torch.cdist(d, src[c0:c0 + 64].float())                 # (v, c)
+        tau = r[None] + o.t()[None].permute(2, 1, 0)                # (s, v, c)
+        k = torch.floor(tau)
+        inside += int(((k >= 0) & (k < N - 1)).sum())
+        total += tau.numel()
+    return inside / max(total, 1)
+
+
 def algorithmic_bytes(wl, x_bytes_per_sample: int) -> int:
     x = wl["x"]
     V = int(np.prod(wl["dstpos"].shape[:-1]))
@@ -345,6 +364,7 @@ def run_ours(args, rank, world) -> dict:
                     "serial": {"value": units * world / (ms_e2e_serial * 1e-3) / 1e9,
                                "api": "ffdas_b200.das per step: copy in, call, copy out"}},
             "gpu_launches": 2 * args.steps,
+            "in_record_fraction": in_record_fraction(wl),
             "clocks": ck}
 
     if rank == 0 and world == 1 and not args.quick:
