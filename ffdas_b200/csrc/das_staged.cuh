@@ -719,6 +719,7 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
     const st *__restrict__ Pg = static_cast<const st *>(p.P);
     const uint32_t kmax_pair = (uint32_t)(p.npad - 1);
     float acc = 0.f;
+    const int cbeg = chan_begin(p), cend = chan_end(p);   // this CTA's channel slice
     float2 acc2 = make_float2(0.f, 0.f);  // packed partial sums (even / odd event)
     int stage = 0;
     uint32_t phase = 0;
@@ -740,7 +741,7 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
             w2[j / 2] = make_float2(w[j], w[j + 1]);
         }
 
-        for (int c0 = chan_begin(p); c0 < chan_end(p); c0 += CC) {
+        for (int c0 = cbeg; c0 < cend; c0 += CC) {
             if (cx.producer) {
                 staged_produce<K, WB, SC>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
             } else {
@@ -857,6 +858,7 @@ __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kerne
     extern __shared__ __align__(128) unsigned char smem_raw[];
     staged_smem<K, WB> sm(smem_raw);
     const staged_ctx cx = staged_setup<K, WB>(p, sm, false, 2);
+    const int cbeg = chan_begin(p), cend = chan_end(p);   // this CTA's channel slice
 
     const st *__restrict__ Pg = static_cast<const st *>(p.P);
     const uint32_t kmax_pair = (uint32_t)(p.npad - 1);
@@ -880,7 +882,7 @@ __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kerne
         float2 ofs2[SC], w2[SC];
         staged_pass_begin2<K, WB, SC>(p, sm, cx, e0, sc, ofs2, w2);
 
-        for (int c0 = chan_begin(p); c0 < chan_end(p); c0 += CC) {
+        for (int c0 = cbeg; c0 < cend; c0 += CC) {
             if (cx.producer) {
                 staged_produce<K, WB, SC>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
             } else {
@@ -1119,6 +1121,7 @@ __global__ void __launch_bounds__(kStThreads) das_staged_batch_kernel(const stag
     const st *__restrict__ Pg = static_cast<const st *>(p.P);
     const uint32_t kmax_pair = (uint32_t)(p.npad - 1);
     float2 acc2[BT];   // per batch item: (even events, odd events)
+    const int cbeg = chan_begin(p), cend = chan_end(p);   // this CTA's channel slice
 #pragma unroll
     for (int bi = 0; bi < BT; bi++) acc2[bi] = make_float2(0.f, 0.f);
     int stage = 0;
@@ -1143,7 +1146,7 @@ __global__ void __launch_bounds__(kStThreads) das_staged_batch_kernel(const stag
             w2[j / 2] = make_float2(w[j], w[j + 1]);
         }
 
-        for (int c0 = chan_begin(p); c0 < chan_end(p); c0 += CC) {
+        for (int c0 = cbeg; c0 < cend; c0 += CC) {
             if (cx.producer) {
                 staged_produce_batch<K, WB, SC, BT>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
             } else {
