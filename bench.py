@@ -54,18 +54,60 @@ FLOP_PER_UNIT = 5.0
 
 # ----------------------------------------------------------------- clocks ---
 class ClockSampler:
-    """nvidia-smi sampling during the timed region (200 ms period)."""
+    """SM clocks and throttle reasons sampled during the timed region.
+
+    NVML is polled every 10 ms from a thread (read-only queries), so that even
+    a timed region of a few hundred milliseconds yields tens of samples; when
+    NVML is unavailable, nvidia-smi is polled every 200 ms instead.
+    """
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, period_s: float = 0.01):
         self.index = index
-        self.rows = []
+        self.period = period_s
+        self.rows = []          # (sm_mhz, sm_max_mhz, set of reasons)
         self.proc = None
         self.thread = None
+        self.stop_evt = threading.Event()
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID("GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
+        try:
+            nv, hd = self._nvml_handle()
+            smax = float(nv.nvmlDeviceGetMaxClockInfo(hd, nv.NVML_CLOCK_SM))
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+
+            def poll():
+                while not self.stop_evt.is_set():
+                    try:
+                        sm = float(nv.nvmlDeviceGetClockInfo(hd, nv.NVML_CLOCK_SM))
+                        r = nv.nvmlDeviceGetCurrentClocksEventReasons(hd)
+                        self.rows.append((sm, smax, {n for n, b in bits.items() if r & b}))
+                    except Exception:
+                        pass
+                    self.stop_evt.wait(self.period)
+
+            self.source = "nvml 10 ms"
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            pass
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -73,38 +115,37 @@ class ClockSampler:
         except Exception:
             self.proc = None
             return
+        self.source = "nvidia-smi 200 ms"
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([c.strip() for c in line.split(",")])
-
-    def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        if self.thread:
-            self.thread.join(timeout=2)
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
+            r = [c.strip() for c in line.split(",")]
             try:
-                sm.append(float(r[1]))
-                smax.append(float(r[2]))
-                for n, v in zip(names, r[5:9]):
-                    if v.strip().lower() == "active":
-                        reasons.add(n)
+                self.rows.append((float(r[1]), float(r[2]),
+                                  {n for n, v in zip(self.NAMES, r[5:9]) if v.lower() == "active"}))
             except (ValueError, IndexError):
                 continue
+
+    def stop(self) -> dict:
+        if self.thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi and NVML unavailable"]}
+        self.stop_evt.set()
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        self.thread.join(timeout=2)
+        sm = [r[0] for r in self.rows]
+        smax = [r[1] for r in self.rows]
+        reasons = set().union(*[r[2] for r in self.rows]) if self.rows else set()
         load = [s for s in sm if smax and s > 0.5 * max(smax)] or sm
         return {"sm_mhz": statistics.median(load) if load else None,
                 "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": self.source}
 
 
 # ------------------------------------------------------------------ utils ---
