@@ -541,7 +541,7 @@ def bwd_extras(args, h) -> dict:
 
     table = []
     bcands = [None] + [dict(variant=2, tile_x=tx, tile_y=256 // tx, window=wb)
-                       for tx in (16, 32, 64) for wb in (32, 64)] + [dict(variant=3)]
+                       for tx in (8, 16, 32) for wb in (32, 64)] + [dict(variant=3)]
     if args.schedule_bwd:
         bcands = [json.loads(args.schedule_bwd)]
     for cfg in bcands:

@@ -339,11 +339,45 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
                 bp.n0 = (pb.D0 + tx - 1) / tx;
                 bp.n1 = (pb.D1 + ty - 1) / ty;
             }
+        } else if (pb.D0 >= 8 && pb.D1 >= 32) {
+            // 8 x 32 tiles: a warp's voxels (one column of the tile under the
+            // spread mapping) cover 32 rows along the second axis, so where that
+            // axis is depth they meet more distinct samples -- fewer same-address
+            // atomics in the scatter -- and where it is not, the cost is that of
+            // 16 x 16 tiles.
+            bp.T0 = 8; bp.T1 = 32; bp.T2 = 1;
+            bp.n0 = (pb.D0 + 7) / 8;
+            bp.n1 = (pb.D1 + 31) / 32;
         }
         const int64_t stiles = (int64_t)bp.n0 * bp.n1 * ((pb.D2 + bp.T2 - 1) / bp.T2);
         if (stiles > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
+        // batch tiles: up to 4 items per CTA share each window's delays
+        const int WB = (h.has_config && h.config.window > 32) ? 64 : 32;
+        const int copy = h.has_config ? h.config.copy_engine : 0;
+        int BT = 1;
+        while (BT * 2 <= std::min(pb.B, 4)) BT *= 2;
+        if (h.has_config && h.config.variant == 2 && h.config.batch_tile) BT = std::min(h.config.batch_tile, 4);
+        if (copy == 2 || !staged_batch_supported()) BT = 1;
+        const int SC = BT > 1 ? 4 : (pb.n_events <= 1 ? 1 : 4);
+        const int bchunks_st = (pb.B + BT - 1) / BT;
+        // Channel slices over blockIdx.z (32+ channels each) while there are
+        // fewer than min_blocks (default 2, the adjoint's CTAs per SM) CTAs per
+        // SM, so that small problems fill the GPU.
+        int csplit = 1;
+        {
+            const int per_sm = (h.has_config && h.config.min_blocks) ? h.config.min_blocks : 2;
+            const int64_t ctas = stiles * bchunks_st;
+            const int64_t want = (int64_t)std::max(h.sm_count, 1) * per_sm;
+            while (ctas * csplit * 2 <= want && pb.C >= 64 * csplit && csplit < 64) csplit *= 2;
+        }
+        int cchunk = 0;
+        if (csplit > 1) {
+            cchunk = ((pb.C + csplit - 1) / csplit + 31) / 32 * 32;   // whole stages of channels
+            csplit = (pb.C + cchunk - 1) / cchunk;
+            if (csplit < 2) cchunk = 0;
+        }
         const size_t ve0 = (size_t)pb.n_events * pb.V * sizeof(float);
-        if (pb.B > 1) {  // several CTAs add into the voxel-side gradients
+        if (pb.B > 1 || csplit > 1) {  // several CTAs add into the voxel-side gradients
             if (gw) FFDAS_CUDA(cudaMemsetAsync(gw, 0, ve0, h.stream));
             if (goff) FFDAS_CUDA(cudaMemsetAsync(goff, 0, ve0, h.stream));
             if (gdst) FFDAS_CUDA(cudaMemsetAsync(gdst, 0, (size_t)pb.V * 3 * sizeof(float), h.stream));
@@ -358,24 +392,17 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
         gp.T0 = bp.T0; gp.T1 = bp.T1; gp.T2 = bp.T2; gp.n0 = bp.n0; gp.n1 = bp.n1;
         gp.srcpos = a.srcpos; gp.dstpos = a.dstpos; gp.offsets = a.offsets; gp.weights = a.weights;
         gp.beta_zero = 1;
+        gp.cchunk = cchunk;
         const staged_grads gr{static_cast<const float *>(gout), pb.out_bstride, gx, goff, gw, gdst, gsrc};
-        const int WB = (h.has_config && h.config.window > 32) ? 64 : 32;
-        const int copy = h.has_config ? h.config.copy_engine : 0;
-        // batch tiles: up to 8 items per CTA share each window's delays
-        int BT = 1;
-        while (BT * 2 <= std::min(pb.B, 4)) BT *= 2;
-        if (h.has_config && h.config.variant == 2 && h.config.batch_tile) BT = std::min(h.config.batch_tile, 4);
-        if (copy == 2 || !staged_batch_supported()) BT = 1;
-        const int SC = BT > 1 ? 4 : (pb.n_events <= 1 ? 1 : 4);
-        const int bchunks_st = (pb.B + BT - 1) / BT;
         h.last = ffdas_kernel_info_t{};
         h.last.variant = 4;
         h.last.tile_x = bp.T0; h.last.tile_y = bp.T1; h.last.tile_z = bp.T2;
         h.last.batch_tile = BT; h.last.event_chunk = SC; h.last.storage = kind;
-        h.last.kernels = 2; h.last.grid = stiles * bchunks_st;
+        h.last.kernels = 2; h.last.grid = stiles * bchunks_st * csplit;
+        if (bchunks_st > 65535) return FFDAS_ERROR_DIMS_TOO_LARGE;
         h.mark_start();
         const ffdas_error_t err = launch_staged_bwd(h, pb, kind, gp, gr, SC, WB, BT, copy,
-                                                    dim3((unsigned)stiles, (unsigned)bchunks_st));
+                                                    dim3((unsigned)stiles, (unsigned)bchunks_st, (unsigned)csplit));
         h.mark_stop();
         return err;
     }

@@ -189,12 +189,64 @@ constexpr size_t staged_smem_bytes() {
     return slot_geom<WB, K>::ring_bytes + kStMiscBytes + 128;
 }
 
-// Adjoint extras: fixed-point gradient slots [kStages][kStWin][WB + 2] int32,
-// the per-stage channel-gradient scratch [kStWin / SC * 3][256] floats and a
-// per-warp reduction scratch.
+// The adjoints keep two copies of their fixed-point gradient bins (cx.par
+// picks one per thread) to halve same-address atomics.  A copy spans `words`
+// rounded up to whole bank rows plus half a row, so the copies' bins sit 16
+// banks apart.
+constexpr int bin_region_words(int words) { return (words + 31) / 32 * 32 + 16; }
+constexpr int kBinCopies = 2;
+// Words per window in the bins: samples kw .. kw + WB (WB + 1 bins) plus one
+// bin that only out-of-window taps touch (always with zero), rounded up to
+// whole 16-byte quads.
+constexpr int bin_stride(int wb) { return (wb + 2 + 3) / 4 * 4; }
+
+// Flush of one stage's fixed-point gradient bins: for every window, gx[kw + r]
+// += (copy 0 + copy 1)[r] * finv for the nonzero bins r = 0..WB, and the bins
+// are cleared.  WB / 4 lanes take a window, four bins each, with 128-bit
+// shared loads and stores (a quarter warp moves 128 consecutive bytes: no bank
+// conflicts); the window's first lane also takes bin WB.  row(win, kw) returns
+// the gx row of the window (nullptr when it adds nothing) and its first sample.
+template <int WB, int REGION, class RowFn>
+__device__ __forceinline__ void flush_bins(int *bins0, int lane, int warp, float finv, RowFn &&row) {
+    constexpr int GS4 = bin_stride(WB);
+    constexpr int LPW = WB / 4;     // lanes per window
+    constexpr int WPI = 32 / LPW;   // windows per warp and pass
+    static_assert(WB % 4 == 0 && 32 % LPW == 0 && REGION % 4 == 0, "flush layout");
+    const int sub = lane / LPW, q = lane % LPW;
+    for (int w0 = warp * WPI; w0 < kStWin; w0 += kStWarps * WPI) {
+        const int win = w0 + sub;
+        int *b = bins0 + win * GS4 + 4 * q;
+        const int4 u = *reinterpret_cast<const int4 *>(b);
+        const int4 v = *reinterpret_cast<const int4 *>(b + REGION);
+        *reinterpret_cast<int4 *>(b) = make_int4(0, 0, 0, 0);
+        *reinterpret_cast<int4 *>(b + REGION) = make_int4(0, 0, 0, 0);
+        int last = 0;
+        if (q == 0) {
+            int *e = bins0 + win * GS4 + WB;
+            last = e[0] + e[REGION];
+            e[0] = 0;
+            e[REGION] = 0;
+        }
+        int kw;
+        float *g = row(win, kw);
+        if (g) {
+            g += kw + 4 * q;
+            const int s0 = u.x + v.x, s1 = u.y + v.y, s2 = u.z + v.z, s3 = u.w + v.w;
+            if (s0) atomicAdd(g, (float)s0 * finv);
+            if (s1) atomicAdd(g + 1, (float)s1 * finv);
+            if (s2) atomicAdd(g + 2, (float)s2 * finv);
+            if (s3) atomicAdd(g + 3, (float)s3 * finv);
+            if (last) atomicAdd(g + WB, (float)last * finv);   // only q == 0 has one
+        }
+    }
+}
+
+// Adjoint extras: two copies of the fixed-point gradient slots [kStWin][WB + 2]
+// int32, the per-stage channel-gradient scratch [kStWin / SC * 3][256] floats
+// and a per-warp reduction scratch.
 template <int WB, int K, int SC>
 constexpr size_t staged_bwd_smem_bytes() {
-    return staged_smem_bytes<WB, K>() + kStages * kStWin * (WB + 2) * 4 + (kStWin / SC) * 3 * kStConsumers * 4 +
+    return staged_smem_bytes<WB, K>() + kBinCopies * bin_region_words(kStWin * bin_stride(WB)) * 4 + (kStWin / SC) * 3 * kStConsumers * 4 +
            kStWarps * 4;
 }
 
@@ -274,6 +326,10 @@ struct staged_ctx {
     bool producer, active;
     int64_t v;
     float vx, vy, vz;
+    // checkerboard parity of the voxel in its tile (i0 + i1 + i2) & 1: the
+    // adjoints' scatter copy, so that neighbouring voxels, which often hit one
+    // sample, add into different copies of the gradient bins
+    int par;
     // second voxel of the thread in 512-voxel tiles (tile index + 256)
     bool active2;
     int64_t v2;
@@ -299,6 +355,7 @@ __device__ __forceinline__ staged_ctx staged_setup(const staged_params &p, stage
     cx.active = false;
     cx.v = 0;
     cx.vx = cx.vy = cx.vz = 0.f;
+    cx.par = 0;
     cx.active2 = false;
     cx.v2 = 0;
     cx.vx2 = cx.vy2 = cx.vz2 = 0.f;
@@ -308,6 +365,7 @@ __device__ __forceinline__ staged_ctx staged_setup(const staged_params &p, stage
         const int lt = spread ? (cx.lane * kStWarps + cx.warp) : cx.tid;
         const int i0 = lt % p.T0, i1 = (lt / p.T0) % p.T1, i2 = lt / (p.T0 * p.T1);
         const int g0 = t0 * p.T0 + i0, g1 = t1 * p.T1 + i1, g2 = t2 * p.T2 + i2;
+        cx.par = (i0 + i1 + i2) & 1;
         cx.active = (g0 < p.D0 && g1 < p.D1 && g2 < p.D2);
         if (cx.active) {
             cx.v = ((int64_t)g2 * p.D1 + g1) * p.D0 + g0;
@@ -1273,19 +1331,24 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
     using SG = slot_geom<WB, K>;
     using st = typename pair_traits<K>::storage;
     constexpr int CC = kStWin / SC;
-    constexpr int GS = WB + 2;  // gradient slot length (int32 entries)
+    constexpr int GS = bin_stride(WB);  // gradient slot stride (int32 entries)
     static_assert(kStWin % SC == 0, "SC must divide the stage");
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     staged_smem<K, WB> sm(smem_raw);
-    int *gslot = reinterpret_cast<int *>(sm.extra);                      // [kStages][kStWin][GS]
-    float *cgrad = reinterpret_cast<float *>(gslot + kStages * kStWin * GS);  // [CC * 3][256]
+    // one set of gradient slots (in two copies): a stage's slots are flushed
+    // and cleared between two consumer barriers before the next stage
+    // scatters into them
+    constexpr int kRegion = bin_region_words(kStWin * GS);
+    int *gslot = reinterpret_cast<int *>(sm.extra);                      // [kBinCopies][kRegion]
+    float *cgrad = reinterpret_cast<float *>(gslot + kBinCopies * kRegion);  // [CC * 3][256]
     float *wmax = cgrad + CC * 3 * kStConsumers;                          // [kStWarps]
-    for (int i = threadIdx.x; i < kStages * kStWin * GS; i += kStThreads) gslot[i] = 0;
+    for (int i = threadIdx.x; i < kBinCopies * kRegion; i += kStThreads) gslot[i] = 0;
     const staged_ctx cx = staged_setup<K, WB>(p, sm, true);   // ends with __syncthreads
-    const uint32_t gslot_u32 = smem_u32(gslot);
+    const uint32_t gslot_u32 = smem_u32(gslot) + cx.par * (kRegion * 4);   // this thread's copy
 
-    const bool multi_b = p.B > 1;
+    const bool multi_b = p.B > 1 || gridDim.z > 1;   // several CTAs add into the voxel-side gradients
+    const int cbeg = chan_begin(p), cend = chan_end(p);
     const float g = (cx.active) ? __ldg(p.gout + (int64_t)cx.b * p.gout_bstride + cx.v) : 0.f;
     const bool want_pos = p.gdst != nullptr || p.gsrc != nullptr;
     float gpx = 0.f, gpy = 0.f, gpz = 0.f;
@@ -1344,14 +1407,14 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
         const float2 magic2 = make_float2(kFloorMagic, kFloorMagic);
         const float2 neg1 = make_float2(-1.f, -1.f);
 
-        for (int c0 = 0; c0 < p.C; c0 += CC) {
+        for (int c0 = cbeg; c0 < cend; c0 += CC) {
             if (cx.producer) {
                 staged_produce<K, WB, SC>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
             } else {
                 const uint32_t full_bar = smem_u32(&sm.full[stage]);
                 const unsigned char *stage_base = sm.ring + stage * SG::stage_bytes;
-                int *gstage = gslot + stage * kStWin * GS;
-                const uint32_t gstage_u32 = gslot_u32 + stage * kStWin * GS * 4;
+                int *gstage = gslot;
+                const uint32_t gstage_u32 = gslot_u32;
                 if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
                 const bool any_ovf = !dead && sm.ovf[stage] != 0;
                 if (!dead && !any_ovf && (fixed || !p.gx)) {
@@ -1362,7 +1425,7 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
                     const uint32_t nlast = (uint32_t)(p.N - 1);
                     for (int cl = 0; cl < CC; cl++) {
                         const int c = c0 + cl;
-                        if (c >= p.C) break;   // a phantom channel's taps would scatter outside gx
+                        if (c >= cend) break;   // a channel past the slice (or a phantom one) is not this CTA's
                         const float4 cp = sm.chan_pos[stage * kStWin + cl];
                         const recv_geom gm = receive_geometry(cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z);
                         uint32_t k0p[SC];
@@ -1415,7 +1478,7 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
                 } else if (!dead) {
                     for (int cl = 0; cl < CC; cl++) {
                         const int c = c0 + cl;
-                        if (c >= p.C) break;   // a phantom channel's taps would scatter outside gx
+                        if (c >= cend) break;   // a channel past the slice (or a phantom one) is not this CTA's
                         const float4 cp = sm.chan_pos[stage * kStWin + cl];
                         const recv_geom gm = receive_geometry(cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z);
                         uint32_t k0p[SC];
@@ -1477,27 +1540,18 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
                 if (!dead) {
                     // flush the stage's gradient slots: one red.add per touched sample
                     if (p.gx && fixed) {
-                        // eight threads per window, bins r0, r0 + 8, ...: no division in the loop
-                        static_assert(kStConsumers == kStWin * 8, "flush layout: eight threads per window");
-                        const int win = cx.tid >> 3, r0 = cx.tid & 7;
-                        const int cl = win / SC, j = win % SC;
-                        const int kw = (int)(sm.meta[stage * kStWin + win] - kFloorMagicBits);
-                        float *grow = p.gx + (((int64_t)cx.b * p.C + (c0 + cl)) * p.S + (e0 + j)) * p.N;
-                        int *bins = gstage + win * GS;
-#pragma unroll
-                        for (int r = r0; r < GS; r += 8) {
-                            const int val = bins[r];
-                            if (val != 0) {
-                                bins[r] = 0;
-                                atomicAdd(grow + kw + r, (float)val * finv);
-                            }
-                        }
+                        flush_bins<WB, kRegion>(gstage, cx.lane, cx.warp, finv, [&](int win, int &kw) -> float * {
+                            const int cl = win / SC, j = win % SC;
+                            kw = (int)(sm.meta[stage * kStWin + win] - kFloorMagicBits);
+                            if (c0 + cl >= cend) return nullptr;
+                            return p.gx + (((int64_t)cx.b * p.C + (c0 + cl)) * p.S + (e0 + j)) * p.N;
+                        });
                     }
                     // channel-position gradients: reduce the tile, one add per channel
                     if (p.gsrc) {
                         for (int o = cx.warp; o < CC * 3; o += kStWarps) {
                             const int cl = o / 3;
-                            if (c0 + cl >= p.C) continue;
+                            if (c0 + cl >= cend) continue;
                             float s = 0.f;
 #pragma unroll
                             for (int i = 0; i < kStConsumers / 32; i++) s += cgrad[o * kStConsumers + cx.lane + 32 * i];
@@ -1561,15 +1615,14 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
 // and position gradients, and the fixed-point scatter of g_b w (1 - t), g_b w t
 // into the item's gradient slot.  amax = max_b |g_b| * max_j |w_j| over the tile.
 //
-// The slot of a window holds two fixed-point bin arrays per sample k of the
-// window: A[k] += g_b w and T[k] += g_b w t for a tap at k, so that the flush
-// adds A[k] - T[k] to gx[k] and T[k] to gx[k+1] -- for 0 <= k <= N-2 only.
-// A tap outside the record therefore needs no test in the loop (its bins are
-// dropped at the flush), and a tap outside its window (always outside the
-// record) lands in the bin past the window, which the flush never reads.
+// The slot of a window holds one fixed-point bin per sample kw .. kw + WB:
+// a tap at sample k adds round(a) - round(a t) to bin k and round(a t) to bin
+// k + 1, a = g_b w scaled, and a tap outside the record adds zeros (one test
+// per voxel, channel and event, shared by the BT items).  A tap outside its
+// window is always outside the record and adds its zeros past the window.
 template <int WB, int K, int SC, int BT>
 constexpr size_t staged_bwd_batch_smem_bytes() {
-    return staged_smem_bytes<WB, K>() + kStages * kStWin * 2 * (WB + 1) * 4 +
+    return staged_smem_bytes<WB, K>() + kBinCopies * bin_region_words(kStWin * bin_stride(WB)) * 4 +
            (group_geom<WB, K, BT>::groups / SC) * 3 * kStConsumers * 4 + kStWarps * 4 + 16 +
            group_geom<WB, K, BT>::data_bytes;
 }
@@ -1581,27 +1634,30 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
     using GG = group_geom<WB, K, BT>;
     using st = typename pair_traits<K>::storage;
     constexpr int CC = GG::groups / SC;
-    constexpr int GS = WB + 1;  // bins per window and array (the last one collects out-of-window taps)
-    constexpr int GW = 2 * GS;  // A bins then T bins
+    constexpr int GS = bin_stride(WB);  // bins per window: samples kw .. kw + WB, then zero-only ones
     static_assert(SC % 2 == 0 && GG::groups % SC == 0, "SC * BT must divide the stage");
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     staged_smem<K, WB> sm(smem_raw);
-    int *gslot = reinterpret_cast<int *>(sm.extra);                      // [kStages][kStWin][2][GS], window = group * BT + item
-    float *cgrad = reinterpret_cast<float *>(gslot + kStages * kStWin * GW);  // [CC * 3][256]
+    // one set of bins (in two copies): a stage's bins are flushed and cleared
+    // between two consumer barriers before the next stage scatters into them
+    constexpr int kRegion = bin_region_words(kStWin * GS);
+    int *gslot = reinterpret_cast<int *>(sm.extra);   // [kBinCopies][kRegion]: [kStWin][GS], window = group * BT + item
+    float *cgrad = reinterpret_cast<float *>(gslot + kBinCopies * kRegion);  // [CC * 3][256]
     float *wmax = cgrad + CC * 3 * kStConsumers;                          // [kStWarps]
     // zero group after the scratch, 16-byte aligned (offset arithmetic on the
     // shared pointer keeps its address space visible to the compiler)
-    constexpr int kZeroOff = ((kStages * kStWin * GW + CC * 3 * kStConsumers + kStWarps) * 4 + 15) & ~15;
+    constexpr int kZeroOff = ((kBinCopies * kRegion + CC * 3 * kStConsumers + kStWarps) * 4 + 15) & ~15;
     unsigned char *zero_group = sm.extra + kZeroOff;
-    for (int i = threadIdx.x; i < kStages * kStWin * GW; i += kStThreads) gslot[i] = 0;
+    for (int i = threadIdx.x; i < kBinCopies * kRegion; i += kStThreads) gslot[i] = 0;
     for (int i = threadIdx.x; i < GG::data_bytes / 4; i += kStThreads) reinterpret_cast<uint32_t *>(zero_group)[i] = 0u;
     const staged_ctx cx = staged_setup<K, WB>(p, sm, true);   // ends with __syncthreads
-    const uint32_t gslot_u32 = smem_u32(gslot);
+    const uint32_t gslot_u32 = smem_u32(gslot) + cx.par * (kRegion * 4);   // this thread's copy
     const uint32_t zero_u32 = smem_u32(zero_group);
 
     const int b0 = cx.b * BT;
-    const bool multi = gridDim.y > 1;   // several CTAs add into the voxel-side gradients
+    const bool multi = gridDim.y > 1 || gridDim.z > 1;   // several CTAs add into the voxel-side gradients
+    const int cbeg = chan_begin(p), cend = chan_end(p);
     float g[BT];
     float gmax = 0.f;
 #pragma unroll
@@ -1669,27 +1725,27 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
 #pragma unroll
         for (int j = 0; j < SC; j++) gsw[j] = w[j] * fscale;
 
-        for (int c0 = 0; c0 < p.C; c0 += CC) {
+        for (int c0 = cbeg; c0 < cend; c0 += CC) {
             if (cx.producer) {
                 staged_produce_batch<K, WB, SC, BT>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
             } else {
                 const uint32_t full_bar = smem_u32(&sm.full[stage]);
                 const uint32_t stage_u32 = smem_u32(sm.ring + stage * SG::stage_bytes);
-                int *gstage = gslot + stage * kStWin * GW;
-                const uint32_t gstage_u32 = gslot_u32 + stage * kStWin * GW * 4;
+                int *gstage = gslot;
+                const uint32_t gstage_u32 = gslot_u32;
                 if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
                 const bool any_ovf = !dead && sm.ovf[stage] != 0;
                 if (!dead) {
                     const uint32_t nlast = (uint32_t)(p.N - 1);
                     for (int cl = 0; cl < CC; cl++) {
                         const int c = c0 + cl;
-                        if (c >= p.C) break;   // a phantom channel's taps would scatter outside gx
+                        if (c >= cend) break;   // a channel past the slice (or a phantom one) is not this CTA's
                         const float4 cp = sm.chan_pos[stage * kStWin + cl];
                         const recv_geom gm = receive_geometry(cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z);
                         uint32_t k0p[SC];
                         load_meta<SC>(sm.meta, stage, cl, k0p);
                         const uint32_t groups_u32 = stage_u32 + (cl * SC) * GG::bytes;
-                        const uint32_t gwin_u32 = gstage_u32 + (cl * SC * BT) * GW * 4;
+                        const uint32_t gwin_u32 = gstage_u32 + (cl * SC * BT) * GS * 4;
                         float q = 0.f;
                         if (!any_ovf && (fixed || !p.gx)) {
                             const unsigned char *groups = sm.ring + stage * SG::stage_bytes + (cl * SC) * GG::bytes;
@@ -1712,7 +1768,10 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                                     const st *tp = rr < (uint32_t)WB
                                                        ? reinterpret_cast<const st *>(groups + jj * GG::bytes) + rr
                                                        : reinterpret_cast<const st *>(zero_group);
-                                    const uint32_t gb = gwin_u32 + ((jj * BT) * GW + min(rr, (uint32_t)WB)) * 4;
+                                    const uint32_t gb = gwin_u32 + ((jj * BT) * GS + min(rr, (uint32_t)WB)) * 4;
+                                    // a tap outside the record scatters zeros (into its window's
+                                    // bins, or the zero-only bins past the window)
+                                    const float gsin = (mb - kFloorMagicBits < nlast) ? gsw[jj] : 0.f;
                                     float2 sg = make_float2(sx[jj], 0.f);   // (sum g_b x0, sum g_b d)
                                     if (p.gx) {
                                         static_for<0, BT>([&](auto bic) {
@@ -1720,9 +1779,10 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                                             float x0, d;
                                             pair_x0_d_ptr<K>(tp + bi * (GG::item_bytes / (int)sizeof(st)), x0, d);
                                             sg = __ffma2_rn(g2[bi], make_float2(x0, d), sg);
-                                            const float as = g[bi] * gsw[jj];
-                                            red_shared_add_at<bi * GW * 4>(gb, fix_round(as));
-                                            red_shared_add_at<(bi * GW + GS) * 4>(gb, fix_round_fma(as, t));
+                                            const float as = g[bi] * gsin;
+                                            const int it = fix_round(as), i1 = fix_round_fma(as, t);
+                                            red_shared_add_at<bi * GS * 4>(gb, it - i1);
+                                            red_shared_add_at<bi * GS * 4 + 4>(gb, i1);
                                         });
                                     } else {
 #pragma unroll
@@ -1769,9 +1829,10 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                                     if (p.gx && a != 0.f && ts.k < nlast && b0 + bi < p.B) {
                                         if (fixed && !ovfw && rr < (uint32_t)WB) {
                                             const float as = g[bi] * gsw[j];
-                                            const uint32_t ga = gwin_u32 + ((j * BT + bi) * GW + rr) * 4;
-                                            red_shared_add(ga, fix_round(as));
-                                            red_shared_add(ga + GS * 4, fix_round_fma(as, ts.t));
+                                            const uint32_t ga = gwin_u32 + ((j * BT + bi) * GS + rr) * 4;
+                                            const int it = fix_round(as), i1 = fix_round_fma(as, ts.t);
+                                            red_shared_add(ga, it - i1);
+                                            red_shared_add(ga + 4, i1);
                                         } else {
                                             const float a1 = a * ts.t;
                                             float *gr = p.gx + (((int64_t)(b0 + bi) * p.C + c) * p.S + (e0 + j)) * p.N + ts.k;
@@ -1801,35 +1862,18 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                 consumer_sync();
                 if (!dead) {
                     if (p.gx && fixed) {
-                        // bins 0..WB-1 of each window: gx[k] += A - T, gx[k+1] += T for 0 <= k <= N-2;
-                        // every bin (the out-of-window one too) is cleared for the stage's next use.
-                        // Eight threads per window, bins r0, r0 + 8, ...: no division in the loop.
-                        static_assert(kStConsumers == kStWin * 8, "flush layout: eight threads per window");
-                        const int win = cx.tid >> 3, r0 = cx.tid & 7;
-                        const int grp = win / BT, bi = win % BT;
-                        const int cl = grp / SC, j = grp % SC;
-                        const int kw = (int)(sm.meta[stage * kStWin + grp] - kFloorMagicBits);
-                        const bool live = b0 + bi < p.B;
-                        float *grow = p.gx + (((int64_t)(b0 + bi) * p.C + (c0 + cl)) * p.S + (e0 + j)) * p.N;
-                        int *bins = gstage + win * GW;
-#pragma unroll
-                        for (int r = r0; r < GS; r += 8) {
-                            const int va = bins[r], vt = bins[GS + r];
-                            if ((va | vt) != 0) {
-                                bins[r] = 0;
-                                bins[GS + r] = 0;
-                                const int k = kw + r;
-                                if (r < WB && live && k >= 0 && k <= p.N - 2) {
-                                    atomicAdd(grow + k, (float)(va - vt) * finv);
-                                    atomicAdd(grow + k + 1, (float)vt * finv);
-                                }
-                            }
-                        }
+                        flush_bins<WB, kRegion>(gstage, cx.lane, cx.warp, finv, [&](int win, int &kw) -> float * {
+                            const int grp = win / BT, bi = win % BT;
+                            const int cl = grp / SC, j = grp % SC;
+                            kw = (int)(sm.meta[stage * kStWin + grp] - kFloorMagicBits);
+                            if (b0 + bi >= p.B || c0 + cl >= cend) return nullptr;
+                            return p.gx + (((int64_t)(b0 + bi) * p.C + (c0 + cl)) * p.S + (e0 + j)) * p.N;
+                        });
                     }
                     if (p.gsrc) {
                         for (int o = cx.warp; o < CC * 3; o += kStWarps) {
                             const int cl = o / 3;
-                            if (c0 + cl >= p.C) continue;
+                            if (c0 + cl >= cend) continue;
                             float s = 0.f;
 #pragma unroll
                             for (int i = 0; i < kStConsumers / 32; i++) s += cgrad[o * kStConsumers + cx.lane + 32 * i];

@@ -144,8 +144,9 @@ typedef struct {
     int32_t tile_z;       /* ... along the outermost spatial dim */
     int32_t batch_tile;   /* batch items per thread (1,2,4,8,16) */
     int32_t event_chunk;  /* events held in registers per pass (1..16) */
-    int32_t min_blocks;   /* staged forward: target CTAs per SM; problems with fewer tiles split
-                             each tile's channels over CTAs that add into the image (default 3) */
+    int32_t min_blocks;   /* staged kernels: target CTAs per SM; problems with fewer tiles split
+                             each tile's channels over CTAs that add into the image or the
+                             voxel-side gradients (default 3 forward, 2 adjoint) */
     int32_t window;       /* TMA-staged kernel: pairs per staged window (32 or 64) */
     int32_t copy_engine;  /* staged kernels: 0 auto, 1 TMA tile loads, 2 per-thread cp.async copies */
 } ffdas_das_config_t;
