@@ -135,11 +135,14 @@ static ffdas_error_t launch_ingest_t(ffdas_context &h, const das_problem &pb, co
                                      int64_t npad, void *P) {
     const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
     if (rows == 0) return FFDAS_SUCCESS;
-    dim3 block(256);
-    dim3 grid((unsigned)((npad + 255) / 256), (unsigned)std::min<int64_t>(rows, 65535));
-    ingest_pairs_kernel<Tin, K><<<grid, block, 0, h.stream>>>(
+    const int64_t bc = (int64_t)pb.B * pb.C;
+    if (bc > INT32_MAX || npad % kIngestVec != 0) return FFDAS_ERROR_INTERNAL;
+    const int64_t per_block = (int64_t)kIngestThreads * kIngestVec;
+    dim3 grid((unsigned)((npad + per_block - 1) / per_block), (unsigned)std::min<int64_t>(pb.S, 65535),
+              (unsigned)std::min<int64_t>(bc, 65535));
+    ingest_pairs_kernel<Tin, K><<<grid, kIngestThreads, 0, h.stream>>>(
         static_cast<const Tin *>(x), pb.x_bstride, pb.x_cstride, pb.x_sstride, pb.C, pb.S, pb.N,
-        rows, npad, static_cast<typename pair_traits<K>::storage *>(P));
+        (int)bc, npad, static_cast<typename pair_traits<K>::storage *>(P));
     return ffdas_launch_check(h.stream);
 }
 

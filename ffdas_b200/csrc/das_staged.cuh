@@ -250,14 +250,18 @@ constexpr size_t staged_bwd_smem_bytes() {
            kStWarps * 4;
 }
 
+// Shared-memory integer adds into the adjoints' gradient bins.  No "memory"
+// clobber: the bins are only read after a consumer barrier (whose asm has
+// one), and without it the compiler may hoist the staged-pair loads of later
+// taps above these adds instead of waiting out each load in turn.
 __device__ __forceinline__ void red_shared_add(uint32_t addr, int v) {
-    asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+    asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(addr), "r"(v));
 }
 // red.shared.add.s32 at addr + OFF bytes (OFF an immediate): no result
 // register, and the offset folds into the instruction.
 template <int OFF>
 __device__ __forceinline__ void red_shared_add_at(uint32_t addr, int v) {
-    asm volatile("red.shared.add.s32 [%0+%2], %1;" ::"r"(addr), "r"(v), "n"(OFF) : "memory");
+    asm volatile("red.shared.add.s32 [%0+%2], %1;" ::"r"(addr), "r"(v), "n"(OFF));
 }
 
 // Calls f(std::integral_constant<int, I>) for I = 0 .. N-1 (compile-time loop).
@@ -277,6 +281,11 @@ __device__ __forceinline__ int fix_round(float v) {
 }
 __device__ __forceinline__ int fix_round_fma(float a, float b) {   // round(a * b), one rounding
     return __float_as_int(__fmaf_rn(a, b, kFloorMagic)) - (int)kFloorMagicBits;
+}
+// round(a * b) + bits(1.5 * 2^23): differences of two such values need no
+// bias correction
+__device__ __forceinline__ int fix_bits_fma(float a, float b) {
+    return __float_as_int(__fmaf_rn(a, b, kFloorMagic));
 }
 
 // Shared-memory layout shared by the forward and adjoint kernels.
@@ -1456,11 +1465,11 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
                                 q = __fmaf_rn(aw[jj], d, q);
                                 if (p.gx) {
                                     const float as = (mb - kFloorMagicBits < nlast) ? asw[jj] : 0.f;
-                                    const int it = fix_round(as);
-                                    const int i1 = fix_round_fma(as, t);
+                                    // round(a) - round(a t) to sample k, round(a t) to k + 1
+                                    const int ab = __float_as_int(as + kFloorMagic), tb = fix_bits_fma(as, t);
                                     const uint32_t ga = gwin_u32 + (jj * GS + rel) * 4;
-                                    red_shared_add(ga, it - i1);
-                                    red_shared_add(ga + 4, i1);
+                                    red_shared_add(ga, ab - tb);
+                                    red_shared_add(ga + 4, tb - (int)kFloorMagicBits);
                                 }
                             }
                         }
@@ -1749,56 +1758,63 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                         float q = 0.f;
                         if (!any_ovf && (fixed || !p.gx)) {
                             const unsigned char *groups = sm.ring + stage * SG::stage_bytes + (cl * SC) * GG::bytes;
-                            // common case: every in-record tap is in its window
+                            // common case: every in-record tap is in its window; the
+                            // scatter's presence is decided once per channel (SCATTER)
                             const float2 rsq2 = make_float2(gm.rsq, gm.rsq), rinv2 = make_float2(gm.rinv, gm.rinv);
+                            auto taps = [&](auto scatter_c) {
+                                constexpr bool SCATTER = decltype(scatter_c)::value;
 #pragma unroll
-                            for (int j = 0; j < SC; j += 2) {
-                                const float2 tau2 = __ffma2_rn(rsq2, rinv2, make_float2(ofs[j], ofs[j + 1]));
-                                const float2 mm2 = __fadd2_rd(tau2, magic2);
-                                const float2 nfl2 = __ffma2_rn(mm2, neg1, magic2);   // -(floor), exact
-                                const float2 t2 = __fadd2_rn(tau2, nfl2);
+                                for (int j = 0; j < SC; j += 2) {
+                                    const float2 tau2 = __ffma2_rn(rsq2, rinv2, make_float2(ofs[j], ofs[j + 1]));
+                                    const float2 mm2 = __fadd2_rd(tau2, magic2);
+                                    const float2 nfl2 = __ffma2_rn(mm2, neg1, magic2);   // -(floor), exact
+                                    const float2 t2 = __fadd2_rn(tau2, nfl2);
 #pragma unroll
-                                for (int h = 0; h < 2; h++) {
-                                    const int jj = j + h;
-                                    const uint32_t mb = __float_as_uint(h ? mm2.y : mm2.x);
-                                    const float t = h ? t2.y : t2.x;
-                                    const uint32_t rr = mb - k0p[jj];
-                                    // plain shared-memory pointers: the per-item offsets fold
-                                    // into the load / atomic instructions as immediates
-                                    const st *tp = rr < (uint32_t)WB
-                                                       ? reinterpret_cast<const st *>(groups + jj * GG::bytes) + rr
-                                                       : reinterpret_cast<const st *>(zero_group);
-                                    const uint32_t gb = gwin_u32 + ((jj * BT) * GS + min(rr, (uint32_t)WB)) * 4;
-                                    // a tap outside the record scatters zeros (into its window's
-                                    // bins, or the zero-only bins past the window)
-                                    const float gsin = (mb - kFloorMagicBits < nlast) ? gsw[jj] : 0.f;
-                                    float2 sg = make_float2(sx[jj], 0.f);   // (sum g_b x0, sum g_b d)
-                                    if (p.gx) {
-                                        static_for<0, BT>([&](auto bic) {
-                                            constexpr int bi = decltype(bic)::value;
-                                            float x0, d;
-                                            pair_x0_d_ptr<K>(tp + bi * (GG::item_bytes / (int)sizeof(st)), x0, d);
-                                            sg = __ffma2_rn(g2[bi], make_float2(x0, d), sg);
-                                            const float as = g[bi] * gsin;
-                                            const int it = fix_round(as), i1 = fix_round_fma(as, t);
-                                            red_shared_add_at<bi * GS * 4>(gb, it - i1);
-                                            red_shared_add_at<bi * GS * 4 + 4>(gb, i1);
-                                        });
-                                    } else {
+                                    for (int h = 0; h < 2; h++) {
+                                        const int jj = j + h;
+                                        const uint32_t mb = __float_as_uint(h ? mm2.y : mm2.x);
+                                        const float t = h ? t2.y : t2.x;
+                                        const uint32_t rr = mb - k0p[jj];
+                                        // plain shared-memory pointers: the per-item offsets fold
+                                        // into the load / atomic instructions as immediates
+                                        const st *tp = rr < (uint32_t)WB
+                                                           ? reinterpret_cast<const st *>(groups + jj * GG::bytes) + rr
+                                                           : reinterpret_cast<const st *>(zero_group);
+                                        float2 sg = make_float2(sx[jj], 0.f);   // (sum g_b x0, sum g_b d)
+                                        if constexpr (SCATTER) {
+                                            const uint32_t gb = gwin_u32 + ((jj * BT) * GS + min(rr, (uint32_t)WB)) * 4;
+                                            // a tap outside the record scatters zeros (into its
+                                            // window's bins, or the zero-only bins past the window)
+                                            const float gsin = (mb - kFloorMagicBits < nlast) ? gsw[jj] : 0.f;
+                                            const float gst = gsin * t;
+                                            static_for<0, BT>([&](auto bic) {
+                                                constexpr int bi = decltype(bic)::value;
+                                                float x0, d;
+                                                pair_x0_d_ptr<K>(tp + bi * (GG::item_bytes / (int)sizeof(st)), x0, d);
+                                                sg = __ffma2_rn(g2[bi], make_float2(x0, d), sg);
+                                                // round(g w) - round(g w t) to sample k, round(g w t) to k + 1
+                                                const int ab = fix_bits_fma(g[bi], gsin), tb = fix_bits_fma(g[bi], gst);
+                                                red_shared_add_at<bi * GS * 4>(gb, ab - tb);
+                                                red_shared_add_at<bi * GS * 4 + 4>(gb, tb - (int)kFloorMagicBits);
+                                            });
+                                        } else {
 #pragma unroll
-                                        for (int bi = 0; bi < BT; bi++) {
-                                            float x0, d;
-                                            pair_x0_d_ptr<K>(tp + bi * (GG::item_bytes / (int)sizeof(st)), x0, d);
-                                            sg = __ffma2_rn(g2[bi], make_float2(x0, d), sg);
+                                            for (int bi = 0; bi < BT; bi++) {
+                                                float x0, d;
+                                                pair_x0_d_ptr<K>(tp + bi * (GG::item_bytes / (int)sizeof(st)), x0, d);
+                                                sg = __ffma2_rn(g2[bi], make_float2(x0, d), sg);
+                                            }
                                         }
+                                        sx[jj] = sg.x;
+                                        const float gd = sg.y;
+                                        sd[jj] += gd;
+                                        std_[jj] = __fmaf_rn(t, gd, std_[jj]);
+                                        q = __fmaf_rn(w[jj], gd, q);
                                     }
-                                    sx[jj] = sg.x;
-                                    const float gd = sg.y;
-                                    sd[jj] += gd;
-                                    std_[jj] = __fmaf_rn(t, gd, std_[jj]);
-                                    q = __fmaf_rn(w[jj], gd, q);
                                 }
-                            }
+                            };
+                            if (p.gx) taps(std::true_type{});
+                            else taps(std::false_type{});
                         } else {
                             const unsigned char *groups = sm.ring + stage * SG::stage_bytes + (cl * SC) * GG::bytes;
 #pragma unroll
