@@ -614,7 +614,37 @@ def config_extras(args, impl: str) -> dict:
         out[name] = e
         del wl, geo
         torch.cuda.empty_cache()
+    out["sparse_select"] = select_extra(args, impl, dev, stream)
     return {"configs": out}
+
+
+def select_extra(args, impl: str, dev, stream) -> dict:
+    """Choosing the das_sparse lists: per voxel the 32 of 64 events with the
+    largest weight (a seeded 0/1 beam mask plus jitter, 400x256 pixels), with
+    weights and delays gathered.  Ours: ffdas_sparse_select on the GPU.  The
+    reference does this step with host-array calls in its example
+    (sparse_compounding.py:141-144, through CuPy, which is not installed here):
+    the reference arm times the same numpy calls on the host."""
+    g = torch.Generator().manual_seed(41)
+    S, k, shape = 64, 32, (400, 256)
+    w = (torch.rand((S, *shape), generator=g) < 0.3).float() + torch.rand((S, *shape), generator=g) * 1e-3
+    o = torch.rand((S, *shape), generator=g) * 1000
+    if impl == "reference":
+        import time
+        wn, on = w.numpy(), o.numpy()
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            i = np.argpartition(wn, -k, axis=0)[-k:]
+            np.take_along_axis(wn, i, axis=0)
+            np.take_along_axis(on, i, axis=0)
+            ts.append(time.perf_counter() - t0)
+        return {"us_per_call": min(ts) * 1e6, "impl": "host numpy argpartition + take_along_axis (the reference "
+                "example's calls; CuPy absent)", "shape": [S, *shape], "k": k}
+    import ffdas_b200
+    wd, od = w.to(dev), o.to(dev)
+    ms = timed(lambda: ffdas_b200.sparse_select(wd, k, offsets=od), max(args.steps, 5), args.warmup, stream, 1)
+    return {"us_per_call": ms * 1e3, "impl": "ffdas_sparse_select (GPU)", "shape": [S, *shape], "k": k}
 
 
 def main() -> int:

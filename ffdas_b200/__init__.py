@@ -10,7 +10,7 @@ loads the compiled library and fails if it is missing.
 from . import _lib
 from ._lib import Algorithm, ComputeType, DataType, DasConfig, FFDASError
 from .library import get_cuda_device, set_cuda_device, get_library_handle
-from .das import das, das_sparse, DowncastWarning
+from .das import das, das_sparse, sparse_select, DowncastWarning
 from .timing import Timer
 
 _lib.load()
@@ -18,6 +18,6 @@ _lib.load()
 __version__ = "0.1.0"
 
 __all__ = [
-    "das", "das_sparse", "Algorithm", "ComputeType", "DataType", "DasConfig", "FFDASError",
+    "das", "das_sparse", "sparse_select", "Algorithm", "ComputeType", "DataType", "DasConfig", "FFDASError",
     "DowncastWarning", "get_cuda_device", "set_cuda_device", "get_library_handle", "Timer",
 ]

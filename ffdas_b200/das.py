@@ -251,3 +251,54 @@ def das_sparse(x, srcpos, dstpos, offsets, weights, sparse_indices, *, srcdir=No
     return _run(x, srcpos, dstpos, offsets, weights, sparse_indices, srcdir=srcdir, wavenum=wavenum,
                 algorithm=algorithm, use_fp16=use_fp16, use_bf16=use_bf16, channels_trailing=channels_trailing,
                 out=out)
+
+
+def sparse_select(weights, k: int, offsets=None):
+    """The inputs of `das_sparse`: per voxel the k events with the largest weight.
+
+    Device version of the host step in the reference's sparse-compounding
+    example (bindings/python/examples/sparse_compounding.py:141-144):
+    ``sparse_indices = argpartition(weights, -k, axis=0)[-k:]`` and
+    ``take_along_axis`` of the weights and delays at those indices.
+
+    Args:
+        weights: per-event apodization (n_events, ...), on a CUDA device.
+        k: events kept per voxel, 1 <= k <= min(n_events, 32).
+        offsets: optional per-event delays of the same shape, gathered too.
+
+    Returns:
+        (sparse_indices int32 (k, ...), sparse_weights (k, ...), sparse_offsets
+        (k, ...) or None).  Entries come in descending weight (NaN above every
+        number, ties to the lower event index); argpartition leaves that order
+        unspecified, and das_sparse's sum depends on it only through rounding.
+    """
+    w_shape = _shape(weights)
+    if len(w_shape) < 2:
+        raise ValueError("weights must have dimensions (n_events, ...)")
+    n = w_shape[0]
+    if not isinstance(k, (int,)) or isinstance(k, bool):
+        raise TypeError("k must be an int")
+    if k < 1 or k > min(n, 32):
+        raise ValueError(f"k must lie in [1, min(n_events, 32)] = [1, {min(n, 32)}], got {k}")
+    if offsets is not None and _shape(offsets) != w_shape:
+        raise ValueError(f"offsets shape {_shape(offsets)} must match weights shape {w_shape}")
+    wt = _to_torch(weights)
+    if not wt.is_cuda:
+        raise ValueError("weights must be a CUDA tensor")
+    dev = wt.device
+    w_t = _astype(wt, torch.float32, dev, "weights")
+    o_t = _astype(offsets, torch.float32, dev, "offsets") if offsets is not None else None
+    spatial = w_shape[1:]
+    V = 1
+    for d in spatial:
+        V *= int(d)
+    idx = torch.empty((k, *spatial), dtype=torch.int32, device=dev)
+    sw = torch.empty((k, *spatial), dtype=torch.float32, device=dev)
+    so = torch.empty((k, *spatial), dtype=torch.float32, device=dev) if o_t is not None else None
+    handle = get_library_handle(dev)
+    handle.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+    ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+    _lib.check(_lib.load().ffdas_sparse_select(handle.h, ptr(w_t), ptr(o_t), int(n), int(V), int(k), ptr(idx),
+                                               ptr(sw), ptr(so)))
+    return (_from_torch_like(idx, weights), _from_torch_like(sw, weights),
+            None if so is None else _from_torch_like(so, weights))

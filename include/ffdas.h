@@ -312,6 +312,30 @@ FFDAS_API ffdas_error_t ffdas_das_static(
     ffdas_alg_t alg
 );
 
+/* New, no counterpart in the reference library: the event lists a
+ * das_sparse call sums, chosen on the device.  Replaces the host-array step
+ * of the reference's sparse-compounding example
+ * (bindings/python/examples/sparse_compounding.py:141-144: argpartition of
+ * the weights over the event axis, then take_along_axis of weights and
+ * delays).  weights and offsets are (n_events, n_voxels) float32 rows;
+ * per voxel the k events with the largest weight (NaN above every number,
+ * ties to the lower event index), in that order, go to sparse_indices
+ * (k, n_voxels) int32, their weights to sparse_weights and their delays to
+ * sparse_offsets (both nullable; offsets may be NULL when sparse_offsets is).
+ * 1 <= k <= min(n_events, 32), else FFDAS_ERROR_INVALID_ARGUMENT.
+ * Asynchronous on the handle's stream; allocates nothing. */
+FFDAS_API ffdas_error_t ffdas_sparse_select(
+    ffdas_handle_t handle,
+    const float *weights,
+    const float *offsets,
+    int n_events,
+    int64_t n_voxels,
+    int k,
+    int *sparse_indices,
+    float *sparse_weights,
+    float *sparse_offsets
+);
+
 /* New: schedule override for the following calls on this handle
  * (NULL restores the planner default). */
 FFDAS_API ffdas_error_t ffdas_das_set_config(ffdas_handle_t handle,

@@ -70,6 +70,24 @@ def test_cpu_tensor_is_rejected_loudly():
         ffdas_b200.das(**_das_args())
 
 
+def test_sparse_select_validation_before_gpu_work():
+    w = torch.ones((8, 5, 6))
+    with pytest.raises(ValueError, match="k must lie"):
+        ffdas_b200.sparse_select(w, 0)
+    with pytest.raises(ValueError, match="k must lie"):
+        ffdas_b200.sparse_select(w, 9)
+    with pytest.raises(ValueError, match="k must lie"):
+        ffdas_b200.sparse_select(torch.ones((40, 6)), 33)
+    with pytest.raises(TypeError):
+        ffdas_b200.sparse_select(w, 2.0)
+    with pytest.raises(ValueError, match="offsets shape"):
+        ffdas_b200.sparse_select(w, 2, offsets=torch.ones((8, 5, 7)))
+    with pytest.raises(ValueError, match="n_events"):
+        ffdas_b200.sparse_select(torch.ones(8), 2)
+    with pytest.raises(ValueError, match="CUDA"):
+        ffdas_b200.sparse_select(w, 2)
+
+
 @pytest.mark.parametrize("name", list(W.CONFIGS))
 def test_workload_shapes(name):
     wl = W.CONFIGS[name](scale=0.05)

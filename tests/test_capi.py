@@ -91,6 +91,7 @@ def test_null_handle_is_rejected_before_any_device_work():
     assert L.ffdas_get_stream(None, None) == Error.INVALID_HANDLE
     assert L.ffdas_destroy(None) == Error.INVALID_HANDLE
     assert L.ffdas_das_set_config(None, None) == Error.INVALID_HANDLE
+    assert L.ffdas_sparse_select(None, None, None, 4, 16, 2, None, None, None) == Error.INVALID_HANDLE
     assert L.ffdas_contiguous_copy(None, None, None, None, None) == Error.INVALID_HANDLE
     assert L.ffdas_event_record(None, 1) == Error.INVALID_HANDLE
     assert L.ffdas_event_synchronize(0) == Error.INVALID_ARGUMENT
