@@ -247,7 +247,7 @@ ffdas_error_t ffdas_das_set_config(ffdas_handle_t h, const ffdas_das_config_t *c
     }
     const ffdas_das_config_t &c = *config;
     auto pow2_or_zero = [](int v, int hi) { return v == 0 || (v > 0 && v <= hi && (v & (v - 1)) == 0); };
-    if (c.variant < 0 || c.variant > 3) return FFDAS_ERROR_INVALID_ARGUMENT;
+    if (c.variant < 0 || c.variant > 5 || c.variant == 4) return FFDAS_ERROR_INVALID_ARGUMENT;
     if (!pow2_or_zero(c.tile_x, 256) || !pow2_or_zero(c.tile_y, 256) || !pow2_or_zero(c.tile_z, 256))
         return FFDAS_ERROR_INVALID_ARGUMENT;
     if (!pow2_or_zero(c.batch_tile, 16)) return FFDAS_ERROR_INVALID_ARGUMENT;
@@ -255,7 +255,9 @@ ffdas_error_t ffdas_das_set_config(ffdas_handle_t h, const ffdas_das_config_t *c
     if (c.min_blocks < 0 || c.min_blocks > 32) return FFDAS_ERROR_INVALID_ARGUMENT;
     if (c.copy_engine < 0 || c.copy_engine > 2) return FFDAS_ERROR_INVALID_ARGUMENT;
     int tx = c.tile_x ? c.tile_x : 1, ty = c.tile_y ? c.tile_y : 1, tz = c.tile_z ? c.tile_z : 1;
-    if ((c.tile_x || c.tile_y || c.tile_z) && (tx * ty * tz < 32 || tx * ty * tz > 1024))
+    // variant 5 reads tile_x as lanes per voxel (1..32)
+    if (c.variant == 5 && (c.tile_x > 32 || c.tile_y > 1 || c.tile_z > 1)) return FFDAS_ERROR_INVALID_ARGUMENT;
+    if (c.variant != 5 && (c.tile_x || c.tile_y || c.tile_z) && (tx * ty * tz < 32 || tx * ty * tz > 1024))
         return FFDAS_ERROR_INVALID_ARGUMENT;
     h->config = c;
     h->has_config = true;

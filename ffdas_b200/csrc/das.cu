@@ -13,6 +13,7 @@
 
 #include "core.h"
 #include "das_problem.h"
+#include "das_direct.h"
 #include "das_gather.cuh"
 
 namespace ffdas {
@@ -411,6 +412,21 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
     if (pb.C > 0 && !a.srcpos) return FFDAS_ERROR_NULL_POINTER;
     if ((int64_t)pb.B * pb.C * pb.S * pb.N > 0 && !a.x) return FFDAS_ERROR_NULL_POINTER;
     if (a.sparse && !a.sparse_indices) return FFDAS_ERROR_NULL_POINTER;
+
+    // ---- small problems: the whole call as one launch straight from x ----
+    if (direct_supported(pb, xd.dtype, od.dtype, kind)) {
+        const bool asked = h.has_config && h.config.variant == 5;
+        const bool planner = !h.has_config || h.config.variant == 0;
+        const int64_t units = pb.V * pb.C * (int64_t)pb.S * pb.B;
+        if (asked || (planner && units <= (pb.B == 1 ? kDirectUnits : kDirectUnitsBatched))) {
+            double br = 0.0, bi = 0.0;
+            int bz = 1;
+            read_beta(od.dtype, a.beta, br, bi, bz);
+            return launch_direct(h, pb, xd.dtype, a.x, a.srcpos, a.srcdir, a.dstpos, a.offsets, a.weights,
+                                 static_cast<float *>(a.out), br, bz, asked ? h.config.batch_tile : 0,
+                                 asked ? h.config.tile_x : 0);
+        }
+    }
 
     // ---- ingest: x -> pair rows (workspace) ----
     const int64_t npad = pair_row_length(pb.N);

@@ -16,6 +16,7 @@ import os
 import threading
 from pathlib import Path
 
+import numpy as np
 import torch
 
 from .library import get_library_handle
@@ -40,6 +41,11 @@ def _grid_dims(dstpos) -> tuple[int, int]:
     d0 = dims[-1] if dims else 1
     d1 = dims[-2] if len(dims) >= 2 else 1
     return d0, d1
+
+
+# Largest problem (voxels x channels x events x items) for which the direct
+# kernel is among the candidates: twice the planner's own threshold.
+DIRECT_UNITS_MAX = 2 << 25
 
 
 def candidates(x, dstpos, offsets, sparse_indices=None) -> list[dict]:
@@ -72,6 +78,17 @@ def candidates(x, dstpos, offsets, sparse_indices=None) -> list[dict]:
                     for ec in sorted({4, 8} if bt <= 4 else {4}):
                         out.append(dict(variant=2, tile_x=t0, tile_y=t1, window=wb, event_chunk=ec, copy_engine=1,
                                         batch_tile=bt))
+    if real and sparse_indices is None and x.dtype != torch.float64:
+        # direct kernel (one launch, no pair workspace) for small problems
+        V = int(np.prod(dstpos.shape[:-1]))
+        C, S = x.shape[-3], offsets.shape[0]
+        if V * C * S * B <= DIRECT_UNITS_MAX:
+            for bt in sorted({1, min(2, B), min(4, B)}):
+                if bt & (bt - 1) == 0:
+                    out.append(dict(variant=5, batch_tile=bt))   # lanes per voxel from the occupancy
+                    for lanes in (2, 4, 8, 16, 32):
+                        if lanes <= C:
+                            out.append(dict(variant=5, batch_tile=bt, tile_x=lanes))
     if real and sparse_indices is None:
         # staged kernel with 512-voxel tiles (two voxels per thread)
         n_ev = offsets.shape[0]

@@ -138,8 +138,11 @@ typedef struct ffdas_tensor_desc* ffdas_tensor_desc_t;
  * means "planner default".  The autotuner sweeps these. */
 typedef struct {
     int32_t variant;      /* 0 auto, 1 L1 gather kernel, 2 TMA-staged kernel (forward and adjoint),
-                             3 gather adjoint in ffdas_das_backward (forward as 0) */
-    int32_t tile_x;       /* voxels per CTA along the innermost spatial dim */
+                             3 gather adjoint in ffdas_das_backward (forward as 0),
+                             5 direct kernel: one launch, no workspace, for small real problems
+                               (forward; the adjoint as 0) */
+    int32_t tile_x;       /* voxels per CTA along the innermost spatial dim
+                             (variant 5: lanes per voxel, 1..32, 0 = from the occupancy) */
     int32_t tile_y;       /* ... along the middle spatial dim */
     int32_t tile_z;       /* ... along the outermost spatial dim */
     int32_t batch_tile;   /* batch items per thread (1,2,4,8,16) */

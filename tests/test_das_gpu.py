@@ -272,3 +272,63 @@ def test_runs_on_current_stream(rng):
     s.synchronize()
     ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w))
     assert oracle.rel_l2(_np(got), ref) < 2e-5
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float16, torch.bfloat16])
+@pytest.mark.parametrize("B,bt", [(1, 1), (3, 2), (5, 4), (2, 4)])
+def test_direct_kernel(dtype, B, bt):
+    # one launch straight from x (no pair workspace): same taps as the f32
+    # pairs of the other kernels, so the FP32 bound holds for all three inputs
+    from ffdas_b200.tune import schedule
+    wl = W.diverging3d(device=DEV, scale=0.125)
+    x = (wl["x"].expand(B, *wl["x"].shape[1:]) * torch.arange(1, B + 1, device=DEV).view(B, 1, 1, 1)).to(dtype)
+    h = ffdas_b200.get_library_handle(DEV)
+    with schedule(dict(variant=5, batch_tile=bt), DEV):
+        got = ffdas_b200.das(x, wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"])
+        info = h.last_kernel_info()
+    assert info["variant"] == 5 and info["kernels"] == 1 and info["batch_tile"] == min(bt, 4 if B >= 4 else (2 if B >= 2 else 1))
+    ref = oracle.das_f64(_np(x.float()), _np(wl["srcpos"]), _np(wl["dstpos"]), _np(wl["offsets"]), _np(wl["weights"]))
+    assert oracle.rel_l2(_np(got), ref) < TOL[torch.float32]
+    with schedule(dict(variant=2, tile_x=32, tile_y=8, window=32), DEV):
+        staged = ffdas_b200.das(x, wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"])
+    if dtype == torch.float32:
+        assert oracle.rel_l2(_np(got), _np(staged)) < 1e-6
+
+
+def test_planner_takes_the_direct_kernel_for_small_frames():
+    h = ffdas_b200.get_library_handle(DEV)
+    h.set_config(None)
+    small = W.plane2d(device=DEV, scale=0.5)
+    out = ffdas_b200.das(small["x"], small["srcpos"], small["dstpos"], small["offsets"], small["weights"])
+    info = h.last_kernel_info()
+    assert info["variant"] == 5 and info["kernels"] == 1
+    assert oracle.rel_l2(_np(out), _oracle_of(small)) < TOL[torch.float32]
+    # complex data, sparse lists and 16-bit pair storage keep the other kernels
+    sp = W.sparse_focus(device=DEV, scale=0.2)
+    _run(sp)
+    assert h.last_kernel_info()["variant"] == 1
+    _run(small, small["x"].float(), use_fp16=True)
+    assert h.last_kernel_info()["variant"] != 5
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 8, 32])
+def test_direct_kernel_lanes_per_voxel(lanes):
+    # lanes share a voxel's channels (ragged: 37 channels over 4-channel
+    # unrolled steps); every split gives the same image up to summation order
+    from ffdas_b200.tune import schedule
+    g = torch.Generator().manual_seed(lanes)
+    C, S, N = 37, 3, 300
+    x = torch.randn((2, C, S, N), generator=g)
+    src = torch.zeros((C, 3))
+    src[:, 0] = torch.linspace(-6, 6, C)
+    zz, xx = torch.meshgrid(torch.linspace(20, 120, 50), torch.linspace(-8, 8, 30), indexing="ij")
+    dst = torch.stack([xx, torch.zeros_like(xx), zz], -1)
+    offs = zz[None].expand(S, -1, -1) + torch.rand((S, 50, 30), generator=g) * 5
+    w = torch.rand((S, 50, 30), generator=g)
+    h = ffdas_b200.get_library_handle(DEV)
+    with schedule(dict(variant=5, tile_x=lanes, batch_tile=2), DEV):
+        got = ffdas_b200.das(x.to(DEV), src.to(DEV), dst.to(DEV), offs.to(DEV), w.to(DEV))
+        info = h.last_kernel_info()
+    assert info["variant"] == 5 and info["tile_x"] == lanes
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w))
+    assert oracle.rel_l2(_np(got), ref) < TOL[torch.float32]

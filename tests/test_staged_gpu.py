@@ -177,7 +177,8 @@ def test_autotune_picks_a_correct_schedule(tmp_path, monkeypatch):
 
 
 @pytest.mark.parametrize("cfg", [dict(variant=1, tile_x=32, tile_y=8), dict(variant=2, tile_x=32, tile_y=8, window=32),
-                                 dict(variant=2, tile_x=32, tile_y=16, window=32)], ids=["gather", "staged256", "staged512"])
+                                 dict(variant=2, tile_x=32, tile_y=16, window=32), dict(variant=5, batch_tile=4)],
+                         ids=["gather", "staged256", "staged512", "direct"])
 def test_beta_accumulates_into_out(cfg):
     # out = beta * out + das(...), through the C-ABI (the Python API has no beta)
     import ctypes
@@ -230,11 +231,12 @@ def test_batch_tiles_16bit(dtype, flag):
 def test_default_planner_picks_staged_for_dense_volumes():
     h = ffdas_b200.get_library_handle(DEV)
     h.set_config(None)
-    wl = W.diverging3d(device=DEV, scale=0.25)
+    wl = W.diverging3d(device=DEV, scale=0.4)   # 1.3e8 units: above the direct kernel's range
     out = ffdas_b200.das(wl["x"], wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"])
     info = h.last_kernel_info()
     assert info["variant"] == 2 and info["tile_x"] * info["tile_y"] * info["tile_z"] == 512
-    assert oracle.rel_l2(_np(out), _ref(wl, wl["x"])) < 2e-5
+    # 1638 samples: delays up to ~1.6e3, so the fp32 delay rounding bound is wider
+    assert oracle.rel_l2(_np(out), _ref(wl, wl["x"])) < 5e-5
     af = W.autofocus(device=DEV, scale=0.25)
     out = ffdas_b200.das(af["x"], af["srcpos"], af["dstpos"], af["offsets"], af["weights"])
     info = h.last_kernel_info()
