@@ -432,7 +432,8 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
     const int64_t npad = pair_row_length(pb.N);
     const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
     workspace P(h);
-    FFDAS_TRY(P.alloc((size_t)std::max<int64_t>(rows, 1) * npad * storage_bytes(kind)));
+    const size_t pair_bytes = ((size_t)std::max<int64_t>(rows, 1) * npad * storage_bytes(kind) + 255) & ~size_t(255);
+    FFDAS_TRY(P.alloc(pair_bytes + (a.sparse ? 256 : 0)));   // das_sparse: a gate word after the pairs
     FFDAS_TRY(launch_ingest(h, pb, xd.dtype, kind, a.x, npad, P.get<void>()));
 
     // ---- forward kernel ----
@@ -506,6 +507,74 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
                                                 dim3((unsigned)tiles, (unsigned)bchunks_st, (unsigned)csplit));
         h.mark_stop();
         return err;
+    }
+    // das_sparse on the 512-voxel staged kernel: each pass runs over x's
+    // events and each voxel takes the list entry naming the event, so the
+    // work is that of the dense call over x's S events.  The planner takes it
+    // for 256+ channels and S at most 4x the list length (measured on B200:
+    // 3-D volumes of 256-1024 channels 1.5-3.1x faster than the gather
+    // kernel; a 128-channel 2-D frame is faster on the gather kernel, whose
+    // per-voxel list walk costs less than the staged pass's list scan), or
+    // when the schedule asks for variant 2.  A
+    // list that names an event twice sets a device gate: the staged kernel
+    // then does nothing and the gather kernel, launched after it and
+    // otherwise idle, computes the call -- no host round trip, and the call
+    // stays capturable in a CUDA graph.
+    const bool real_pairs = (kind == ST_F32 || kind == ST_F16 || kind == ST_BF16);
+    if (a.sparse && real_pairs && od.dtype == FFDAS_R_32F && staged_batch_supported() && npad >= 64 &&
+        rows < INT32_MAX && !(h.has_config && h.config.variant == 1) &&
+        ((h.has_config && h.config.variant == 2) ||
+         (!h.has_config && pb.C >= 256 && (int64_t)pb.S <= 4 * (int64_t)pb.n_events))) {
+        gather_params sg = gp;
+        const ffdas_das_config_t *c = h.has_config ? &h.config : nullptr;
+        int T0, T1;
+        if (c && c->tile_x * (c->tile_y ? c->tile_y : 1) == 512) {
+            T0 = c->tile_x; T1 = c->tile_y ? c->tile_y : 1;
+        } else if (pb.D1 <= 1) {
+            T0 = 512; T1 = 1;
+        } else {
+            T0 = std::min(32, std::max(1, floor_pow2(pb.D0))); T1 = 512 / T0;
+        }
+        sg.T0 = T0; sg.T1 = T1; sg.T2 = 1;
+        sg.n0 = (pb.D0 + T0 - 1) / T0;
+        sg.n1 = (pb.D1 + T1 - 1) / T1;
+        sg.cchunk = 0;
+        const int64_t stiles = (int64_t)sg.n0 * sg.n1 * pb.D2;
+        // channel slices for grids that leave SMs idle, as in the dense call
+        int csplit = 1;
+        {
+            const int per_sm = (c && c->min_blocks) ? c->min_blocks : 3;
+            const int64_t want = (int64_t)std::max(h.sm_count, 1) * per_sm;
+            while (stiles * pb.B * csplit * 2 <= want && pb.C >= 64 * csplit && csplit < 64) csplit *= 2;
+        }
+        if (csplit > 1) {
+            const int chunk = ((pb.C + csplit - 1) / csplit + 31) / 32 * 32;   // whole stages of channels
+            csplit = (pb.C + chunk - 1) / chunk;
+            sg.cchunk = csplit > 1 ? chunk : 0;
+        }
+        const int SCs = (c && c->event_chunk) ? (c->event_chunk <= 1 ? 1 : (c->event_chunk <= 4 ? 4 : 8))
+                                              : (pb.S <= 1 ? 1 : (pb.S <= 4 ? 4 : 8));
+        const int WBs = (c && c->window > 32) ? 64 : 32;
+        const int copy = c ? c->copy_engine : 0;
+        if (stiles <= INT32_MAX && pb.B <= 65535) {
+            int *gate = reinterpret_cast<int *>(static_cast<char *>(P.get<void>()) + pair_bytes);
+            h.last.variant = 2;
+            h.last.tile_x = T0; h.last.tile_y = T1; h.last.tile_z = 1;
+            h.last.batch_tile = 1;
+            h.last.event_chunk = SCs;
+            h.last.kernels = csplit > 1 ? 5 : 4;   // ingest, list check, (image preparation,) staged, gated gather
+            h.last.grid = stiles * pb.B * csplit;
+            h.mark_start();
+            ffdas_error_t err = launch_staged_sparse(h, pb, kind, sg, SCs, WBs, copy,
+                                                     dim3((unsigned)stiles, (unsigned)pb.B, (unsigned)csplit), gate);
+            if (err == FFDAS_SUCCESS) {
+                gather_params fg = gp;
+                fg.run_if = gate;
+                err = launch_gather<true>(h, kind, od.dtype, fg, s, grid);
+            }
+            h.mark_stop();
+            return err;
+        }
     }
     h.mark_start();
     const ffdas_error_t err = a.sparse ? launch_gather<true>(h, kind, od.dtype, gp, s, grid)

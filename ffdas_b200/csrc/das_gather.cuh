@@ -40,6 +40,7 @@ struct gather_params {
     double beta_re, beta_im;
     int beta_zero;
     int cchunk;               // staged forward: channels per blockIdx.z slice (0: no split)
+    const int *run_if;        // when set, the kernel runs only if *run_if != 0 (das_sparse fallback)
 };
 
 template <typename A> struct acc_ops;
@@ -156,6 +157,7 @@ __global__ void __launch_bounds__(256) das_gather_kernel(const gather_params p) 
     using tr = pair_traits<K>;
     using st = typename tr::storage;
     using acc_t = typename tr::acc;
+    if (p.run_if && *(volatile const int *)p.run_if == 0) return;   // uniform for the grid
 
     int tid = threadIdx.x;
     const int tile = blockIdx.x;

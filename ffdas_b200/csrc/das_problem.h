@@ -83,6 +83,10 @@ struct staged_grads {
     int64_t gout_bstride;
     float *gx, *goff, *gw, *gdst, *gsrc;
 };
+// das_sparse on the 512-voxel staged kernel: zeroes *gate, flags lists that
+// name an event twice, then runs the kernel (which does nothing when flagged).
+ffdas_error_t launch_staged_sparse(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,
+                                   int SC, int WB, int copy, dim3 grid, int *gate);
 ffdas_error_t launch_staged_bwd(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,
                                 const staged_grads &gr, int SC, int WB, int BT, int copy, dim3 grid);
 

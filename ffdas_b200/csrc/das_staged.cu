@@ -220,7 +220,7 @@ ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, c
         if (grid.z < 2) return FFDAS_ERROR_INTERNAL;
         dim3 sg((unsigned)((pb.V + 255) / 256), (unsigned)std::min(pb.B, 65535));
         scale_image_kernel<<<sg, 256, 0, h.stream>>>(static_cast<float *>(gp.out), pb.out_bstride, pb.V, pb.B,
-                                                     (float)gp.beta_re, gp.beta_zero);
+                                                     (float)gp.beta_re, gp.beta_zero, nullptr);
         FFDAS_TRY(ffdas_launch_check(h.stream));
     }
     if (BT > 1) copy = 1;   // batch tiles stage their windows with 3-D TMA boxes
@@ -248,6 +248,73 @@ ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, c
                                 : launch_fwd_batch<ST_BF16, 32>(h, sp, map, SC, BT, grid);
         }
     }
+    switch (kind) {
+        case ST_F32:
+            return WB == 64 ? launch_fwd_sc<ST_F32, 64>(h, sp, map, SC, grid) : launch_fwd_sc<ST_F32, 32>(h, sp, map, SC, grid);
+        case ST_F16:
+            return WB == 64 ? launch_fwd_sc<ST_F16, 64>(h, sp, map, SC, grid) : launch_fwd_sc<ST_F16, 32>(h, sp, map, SC, grid);
+        default:
+            return WB == 64 ? launch_fwd_sc<ST_BF16, 64>(h, sp, map, SC, grid) : launch_fwd_sc<ST_BF16, 32>(h, sp, map, SC, grid);
+    }
+}
+
+// das_sparse lists that name an event twice with nonzero weights (the staged
+// pass holds one entry per voxel and event): sets *gate.  Zero-weight entries
+// and events outside x are ignored, as both kernels ignore them.
+__global__ void __launch_bounds__(256) sparse_duplicate_kernel(const int *__restrict__ idx,
+                                                               const float *__restrict__ w, int n, int S,
+                                                               int64_t V, int *gate) {
+    const int64_t v = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (v >= V) return;
+    bool dup = false;
+    if (S <= 64) {
+        unsigned long long seen = 0ull;
+        for (int i = 0; i < n && !dup; i++) {
+            const int s = __ldg(idx + (int64_t)i * V + v);
+            if ((unsigned)s < (unsigned)S && __ldg(w + (int64_t)i * V + v) != 0.f) {
+                const unsigned long long bit = 1ull << s;
+                dup = (seen & bit) != 0ull;
+                seen |= bit;
+            }
+        }
+    } else {
+        for (int i = 1; i < n && !dup; i++) {
+            const int s = __ldg(idx + (int64_t)i * V + v);
+            if ((unsigned)s >= (unsigned)S || __ldg(w + (int64_t)i * V + v) == 0.f) continue;
+            for (int j = 0; j < i && !dup; j++)
+                dup = __ldg(idx + (int64_t)j * V + v) == s && __ldg(w + (int64_t)j * V + v) != 0.f;
+        }
+    }
+    if (dup) atomicExch(gate, 1);
+}
+
+ffdas_error_t launch_staged_sparse(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,
+                                   int SC, int WB, int copy, dim3 grid, int *gate) {
+    if (gp.T0 * gp.T1 * gp.T2 != 2 * kStConsumers || !gp.sparse_idx) return FFDAS_ERROR_INTERNAL;
+    if (gp.cchunk && grid.z < 2) return FFDAS_ERROR_INTERNAL;
+    FFDAS_CUDA(cudaMemsetAsync(gate, 0, sizeof(int), h.stream));
+    const int64_t vb = (pb.V + 255) / 256;
+    if (vb > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
+    sparse_duplicate_kernel<<<(unsigned)vb, 256, 0, h.stream>>>(gp.sparse_idx, gp.weights, pb.n_events, pb.S, pb.V,
+                                                               gate);
+    FFDAS_TRY(ffdas_launch_check(h.stream));
+    if (gp.cchunk) {   // channel slices add into the image: prepare it unless the call falls back
+        dim3 sg((unsigned)vb, (unsigned)std::min(pb.B, 65535));
+        scale_image_kernel<<<sg, 256, 0, h.stream>>>(static_cast<float *>(gp.out), pb.out_bstride, pb.V, pb.B,
+                                                     (float)gp.beta_re, gp.beta_zero, gate);
+        FFDAS_TRY(ffdas_launch_check(h.stream));
+    }
+    copy = resolve_copy(copy);
+    CUtensorMap map;
+    std::memset(&map, 0, sizeof(map));
+    if (copy == 1) FFDAS_TRY(pair_row_map(map, gp.P, gp.npad, (int64_t)pb.B * pb.C * pb.S, kind, WB));
+    staged_params sp = base_params(h, pb, gp);
+    sp.copy_async = copy == 2;
+    sp.n_events = pb.S;            // passes run over x's events
+    sp.sparse_idx = gp.sparse_idx;
+    sp.sparse_n = pb.n_events;     // list length
+    sp.gate = gate;
+    h.last.copy_engine = copy;
     switch (kind) {
         case ST_F32:
             return WB == 64 ? launch_fwd_sc<ST_F32, 64>(h, sp, map, SC, grid) : launch_fwd_sc<ST_F32, 32>(h, sp, map, SC, grid);

@@ -62,6 +62,11 @@ struct staged_params {
     int debug_drop_stage;  // test hook: the producer never fills the first stage
     int copy_async;        // 1: windows staged by per-lane cp.async copies instead of TMA tile loads
     int cchunk;            // forward: channels per blockIdx.z slice (0: all channels in one CTA)
+    // das_sparse on the 512-voxel kernel: per-voxel lists (sparse_n, V) of events of x;
+    // the passes run over x's events and each voxel takes the list entry naming the event
+    const int *sparse_idx;
+    int sparse_n;
+    const int *gate;       // when set and *gate != 0 the kernel does nothing (a duplicate listed event)
     // adjoint only
     const float *gout;
     int64_t gout_bstride;
@@ -501,26 +506,63 @@ __device__ __forceinline__ void staged_pass_begin2(const staged_params &p, stage
                                                    const staged_ctx &cx, int e0, int sc, float2 (&ofs2)[SC],
                                                    float2 (&w2)[SC]) {
     if (!cx.producer) {
+        // absent taps: delay 1e30 (its index clamps to the zero pair, its
+        // fraction is 0) and weight 0, left out of the tile's delay range
+        uint32_t present = 0u;   // bit 2j: voxel 1 has event e0 + j, bit 2j+1: voxel 2
 #pragma unroll
         for (int j = 0; j < SC; j++) {
             ofs2[j] = make_float2(1e30f, 1e30f);
             w2[j] = make_float2(0.f, 0.f);
-            if (j < sc) {
-                const int64_t base = (int64_t)(e0 + j) * p.V;
+        }
+        if (!p.sparse_idx) {
+#pragma unroll
+            for (int j = 0; j < SC; j++) {
+                if (j < sc) {
+                    const int64_t base = (int64_t)(e0 + j) * p.V;
+                    if (cx.active) {
+                        ofs2[j].x = __ldg(p.offsets + base + cx.v);
+                        w2[j].x = __ldg(p.weights + base + cx.v);
+                        present |= 1u << (2 * j);
+                    }
+                    if (cx.active2) {
+                        ofs2[j].y = __ldg(p.offsets + base + cx.v2);
+                        w2[j].y = __ldg(p.weights + base + cx.v2);
+                        present |= 2u << (2 * j);
+                    }
+                }
+            }
+        } else {
+            // das_sparse: each voxel's list entry that names event e0 + j
+            // (zero-weight entries and events outside x add nothing, as in the
+            // gather kernel; a doubly listed event never reaches this kernel)
+            for (int i = 0; i < p.sparse_n; i++) {
+                const int64_t base = (int64_t)i * p.V;
                 if (cx.active) {
-                    ofs2[j].x = __ldg(p.offsets + base + cx.v);
-                    w2[j].x = __ldg(p.weights + base + cx.v);
+                    const uint32_t j = (uint32_t)(__ldg(p.sparse_idx + base + cx.v) - e0);
+                    const float wv = __ldg(p.weights + base + cx.v);
+                    if (j < (uint32_t)sc && wv != 0.f) {
+                        const float ov = __ldg(p.offsets + base + cx.v);
+#pragma unroll
+                        for (int jj = 0; jj < SC; jj++)
+                            if (j == (uint32_t)jj) { ofs2[jj].x = ov; w2[jj].x = wv; present |= 1u << (2 * jj); }
+                    }
                 }
                 if (cx.active2) {
-                    ofs2[j].y = __ldg(p.offsets + base + cx.v2);
-                    w2[j].y = __ldg(p.weights + base + cx.v2);
+                    const uint32_t j = (uint32_t)(__ldg(p.sparse_idx + base + cx.v2) - e0);
+                    const float wv = __ldg(p.weights + base + cx.v2);
+                    if (j < (uint32_t)sc && wv != 0.f) {
+                        const float ov = __ldg(p.offsets + base + cx.v2);
+#pragma unroll
+                        for (int jj = 0; jj < SC; jj++)
+                            if (j == (uint32_t)jj) { ofs2[jj].y = ov; w2[jj].y = wv; present |= 2u << (2 * jj); }
+                    }
                 }
             }
         }
 #pragma unroll
         for (int j = 0; j < SC; j++) {
-            const bool oka = cx.active && j < sc && isfinite(ofs2[j].x);
-            const bool okb = cx.active2 && j < sc && isfinite(ofs2[j].y);
+            const bool oka = ((present >> (2 * j)) & 1u) && isfinite(ofs2[j].x);
+            const bool okb = ((present >> (2 * j)) & 2u) && isfinite(ofs2[j].y);
             float lo = fminf(oka ? ofs2[j].x : INFINITY, okb ? ofs2[j].y : INFINITY);
             float hi = fmaxf(oka ? ofs2[j].x : -INFINITY, okb ? ofs2[j].y : -INFINITY);
 #pragma unroll
@@ -922,6 +964,9 @@ __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kerne
     constexpr int CC = kStWin / SC;  // channels per stage
     static_assert(kStWin % SC == 0, "SC must divide the stage");
 
+    // a das_sparse call whose lists name an event twice runs on the gather
+    // kernel instead (uniform for the whole grid, before any barrier or copy)
+    if (p.gate && *(volatile const int *)p.gate) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     staged_smem<K, WB> sm(smem_raw);
     const staged_ctx cx = staged_setup<K, WB>(p, sm, false, 2);
@@ -1948,7 +1993,8 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
 // Prepares the image for channel slices that add into it: out = beta * out
 // (or 0) for every batch item and voxel.
 __global__ void __launch_bounds__(256) scale_image_kernel(float *out, int64_t bstride, int64_t V, int B,
-                                                          float beta, int beta_zero) {
+                                                          float beta, int beta_zero, const int *gate) {
+    if (gate && *(volatile const int *)gate) return;   // the staged call is off: the gather kernel applies beta
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= V) return;
     for (int b = blockIdx.y; b < B; b += gridDim.y) {

@@ -89,6 +89,16 @@ def candidates(x, dstpos, offsets, sparse_indices=None) -> list[dict]:
                     for lanes in (2, 4, 8, 16, 32):
                         if lanes <= C:
                             out.append(dict(variant=5, batch_tile=bt, tile_x=lanes))
+    if real and sparse_indices is not None and x.dtype != torch.float64:
+        # das_sparse on the staged kernel: 512-voxel tiles, passes over x's events
+        S = x.shape[-2]
+        for t0 in (128, 64, 32, 16, 8):
+            t1 = 512 // t0
+            if t0 <= max(d0, 8) * 2 and t1 <= max(d1, 1) * 2:
+                for wb in (32, 64):
+                    for ec in sorted({min(c, max(S, 1)) for c in (4, 8)}):
+                        out.append(dict(variant=2, tile_x=t0, tile_y=t1, window=wb, event_chunk=ec, copy_engine=1,
+                                        batch_tile=1))
     if real and sparse_indices is None:
         # staged kernel with 512-voxel tiles (two voxels per thread)
         n_ev = offsets.shape[0]

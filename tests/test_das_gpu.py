@@ -306,7 +306,7 @@ def test_planner_takes_the_direct_kernel_for_small_frames():
     # complex data, sparse lists and 16-bit pair storage keep the other kernels
     sp = W.sparse_focus(device=DEV, scale=0.2)
     _run(sp)
-    assert h.last_kernel_info()["variant"] == 1
+    assert h.last_kernel_info()["variant"] != 5
     _run(small, small["x"].float(), use_fp16=True)
     assert h.last_kernel_info()["variant"] != 5
 
@@ -332,3 +332,92 @@ def test_direct_kernel_lanes_per_voxel(lanes):
     assert info["variant"] == 5 and info["tile_x"] == lanes
     ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w))
     assert oracle.rel_l2(_np(got), ref) < TOL[torch.float32]
+
+
+@pytest.mark.parametrize("B", [1, 2])
+def test_sparse_on_the_staged_kernel(rng, B):
+    # lists over x's events run on the 512-voxel staged kernel (each pass takes
+    # the entry naming its event); same image as the gather kernel and the oracle
+    from ffdas_b200.tune import schedule
+    x, src, dst, offs, w = _small(rng, B=B, C=9, S=8, N=200, V=(40, 30))
+    g = torch.Generator().manual_seed(21)
+    n = 5
+    V = dst.shape[:-1]
+    perm = torch.argsort(torch.rand((8, *V), generator=g), dim=0)[:n].int()   # distinct events per voxel
+    ofs_s = (torch.rand((n, *V), generator=g) * 60 - 10).float()
+    w_s = (torch.rand((n, *V), generator=g) + 0.1).float()
+    w_s[-1, ::3] = 0.0                                                     # zero-weight padding
+    perm[-1, ::3] = perm[0, ::3]                                           # ... repeating an index
+    idx, ofs_s, w_s = perm.to(DEV), ofs_s.to(DEV), w_s.to(DEV)
+    h = ffdas_b200.get_library_handle(DEV)
+    with schedule(dict(variant=2), DEV):
+        got = ffdas_b200.das_sparse(x, src, dst, ofs_s, w_s, idx)
+        info = h.last_kernel_info()
+    assert info["variant"] == 2 and info["kernels"] == 4 and info["tile_x"] * info["tile_y"] == 512
+    with schedule(dict(variant=1), DEV):
+        gat = ffdas_b200.das_sparse(x, src, dst, ofs_s, w_s, idx)
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(ofs_s), _np(w_s), sparse_indices=_np(idx))
+    assert oracle.rel_l2(_np(got), ref) < TOL[torch.float32]
+    assert oracle.rel_l2(_np(got), _np(gat)) < 1e-6
+
+
+def test_sparse_list_naming_an_event_twice_falls_back_on_the_device(rng):
+    # the staged pass holds one entry per voxel and event: a doubly named event
+    # (both weights nonzero) sets the device gate and the gather kernel
+    # computes the call; the result is the oracle's either way
+    x, src, dst, offs, w = _small(rng, C=6, S=4, N=150, V=(20, 16))
+    V = dst.shape[:-1]
+    g = torch.Generator().manual_seed(5)
+    idx = torch.stack([torch.full(V, e, dtype=torch.int32) for e in (0, 1, 2, 3)])
+    idx[3, 4, 5] = 1                                                       # voxel (4, 5) names event 1 twice
+    ofs_s = (torch.rand((4, *V), generator=g) * 40).float()
+    w_s = (torch.rand((4, *V), generator=g) + 0.1).float()
+    idx, ofs_s, w_s = idx.to(DEV), ofs_s.to(DEV), w_s.to(DEV)
+    from ffdas_b200.tune import schedule
+    h = ffdas_b200.get_library_handle(DEV)
+    with schedule(dict(variant=2), DEV):
+        got = ffdas_b200.das_sparse(x, src, dst, ofs_s, w_s, idx)
+        assert h.last_kernel_info()["kernels"] == 4
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(ofs_s), _np(w_s), sparse_indices=_np(idx))
+    assert oracle.rel_l2(_np(got), ref) < TOL[torch.float32]
+
+
+@pytest.mark.parametrize("dup", [False, True], ids=["staged", "fallback"])
+def test_sparse_channel_slices_with_beta(dup):
+    # 96 channels over a small grid: the staged sparse call (asked for with
+    # variant 2) splits the channels
+    # over CTAs that add into a prepared image (beta * out); with a doubly
+    # listed event the preparation is skipped and the gather kernel applies
+    # beta instead -- out = beta * out + das_sparse either way
+    import ctypes
+    from ffdas_b200 import _lib
+    from ffdas_b200._lib import DataType
+    rng = np.random.default_rng(3)
+    x, src, dst, offs, w = _small(rng, C=96, S=6, N=160, V=(24, 20))
+    V = dst.shape[:-1]
+    g = torch.Generator().manual_seed(9)
+    idx = torch.argsort(torch.rand((6, *V), generator=g), dim=0)[:4].int()
+    if dup:
+        idx[2, 3, 3] = idx[0, 3, 3]
+    ofs_s = (torch.rand((4, *V), generator=g) * 50).float()
+    w_s = (torch.rand((4, *V), generator=g) + 0.1).float()
+    idx, ofs_s, w_s = idx.to(DEV), ofs_s.to(DEV), w_s.to(DEV)
+    h = ffdas_b200.get_library_handle(DEV)
+    h.set_config(dict(variant=2))
+    L = _lib.load()
+    prev = torch.randn((1, *V), device=DEV)
+    out = prev.clone()
+    xd = _lib.TensorDesc(list(x.shape), None, DataType.R_32F)
+    od = _lib.TensorDesc(list(out.shape), None, DataType.R_32F)
+    beta = (ctypes.c_float * 2)(0.5, 0.0)
+    h.set_stream(torch.cuda.current_stream().cuda_stream)
+    _lib.check(L.ffdas_das_sparse(h.h, src.data_ptr(), None, 0.0, xd.desc, x.data_ptr(), dst.data_ptr(),
+                                  ofs_s.data_ptr(), w_s.data_ptr(), 4, idx.data_ptr(),
+                                  ctypes.cast(beta, ctypes.c_void_p), od.desc, out.data_ptr(), 0, 0))
+    info = h.last_kernel_info()
+    h.set_config(None)
+    torch.cuda.synchronize()
+    assert info["variant"] == 2 and info["kernels"] == 5
+    ref = 0.5 * _np(prev) + oracle.das_f64(_np(x), _np(src), _np(dst), _np(ofs_s), _np(w_s),
+                                          sparse_indices=_np(idx))
+    assert oracle.rel_l2(_np(out), ref) < TOL[torch.float32]
