@@ -478,6 +478,29 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
     h.last.kernels = 2;
     h.last.grid = tiles * bchunks;
 
+    // Complex (IQ) data on the staged complex kernel when the schedule asks
+    // for variant 2: 256-voxel tiles, the gather kernel's event chunk so that
+    // both sum in the same order.  The planner keeps complex data on the
+    // gather kernel: measured on B200 the two are level for single frames
+    // (3-D diverging volume, 1024 channels: 146 ms staged, 152 ms gather,
+    // 284 ms reference ALG1) -- both bound by the per-tap sincos and complex
+    // multiply-add -- and the gather kernel's batch tiles share the phase
+    // over frames (50-frame ensemble: 9.9 ms gather, 34.6 ms staged).
+    if ((kind == ST_C32 || kind == ST_C16) && od.dtype == FFDAS_C_32F && !a.sparse && staged_batch_supported() &&
+        npad >= 64 && rows < INT32_MAX && pb.B <= 65535 && h.has_config && h.config.variant == 2) {
+        gather_params cg = gp;
+        cg.cchunk = 0;
+        const int SCc = (h.has_config && h.config.event_chunk >= 8) ? 8 : 4;
+        h.last.variant = 2;
+        h.last.event_chunk = SCc;
+        h.last.batch_tile = 1;
+        h.last.grid = tiles * pb.B;
+        h.mark_start();
+        const ffdas_error_t err = launch_staged_cplx(h, pb, kind, cg, SCc, dim3((unsigned)tiles, (unsigned)pb.B));
+        h.mark_stop();
+        return err;
+    }
+
     const bool staged = s.variant == 2;
     if (staged) {
         const int bchunks_st = (pb.B + s.BT - 1) / s.BT;

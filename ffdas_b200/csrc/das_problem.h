@@ -83,6 +83,10 @@ struct staged_grads {
     int64_t gout_bstride;
     float *gx, *goff, *gw, *gdst, *gsrc;
 };
+// Complex (IQ) data on the staged kernel: 256-voxel tiles, 32-pair windows,
+// TMA copies, event chunk 4 or 8.
+ffdas_error_t launch_staged_cplx(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,
+                                 int SC, dim3 grid);
 // das_sparse on the 512-voxel staged kernel: zeroes *gate, flags lists that
 // name an event twice, then runs the kernel (which does nothing when flagged).
 ffdas_error_t launch_staged_sparse(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,

@@ -50,15 +50,23 @@ static int resolve_copy(int copy) {
 }
 
 // Tensor map over the pair rows: dims {npad, rows}, box {WB, 1}, zero OOB fill.
+static int staged_pair_bytes(int kind) {
+    return kind == ST_C32 ? 16 : ((kind == ST_F32 || kind == ST_C16) ? 8 : 4);
+}
+
+// 2-D map over the pair rows (one row per item, channel, event); a 16-byte
+// (complex f32) pair is two 8-byte elements, so its x coordinates and box
+// width count elements, not pairs.
 static ffdas_error_t pair_row_map(CUtensorMap &map, const void *P, int64_t npad, int64_t rows, int kind, int WB) {
     auto encode = tensor_map_encoder();
     if (!encode) return FFDAS_ERROR_CUDA_DRIVER;
-    const int pair_bytes = (kind == ST_F32) ? 8 : 4;
-    const cuuint64_t dims[2] = {(cuuint64_t)npad, (cuuint64_t)rows};
+    const int pair_bytes = staged_pair_bytes(kind);
+    const int units = pair_bytes == 16 ? 2 : 1;
+    const cuuint64_t dims[2] = {(cuuint64_t)(npad * units), (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)npad * pair_bytes};
-    const cuuint32_t box[2] = {(cuuint32_t)WB, 1u};
+    const cuuint32_t box[2] = {(cuuint32_t)(WB * units), 1u};
     const cuuint32_t estr[2] = {1u, 1u};
-    const CUresult r = encode(&map, pair_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32,
+    const CUresult r = encode(&map, pair_bytes >= 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32,
                               2, const_cast<void *>(P), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -207,7 +215,8 @@ static staged_params base_params(ffdas_context &h, const das_problem &pb, const 
     sp.srcpos = gp.srcpos; sp.srcdir = gp.srcdir; sp.dstpos = gp.dstpos;
     sp.offsets = gp.offsets; sp.weights = gp.weights;
     sp.out = gp.out; sp.out_bstride = gp.out_bstride;
-    sp.beta_re = gp.beta_re; sp.beta_zero = gp.beta_zero;
+    sp.beta_re = gp.beta_re; sp.beta_im = gp.beta_im; sp.beta_zero = gp.beta_zero;
+    sp.wavenum = gp.wavenum;
     sp.status = h.status;
     sp.debug_drop_stage = ffdas_take_debug_drop_stage();
     sp.cchunk = gp.cchunk;
@@ -256,6 +265,31 @@ ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, c
         default:
             return WB == 64 ? launch_fwd_sc<ST_BF16, 64>(h, sp, map, SC, grid) : launch_fwd_sc<ST_BF16, 32>(h, sp, map, SC, grid);
     }
+}
+
+template <int K, int SC>
+static ffdas_error_t launch_cplx_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
+    constexpr size_t smem = staged_smem_bytes<32, K>();
+    static bool ready = false;
+    if (!ready) {
+        FFDAS_TRY(prepare_kernel(das_staged_cplx_kernel<K, SC, 32>, smem));
+        ready = true;
+    }
+    das_staged_cplx_kernel<K, SC, 32><<<grid, kStThreads, smem, h.stream>>>(sp, map);
+    return ffdas_launch_check(h.stream);
+}
+
+ffdas_error_t launch_staged_cplx(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,
+                                 int SC, dim3 grid) {
+    if (kind != ST_C32 && kind != ST_C16) return FFDAS_ERROR_INTERNAL;
+    if (gp.cchunk || gp.T0 * gp.T1 * gp.T2 != kStConsumers) return FFDAS_ERROR_INTERNAL;
+    CUtensorMap map;
+    std::memset(&map, 0, sizeof(map));
+    FFDAS_TRY(pair_row_map(map, gp.P, gp.npad, (int64_t)pb.B * pb.C * pb.S, kind, 32));
+    staged_params sp = base_params(h, pb, gp);
+    h.last.copy_engine = 1;
+    if (kind == ST_C32) return SC >= 8 ? launch_cplx_t<ST_C32, 8>(h, sp, map, grid) : launch_cplx_t<ST_C32, 4>(h, sp, map, grid);
+    return SC >= 8 ? launch_cplx_t<ST_C16, 8>(h, sp, map, grid) : launch_cplx_t<ST_C16, 4>(h, sp, map, grid);
 }
 
 // das_sparse lists that name an event twice with nonzero weights (the staged

@@ -54,9 +54,10 @@ struct staged_params {
     const float *srcpos;
     const float4 *srcdir;
     const float *dstpos, *offsets, *weights;
+    float wavenum;             // complex data: phase rotation per sample of delay
     void *out;
     int64_t out_bstride;
-    double beta_re;
+    double beta_re, beta_im;   // beta_im: complex output only
     int beta_zero;
     int *status;
     int debug_drop_stage;  // test hook: the producer never fills the first stage
@@ -149,7 +150,9 @@ __device__ __forceinline__ bool bounded_wait(uint32_t bar, uint32_t parity, vola
 template <int K> struct staged_traits {
     using st = typename pair_traits<K>::storage;
     static constexpr int bytes = sizeof(st);
-    static constexpr int align_pairs = 16 / bytes;     // TMA x coordinate granularity
+    static constexpr int align_pairs = bytes >= 16 ? 1 : 16 / bytes;   // TMA x coordinate granularity
+    // TMA elements per pair: 16-byte (complex f32) pairs are two 8-byte elements
+    static constexpr int tma_units = bytes == 16 ? 2 : 1;
 };
 
 template <int WB, int K> struct slot_geom {
@@ -648,7 +651,8 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
                 if (k1 - k0 + 1 <= WB) {
                     if (!p.copy_async) {
                         const int row = (bb * p.C + c) * p.S + (e0 + j);
-                        tma_load_row(smem_u32(stage_base + lane * SG::bytes), tmap, k0, row, full_bar);
+                        tma_load_row(smem_u32(stage_base + lane * SG::bytes), tmap, k0 * staged_traits<K>::tma_units,
+                                     row, full_bar);
                     }
                     k0w = k0;
                     m = kFloorMagicBits + (uint32_t)k0;
@@ -1988,6 +1992,116 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
             p.gdst[3 * cx.v + 2] = gpz;
         }
     }
+}
+
+// ------------------------------------------------------- complex (IQ) data ---
+// Forward for complex channel data (complex64 pairs (x0, x1 - x0), or
+// complex32 pairs (x0, x1)) on the same producer and ring: one voxel per
+// consumer thread, SC events per pass.  A tap adds w (cos, sin)(wavenum tau)
+// x lerp with the reference's cmadd ordering (src/das/das_alg1_kernels.cuh:
+// 78-98); a tap outside the record reads the zero pair and adds an exact zero,
+// as in the gather kernel.  Channels, event chunks and events within a chunk
+// are summed in the gather kernel's order, so with the same event chunk the
+// two kernels agree bit for bit.
+template <int K, int SC, int WB>
+__global__ void __launch_bounds__(kStThreads) das_staged_cplx_kernel(const staged_params p,
+                                                                     const __grid_constant__ CUtensorMap tmap) {
+    using st = typename pair_traits<K>::storage;
+    using SG = slot_geom<WB, K>;
+    constexpr int CC = kStWin / SC;
+    static_assert(kStWin % SC == 0, "SC must divide the stage");
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    staged_smem<K, WB> sm(smem_raw);
+    const staged_ctx cx = staged_setup<K, WB>(p, sm);
+    const int cbeg = chan_begin(p), cend = chan_end(p);
+    const st *__restrict__ Pg = static_cast<const st *>(p.P);
+    const uint32_t kmax_pair = (uint32_t)(p.npad - 1);
+    const uint32_t nlast = (uint32_t)(p.N - 1);
+    const float wavenum = p.wavenum;
+    const bool srcdir = p.srcdir != nullptr;
+    float2 acc = make_float2(0.f, 0.f);
+    int stage = 0;
+    uint32_t phase = 0;
+    bool dead = false;
+    uint32_t issued_mask = 0;
+
+    for (int e0 = 0; e0 < p.n_events; e0 += SC) {
+        const int sc = min(SC, p.n_events - e0);
+        float ofs[SC], w[SC];
+        staged_pass_begin<K, WB, SC>(p, sm, cx, e0, sc, ofs, w);
+        for (int c0 = cbeg; c0 < cend; c0 += CC) {
+            if (cx.producer) {
+                staged_produce<K, WB, SC>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
+            } else {
+                const uint32_t full_bar = smem_u32(&sm.full[stage]);
+                if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
+                if (!dead && cx.active) {
+                    const unsigned char *stage_base = sm.ring + stage * SG::stage_bytes;
+                    const bool any_ovf = sm.ovf[stage] != 0;
+                    for (int cl = 0; cl < CC; cl++) {
+                        const int c = c0 + cl;
+                        if (c >= cend) break;
+                        const float4 cp = sm.chan_pos[stage * kStWin + cl];
+                        recv_geom gm = receive_geometry(cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z);
+                        if (srcdir)
+                            apply_directivity(gm, cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z, sm.chan_dir[stage * kStWin + cl]);
+                        uint32_t k0p[SC];
+                        load_meta<SC>(sm.meta, stage, cl, k0p);
+                        const unsigned char *slots = stage_base + (cl * SC) * SG::bytes;
+                        if (!any_ovf) {
+                            // branch-free: a tap outside the record reads the zero pair
+                            // (its window index clamps there) and adds an exact zero
+#pragma unroll
+                            for (int j = 0; j < SC; j++) {
+                                const float tau = __fmaf_rn(gm.rsq, gm.rinv, ofs[j]);
+                                const tau_split ts = split_tau(tau);
+                                const uint32_t rel = min(ts.k + kFloorMagicBits - k0p[j], (uint32_t)WB);
+                                const st pr = *reinterpret_cast<const st *>(slots + j * SG::bytes + rel * sizeof(st));
+                                float sn, cs;
+                                __sincosf(wavenum * tau, &sn, &cs);
+                                acc = cfma(make_float2(cs * w[j], sn * w[j]), pair_traits<K>::tap(pr, ts.t), acc);
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < SC; j++) {
+                                const float tau = __fmaf_rn(gm.rsq, gm.rinv, ofs[j]);
+                                const tau_split ts = split_tau(tau);
+                                if (ts.k < nlast) {
+                                    st pr;
+                                    if (k0p[j] == kOvf) {
+                                        const int64_t row = ((int64_t)cx.b * p.C + c) * p.S + (e0 + min(j, sc - 1));
+                                        pr = Pg[row * p.npad + min(ts.k, kmax_pair)];
+                                    } else {
+                                        const uint32_t rel = min(ts.k + kFloorMagicBits - k0p[j], (uint32_t)WB);
+                                        pr = *reinterpret_cast<const st *>(slots + j * SG::bytes + rel * sizeof(st));
+                                    }
+                                    float sn, cs;
+                                    __sincosf(wavenum * tau, &sn, &cs);
+                                    acc = cfma(make_float2(cs * w[j], sn * w[j]), pair_traits<K>::tap(pr, ts.t), acc);
+                                }
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+                if (cx.lane == 0) mbar_arrive(smem_u32(&sm.empty[stage]));
+            }
+            if (++stage == kStages) {
+                stage = 0;
+                phase ^= 1u;
+            }
+        }
+        __syncthreads();
+    }
+
+    if (cx.producer) {
+        staged_drain<K, WB>(sm, cx, stage, phase, issued_mask);
+        return;
+    }
+    if (dead || !cx.active) return;
+    float2 *o = static_cast<float2 *>(p.out) + (int64_t)cx.b * p.out_bstride + cx.v;
+    *o = p.beta_zero ? acc : cfma(make_float2((float)p.beta_re, (float)p.beta_im), *o, acc);
 }
 
 // Prepares the image for channel slices that add into it: out = beta * out

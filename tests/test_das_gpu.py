@@ -421,3 +421,38 @@ def test_sparse_channel_slices_with_beta(dup):
     ref = 0.5 * _np(prev) + oracle.das_f64(_np(x), _np(src), _np(dst), _np(ofs_s), _np(w_s),
                                           sparse_indices=_np(idx))
     assert oracle.rel_l2(_np(out), ref) < TOL[torch.float32]
+
+
+@pytest.mark.parametrize("dtype", [torch.complex64, torch.complex32])
+@pytest.mark.parametrize("B", [1, 2])
+def test_complex_on_the_staged_kernel(dtype, B):
+    # IQ data with phase rotation and directivity on 64x80 pixels: the staged
+    # complex kernel (schedule variant 2) sums in the gather kernel's order, so the two agree to
+    # rounding of exact zeros; both match the FP64 oracle
+    from ffdas_b200.tune import schedule
+    rng = np.random.default_rng(17 + B)
+    C, S, N = 24, 5, 400
+    x = (rng.standard_normal((B, C, S, N)) + 1j * rng.standard_normal((B, C, S, N))).astype(np.complex64)
+    src = np.zeros((C, 3), np.float32)
+    src[:, 0] = np.linspace(-10, 10, C)
+    zz, xx = np.meshgrid(np.linspace(30, 160, 64), np.linspace(-12, 12, 80), indexing="ij")
+    dst = np.stack([xx, np.zeros_like(xx), zz], -1).astype(np.float32)
+    offs = (zz[None] + rng.uniform(-5, 5, (S, 64, 80))).astype(np.float32)
+    w = rng.uniform(0.2, 1.0, (S, 64, 80)).astype(np.float32)
+    srcdir = np.zeros((C, 4), np.float32)
+    srcdir[:, 2] = 1.0
+    srcdir[:, 3] = 0.3
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
+    xt = t(x).to(dtype)
+    wn = -2 * np.pi * 0.23
+    h = ffdas_b200.get_library_handle(DEV)
+    with schedule(dict(variant=2), DEV):
+        got = ffdas_b200.das(xt, t(src), t(dst), t(offs), t(w), srcdir=t(srcdir), wavenum=wn)
+        info = h.last_kernel_info()
+    assert info["variant"] == 2 and got.dtype == torch.complex64
+    with schedule(dict(variant=1), DEV):
+        gat = ffdas_b200.das(xt, t(src), t(dst), t(offs), t(w), srcdir=t(srcdir), wavenum=wn)
+    assert oracle.rel_l2(_np(got), _np(gat)) < 1e-7
+    xr = xt.to(torch.complex64).cpu().numpy()
+    ref = oracle.das_f64(xr, src, dst, offs, w, srcdir=srcdir, wavenum=wn)
+    assert oracle.rel_l2(_np(got), ref) < 1e-3   # __sincosf of phases up to ~500 rad, as the reference
