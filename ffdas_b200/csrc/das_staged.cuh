@@ -1795,9 +1795,20 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                 const bool any_ovf = !dead && sm.ovf[stage] != 0;
                 if (!dead) {
                     const uint32_t nlast = (uint32_t)(p.N - 1);
-                    for (int cl = 0; cl < CC; cl++) {
+                    // One channel of the stage.  FAST: every in-record tap is in its
+                    // window and the scatter (SCATTER) is fixed point; POS: position
+                    // gradients.  The flags are decided once per stage, so the fast
+                    // path's channels unroll into one straight run (independent work
+                    // for the scheduler); its phantom channels past the slice read
+                    // zero windows and add exact zeros (their bins are never flushed
+                    // to gx, their channel gradients never reduced).
+                    auto channel = [&](const int cl, auto fast_c, auto scatter_c, auto pos_c) {
+                        constexpr bool FAST = decltype(fast_c)::value;
+                        constexpr bool SCATTER = decltype(scatter_c)::value;
+                        constexpr bool POS = decltype(pos_c)::value;
+                        (void)SCATTER;
+
                         const int c = c0 + cl;
-                        if (c >= cend) break;   // a channel past the slice (or a phantom one) is not this CTA's
                         const float4 cp = sm.chan_pos[stage * kStWin + cl];
                         const recv_geom gm = receive_geometry(cx.vx, cx.vy, cx.vz, cp.x, cp.y, cp.z);
                         uint32_t k0p[SC];
@@ -1805,13 +1816,11 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                         const uint32_t groups_u32 = stage_u32 + (cl * SC) * GG::bytes;
                         const uint32_t gwin_u32 = gstage_u32 + (cl * SC * BT) * GS * 4;
                         float q = 0.f;
-                        if (!any_ovf && (fixed || !p.gx)) {
+                        if constexpr (FAST) {
                             const unsigned char *groups = sm.ring + stage * SG::stage_bytes + (cl * SC) * GG::bytes;
-                            // common case: every in-record tap is in its window; the
-                            // scatter's presence is decided once per channel (SCATTER)
+                            // common case: every in-record tap is in its window
                             const float2 rsq2 = make_float2(gm.rsq, gm.rsq), rinv2 = make_float2(gm.rinv, gm.rinv);
-                            auto taps = [&](auto scatter_c) {
-                                constexpr bool SCATTER = decltype(scatter_c)::value;
+                            {
 #pragma unroll
                                 for (int j = 0; j < SC; j += 2) {
                                     const float2 tau2 = __ffma2_rn(rsq2, rinv2, make_float2(ofs[j], ofs[j + 1]));
@@ -1861,9 +1870,7 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                                         q = __fmaf_rn(w[jj], gd, q);
                                     }
                                 }
-                            };
-                            if (p.gx) taps(std::true_type{});
-                            else taps(std::false_type{});
+                            }
                         } else {
                             const unsigned char *groups = sm.ring + stage * SG::stage_bytes + (cl * SC) * GG::bytes;
 #pragma unroll
@@ -1911,7 +1918,7 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                                 q = __fmaf_rn(w[j], gd, q);
                             }
                         }
-                        if (want_pos) {
+                        if constexpr (POS) {
                             const float qr = q * gm.rinv;
                             const float ex = (cx.vx - cp.x) * qr, ey = (cx.vy - cp.y) * qr, ez = (cx.vz - cp.z) * qr;
                             gpx += ex; gpy += ey; gpz += ez;
@@ -1921,6 +1928,28 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                                 cgrad[(cl * 3 + 2) * kStConsumers + cx.tid] = -ez;
                             }
                         }
+                                        };
+                    auto run = [&](auto fast_c, auto scatter_c, auto pos_c) {
+                        if constexpr (decltype(fast_c)::value) {
+#pragma unroll
+                            for (int cl = 0; cl < CC; cl++) channel(cl, fast_c, scatter_c, pos_c);
+                        } else {
+                            for (int cl = 0; cl < CC; cl++) {
+                                if (c0 + cl >= cend) break;   // a channel past the slice (or a phantom one)
+                                channel(cl, fast_c, scatter_c, pos_c);
+                            }
+                        }
+                    };
+                    using T_ = std::true_type;
+                    using F_ = std::false_type;
+                    if (!any_ovf && (fixed || !p.gx)) {
+                        if (p.gx) {
+                            if (want_pos) run(T_{}, T_{}, T_{}); else run(T_{}, T_{}, F_{});
+                        } else {
+                            if (want_pos) run(T_{}, F_{}, T_{}); else run(T_{}, F_{}, F_{});
+                        }
+                    } else {
+                        if (want_pos) run(F_{}, F_{}, T_{}); else run(F_{}, F_{}, F_{});
                     }
                 }
                 // every consumer warp finished this stage's scatter
