@@ -1680,8 +1680,8 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_kernel(const sta
 // window is always outside the record and adds its zeros past the window.
 template <int WB, int K, int SC, int BT>
 constexpr size_t staged_bwd_batch_smem_bytes() {
-    return staged_smem_bytes<WB, K>() + kBinCopies * bin_region_words(kStWin * bin_stride(WB)) * 4 +
-           (group_geom<WB, K, BT>::groups / SC) * 3 * kStConsumers * 4 + kStWarps * 4 + 16 +
+    return staged_smem_bytes<WB, K>() + 2 * kBinCopies * bin_region_words(kStWin * bin_stride(WB)) * 4 +
+           2 * (group_geom<WB, K, BT>::groups / SC) * 3 * kStConsumers * 4 + kStWarps * 4 + 16 +
            group_geom<WB, K, BT>::data_bytes;
 }
 
@@ -1697,17 +1697,24 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     staged_smem<K, WB> sm(smem_raw);
-    // one set of bins (in two copies): a stage's bins are flushed and cleared
-    // between two consumer barriers before the next stage scatters into them
+    // Two sets of bins (each in two copies) and of channel-gradient scratch,
+    // used by stages of alternate parity (kStages is even): a warp that has
+    // flushed stage s's set scatters stage s + 1 into the other while slower
+    // warps still read s's, and the barrier after stage s + 1's scatter orders
+    // every flush of s's set before stage s + 2 writes it -- one consumer
+    // barrier per stage.
+    static_assert(kStages % 2 == 0, "stage parity must alternate around the ring");
     constexpr int kRegion = bin_region_words(kStWin * GS);
-    int *gslot = reinterpret_cast<int *>(sm.extra);   // [kBinCopies][kRegion]: [kStWin][GS], window = group * BT + item
-    float *cgrad = reinterpret_cast<float *>(gslot + kBinCopies * kRegion);  // [CC * 3][256]
-    float *wmax = cgrad + CC * 3 * kStConsumers;                          // [kStWarps]
+    constexpr int kSet = kBinCopies * kRegion;                           // words per set of bins
+    constexpr int kCg = CC * 3 * kStConsumers;                           // floats per channel-gradient set
+    int *gslot = reinterpret_cast<int *>(sm.extra);   // [2][kBinCopies][kRegion]: [kStWin][GS], window = group * BT + item
+    float *cgrad0 = reinterpret_cast<float *>(gslot + 2 * kSet);        // [2][CC * 3][256]
+    float *wmax = cgrad0 + 2 * kCg;                                      // [kStWarps]
     // zero group after the scratch, 16-byte aligned (offset arithmetic on the
     // shared pointer keeps its address space visible to the compiler)
-    constexpr int kZeroOff = ((kBinCopies * kRegion + CC * 3 * kStConsumers + kStWarps) * 4 + 15) & ~15;
+    constexpr int kZeroOff = ((2 * kSet + 2 * kCg + kStWarps) * 4 + 15) & ~15;
     unsigned char *zero_group = sm.extra + kZeroOff;
-    for (int i = threadIdx.x; i < kBinCopies * kRegion; i += kStThreads) gslot[i] = 0;
+    for (int i = threadIdx.x; i < 2 * kSet; i += kStThreads) gslot[i] = 0;
     for (int i = threadIdx.x; i < GG::data_bytes / 4; i += kStThreads) reinterpret_cast<uint32_t *>(zero_group)[i] = 0u;
     const staged_ctx cx = staged_setup<K, WB>(p, sm, true);   // ends with __syncthreads
     const uint32_t gslot_u32 = smem_u32(gslot) + cx.par * (kRegion * 4);   // this thread's copy
@@ -1789,8 +1796,9 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
             } else {
                 const uint32_t full_bar = smem_u32(&sm.full[stage]);
                 const uint32_t stage_u32 = smem_u32(sm.ring + stage * SG::stage_bytes);
-                int *gstage = gslot;
-                const uint32_t gstage_u32 = gslot_u32;
+                int *gstage = gslot + (stage & 1) * kSet;
+                const uint32_t gstage_u32 = gslot_u32 + (stage & 1) * (kSet * 4);
+                float *cgrad = cgrad0 + (stage & 1) * kCg;
                 if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
                 const bool any_ovf = !dead && sm.ovf[stage] != 0;
                 if (!dead) {
@@ -1977,7 +1985,8 @@ __global__ void __launch_bounds__(kStThreads, 2) das_staged_bwd_batch_kernel(con
                         }
                     }
                 }
-                consumer_sync();  // scratch reused by the next stage
+                // no barrier: the next stage uses the other set of scratch, and
+                // the producer refills this ring stage once every warp arrived
                 __syncwarp();
                 if (cx.lane == 0) mbar_arrive(smem_u32(&sm.empty[stage]));
             }
