@@ -3,7 +3,7 @@
 The reference's das path is compiled from its sources into
 oracle/_ref/libffdas_ref.so (`make -C oracle ref`) and driven through its own
 C-ABI by oracle/reference.py, which pads x so the reference's unmasked loads
-stay inside memory it owns.  Tolerance (relative L2): FP32
+stay inside memory it owns.  Tolerance (relative L2, the parity bar): FP32
 1e-5 against the reference's FP32 das on the same inputs.
 """
 import numpy as np
