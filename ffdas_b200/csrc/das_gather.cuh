@@ -14,6 +14,8 @@
 // accumulation; only the order of the sum over (channel, event) differs.
 #pragma once
 
+#include <type_traits>
+
 #include "das_pairs.cuh"
 
 namespace ffdas {
@@ -228,7 +230,10 @@ __global__ void __launch_bounds__(256) das_gather_kernel(const gather_params p) 
             }
         }
 
-        for (int c = 0; c < p.C; c++) {
+        // channel slice of this CTA (blockIdx.z) when the call splits channels
+        const int cbeg = p.cchunk ? (int)blockIdx.z * p.cchunk : 0;
+        const int cend = p.cchunk ? min(p.C, cbeg + p.cchunk) : p.C;
+        for (int c = cbeg; c < cend; c++) {
             const float cx = __ldg(p.srcpos + 3 * c + 0);
             const float cy = __ldg(p.srcpos + 3 * c + 1);
             const float cz = __ldg(p.srcpos + 3 * c + 2);
@@ -267,6 +272,12 @@ __global__ void __launch_bounds__(256) das_gather_kernel(const gather_params p) 
     for (int b = 0; b < BT; b++) {
         if (BT == 1 || b0 + b < p.B) {
             OutT *o = out + (int64_t)(b0 + b) * p.out_bstride + v;
+            if constexpr (std::is_same_v<OutT, float> && std::is_same_v<acc_t, float>) {
+                if (p.cchunk) {   // channel slices add into the prepared image
+                    atomicAdd(o, acc[b]);
+                    continue;
+                }
+            }
             if constexpr (sizeof(OutT) == sizeof(acc_t)) {
                 store_out<OutT>(o, acc[b], p);
             } else if constexpr (sizeof(OutT) == 8 && sizeof(acc_t) == 4) {

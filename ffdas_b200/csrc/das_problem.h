@@ -73,6 +73,9 @@ bool staged_supported(const das_problem &pb, int kind);
 // driver's tensor-map encoder is unavailable).  Records it in h.last.
 // Batch tiles need the TMA tensor-map encoder (3-D boxes).
 bool staged_batch_supported();
+// out = beta * out (or 0) for every item and voxel of an f32 image, before
+// channel slices add into it.
+ffdas_error_t launch_scale_image(ffdas_context &h, const das_problem &pb, float *out, float beta, int beta_zero);
 // BT > 1: batch tiles of BT items per CTA (256-voxel tiles, SC * BT <= 32).
 ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp, int SC,
                             int WB, int BT, int copy, dim3 grid);

@@ -223,6 +223,12 @@ static staged_params base_params(ffdas_context &h, const das_problem &pb, const 
     return sp;
 }
 
+ffdas_error_t launch_scale_image(ffdas_context &h, const das_problem &pb, float *out, float beta, int beta_zero) {
+    dim3 sg((unsigned)((pb.V + 255) / 256), (unsigned)std::min(pb.B, 65535));
+    scale_image_kernel<<<sg, 256, 0, h.stream>>>(out, pb.out_bstride, pb.V, pb.B, beta, beta_zero, nullptr);
+    return ffdas_launch_check(h.stream);
+}
+
 ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp, int SC,
                             int WB, int BT, int copy, dim3 grid) {
     if (gp.cchunk) {   // channel slices add into the image: prepare it (beta * out, or 0)

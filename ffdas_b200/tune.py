@@ -63,6 +63,13 @@ def candidates(x, dstpos, offsets, sparse_indices=None) -> list[dict]:
             if bt & (bt - 1):
                 continue
             out.append(dict(variant=1, tile_x=t0, tile_y=t1, batch_tile=bt))
+            if real and sparse_indices is not None and bt <= 4:
+                # event chunks of 8 and 4: fewer registers, more resident warps for latency-bound lists
+                for ec in (8, 4):
+                    out.append(dict(variant=1, tile_x=t0, tile_y=t1, batch_tile=bt, event_chunk=ec))
+                    for mb in (8, 16):   # more channel slices than the default target of 4 CTAs per SM
+                        out.append(dict(variant=1, tile_x=t0, tile_y=t1, batch_tile=bt, event_chunk=ec,
+                                        min_blocks=mb))
         if real and sparse_indices is None:
             n_ev = offsets.shape[0]
             chunks = sorted({min(c, max(n_ev, 1)) for c in (4, 8, 16)})

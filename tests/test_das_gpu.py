@@ -456,3 +456,42 @@ def test_complex_on_the_staged_kernel(dtype, B):
     xr = xt.to(torch.complex64).cpu().numpy()
     ref = oracle.das_f64(xr, src, dst, offs, w, srcdir=srcdir, wavenum=wn)
     assert oracle.rel_l2(_np(got), ref) < 1e-3   # __sincosf of phases up to ~500 rad, as the reference
+
+
+def test_sparse_gather_channel_slices_with_beta():
+    # the gather kernel splits a small sparse call's channels over CTAs that
+    # add into a prepared image: out = beta * out + das_sparse
+    import ctypes
+    from ffdas_b200 import _lib
+    from ffdas_b200._lib import DataType
+    rng = np.random.default_rng(8)
+    x, src, dst, offs, w = _small(rng, C=96, S=6, N=160, V=(24, 20))
+    V = dst.shape[:-1]
+    g = torch.Generator().manual_seed(10)
+    idx = torch.randint(0, 6, (5, *V), generator=g).int()
+    ofs_s = (torch.rand((5, *V), generator=g) * 50).float()
+    w_s = (torch.rand((5, *V), generator=g) + 0.1).float()
+    idx, ofs_s, w_s = idx.to(DEV), ofs_s.to(DEV), w_s.to(DEV)
+    h = ffdas_b200.get_library_handle(DEV)
+    L = _lib.load()
+    prev = torch.randn((1, *V), device=DEV)
+    xd = _lib.TensorDesc(list(x.shape), None, DataType.R_32F)
+    outs = []
+    for cfg in (dict(variant=1, event_chunk=8), dict(variant=1, event_chunk=4, min_blocks=16)):
+        out = prev.clone()
+        od = _lib.TensorDesc(list(out.shape), None, DataType.R_32F)
+        beta = (ctypes.c_float * 2)(-0.25, 0.0)
+        h.set_config(cfg)
+        h.set_stream(torch.cuda.current_stream().cuda_stream)
+        _lib.check(L.ffdas_das_sparse(h.h, src.data_ptr(), None, 0.0, xd.desc, x.data_ptr(), dst.data_ptr(),
+                                      ofs_s.data_ptr(), w_s.data_ptr(), 5, idx.data_ptr(),
+                                      ctypes.cast(beta, ctypes.c_void_p), od.desc, out.data_ptr(), 0, 0))
+        info = h.last_kernel_info()
+        h.set_config(None)
+        assert info["variant"] == 1 and info["kernels"] == 3, info
+        outs.append(out)
+    torch.cuda.synchronize()
+    ref = -0.25 * _np(prev) + oracle.das_f64(_np(x), _np(src), _np(dst), _np(ofs_s), _np(w_s),
+                                            sparse_indices=_np(idx))
+    for out in outs:
+        assert oracle.rel_l2(_np(out), ref) < TOL[torch.float32]
