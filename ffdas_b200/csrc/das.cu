@@ -95,6 +95,13 @@ int select_storage(ffdas_datatype_t xt, ffdas_datatype_t ot, ffdas_compute_type_
             if (ct == FFDAS_COMPUTE_16F) return ST_F16;
             if (ct == FFDAS_COMPUTE_16BF) return ST_BF16;
             return ST_F32;
+        // int16 channel data (raw ADC samples; the reference rejects the type):
+        // FP32 pairs hold every int16 exactly, 16-bit pairs only when asked for
+        case FFDAS_R_16I:
+            if (ot != FFDAS_R_32F) return -1;
+            if (ct == FFDAS_COMPUTE_16F) return ST_F16;
+            if (ct == FFDAS_COMPUTE_16BF) return ST_BF16;
+            return ST_F32;
         case FFDAS_C_16F:
             if (ot != FFDAS_C_32F) return -1;
             if (ct == FFDAS_COMPUTE_16F || ct == FFDAS_COMPUTE_16BF) return -1;
@@ -159,6 +166,11 @@ static ffdas_error_t launch_ingest(ffdas_context &h, const das_problem &pb, ffda
             if (kind == ST_F32) return launch_ingest_t<__half, ST_F32>(h, pb, x, npad, P);
             if (kind == ST_F16) return launch_ingest_t<__half, ST_F16>(h, pb, x, npad, P);
             if (kind == ST_BF16) return launch_ingest_t<__half, ST_BF16>(h, pb, x, npad, P);
+            break;
+        case FFDAS_R_16I:
+            if (kind == ST_F32) return launch_ingest_t<int16_t, ST_F32>(h, pb, x, npad, P);
+            if (kind == ST_F16) return launch_ingest_t<int16_t, ST_F16>(h, pb, x, npad, P);
+            if (kind == ST_BF16) return launch_ingest_t<int16_t, ST_BF16>(h, pb, x, npad, P);
             break;
         case FFDAS_R_16BF:
             if (kind == ST_F32) return launch_ingest_t<__nv_bfloat16, ST_F32>(h, pb, x, npad, P);
@@ -389,6 +401,7 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
     const bool combo_ok =
         (xd.dtype == FFDAS_R_16F && od.dtype == FFDAS_R_32F) ||
         (xd.dtype == FFDAS_R_16BF && od.dtype == FFDAS_R_32F) ||
+        (xd.dtype == FFDAS_R_16I && od.dtype == FFDAS_R_32F) ||
         (xd.dtype == FFDAS_R_32F && od.dtype == FFDAS_R_32F) ||
         (xd.dtype == FFDAS_C_16F && od.dtype == FFDAS_C_32F) ||
         (xd.dtype == FFDAS_C_32F && od.dtype == FFDAS_C_32F) ||
@@ -733,7 +746,8 @@ extern "C" ffdas_error_t ffdas_das_static(uintptr_t stream, const float *srcpos,
     if (!x_desc || !out_desc) return FFDAS_ERROR_NULL_POINTER;
     const ffdas_tensor_desc &xd = *x_desc;
     const ffdas_tensor_desc &od = *out_desc;
-    const bool combo_ok = (xd.dtype == FFDAS_R_16F || xd.dtype == FFDAS_R_16BF || xd.dtype == FFDAS_R_32F) &&
+    const bool combo_ok = (xd.dtype == FFDAS_R_16F || xd.dtype == FFDAS_R_16BF || xd.dtype == FFDAS_R_32F ||
+                           xd.dtype == FFDAS_R_16I) &&
                           od.dtype == FFDAS_R_32F;
     if (!combo_ok) return FFDAS_ERROR_UNSUPPORTED_TYPE;   // real channel data, float output
     if (!fits_int32_indexing(xd) || !fits_int32_indexing(od)) return FFDAS_ERROR_INVALID_DIMS;

@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(kDirectThreads) das_direct_kernel(const direct
 
 bool direct_supported(const das_problem &pb, ffdas_datatype_t xt, ffdas_datatype_t ot, int kind) {
     if (pb.sparse || kind != ST_F32 || ot != FFDAS_R_32F) return false;
-    if (xt != FFDAS_R_32F && xt != FFDAS_R_16F && xt != FFDAS_R_16BF) return false;
+    if (xt != FFDAS_R_32F && xt != FFDAS_R_16F && xt != FFDAS_R_16BF && xt != FFDAS_R_16I) return false;
     return pb.C > 0 && pb.S > 0 && pb.B <= 65535 * 4;
 }
 
@@ -177,6 +177,11 @@ static int direct_blocks_per_sm(ffdas_datatype_t xt, int batch_tile, int C) {
             e = bt == 4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, das_direct_kernel<__half, 4>, kDirectThreads, smem)
               : bt == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, das_direct_kernel<__half, 2>, kDirectThreads, smem)
                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, das_direct_kernel<__half, 1>, kDirectThreads, smem);
+            break;
+        case FFDAS_R_16I:
+            e = bt == 4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, das_direct_kernel<int16_t, 4>, kDirectThreads, smem)
+              : bt == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, das_direct_kernel<int16_t, 2>, kDirectThreads, smem)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, das_direct_kernel<int16_t, 1>, kDirectThreads, smem);
             break;
         case FFDAS_R_16BF:
             e = bt == 4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, das_direct_kernel<__nv_bfloat16, 4>, kDirectThreads, smem)
@@ -246,6 +251,7 @@ ffdas_error_t launch_direct(ffdas_context &h, const das_problem &pb, ffdas_datat
         case FFDAS_R_32F: err = launch_direct_bt<float>(h, dp, BT); break;
         case FFDAS_R_16F: err = launch_direct_bt<__half>(h, dp, BT); break;
         case FFDAS_R_16BF: err = launch_direct_bt<__nv_bfloat16>(h, dp, BT); break;
+        case FFDAS_R_16I: err = launch_direct_bt<int16_t>(h, dp, BT); break;
         default: err = FFDAS_ERROR_INTERNAL; break;
     }
     h.mark_stop();

@@ -137,6 +137,7 @@ template <> struct sample_io<float> { using w = float; __device__ static w load(
 template <> struct sample_io<double> { using w = double; __device__ static w load(const double *p) { return __ldg(p); } };
 template <> struct sample_io<__half> { using w = float; __device__ static w load(const __half *p) { return __half2float(*p); } };
 template <> struct sample_io<__nv_bfloat16> { using w = float; __device__ static w load(const __nv_bfloat16 *p) { return __bfloat162float(*p); } };
+template <> struct sample_io<int16_t> { using w = float; __device__ static w load(const int16_t *p) { return (float)__ldg(p); } };
 template <> struct sample_io<float2> { using w = float2; __device__ static w load(const float2 *p) { return __ldg(p); } };
 template <> struct sample_io<double2> { using w = double2; __device__ static w load(const double2 *p) { return __ldg(p); } };
 template <> struct sample_io<__half2> { using w = float2; __device__ static w load(const __half2 *p) { return __half22float2(*p); } };

@@ -19,6 +19,8 @@ Differences from the reference (documented, deliberate):
     event 0's row when x has no batch dim);
   * the output of 16-bit real input is float32 and of complex32 input
     complex64 (the C-ABI's output dtypes);
+  * int16 channel data (raw ADC samples) is accepted and interpolated in FP32
+    (the reference's C-ABI has the int16 type code but rejects it for das);
   * `use_bf16=True` selects the new bf16 pair storage;
   * calls run on torch's current CUDA stream (the reference always uses the
     legacy default stream);
@@ -46,6 +48,7 @@ _FFDAS_DTYPE = {
     torch.float32: DataType.R_32F,
     torch.float16: DataType.R_16F,
     torch.bfloat16: DataType.R_16BF,
+    torch.int16: DataType.R_16I,
     torch.float64: DataType.R_64F,
     torch.complex64: DataType.C_32F,
     torch.complex32: DataType.C_16F,
@@ -55,6 +58,7 @@ _OUT_DTYPE = {
     torch.float32: torch.float32,
     torch.float16: torch.float32,
     torch.bfloat16: torch.float32,
+    torch.int16: torch.float32,
     torch.float64: torch.float64,
     torch.complex64: torch.complex64,
     torch.complex32: torch.complex64,
@@ -214,7 +218,7 @@ def das(x, srcpos, dstpos, offsets, weights, *, srcdir=None, wavenum: float = 0.
 
     Args:
         x: RF data, (channels, sequence, samples) or (batch, channels, sequence, samples);
-            float32, float16, bfloat16, float64, complex64, complex32 or complex128.
+            float32, float16, bfloat16, int16, float64, complex64, complex32 or complex128.
         srcpos: channel positions (channels, 3).
         dstpos: target positions (..., 3); the output has shape ([batch,] ...).
         offsets: per-target delays in samples (sequence, ...).

@@ -10,6 +10,9 @@
  *
  * Additions (new codes and new symbols only; nothing existing is altered):
  *   - FFDAS_R_16BF: bfloat16 channel data (unused code 18).
+ *   - FFDAS_R_16I channel data (the reference's code 14) into FFDAS_R_32F output:
+ *     raw int16 ADC samples, interpolated in FP32 (the reference rejects the
+ *     type for das with FFDAS_ERROR_UNSUPPORTED_TYPE).
  *   - ffdas_das_backward: adjoint of ffdas_das / ffdas_das_sparse.
  *   - ffdas_das_set_config / ffdas_das_get_config: kernel schedule override
  *     used by the autotuner.
@@ -293,7 +296,7 @@ FFDAS_API ffdas_error_t ffdas_das_backward(
  * is a 16 MiB array in the library's device image (every GPU that loads the
  * library holds it until exit), so B * C * S * roundup(N, 4) * 8 bytes (4 for
  * 16-bit channel data) must not exceed 16 MiB, else FFDAS_ERROR_DIMS_TOO_LARGE.
- * Real channel data (float32, float16, bfloat16) with float32 output only.
+ * Real channel data (float32, float16, bfloat16, int16) with float32 output only.
  * The first call on a device looks up the array's device address (once per
  * device); make that first call before any stream capture.  All calls share
  * the one array: calls that overlap on the GPU (other streams, other host

@@ -495,3 +495,39 @@ def test_sparse_gather_channel_slices_with_beta():
                                             sparse_indices=_np(idx))
     for out in outs:
         assert oracle.rel_l2(_np(out), ref) < TOL[torch.float32]
+
+
+@pytest.mark.parametrize("cfg", [None, dict(variant=1), dict(variant=2, tile_x=16, tile_y=16, window=32),
+                                 dict(variant=5)], ids=["planner", "gather", "staged", "direct"])
+def test_int16_channel_data(cfg):
+    # raw ADC samples: int16 x is interpolated in FP32 (FP32 pairs hold every
+    # int16 exactly), so every kernel matches the oracle of the same integers
+    from ffdas_b200.tune import schedule
+    wl = W.diverging3d(device=DEV, scale=0.125)
+    g = torch.Generator().manual_seed(3)
+    x16 = (wl["x"].cpu() * 8000 + torch.randn(wl["x"].shape, generator=g) * 30).round().clamp(-32768, 32767)
+    x16 = x16.to(torch.int16).to(DEV)
+    h = ffdas_b200.get_library_handle(DEV)
+    with schedule(cfg, DEV):
+        got = ffdas_b200.das(x16, wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"])
+        info = h.last_kernel_info()
+    assert got.dtype == torch.float32 and info["storage"] == 0
+    if cfg is not None:
+        assert info["variant"] == cfg["variant"]
+    ref = oracle.das_f64(_np(x16).astype(np.float64), _np(wl["srcpos"]), _np(wl["dstpos"]), _np(wl["offsets"]),
+                         _np(wl["weights"]))
+    assert oracle.rel_l2(_np(got), ref) < TOL[torch.float32]
+
+
+def test_int16_channel_data_gradients():
+    # the adjoint runs on the same FP32 pairs; an int16 tensor carries no gradient
+    # itself, the geometry does
+    wl = W.autofocus(device=DEV, scale=0.2)
+    x16 = (wl["x"] * 3000).round().to(torch.int16)
+    xf = x16.float()
+    leaves16 = [t.clone().requires_grad_(True) for t in (wl["offsets"], wl["weights"])]
+    leavesf = [t.clone().requires_grad_(True) for t in (wl["offsets"], wl["weights"])]
+    ffdas_b200.das(x16, wl["srcpos"], wl["dstpos"], *leaves16).square().sum().backward()
+    ffdas_b200.das(xf, wl["srcpos"], wl["dstpos"], *leavesf).square().sum().backward()
+    for a, b in zip(leaves16, leavesf):
+        assert oracle.rel_l2(_np(a.grad), _np(b.grad)) < 1e-6
