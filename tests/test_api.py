@@ -109,3 +109,25 @@ def test_full_size_workload_geometry():
     assert tuple(wl["x"].shape) == (1, 128, 1, 2048)
     assert tuple(wl["dstpos"].shape) == (256, 1, 128, 3)
     assert wl["units"] == 256 * 128 * 128
+
+
+def test_tuner_candidates_cover_each_kernel_family():
+    # host-side schedule search space (no GPU): the one-launch direct kernel
+    # for small real frames, the staged kernels (512-voxel tiles for sparse
+    # lists), gather chunks and channel-slice targets for sparse lists, and
+    # only the gather kernel for complex data
+    from ffdas_b200.tune import candidates
+    small = W.plane2d(scale=0.25)
+    c = candidates(small["x"], small["dstpos"], small["offsets"])
+    assert any(k["variant"] == 5 for k in c) and any(k["variant"] == 2 for k in c)
+    assert {k.get("tile_x") for k in c if k["variant"] == 5} >= {None, 2, 32}
+    big = W.diverging3d(scale=0.5)
+    assert not any(k["variant"] == 5 for k in candidates(big["x"], big["dstpos"], big["offsets"]))
+    sp = W.sparse_focus(scale=0.25)
+    cs = candidates(sp["x"], sp["dstpos"], sp["offsets"], sp["sparse_indices"])
+    assert any(k["variant"] == 2 and k["tile_x"] * k["tile_y"] == 512 for k in cs)
+    assert any(k["variant"] == 1 and k.get("event_chunk") == 8 and k.get("min_blocks") == 16 for k in cs)
+    assert not any(k["variant"] == 5 for k in cs)
+    xc = small["x"].to(torch.complex64)
+    cc = candidates(xc, small["dstpos"], small["offsets"])
+    assert cc and all(k["variant"] == 1 for k in cc)
