@@ -16,6 +16,7 @@
 // (0 <= k < N - 1 fails) reads nothing and contributes fma(w, 0, acc), as a
 // zero pair would.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 #include "core.h"
@@ -147,12 +148,15 @@ static ffdas_error_t launch_direct_t(ffdas_context &h, const direct_params &dp) 
     const int64_t bchunks = (dp.B + BT - 1) / BT;
     if (blocks > INT32_MAX || bchunks > 65535) return FFDAS_ERROR_DIMS_TOO_LARGE;
     const size_t smem = dp.chan_smem ? (size_t)dp.C * sizeof(float4) : 0;
-    if (smem > 48 * 1024) {
-        static bool ready = false;
-        if (!ready) {
+    if (smem > 48 * 1024) {   // the attribute belongs to the device: set it for each one
+        static std::atomic<unsigned long long> done{0ull};
+        int dev = 0;
+        FFDAS_CUDA(cudaGetDevice(&dev));
+        const unsigned long long bit = 1ull << (dev & 63);
+        if (!(done.load(std::memory_order_acquire) & bit)) {
             FFDAS_CUDA(cudaFuncSetAttribute(das_direct_kernel<Tin, BT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)smem));
-            ready = true;
+                                            (int)(kDirectSmemChannels * sizeof(float4))));
+            done.fetch_or(bit, std::memory_order_release);
         }
     }
     das_direct_kernel<Tin, BT><<<dim3((unsigned)blocks, (unsigned)bchunks), kDirectThreads, smem, h.stream>>>(dp);

@@ -9,6 +9,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 
@@ -102,14 +103,24 @@ static ffdas_error_t prepare_kernel(Kernel kernel, size_t smem) {
     return FFDAS_SUCCESS;
 }
 
+// Kernel attributes (dynamic shared memory above 48 KB, carveout) belong to a
+// device: set them once for every device the process launches the kernel on.
+template <auto Kernel>
+static ffdas_error_t prepare_once(size_t smem) {
+    static std::atomic<unsigned long long> done{0ull};
+    int dev = 0;
+    FFDAS_CUDA(cudaGetDevice(&dev));
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return FFDAS_SUCCESS;
+    FFDAS_TRY(prepare_kernel(Kernel, smem));
+    done.fetch_or(bit, std::memory_order_release);
+    return FFDAS_SUCCESS;
+}
+
 template <int K, int SC, int WB>
 static ffdas_error_t launch_fwd_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
     constexpr size_t smem = staged_smem_bytes<WB, K>();
-    static bool ready = false;  // per instantiation; idempotent
-    if (!ready) {
-        FFDAS_TRY(prepare_kernel(das_staged_kernel<K, SC, WB>, smem));
-        ready = true;
-    }
+    FFDAS_TRY((prepare_once<das_staged_kernel<K, SC, WB>>(smem)));
     das_staged_kernel<K, SC, WB><<<grid, kStThreads, smem, h.stream>>>(sp, map);
     return ffdas_launch_check(h.stream);
 }
@@ -117,11 +128,7 @@ static ffdas_error_t launch_fwd_t(ffdas_context &h, const staged_params &sp, con
 template <int K, int SC, int WB>
 static ffdas_error_t launch_fwd2_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
     constexpr size_t smem = staged_smem_bytes<WB, K>();
-    static bool ready = false;
-    if (!ready) {
-        FFDAS_TRY(prepare_kernel(das_staged2_kernel<K, SC, WB>, smem));
-        ready = true;
-    }
+    FFDAS_TRY((prepare_once<das_staged2_kernel<K, SC, WB>>(smem)));
     das_staged2_kernel<K, SC, WB><<<grid, kStThreads, smem, h.stream>>>(sp, map);
     return ffdas_launch_check(h.stream);
 }
@@ -129,11 +136,7 @@ static ffdas_error_t launch_fwd2_t(ffdas_context &h, const staged_params &sp, co
 template <int K, int SC, int WB, int BT>
 static ffdas_error_t launch_fwdb_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
     constexpr size_t smem = staged_batch_smem_bytes<WB, K, BT>();
-    static bool ready = false;
-    if (!ready) {
-        FFDAS_TRY(prepare_kernel(das_staged_batch_kernel<K, SC, WB, BT>, smem));
-        ready = true;
-    }
+    FFDAS_TRY((prepare_once<das_staged_batch_kernel<K, SC, WB, BT>>(smem)));
     das_staged_batch_kernel<K, SC, WB, BT><<<grid, kStThreads, smem, h.stream>>>(sp, map);
     return ffdas_launch_check(h.stream);
 }
@@ -149,11 +152,7 @@ static ffdas_error_t launch_fwd_batch(ffdas_context &h, const staged_params &sp,
 template <int K, int SC, int WB>
 static ffdas_error_t launch_bwd_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
     constexpr size_t smem = staged_bwd_smem_bytes<WB, K, SC>();
-    static bool ready = false;
-    if (!ready) {
-        FFDAS_TRY(prepare_kernel(das_staged_bwd_kernel<K, SC, WB>, smem));
-        ready = true;
-    }
+    FFDAS_TRY((prepare_once<das_staged_bwd_kernel<K, SC, WB>>(smem)));
     das_staged_bwd_kernel<K, SC, WB><<<grid, kStThreads, smem, h.stream>>>(sp, map);
     return ffdas_launch_check(h.stream);
 }
@@ -180,11 +179,7 @@ static ffdas_error_t launch_fwd_sc(ffdas_context &h, const staged_params &sp, co
 template <int K, int WB, int BT>
 static ffdas_error_t launch_bwdb_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
     constexpr size_t smem = staged_bwd_batch_smem_bytes<WB, K, 4, BT>();
-    static bool ready = false;
-    if (!ready) {
-        FFDAS_TRY(prepare_kernel(das_staged_bwd_batch_kernel<K, 4, WB, BT>, smem));
-        ready = true;
-    }
+    FFDAS_TRY((prepare_once<das_staged_bwd_batch_kernel<K, 4, WB, BT>>(smem)));
     das_staged_bwd_batch_kernel<K, 4, WB, BT><<<grid, kStThreads, smem, h.stream>>>(sp, map);
     return ffdas_launch_check(h.stream);
 }
@@ -276,11 +271,7 @@ ffdas_error_t launch_staged(ffdas_context &h, const das_problem &pb, int kind, c
 template <int K, int SC>
 static ffdas_error_t launch_cplx_t(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, dim3 grid) {
     constexpr size_t smem = staged_smem_bytes<32, K>();
-    static bool ready = false;
-    if (!ready) {
-        FFDAS_TRY(prepare_kernel(das_staged_cplx_kernel<K, SC, 32>, smem));
-        ready = true;
-    }
+    FFDAS_TRY((prepare_once<das_staged_cplx_kernel<K, SC, 32>>(smem)));
     das_staged_cplx_kernel<K, SC, 32><<<grid, kStThreads, smem, h.stream>>>(sp, map);
     return ffdas_launch_check(h.stream);
 }
