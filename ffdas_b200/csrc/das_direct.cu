@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <type_traits>
 
 #include "core.h"
 #include "das_common.cuh"
@@ -73,27 +74,33 @@ __global__ void __launch_bounds__(kDirectThreads) das_direct_kernel(const direct
         const uint32_t nlast = (uint32_t)(p.N - 1);
         const float *po0 = p.offsets + v, *pw0 = p.weights + v;
         const int cstride = p.cstride, sstride = p.sstride;
-        // kDirectUnroll channels per iteration: their gathers are independent,
-        // so a thread keeps several L2 requests in flight instead of waiting
-        // out each tap in turn
-        for (int c0 = part; c0 < C; c0 += kDirectUnroll * split) {
+        const bool chan_smem = p.chan_smem;
+        const float *srcpos = p.srcpos;
+        const float4 *srcdir = p.srcdir;
+        // kDirectUnroll channels per step: their gathers are independent, so a
+        // thread keeps several L2 requests in flight instead of waiting out
+        // each tap in turn.  Whole steps run without channel tests; the last,
+        // partial step (CHECK) masks the channels past C.
+        auto step = [&](const int c0, auto check_c) {
+            constexpr bool CHECK = decltype(check_c)::value;
             recv_geom gm[kDirectUnroll];
             int row[kDirectUnroll];
             bool live[kDirectUnroll];
 #pragma unroll
             for (int u = 0; u < kDirectUnroll; u++) {
                 const int c = c0 + u * split;
-                live[u] = c < C;
+                live[u] = !CHECK || c < C;
                 const int cc = live[u] ? c : 0;
-                const float4 cp = p.chan_smem ? chan[cc]
-                                              : make_float4(__ldg(p.srcpos + 3 * cc), __ldg(p.srcpos + 3 * cc + 1),
-                                                            __ldg(p.srcpos + 3 * cc + 2), 0.f);
+                const float4 cp = chan_smem ? chan[cc]
+                                            : make_float4(__ldg(srcpos + 3 * cc), __ldg(srcpos + 3 * cc + 1),
+                                                          __ldg(srcpos + 3 * cc + 2), 0.f);
                 gm[u] = receive_geometry(vx, vy, vz, cp.x, cp.y, cp.z);
-                if (p.srcdir) apply_directivity(gm[u], vx, vy, vz, cp.x, cp.y, cp.z, __ldg(p.srcdir + cc));
+                if (srcdir) apply_directivity(gm[u], vx, vy, vz, cp.x, cp.y, cp.z, __ldg(srcdir + cc));
                 row[u] = cc * cstride;
             }
             const float *po = po0, *pw = pw0;
-            for (int s = 0; s < S; s++, po += V, pw += V) {
+            int srow = 0;
+            for (int s = 0; s < S; s++, po += V, pw += V, srow += sstride) {
                 const float ofs = __ldg(po), w = __ldg(pw);
                 float t[kDirectUnroll];
                 int e[kDirectUnroll];
@@ -103,7 +110,7 @@ __global__ void __launch_bounds__(kDirectThreads) das_direct_kernel(const direct
                     const tau_split ts = split_tau(__fmaf_rn(gm[u].rsq, gm[u].rinv, ofs));
                     in[u] = live[u] && ts.k < nlast;
                     t[u] = ts.t;
-                    e[u] = row[u] + s * sstride + (in[u] ? (int)ts.k : 0);
+                    e[u] = row[u] + srow + (in[u] ? (int)ts.k : 0);
                 }
 #pragma unroll
                 for (int bi = 0; bi < BT; bi++) {
@@ -118,7 +125,11 @@ __global__ void __launch_bounds__(kDirectThreads) das_direct_kernel(const direct
                         if (live[u]) acc[bi] = __fmaf_rn(w, __fmaf_rn(t[u], x1[u] - x0[u], x0[u]), acc[bi]);
                 }
             }
-        }
+        };
+        const int stride = kDirectUnroll * split;
+        int c0 = part;
+        for (; c0 + (kDirectUnroll - 1) * split < C; c0 += stride) step(c0, std::false_type{});
+        if (c0 < C) step(c0, std::true_type{});
     }
     // partial sums of the voxel's split lanes (consecutive lanes of one warp)
     for (int off = split >> 1; off > 0; off >>= 1) {
