@@ -22,8 +22,11 @@ copied from pinned host memory and the image read back each step), `bf16` /
 `fp16` (reduced-precision pair storage: throughput, speed-up over FP32 and
 error against this library's FP64-pair pipeline), `bwd_fwd` (backward /
 forward time on the differentiable 128-channel, 8-plane-wave, batch-4
-workload, with the kernels that ran) and `configs` (the 2-D plane-wave frame
-under graph replay, the 200-frame FP16 ensemble and uneven das_sparse).
+workload, with the kernels that ran), `configs` (the 2-D plane-wave frame
+under graph replay, the 200-frame FP16 ensemble, uneven das_sparse and the
+GPU selection of das_sparse lists), `in_record_fraction` (share of the units
+whose tap lies inside the record) and `clocks` (SM clock and throttle reasons
+sampled through NVML during the timed region).
 `--impl reference` times the reference implementation (its CUDA das, built
 from its sources into oracle/_ref) on the same workloads and GPU.
 `--section bwd|configs` runs one part alone (for profiling).
