@@ -67,7 +67,7 @@ def candidates(x, dstpos, offsets, sparse_indices=None) -> list[dict]:
                 # event chunks of 8 and 4: fewer registers, more resident warps for latency-bound lists
                 for ec in (8, 4):
                     out.append(dict(variant=1, tile_x=t0, tile_y=t1, batch_tile=bt, event_chunk=ec))
-                    for mb in (8, 16):   # more channel slices than the default target of 4 CTAs per SM
+                    for mb in (8, 16, 32):   # channel-slice targets around the default of 16 CTAs per SM
                         out.append(dict(variant=1, tile_x=t0, tile_y=t1, batch_tile=bt, event_chunk=ec,
                                         min_blocks=mb))
         if real and sparse_indices is None:
