@@ -132,17 +132,34 @@ def schedule(cfg: dict | None, device=None):
         h.set_config(prev if any(prev.values()) else None)
 
 
+_MIN_TIMED_MS = 2.0      # a timed run of a small call repeats it until about this much device time
+_MAX_REPS = 256
+
+
 def _time(fn, reps: int) -> float:
+    """Per-call milliseconds: the best of three timed runs of at least `reps` calls.
+
+    Calls of a few microseconds are repeated until a run holds about 2 ms of
+    device time, so that launch jitter does not decide between schedules whose
+    difference is a few percent."""
     fn()
     torch.cuda.synchronize()
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
-    a.record()
-    for _ in range(reps):
-        fn()
-    b.record()
-    b.synchronize()
-    return a.elapsed_time(b) / reps
+
+    def run(n):
+        a.record()
+        for _ in range(n):
+            fn()
+        b.record()
+        b.synchronize()
+        return a.elapsed_time(b) / n
+
+    first = run(reps)
+    n = reps
+    if first * reps < _MIN_TIMED_MS:
+        n = min(_MAX_REPS, max(reps, int(_MIN_TIMED_MS / max(first, 1e-3))))
+    return min(first if n == reps else run(n), run(n), run(n))
 
 
 def autotune(x, srcpos, dstpos, offsets, weights, sparse_indices=None, *, use_fp16=False, use_bf16=False,
