@@ -121,6 +121,7 @@ SIGNATURES = {
                                    ctypes.c_int, c_ptr, c_desc, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr]),
     "ffdas_sparse_select": (c_err, [c_handle, c_ptr, c_ptr, ctypes.c_int, ctypes.c_int64, ctypes.c_int, c_ptr,
                                     c_ptr, c_ptr]),
+    "ffdas_truncate_rank": (c_err, [c_handle, c_desc, c_ptr, ctypes.c_int64, ctypes.c_int64, c_desc, c_ptr]),
     "ffdas_das_set_config": (c_err, [c_handle, ctypes.POINTER(DasConfig)]),
     "ffdas_das_get_config": (c_err, [c_handle, ctypes.POINTER(DasConfig)]),
     "ffdas_get_last_kernel_info": (c_err, [c_handle, ctypes.POINTER(KernelInfo)]),

@@ -220,6 +220,7 @@ ffdas_error_t ffdas_destroy(ffdas_handle_t h) {
     if (h->ev_start) cudaEventDestroy(h->ev_start);
     if (h->ev_stop) cudaEventDestroy(h->ev_stop);
     if (h->status) cudaFree(h->status);
+    if (h->solver && h->solver_release) h->solver_release(h->solver);
     cudaGetLastError();
     delete h;
     return err;

@@ -2,8 +2,9 @@
 //
 // The handle mirrors the reference's ffdas_context (src/core/context.cuh:21):
 // device id, arch code, stream, and a stream-ordered workspace allocator.
-// cuBLAS/cuSOLVER handles are dropped because no delay-and-sum kernel uses
-// them.  Workspace comes from a per-handle CUDA memory pool
+// No cuBLAS handle: no kernel here calls it.  The cuSOLVER state that
+// ffdas_truncate_rank needs is created on that function's first call.
+// Workspace comes from a per-handle CUDA memory pool
 // (cudaMallocFromPoolAsync) with a high release threshold, which makes it a
 // caching, graph-capturable allocator (the reference uses
 // cub::CachingDeviceAllocator, src/core/context.cu:143-158).
@@ -55,6 +56,10 @@ struct ffdas_context {
     bool timing = false;
     bool timing_recorded = false;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    // eigensolver state of ffdas_truncate_rank, created on its first call and
+    // released with the handle
+    void *solver = nullptr;
+    void (*solver_release)(void *) = nullptr;
 
     // Brackets the main kernel launch with events when timing is enabled.
     void mark_start() { if (timing) cudaEventRecord(ev_start, stream); }

@@ -1,0 +1,544 @@
+// truncate_rank.cu -- ffdas_truncate_rank: keep the singular components
+// [start, stop) of a 2-D matrix.  This is the slow-time clutter filter that
+// follows delay-and-sum on a frame ensemble: frames x voxels, with the
+// leading components (tissue) removed.
+//
+// Reference: src/truncate_rank/truncate_rank.cu:6-42 (entry point, dtype
+// switch) and src/truncate_rank/truncate_rank_impl.cuh:426-513 (Gram matrix of
+// the smaller side, eigendecomposition, projection).  The result is
+//     out = U_k U_k^H A,   U_k = left singular vectors start..stop-1 of A,
+// where A is x viewed as a (p, q) matrix with p = min(m, n) rows: x itself
+// when m <= n, else its transpose (then the filter reads out = x V_k V_k^H
+// with V the right singular vectors, the same result).
+//
+// Steps on the device:
+//  1. G = A A^H / q, p x p: a tiled SIMT product over the upper-triangle
+//     tiles only, split over q into partial sums that a second kernel adds in
+//     a fixed order in double.  The sum is therefore the same on every run.
+//     It is written as the column-major Hermitian matrix that the solver
+//     takes.  The reference forms the full product with one cuBLAS GEMM.
+//  2. Eigendecomposition of G with cuSOLVER's syevd, as the reference does.
+//     The library is loaded on first use, so the delay-and-sum path never
+//     depends on it.  Eigenvalues come back ascending, so singular rank s is
+//     eigenvector p-1-s.
+//  3. Projection with the smaller basis.  With k = stop-start kept vectors
+//     and c = p-k removed ones, out = U_k (U_k^H A) when k <= c, else
+//     out = A - U_c (U_c^H A).  Both are exact for an orthonormal
+//     eigenbasis.  The reference forms P = V_k V_k^H (SYRK) and applies it
+//     with one SYMM: 2 p^2 q multiply-adds.  Here the clutter filter
+//     (start = a few tissue ranks, stop = p) costs 4 c p q, and with up to 32
+//     basis vectors it is one pass over A: each thread owns one column,
+//     keeps U^H a in registers, and writes the filtered column.  Larger
+//     bases run as two tiled products through a (r, q) workspace.
+//  With k = p (keep everything) out is x, copied.
+//
+// The tensor cores are not used.  The reference computes in FP32/FP64, and
+// the filter subtracts a dominant component.  A TF32 product carries errors
+// of about 1e-3 of |x|, which is the size of the signal that remains.
+#include "core.h"
+
+#include <cusolverDn.h>
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstdint>
+#include <vector>
+
+namespace ffdas {
+namespace {
+
+// ---------------------------------------------------------------- elements
+
+template <typename T> struct tr_elem;
+template <> struct tr_elem<float> {
+    using real = float;
+    using acc = double;
+    static constexpr cudaDataType cuda = CUDA_R_32F, cuda_real = CUDA_R_32F;
+};
+template <> struct tr_elem<double> {
+    using real = double;
+    using acc = double;
+    static constexpr cudaDataType cuda = CUDA_R_64F, cuda_real = CUDA_R_64F;
+};
+template <> struct tr_elem<float2> {
+    using real = float;
+    using acc = double2;
+    static constexpr cudaDataType cuda = CUDA_C_32F, cuda_real = CUDA_R_32F;
+};
+template <> struct tr_elem<double2> {
+    using real = double;
+    using acc = double2;
+    static constexpr cudaDataType cuda = CUDA_C_64F, cuda_real = CUDA_R_64F;
+};
+
+template <typename T> __device__ __forceinline__ T tr_zero();
+template <> __device__ __forceinline__ float tr_zero<float>() { return 0.f; }
+template <> __device__ __forceinline__ double tr_zero<double>() { return 0.0; }
+template <> __device__ __forceinline__ float2 tr_zero<float2>() { return make_float2(0.f, 0.f); }
+template <> __device__ __forceinline__ double2 tr_zero<double2>() { return make_double2(0.0, 0.0); }
+
+__device__ __forceinline__ float tr_conj(float a) { return a; }
+__device__ __forceinline__ double tr_conj(double a) { return a; }
+__device__ __forceinline__ float2 tr_conj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ double2 tr_conj(double2 a) { return make_double2(a.x, -a.y); }
+
+// c += a * b
+__device__ __forceinline__ void tr_mac(float &c, float a, float b) { c = fmaf(a, b, c); }
+__device__ __forceinline__ void tr_mac(double &c, double a, double b) { c = fma(a, b, c); }
+__device__ __forceinline__ void tr_mac(float2 &c, float2 a, float2 b) {
+    c.x = fmaf(a.x, b.x, c.x);
+    c.x = fmaf(-a.y, b.y, c.x);
+    c.y = fmaf(a.x, b.y, c.y);
+    c.y = fmaf(a.y, b.x, c.y);
+}
+__device__ __forceinline__ void tr_mac(double2 &c, double2 a, double2 b) {
+    c.x = fma(a.x, b.x, c.x);
+    c.x = fma(-a.y, b.y, c.x);
+    c.y = fma(a.x, b.y, c.y);
+    c.y = fma(a.y, b.x, c.y);
+}
+
+// a + s * b (s = +1 or -1)
+__device__ __forceinline__ float tr_axpy(float a, float s, float b) { return fmaf(s, b, a); }
+__device__ __forceinline__ double tr_axpy(double a, double s, double b) { return fma(s, b, a); }
+__device__ __forceinline__ float2 tr_axpy(float2 a, float s, float2 b) {
+    return make_float2(fmaf(s, b.x, a.x), fmaf(s, b.y, a.y));
+}
+__device__ __forceinline__ double2 tr_axpy(double2 a, double s, double2 b) {
+    return make_double2(fma(s, b.x, a.x), fma(s, b.y, a.y));
+}
+
+// double accumulation of the Gram partials
+__device__ __forceinline__ void tr_acc_add(double &c, float a) { c += (double)a; }
+__device__ __forceinline__ void tr_acc_add(double &c, double a) { c += a; }
+__device__ __forceinline__ void tr_acc_add(double2 &c, float2 a) { c.x += (double)a.x; c.y += (double)a.y; }
+__device__ __forceinline__ void tr_acc_add(double2 &c, double2 a) { c.x += a.x; c.y += a.y; }
+template <typename T> __device__ __forceinline__ typename tr_elem<T>::acc tr_acc_zero();
+template <> __device__ __forceinline__ double tr_acc_zero<float>() { return 0.0; }
+template <> __device__ __forceinline__ double tr_acc_zero<double>() { return 0.0; }
+template <> __device__ __forceinline__ double2 tr_acc_zero<float2>() { return make_double2(0.0, 0.0); }
+template <> __device__ __forceinline__ double2 tr_acc_zero<double2>() { return make_double2(0.0, 0.0); }
+__device__ __forceinline__ void tr_store(float &o, double v, double s) { o = (float)(v * s); }
+__device__ __forceinline__ void tr_store(double &o, double v, double s) { o = v * s; }
+__device__ __forceinline__ void tr_store(float2 &o, double2 v, double s) {
+    o = make_float2((float)(v.x * s), (float)(v.y * s));
+}
+__device__ __forceinline__ void tr_store(double2 &o, double2 v, double s) { o = make_double2(v.x * s, v.y * s); }
+
+// ---------------------------------------------------------- tiled product
+
+constexpr int kTrTile = 64;       // C tile edge
+constexpr int kTrTileK = 16;      // k depth staged per step
+constexpr int kTrThreads = 256;   // 16 x 16 threads, 4 x 4 outputs each (rows ty + 16 a, columns tx + 16 b)
+
+template <typename T>
+struct tr_gemm_args {
+    const T *L;          // L(i, k) = L[i * li + k * lk]
+    int64_t li, lk;
+    const T *R;          // R(k, j) = R[k * rk + j * rj]
+    int64_t rk, rj;
+    T *C;                // C(i, j) = C[z * zstride + i * ci + j * cj]
+    int64_t ci, cj;
+    const T *base;       // when set, C = base + sign * sum (base has C's strides)
+    int64_t M, N, K;
+    int64_t kchunk;      // blockIdx.z sums k in [z * kchunk, (z + 1) * kchunk), a multiple of kTrTileK
+    int64_t zstride;
+    int conj_l, conj_r, upper;   // conjugate an operand; skip tiles below the diagonal
+    typename tr_elem<T>::real sign;
+};
+
+// C = op(L) op(R) over a 64 x 64 tile of C per CTA.  Each operand tile is
+// loaded with consecutive threads on its unit-stride index, so the loads
+// coalesce whichever way the operand is laid out.
+template <typename T>
+__global__ void __launch_bounds__(kTrThreads) tr_gemm_kernel(const tr_gemm_args<T> a) {
+    const int64_t bi = blockIdx.y, bj = blockIdx.x;
+    if (a.upper && bi > bj) return;
+    __shared__ T sL[kTrTileK][kTrTile + 1];
+    __shared__ T sR[kTrTileK][kTrTile + 1];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int64_t i0 = bi * kTrTile, j0 = bj * kTrTile;
+    const int64_t kbeg = (int64_t)blockIdx.z * a.kchunk;
+    const int64_t kend = min(a.K, kbeg + a.kchunk);
+    const bool l_kfast = a.lk == 1, r_kfast = a.rk == 1;
+    T acc[4][4];
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) acc[x][y] = tr_zero<T>();
+
+    for (int64_t k0 = kbeg; k0 < kend; k0 += kTrTileK) {
+#pragma unroll
+        for (int u = 0; u < (kTrTile * kTrTileK) / kTrThreads; u++) {
+            const int e = tid + u * kTrThreads;
+            int kk = l_kfast ? (e & (kTrTileK - 1)) : (e / kTrTile);
+            const int ii = l_kfast ? (e / kTrTileK) : (e & (kTrTile - 1));
+            int64_t k = k0 + kk;
+            T v = tr_zero<T>();
+            if (i0 + ii < a.M && k < kend) {
+                v = a.L[(i0 + ii) * a.li + k * a.lk];
+                if (a.conj_l) v = tr_conj(v);
+            }
+            sL[kk][ii] = v;
+            kk = r_kfast ? (e & (kTrTileK - 1)) : (e / kTrTile);
+            const int jj = r_kfast ? (e / kTrTileK) : (e & (kTrTile - 1));
+            k = k0 + kk;
+            T w = tr_zero<T>();
+            if (j0 + jj < a.N && k < kend) {
+                w = a.R[k * a.rk + (j0 + jj) * a.rj];
+                if (a.conj_r) w = tr_conj(w);
+            }
+            sR[kk][jj] = w;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < kTrTileK; kk++) {
+            T l[4], r[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                l[q] = sL[kk][ty + 16 * q];
+                r[q] = sR[kk][tx + 16 * q];
+            }
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++) tr_mac(acc[x][y], l[x], r[y]);
+        }
+        __syncthreads();
+    }
+    T *C = a.C + (int64_t)blockIdx.z * a.zstride;
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+        const int64_t i = i0 + ty + 16 * x;
+        if (i >= a.M) continue;
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+            const int64_t j = j0 + tx + 16 * y;
+            if (j >= a.N) continue;
+            T v = acc[x][y];
+            if (a.base) v = tr_axpy(a.base[i * a.ci + j * a.cj], a.sign, v);
+            C[i * a.ci + j * a.cj] = v;
+        }
+    }
+}
+
+// G (column-major, p x p, both triangles) = scale * sum over the splits of
+// the row-major partials, added in split order in double.  Only i <= j is
+// read: every upper-triangle element lies in a computed tile.
+template <typename T>
+__global__ void tr_gram_reduce_kernel(const T *__restrict__ part, int splits, int64_t p, double scale,
+                                      T *__restrict__ G) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= p * p) return;
+    const int64_t i = e / p, j = e - i * p;
+    if (i > j) return;
+    typename tr_elem<T>::acc s = tr_acc_zero<T>();
+    for (int z = 0; z < splits; z++) tr_acc_add(s, part[(int64_t)z * p * p + e]);
+    T v;
+    tr_store(v, s, scale);
+    G[i + j * p] = v;
+    G[j + i * p] = tr_conj(v);
+}
+
+// U[i * r + t] = V[i + e(t) * p] (row-major p x r basis), e(t) = e0 + t for
+// t < r0, else e1 + t - r0.
+template <typename T>
+__global__ void tr_gather_basis_kernel(const T *__restrict__ V, int64_t p, int r, int64_t e0, int r0, int64_t e1,
+                                       T *__restrict__ U) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= p * r) return;
+    const int64_t i = e / r;
+    const int t = (int)(e - i * r);
+    const int64_t col = t < r0 ? e0 + t : e1 + (t - r0);
+    U[e] = V[i + col * p];
+}
+
+// One pass over A for bases of up to RMAX vectors: a thread owns column j,
+// forms w = U^H a_j in registers, then writes U w (or a_j - U w).  The basis
+// sits in shared memory and is read as a broadcast.  out may alias x: a
+// column is read in full before it is written.
+template <typename T, int RMAX>
+__global__ void __launch_bounds__(256) tr_project_small_kernel(const T *x, int64_t sp, int64_t sq, int64_t p,
+                                                               int64_t q, const T *__restrict__ U, int r,
+                                                               int subtract, T *out) {
+    extern __shared__ unsigned char tr_smem[];
+    T *sU = reinterpret_cast<T *>(tr_smem);
+    for (int64_t e = threadIdx.x; e < p * r; e += blockDim.x) sU[e] = U[e];
+    __syncthreads();
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= q) return;
+    T w[RMAX];
+#pragma unroll
+    for (int t = 0; t < RMAX; t++) w[t] = tr_zero<T>();
+    const T *col = x + j * sq;
+    for (int64_t l = 0; l < p; l++) {
+        const T v = col[l * sp];
+        const T *u = sU + l * r;
+#pragma unroll
+        for (int t = 0; t < RMAX; t++)
+            if (t < r) tr_mac(w[t], tr_conj(u[t]), v);
+    }
+    T *oc = out + j * sq;
+    for (int64_t l = 0; l < p; l++) {
+        const T *u = sU + l * r;
+        T s = tr_zero<T>();
+#pragma unroll
+        for (int t = 0; t < RMAX; t++)
+            if (t < r) tr_mac(s, u[t], w[t]);
+        oc[l * sp] = subtract ? tr_axpy(col[l * sp], (typename tr_elem<T>::real)-1, s) : s;
+    }
+}
+
+// ------------------------------------------------------------- cuSOLVER
+
+struct solver_api {
+    decltype(&cusolverDnCreate) create = nullptr;
+    decltype(&cusolverDnDestroy) destroy = nullptr;
+    decltype(&cusolverDnSetStream) set_stream = nullptr;
+    decltype(&cusolverDnCreateParams) create_params = nullptr;
+    decltype(&cusolverDnDestroyParams) destroy_params = nullptr;
+    decltype(&cusolverDnXsyevd_bufferSize) buffer_size = nullptr;
+    decltype(&cusolverDnXsyevd) syevd = nullptr;
+    bool ok = false;
+};
+
+const solver_api &solver() {
+    static const solver_api api = [] {
+        solver_api s;
+        void *lib = dlopen("libcusolver.so.11", RTLD_NOW | RTLD_LOCAL);
+        if (!lib) lib = dlopen("libcusolver.so", RTLD_NOW | RTLD_LOCAL);
+        if (!lib) return s;
+        s.create = reinterpret_cast<decltype(s.create)>(dlsym(lib, "cusolverDnCreate"));
+        s.destroy = reinterpret_cast<decltype(s.destroy)>(dlsym(lib, "cusolverDnDestroy"));
+        s.set_stream = reinterpret_cast<decltype(s.set_stream)>(dlsym(lib, "cusolverDnSetStream"));
+        s.create_params = reinterpret_cast<decltype(s.create_params)>(dlsym(lib, "cusolverDnCreateParams"));
+        s.destroy_params = reinterpret_cast<decltype(s.destroy_params)>(dlsym(lib, "cusolverDnDestroyParams"));
+        s.buffer_size = reinterpret_cast<decltype(s.buffer_size)>(dlsym(lib, "cusolverDnXsyevd_bufferSize"));
+        s.syevd = reinterpret_cast<decltype(s.syevd)>(dlsym(lib, "cusolverDnXsyevd"));
+        s.ok = s.create && s.destroy && s.set_stream && s.create_params && s.destroy_params && s.buffer_size &&
+               s.syevd;
+        return s;
+    }();
+    return api;
+}
+
+struct solver_state {
+    cusolverDnHandle_t h = nullptr;
+    cusolverDnParams_t params = nullptr;
+};
+
+void release_solver(void *p) {
+    auto *s = static_cast<solver_state *>(p);
+    if (solver().ok) {
+        if (s->params) solver().destroy_params(s->params);
+        if (s->h) solver().destroy(s->h);
+    }
+    delete s;
+}
+
+// The handle's solver state, created on first use (binds to the current
+// device, which check_device has matched to the handle's).
+ffdas_error_t get_solver(ffdas_context &ctx, solver_state **out) {
+    if (!solver().ok) return FFDAS_ERROR_CUSOLVER;
+    if (!ctx.solver) {
+        auto *s = new solver_state;
+        if (solver().create(&s->h) != CUSOLVER_STATUS_SUCCESS) {
+            delete s;
+            return FFDAS_ERROR_CUSOLVER;
+        }
+        if (solver().create_params(&s->params) != CUSOLVER_STATUS_SUCCESS) {
+            solver().destroy(s->h);
+            delete s;
+            return FFDAS_ERROR_CUSOLVER;
+        }
+        ctx.solver = s;
+        ctx.solver_release = release_solver;
+    }
+    *out = static_cast<solver_state *>(ctx.solver);
+    return solver().set_stream((*out)->h, ctx.stream) == CUSOLVER_STATUS_SUCCESS ? FFDAS_SUCCESS
+                                                                              : FFDAS_ERROR_CUSOLVER;
+}
+
+// ------------------------------------------------------------------ driver
+
+constexpr size_t kSmallBasisSmem = 48 * 1024;
+constexpr size_t kGramPartialBytes = size_t(256) << 20;
+
+template <typename T, int RMAX>
+ffdas_error_t launch_small(ffdas_context &h, const T *x, int64_t sp, int64_t sq, int64_t p, int64_t q, const T *U,
+                           int r, int subtract, T *out) {
+    const int64_t blocks = (q + 255) / 256;
+    if (blocks > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
+    tr_project_small_kernel<T, RMAX><<<(unsigned)blocks, 256, (size_t)p * r * sizeof(T), h.stream>>>(
+        x, sp, sq, p, q, U, r, subtract, out);
+    return ffdas_launch_check(h.stream);
+}
+
+template <typename T>
+ffdas_error_t launch_gemm(ffdas_context &h, const tr_gemm_args<T> &a, int splits) {
+    const int64_t gx = (a.N + kTrTile - 1) / kTrTile, gy = (a.M + kTrTile - 1) / kTrTile;
+    if (gx > INT32_MAX || gy > 65535) return FFDAS_ERROR_DIMS_TOO_LARGE;
+    tr_gemm_kernel<T><<<dim3((unsigned)gx, (unsigned)gy, (unsigned)splits), kTrThreads, 0, h.stream>>>(a);
+    return ffdas_launch_check(h.stream);
+}
+
+template <typename T>
+ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x, T *out, int64_t start,
+                              int64_t stop) {
+    using real = typename tr_elem<T>::real;
+    // A = x (p = m) when m <= n, else x^T (p = n): truncate_rank_impl.cuh:451-453
+    const bool rows = m <= n;
+    const int64_t p = rows ? m : n, q = rows ? n : m;
+    const int64_t sp = rows ? n : 1, sq = rows ? 1 : n;
+    const int64_t keep = stop - start, drop = p - keep;
+    if (drop == 0) {
+        if (out != x) FFDAS_CUDA(cudaMemcpyAsync(out, x, (size_t)(m * n) * sizeof(T), cudaMemcpyDeviceToDevice,
+                                                 h.stream));
+        return FFDAS_SUCCESS;
+    }
+    solver_state *sv = nullptr;
+    FFDAS_TRY(get_solver(h, &sv));
+
+    // 1. Gram matrix, upper tiles, split over q
+    const int64_t tiles = (p + kTrTile - 1) / kTrTile;
+    const int64_t tri = tiles * (tiles + 1) / 2;
+    int64_t splits = (4 * (int64_t)h.sm_count + tri - 1) / tri;
+    splits = std::max<int64_t>(1, std::min<int64_t>(splits, (q + kTrTileK - 1) / kTrTileK));
+    splits = std::max<int64_t>(1, std::min<int64_t>(splits, (int64_t)(kGramPartialBytes / ((size_t)p * p * sizeof(T)))));
+    splits = std::min<int64_t>(splits, 65535);
+    int64_t kchunk = (q + splits - 1) / splits;
+    kchunk = (kchunk + kTrTileK - 1) / kTrTileK * kTrTileK;
+    splits = (q + kchunk - 1) / kchunk;
+
+    workspace part(h), gram(h), eig(h), info(h);
+    FFDAS_TRY(part.alloc((size_t)(splits * p * p) * sizeof(T)));
+    FFDAS_TRY(gram.alloc((size_t)(p * p) * sizeof(T)));
+    FFDAS_TRY(eig.alloc((size_t)p * sizeof(real)));
+    FFDAS_TRY(info.alloc(sizeof(int)));
+
+    tr_gemm_args<T> g{};
+    g.L = x; g.li = sp; g.lk = sq;
+    g.R = x; g.rk = sq; g.rj = sp; g.conj_r = 1;
+    g.C = part.get<T>(); g.ci = p; g.cj = 1; g.zstride = p * p;
+    g.M = p; g.N = p; g.K = q; g.kchunk = kchunk; g.upper = 1; g.sign = 1;
+    FFDAS_TRY(launch_gemm(h, g, (int)splits));
+    {
+        const int64_t blocks = (p * p + 255) / 256;
+        tr_gram_reduce_kernel<T><<<(unsigned)blocks, 256, 0, h.stream>>>(part.get<T>(), (int)splits, p,
+                                                                         1.0 / (double)q, gram.get<T>());
+        FFDAS_TRY(ffdas_launch_check(h.stream));
+    }
+
+    // 2. eigendecomposition (truncate_rank_impl.cuh:481-500, 68-90)
+    size_t dev_bytes = 0, host_bytes = 0;
+    if (solver().buffer_size(sv->h, sv->params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, p,
+                             tr_elem<T>::cuda, gram.get<T>(), p, tr_elem<T>::cuda_real, eig.get<real>(),
+                             tr_elem<T>::cuda, &dev_bytes, &host_bytes) != CUSOLVER_STATUS_SUCCESS)
+        return FFDAS_ERROR_CUSOLVER;
+    // The reference allocates p times the reported device workspace (its
+    // note: the size is underestimated on some architectures); the same
+    // margin here, bounded for large p.
+    size_t margin = (size_t)p * dev_bytes;
+    if (dev_bytes && margin / dev_bytes != (size_t)p) margin = SIZE_MAX;
+    const size_t cap = std::max<size_t>(size_t(1) << 30, 8 * dev_bytes);
+    const size_t dev_alloc = std::max<size_t>(std::min(margin, cap), dev_bytes);
+    workspace sdev(h);
+    FFDAS_TRY(sdev.alloc(dev_alloc));
+    std::vector<unsigned char> shost(std::max<size_t>(host_bytes, 1));
+    if (solver().syevd(sv->h, sv->params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, p, tr_elem<T>::cuda,
+                       gram.get<T>(), p, tr_elem<T>::cuda_real, eig.get<real>(), tr_elem<T>::cuda,
+                       sdev.get<void>(), dev_bytes, shost.data(), host_bytes,
+                       info.get<int>()) != CUSOLVER_STATUS_SUCCESS)
+        return FFDAS_ERROR_CUSOLVER;
+
+    // 3. projection with the smaller basis; eigenvector e = p-1-rank
+    const bool direct = keep <= drop;
+    const int r = (int)(direct ? keep : drop);
+    const int64_t e0 = direct ? p - stop : 0;
+    const int r0 = (int)(direct ? keep : p - stop);
+    const int64_t e1 = p - start;
+    workspace basis(h);
+    FFDAS_TRY(basis.alloc((size_t)(p * r) * sizeof(T)));
+    {
+        const int64_t blocks = (p * r + 255) / 256;
+        tr_gather_basis_kernel<T><<<(unsigned)blocks, 256, 0, h.stream>>>(gram.get<T>(), p, r, e0, r0, e1,
+                                                                          basis.get<T>());
+        FFDAS_TRY(ffdas_launch_check(h.stream));
+    }
+    const int subtract = direct ? 0 : 1;
+    if (r <= 32 && (size_t)(p * r) * sizeof(T) <= kSmallBasisSmem) {
+        const T *U = basis.get<T>();
+        if (r <= 4) FFDAS_TRY((launch_small<T, 4>(h, x, sp, sq, p, q, U, r, subtract, out)));
+        else if (r <= 8) FFDAS_TRY((launch_small<T, 8>(h, x, sp, sq, p, q, U, r, subtract, out)));
+        else if (r <= 16) FFDAS_TRY((launch_small<T, 16>(h, x, sp, sq, p, q, U, r, subtract, out)));
+        else FFDAS_TRY((launch_small<T, 32>(h, x, sp, sq, p, q, U, r, subtract, out)));
+    } else {
+        workspace wbuf(h);
+        FFDAS_TRY(wbuf.alloc((size_t)r * (size_t)q * sizeof(T)));
+        tr_gemm_args<T> w{};          // W = U^H A  (r x q)
+        w.L = basis.get<T>(); w.li = 1; w.lk = r; w.conj_l = 1;
+        w.R = x; w.rk = sp; w.rj = sq;
+        w.C = wbuf.get<T>(); w.ci = q; w.cj = 1;
+        w.M = r; w.N = q; w.K = p; w.kchunk = (p + kTrTileK - 1) / kTrTileK * kTrTileK; w.sign = 1;
+        FFDAS_TRY(launch_gemm(h, w, 1));
+        tr_gemm_args<T> o{};          // out = U W, or A - U W
+        o.L = basis.get<T>(); o.li = r; o.lk = 1;
+        o.R = wbuf.get<T>(); o.rk = q; o.rj = 1;
+        o.C = out; o.ci = sp; o.cj = sq;
+        o.base = subtract ? x : nullptr; o.sign = subtract ? (real)-1 : (real)1;
+        o.M = p; o.N = q; o.K = r; o.kchunk = ((int64_t)r + kTrTileK - 1) / kTrTileK * kTrTileK;
+        FFDAS_TRY(launch_gemm(h, o, 1));
+    }
+
+    // The solver's status, read once everything is queued (the reference
+    // reads it before the projection, truncate_rank_impl.cuh:92-97).
+    int h_info = 0;
+    FFDAS_CUDA(cudaMemcpyAsync(&h_info, info.get<int>(), sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+    FFDAS_CUDA(cudaStreamSynchronize(h.stream));
+    return h_info == 0 ? FFDAS_SUCCESS : FFDAS_ERROR_CUSOLVER;
+}
+
+bool c_contiguous_2d(const ffdas_tensor_desc &d) {
+    return (d.dims[1] <= 1 || d.strides[1] == 1) && (d.dims[0] <= 1 || d.strides[0] == d.dims[1]);
+}
+
+}  // namespace
+}  // namespace ffdas
+
+using namespace ffdas;
+
+extern "C" ffdas_error_t ffdas_truncate_rank(ffdas_handle_t handle, ffdas_tensor_desc_t x_desc, const void *x,
+                                             int64_t start, int64_t stop, ffdas_tensor_desc_t out_desc,
+                                             void *out) {
+    // validation order: truncate_rank.cu:15-26, truncate_rank_impl.cuh:432-443
+    if (!handle) return FFDAS_ERROR_INVALID_HANDLE;
+    if (!x_desc || !out_desc) return FFDAS_ERROR_NULL_POINTER;
+    FFDAS_TRY(handle->check_device());
+    const ffdas_tensor_desc &xd = *x_desc, &od = *out_desc;
+    if (xd.dtype != od.dtype) return FFDAS_ERROR_UNSUPPORTED_TYPE;
+    if (xd.dtype != FFDAS_R_32F && xd.dtype != FFDAS_C_32F && xd.dtype != FFDAS_R_64F && xd.dtype != FFDAS_C_64F)
+        return FFDAS_ERROR_UNSUPPORTED_TYPE;
+    if (xd.ndim != 2 || od.ndim != 2) return FFDAS_ERROR_INVALID_DIMS;
+    if (xd.dims[0] != od.dims[0] || xd.dims[1] != od.dims[1]) return FFDAS_ERROR_INVALID_DIMS;
+    if (xd.dims[0] > INT_MAX || xd.dims[1] > INT_MAX) return FFDAS_ERROR_INVALID_DIMS;
+    if (!c_contiguous_2d(xd) || !c_contiguous_2d(od)) return FFDAS_ERROR_NON_CONTIGUOUS;
+    const int64_t m = xd.dims[0], n = xd.dims[1];
+    const int64_t p = std::min(m, n);
+    if (start < 0 || start >= p || stop <= start || stop > p) return FFDAS_ERROR_INVALID_ARGUMENT;
+    if (!x || !out) return FFDAS_ERROR_NULL_POINTER;
+    ffdas_context &h = *handle;
+    switch (xd.dtype) {
+    case FFDAS_R_32F:
+        return truncate_rank_t<float>(h, m, n, static_cast<const float *>(x), static_cast<float *>(out), start, stop);
+    case FFDAS_R_64F:
+        return truncate_rank_t<double>(h, m, n, static_cast<const double *>(x), static_cast<double *>(out), start,
+                                       stop);
+    case FFDAS_C_32F:
+        return truncate_rank_t<float2>(h, m, n, static_cast<const float2 *>(x), static_cast<float2 *>(out), start,
+                                       stop);
+    default:
+        return truncate_rank_t<double2>(h, m, n, static_cast<const double2 *>(x), static_cast<double2 *>(out),
+                                        start, stop);
+    }
+}

@@ -342,6 +342,24 @@ FFDAS_API ffdas_error_t ffdas_sparse_select(
     float *sparse_offsets
 );
 
+/* Rank filter: out = the singular components start..stop-1 of x (m, n)
+ * (reference include/ffdas.h:178-186, src/truncate_rank/truncate_rank.cu:6).
+ * x and out: 2-D, same dims, C-contiguous (else FFDAS_ERROR_NON_CONTIGUOUS),
+ * same dtype in {R_32F, C_32F, R_64F, C_64F}; 0 <= start < stop <=
+ * min(m, n), else FFDAS_ERROR_INVALID_ARGUMENT.  out may be x.  The
+ * eigensolver (cuSOLVER syevd, loaded at the first call) reports through
+ * FFDAS_ERROR_CUSOLVER; the call waits for its status, so it returns with
+ * the handle's stream drained, as the reference's does. */
+FFDAS_API ffdas_error_t ffdas_truncate_rank(
+    ffdas_handle_t handle,
+    ffdas_tensor_desc_t x_desc,
+    const void *x,
+    int64_t start,
+    int64_t stop,
+    ffdas_tensor_desc_t out_desc,
+    void *out
+);
+
 /* New: schedule override for the following calls on this handle
  * (NULL restores the planner default). */
 FFDAS_API ffdas_error_t ffdas_das_set_config(ffdas_handle_t handle,

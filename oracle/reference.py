@@ -54,6 +54,7 @@ def lib():
         L.ffdas_das.argtypes = [vp, vp, vp, ctypes.c_float, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_int]
         L.ffdas_das_sparse.argtypes = [vp, vp, vp, ctypes.c_float, vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp, vp,
                                        ctypes.c_int, ctypes.c_int]
+        L.ffdas_truncate_rank.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_int64, vp, vp]
         L.ffdas_error_string.restype = ctypes.c_char_p
         _lib = L
     return _lib
@@ -205,3 +206,49 @@ class Prepared:
         L.ffdas_destroy_tensor_desc(self.od)
         if self.tile is not None:
             os.environ.pop("FFDAS_ALG1_TILE_SIZE", None)
+
+
+DT_RANK = {torch.float32: 0, torch.float64: 16, torch.complex64: 4, torch.complex128: 17}
+
+
+class PreparedRank:
+    """The reference's rank filter (src/truncate_rank/truncate_rank.cu:6-42) on a
+    contiguous 2-D CUDA tensor, descriptors made once, for parity and timing.
+    It reads x within its bounds, so no guard is needed; the window is checked
+    here the way the reference's Python wrapper checks it."""
+
+    def __init__(self, x: torch.Tensor, start: int, stop: int | None = None):
+        if x.ndim != 2 or not x.is_contiguous() or x.dtype not in DT_RANK:
+            raise ValueError("need a contiguous 2-D float32/float64/complex64/complex128 tensor")
+        m, n = x.shape
+        stop = min(m, n) if stop is None else stop
+        if not (0 <= start < stop <= min(m, n)):
+            raise ValueError("need 0 <= start < stop <= min(m, n)")
+        self.x, self.start, self.stop = x, int(start), int(stop)
+        self.out = torch.empty_like(x)
+        self.xd = _desc([m, n], DT_RANK[x.dtype])
+        self.od = _desc([m, n], DT_RANK[x.dtype])
+        self.h = handle(x.device.index)
+        self.dev = x.device
+
+    def __call__(self):
+        L = lib()
+        L.ffdas_set_stream(self.h, torch.cuda.current_stream(self.dev).cuda_stream)
+        rc = L.ffdas_truncate_rank(self.h, self.xd, self.x.data_ptr(), self.start, self.stop, self.od,
+                                   self.out.data_ptr())
+        if rc != 0:
+            raise RuntimeError(f"reference truncate_rank failed: {L.ffdas_error_string(rc).decode()}")
+        return self.out
+
+    def close(self):
+        L = lib()
+        L.ffdas_destroy_tensor_desc(self.xd)
+        L.ffdas_destroy_tensor_desc(self.od)
+
+
+def truncate_rank(x: torch.Tensor, start: int, stop: int | None = None) -> torch.Tensor:
+    call = PreparedRank(x.contiguous(), start, stop)
+    try:
+        return call().clone()
+    finally:
+        call.close()

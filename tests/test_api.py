@@ -131,3 +131,28 @@ def test_tuner_candidates_cover_each_kernel_family():
     xc = small["x"].to(torch.complex64)
     cc = candidates(xc, small["dstpos"], small["offsets"])
     assert cc and all(k["variant"] == 1 for k in cc)
+
+
+# ------------------------------------------------ truncate_rank argument checks
+# reference bindings/python/tests/test_truncate_rank.py:11-33: ValueError before
+# any device work (CPU tensors suffice).
+
+def test_truncate_rank_1d_rejected():
+    with pytest.raises(ValueError):
+        ffdas_b200.truncate_rank(torch.ones(10), start=0)
+
+
+@pytest.mark.parametrize("start, stop", [(-1, None), (4, None), (2, 1), (0, 5)])
+def test_truncate_rank_window_rejected(start, stop):
+    with pytest.raises(ValueError):
+        ffdas_b200.truncate_rank(torch.ones((4, 8)), start=start, stop=stop)
+
+
+def test_truncate_rank_out_shape_rejected():
+    with pytest.raises(ValueError):
+        ffdas_b200.truncate_rank(torch.ones((4, 8)), 0, out=torch.ones((8, 4)))
+
+
+def test_truncate_rank_needs_cuda():
+    with pytest.raises(ValueError, match="CUDA"):
+        ffdas_b200.truncate_rank(torch.ones((4, 8)), 0)

@@ -30,7 +30,8 @@ def test_header_declares_the_das_path():
     names = declared_functions()
     for n in ("ffdas_das", "ffdas_das_sparse", "ffdas_create", "ffdas_destroy", "ffdas_set_stream",
               "ffdas_get_stream", "ffdas_create_tensor_desc", "ffdas_destroy_tensor_desc", "ffdas_error_string",
-              "ffdas_type_size", "ffdas_event_create", "ffdas_event_elapsed_time", "ffdas_das_backward"):
+              "ffdas_type_size", "ffdas_event_create", "ffdas_event_elapsed_time", "ffdas_das_backward",
+              "ffdas_truncate_rank"):
         assert n in names
 
 
@@ -92,6 +93,7 @@ def test_null_handle_is_rejected_before_any_device_work():
     assert L.ffdas_destroy(None) == Error.INVALID_HANDLE
     assert L.ffdas_das_set_config(None, None) == Error.INVALID_HANDLE
     assert L.ffdas_sparse_select(None, None, None, 4, 16, 2, None, None, None) == Error.INVALID_HANDLE
+    assert L.ffdas_truncate_rank(None, None, None, 0, 1, None, None) == Error.INVALID_HANDLE
     assert L.ffdas_contiguous_copy(None, None, None, None, None) == Error.INVALID_HANDLE
     assert L.ffdas_event_record(None, 1) == Error.INVALID_HANDLE
     assert L.ffdas_event_synchronize(0) == Error.INVALID_ARGUMENT

@@ -189,3 +189,38 @@ def test_oracle_matches_reference_outputs(path):
                          q1=q1, **kw)
     tol = float(z["tol"])
     assert oracle.rel_l2(ref_out, got) < tol
+
+
+# ---------------------------------------------------------------- rank filter
+
+from oracle import truncate_rank as tro  # noqa: E402
+
+
+@pytest.mark.parametrize("shape", [(16, 64), (64, 16), (32, 32), (8, 4, 16)])
+@pytest.mark.parametrize("cplx", [False, True])
+def test_rank_filter_oracle_matches_svd(shape, cplx):
+    # the eigen route of the reference equals the SVD reconstruction its tests
+    # use (test_truncate_rank.py:38-43) on spectra with a gap at the cut
+    m = shape[0]
+    n = int(np.prod(shape[1:]))
+    x = tro.clutter_ensemble(m, n, rank=3, complex_=cplx, seed=1).reshape(shape)
+    for start, stop in [(0, 3), (3, None), (1, 3), (0, min(m, n))]:
+        a = tro.truncate_rank_f64(x, start, stop)
+        b = tro.svd_filter_f64(x, start, stop)
+        assert a.shape == x.shape
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-9 * np.abs(x).max())
+
+
+def test_rank_filter_oracle_keep_all_is_identity(rng):
+    # reference test_truncate_rank.py:46-50
+    x = rng.standard_normal((8, 32))
+    np.testing.assert_allclose(tro.truncate_rank_f64(x, 0, 8), x, atol=1e-12)
+
+
+def test_rank_filter_oracle_projection_properties(rng):
+    # idempotent, and the kept and dropped parts add up to x
+    x = rng.standard_normal((12, 40)) + 1j * rng.standard_normal((12, 40))
+    a = tro.truncate_rank_f64(x, 2, 7)
+    np.testing.assert_allclose(tro.truncate_rank_f64(a, 0, 5), a, atol=1e-10)
+    parts = tro.truncate_rank_f64(x, 0, 2) + a + tro.truncate_rank_f64(x, 7, 12)
+    np.testing.assert_allclose(parts, x, atol=1e-10)
