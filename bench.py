@@ -23,8 +23,9 @@ copied from pinned host memory and the image read back each step), `bf16` /
 error against this library's FP64-pair pipeline), `bwd_fwd` (backward /
 forward time on the differentiable 128-channel, 8-plane-wave, batch-4
 workload, with the kernels that ran), `configs` (the 2-D plane-wave frame
-under graph replay, the 200-frame FP16 ensemble, uneven das_sparse and the
-GPU selection of das_sparse lists), `in_record_fraction` (share of the units
+under graph replay, the 200-frame FP16 ensemble, uneven das_sparse, the
+GPU selection of das_sparse lists and the truncate_rank clutter filter on
+beamformed ensembles), `in_record_fraction` (share of the units
 whose tap lies inside the record) and `clocks` (SM clock and throttle reasons
 sampled through NVML during the timed region).
 `--impl reference` times the reference implementation (its CUDA das, built
@@ -618,7 +619,61 @@ def config_extras(args, impl: str) -> dict:
         del wl, geo
         torch.cuda.empty_cache()
     out["sparse_select"] = select_extra(args, impl, dev, stream)
+    out["rank_filter"] = rank_filter_extra(args, impl, dev, stream)
     return {"configs": out}
+
+
+def slow_time_ensemble(m: int, shape: tuple, dtype: torch.dtype, dev, seed: int) -> torch.Tensor:
+    """Seeded beamformed ensemble (m frames of `shape` voxels): 5 'tissue'
+    components, each 4x weaker than the previous, plus weak full-rank 'blood'."""
+    g = torch.Generator().manual_seed(seed)
+    n = int(np.prod(shape))
+    cplx = dtype.is_complex
+    rdt = torch.float64
+
+    def draw(*sz):
+        a = torch.randn(*sz, generator=g, dtype=rdt)
+        return torch.complex(a, torch.randn(*sz, generator=g, dtype=rdt)) if cplx else a
+
+    u = torch.linalg.qr(draw(m, 5))[0].to(dev)
+    v = (draw(n, 5) / np.sqrt(n)).to(dev)
+    s = (10.0 * np.sqrt(n)) * 4.0 ** -torch.arange(5, dtype=rdt, device=dev)
+    x = (u * s) @ v.conj().T + 1e-2 * draw(m, n).to(dev)
+    return x.to(dtype).reshape(m, *shape).contiguous()
+
+
+def rank_filter_extra(args, impl: str, dev, stream) -> dict:
+    """The clutter filter that follows beamforming: truncate_rank with the 5
+    leading (tissue) ranks removed, on a 200-frame 400x256 FP32 image
+    ensemble (the ensemble configuration's output shape) and on a 64-frame
+    64^3 complex64 volume (the reference's clutter_filter example).  Ours:
+    ffdas_truncate_rank; reference: its ffdas_truncate_rank built from its
+    sources (cuBLAS GEMM, cuSOLVER syevd, SYRK + SYMM).  Both calls return
+    with the stream drained (the solver status is read on the host)."""
+    out = {}
+    steps, warm = max(args.steps, 5), args.warmup
+    for name, (m, shape, dtype, seed) in {"ensemble_f32": (200, (400, 256), torch.float32, 51),
+                                          "volume_c64": (64, (64, 64, 64), torch.complex64, 52)}.items():
+        x = slow_time_ensemble(m, shape, dtype, dev, seed)
+        if impl == "reference":
+            from oracle import reference
+            if not reference.available():
+                out[name] = {"unavailable": "oracle/_ref/libffdas_ref.so not built"}
+                continue
+            call = reference.PreparedRank(x.view(m, -1), 5)
+            ms = timed(call, steps, warm, stream, 1)
+            call.close()
+            kind = "reference ffdas_truncate_rank"
+        else:
+            import ffdas_b200
+            res = torch.empty_like(x)
+            ms = timed(lambda: ffdas_b200.truncate_rank(x, 5, out=res), steps, warm, stream, 1)
+            kind = "ffdas_b200 ffdas_truncate_rank"
+        out[name] = {"ms_per_call": ms, "shape": [m, *shape], "dtype": str(dtype).replace("torch.", ""),
+                     "start": 5, "impl": kind}
+        del x
+        torch.cuda.empty_cache()
+    return out
 
 
 def select_extra(args, impl: str, dev, stream) -> dict:

@@ -129,8 +129,8 @@ __device__ __forceinline__ void tr_store(double2 &o, double2 v, double s) { o = 
 // ---------------------------------------------------------- tiled product
 
 constexpr int kTrTile = 64;       // C tile edge
-constexpr int kTrTileK = 16;      // k depth staged per step
-constexpr int kTrThreads = 256;   // 16 x 16 threads, 4 x 4 outputs each (rows ty + 16 a, columns tx + 16 b)
+constexpr int kTrTileK = 16;      // host-side k granularity (a multiple of every tr_tile_k)
+constexpr int kTrThreads = 256;   // 16 x 16 threads, 4 x 4 outputs each (rows 4 ty + a, columns 4 tx + b)
 
 template <typename T>
 struct tr_gemm_args {
@@ -148,15 +148,32 @@ struct tr_gemm_args {
     typename tr_elem<T>::real sign;
 };
 
+// four consecutive elements, read from shared memory as 16-byte vectors
+template <typename T> struct __align__(16) tr_quad { T v[4]; };
+
+// k depth staged per step: 16, or 8 for 16-byte elements (two stages of both
+// operand tiles stay within the 48 KB of static shared memory)
+template <typename T> constexpr int tr_tile_k() { return sizeof(T) > 8 ? 8 : 16; }
+
 // C = op(L) op(R) over a 64 x 64 tile of C per CTA.  Each operand tile is
 // loaded with consecutive threads on its unit-stride index, so the loads
-// coalesce whichever way the operand is laid out.
+// coalesce whichever way the operand is laid out.  Two shared-memory stages:
+// the next tiles are loaded into registers while the current ones are used,
+// one barrier per step.
+// resident CTAs per SM the register budget is sized for: 3 for float (79
+// registers), 2 for the 8- and 16-byte elements (their 4 x 4 accumulators)
+template <typename T> constexpr int tr_min_blocks() { return sizeof(T) == 4 ? 3 : 2; }
+
 template <typename T>
-__global__ void __launch_bounds__(kTrThreads) tr_gemm_kernel(const tr_gemm_args<T> a) {
+__global__ void __launch_bounds__(kTrThreads, tr_min_blocks<T>()) tr_gemm_kernel(const tr_gemm_args<T> a) {
+    constexpr int BK = tr_tile_k<T>();
+    constexpr int U = kTrTile * BK / kTrThreads;   // elements of each operand a thread stages per step
     const int64_t bi = blockIdx.y, bj = blockIdx.x;
     if (a.upper && bi > bj) return;
-    __shared__ T sL[kTrTileK][kTrTile + 1];
-    __shared__ T sR[kTrTileK][kTrTile + 1];
+    // rows padded by 4 elements: a thread's 4 consecutive entries start on a
+    // 16-byte boundary and are read with 16-byte shared loads
+    __shared__ __align__(16) T sL[2][BK][kTrTile + 4];
+    __shared__ __align__(16) T sR[2][BK][kTrTile + 4];
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     const int64_t i0 = bi * kTrTile, j0 = bj * kTrTile;
     const int64_t kbeg = (int64_t)blockIdx.z * a.kchunk;
@@ -168,53 +185,71 @@ __global__ void __launch_bounds__(kTrThreads) tr_gemm_kernel(const tr_gemm_args<
 #pragma unroll
         for (int y = 0; y < 4; y++) acc[x][y] = tr_zero<T>();
 
-    for (int64_t k0 = kbeg; k0 < kend; k0 += kTrTileK) {
+    T rl[U], rr[U];
+    auto fetch = [&](int64_t k0) {
 #pragma unroll
-        for (int u = 0; u < (kTrTile * kTrTileK) / kTrThreads; u++) {
+        for (int u = 0; u < U; u++) {
             const int e = tid + u * kTrThreads;
-            int kk = l_kfast ? (e & (kTrTileK - 1)) : (e / kTrTile);
-            const int ii = l_kfast ? (e / kTrTileK) : (e & (kTrTile - 1));
+            int kk = l_kfast ? (e % BK) : (e / kTrTile);
+            const int ii = l_kfast ? (e / BK) : (e % kTrTile);
             int64_t k = k0 + kk;
             T v = tr_zero<T>();
             if (i0 + ii < a.M && k < kend) {
                 v = a.L[(i0 + ii) * a.li + k * a.lk];
                 if (a.conj_l) v = tr_conj(v);
             }
-            sL[kk][ii] = v;
-            kk = r_kfast ? (e & (kTrTileK - 1)) : (e / kTrTile);
-            const int jj = r_kfast ? (e / kTrTileK) : (e & (kTrTile - 1));
+            rl[u] = v;
+            kk = r_kfast ? (e % BK) : (e / kTrTile);
+            const int jj = r_kfast ? (e / BK) : (e % kTrTile);
             k = k0 + kk;
             T w = tr_zero<T>();
             if (j0 + jj < a.N && k < kend) {
                 w = a.R[k * a.rk + (j0 + jj) * a.rj];
                 if (a.conj_r) w = tr_conj(w);
             }
-            sR[kk][jj] = w;
+            rr[u] = w;
         }
-        __syncthreads();
+    };
+    auto stage = [&](int buf) {
 #pragma unroll
-        for (int kk = 0; kk < kTrTileK; kk++) {
-            T l[4], r[4];
+        for (int u = 0; u < U; u++) {
+            const int e = tid + u * kTrThreads;
+            sL[buf][l_kfast ? (e % BK) : (e / kTrTile)][l_kfast ? (e / BK) : (e % kTrTile)] = rl[u];
+            sR[buf][r_kfast ? (e % BK) : (e / kTrTile)][r_kfast ? (e / BK) : (e % kTrTile)] = rr[u];
+        }
+    };
+
+    if (kbeg < kend) {
+        fetch(kbeg);
+        stage(0);
+    }
+    __syncthreads();
+    int buf = 0;
+    for (int64_t k0 = kbeg; k0 < kend; k0 += BK) {
+        const bool more = k0 + BK < kend;
+        if (more) fetch(k0 + BK);       // in flight while this step computes
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                l[q] = sL[kk][ty + 16 * q];
-                r[q] = sR[kk][tx + 16 * q];
-            }
+        for (int kk = 0; kk < BK; kk++) {
+            const tr_quad<T> l = *reinterpret_cast<const tr_quad<T> *>(&sL[buf][kk][4 * ty]);
+            const tr_quad<T> r = *reinterpret_cast<const tr_quad<T> *>(&sR[buf][kk][4 * tx]);
 #pragma unroll
             for (int x = 0; x < 4; x++)
 #pragma unroll
-                for (int y = 0; y < 4; y++) tr_mac(acc[x][y], l[x], r[y]);
+                for (int y = 0; y < 4; y++) tr_mac(acc[x][y], l.v[x], r.v[y]);
         }
+        // the other stage was last read before the previous barrier
+        if (more) stage(buf ^ 1);
         __syncthreads();
+        buf ^= 1;
     }
     T *C = a.C + (int64_t)blockIdx.z * a.zstride;
 #pragma unroll
     for (int x = 0; x < 4; x++) {
-        const int64_t i = i0 + ty + 16 * x;
+        const int64_t i = i0 + 4 * ty + x;
         if (i >= a.M) continue;
 #pragma unroll
         for (int y = 0; y < 4; y++) {
-            const int64_t j = j0 + tx + 16 * y;
+            const int64_t j = j0 + 4 * tx + y;
             if (j >= a.N) continue;
             T v = acc[x][y];
             if (a.base) v = tr_axpy(a.base[i * a.ci + j * a.cj], a.sign, v);
@@ -224,19 +259,36 @@ __global__ void __launch_bounds__(kTrThreads) tr_gemm_kernel(const tr_gemm_args<
 }
 
 // G (column-major, p x p, both triangles) = scale * sum over the splits of
-// the row-major partials, added in split order in double.  Only i <= j is
-// read: every upper-triangle element lies in a computed tile.
+// the row-major partials, in double and in a fixed order: a CTA takes 32
+// consecutive elements, warp w adds splits w, w+8, ..., and the eight warp
+// sums are added in warp order.  Only i <= j is read: every upper-triangle
+// element lies in a computed tile.
+constexpr int kReduceWarps = 8;
+
 template <typename T>
-__global__ void tr_gram_reduce_kernel(const T *__restrict__ part, int splits, int64_t p, double scale,
-                                      T *__restrict__ G) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= p * p) return;
+__global__ void __launch_bounds__(32 * kReduceWarps) tr_gram_reduce_kernel(const T *__restrict__ part, int splits,
+                                                                          int64_t p, double scale,
+                                                                          T *__restrict__ G) {
+    using acc_t = typename tr_elem<T>::acc;
+    __shared__ acc_t red[kReduceWarps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t e = (int64_t)blockIdx.x * 32 + lane;
     const int64_t i = e / p, j = e - i * p;
-    if (i > j) return;
-    typename tr_elem<T>::acc s = tr_acc_zero<T>();
-    for (int z = 0; z < splits; z++) tr_acc_add(s, part[(int64_t)z * p * p + e]);
+    const bool use = e < p * p && i <= j;
+    acc_t s = tr_acc_zero<T>();
+    if (use) {
+        const int64_t pp = p * p;
+#pragma unroll 4
+        for (int z = w; z < splits; z += kReduceWarps) tr_acc_add(s, part[(int64_t)z * pp + e]);
+    }
+    red[w][lane] = s;
+    __syncthreads();
+    if (w != 0 || !use) return;
+    acc_t t = red[0][lane];
+#pragma unroll
+    for (int k = 1; k < kReduceWarps; k++) tr_acc_add(t, red[k][lane]);
     T v;
-    tr_store(v, s, scale);
+    tr_store(v, t, scale);
     G[i + j * p] = v;
     G[j + i * p] = tr_conj(v);
 }
@@ -254,40 +306,114 @@ __global__ void tr_gather_basis_kernel(const T *__restrict__ V, int64_t p, int r
     U[e] = V[i + col * p];
 }
 
-// One pass over A for bases of up to RMAX vectors: a thread owns column j,
-// forms w = U^H a_j in registers, then writes U w (or a_j - U w).  The basis
-// sits in shared memory and is read as a broadcast.  out may alias x: a
-// column is read in full before it is written.
+// One pass over A for bases of up to RMAX vectors.  A CTA takes 32
+// consecutive columns (one per lane, so every row read is one coalesced
+// segment) and splits the rows among its warps: warp g forms its partial
+// U^H a_j over its block of rows, the partials meet in shared memory and each
+// warp adds them in group order (the same order in every warp, so every warp
+// holds the same w), then writes U w (or a_j - U w) over its rows.  The basis
+// sits in shared memory and is read as a broadcast.  Rows are read in
+// batches of kProjBatch so that several loads are in flight per thread.
+// out may alias x: each element is read before it is written, by the thread
+// that writes it, and all reads of phase 1 end at the barrier.
+constexpr int kProjBatch = 8;
+constexpr int kProjMaxGroups = 8;
+constexpr size_t kSmallBasisSmem = 48 * 1024;   // dynamic shared memory without an opt-in
+
 template <typename T, int RMAX>
-__global__ void __launch_bounds__(256) tr_project_small_kernel(const T *x, int64_t sp, int64_t sq, int64_t p,
-                                                               int64_t q, const T *__restrict__ U, int r,
-                                                               int subtract, T *out) {
-    extern __shared__ unsigned char tr_smem[];
-    T *sU = reinterpret_cast<T *>(tr_smem);
+__global__ void __launch_bounds__(32 * kProjMaxGroups) tr_project_small_kernel(
+    const T *x, int64_t sp, int64_t sq, int64_t p, int64_t q, const T *__restrict__ U, int r, int subtract,
+    T *out) {
+    extern __shared__ __align__(16) unsigned char tr_smem[];
+    T *sU = reinterpret_cast<T *>(tr_smem);      // p x r
+    T *red = sU + p * r;                          // [groups][r][32]
+    const int groups = blockDim.x >> 5, g = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int64_t e = threadIdx.x; e < p * r; e += blockDim.x) sU[e] = U[e];
     __syncthreads();
-    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= q) return;
+    const int64_t j = (int64_t)blockIdx.x * 32 + lane;
+    const bool ok = j < q;
+    const int64_t rows = (p + groups - 1) / groups;
+    const int64_t l0 = min(p, g * rows), l1 = min(p, l0 + rows);
+    const T *col = x + (ok ? j : 0) * sq;
     T w[RMAX];
 #pragma unroll
     for (int t = 0; t < RMAX; t++) w[t] = tr_zero<T>();
-    const T *col = x + j * sq;
-    for (int64_t l = 0; l < p; l++) {
-        const T v = col[l * sp];
-        const T *u = sU + l * r;
+    if (ok) {
+        int64_t l = l0;
+        for (; l + kProjBatch <= l1; l += kProjBatch) {
+            T v[kProjBatch];
 #pragma unroll
-        for (int t = 0; t < RMAX; t++)
-            if (t < r) tr_mac(w[t], tr_conj(u[t]), v);
+            for (int b = 0; b < kProjBatch; b++) v[b] = col[(l + b) * sp];
+#pragma unroll
+            for (int b = 0; b < kProjBatch; b++) {
+                const T *u = sU + (l + b) * r;
+#pragma unroll
+                for (int t = 0; t < RMAX; t++)
+                    if (t < r) tr_mac(w[t], tr_conj(u[t]), v[b]);
+            }
+        }
+        for (; l < l1; l++) {
+            const T v = col[l * sp];
+            const T *u = sU + l * r;
+#pragma unroll
+            for (int t = 0; t < RMAX; t++)
+                if (t < r) tr_mac(w[t], tr_conj(u[t]), v);
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < RMAX; t++)
+        if (t < r) red[((int64_t)g * r + t) * 32 + lane] = w[t];
+    __syncthreads();
+    if (!ok) return;
+    const typename tr_elem<T>::real one = 1;
+#pragma unroll
+    for (int t = 0; t < RMAX; t++) {
+        if (t >= r) continue;
+        T s = red[(int64_t)t * 32 + lane];
+        for (int k = 1; k < groups; k++) s = tr_axpy(s, one, red[((int64_t)k * r + t) * 32 + lane]);
+        w[t] = s;
     }
     T *oc = out + j * sq;
-    for (int64_t l = 0; l < p; l++) {
+    const typename tr_elem<T>::real minus = -1;
+    int64_t l = l0;
+    for (; l + kProjBatch <= l1; l += kProjBatch) {
+        T v[kProjBatch];
+        if (subtract) {
+#pragma unroll
+            for (int b = 0; b < kProjBatch; b++) v[b] = col[(l + b) * sp];
+        }
+#pragma unroll
+        for (int b = 0; b < kProjBatch; b++) {
+            const T *u = sU + (l + b) * r;
+            T s = tr_zero<T>();
+#pragma unroll
+            for (int t = 0; t < RMAX; t++)
+                if (t < r) tr_mac(s, u[t], w[t]);
+            oc[(l + b) * sp] = subtract ? tr_axpy(v[b], minus, s) : s;
+        }
+    }
+    for (; l < l1; l++) {
         const T *u = sU + l * r;
         T s = tr_zero<T>();
 #pragma unroll
         for (int t = 0; t < RMAX; t++)
             if (t < r) tr_mac(s, u[t], w[t]);
-        oc[l * sp] = subtract ? tr_axpy(col[l * sp], (typename tr_elem<T>::real)-1, s) : s;
+        oc[l * sp] = subtract ? tr_axpy(col[l * sp], minus, s) : s;
     }
+}
+
+// Row groups (warps) per CTA of the one-pass projection: at least 32 rows
+// per warp (fewer leaves each warp too little work for the basis load and
+// the barrier), at most 8, and shared memory (basis + partials) within the
+// static limit; 0 when even one group does not fit.
+template <typename T>
+int small_groups(int64_t p, int r) {
+    if (r > 32) return 0;
+    int g = 1;
+    while (g < kProjMaxGroups && (int64_t)(2 * g) * 32 <= p) g *= 2;
+    for (; g >= 1; g /= 2)
+        if ((size_t)(p * r + (int64_t)g * r * 32) * sizeof(T) <= kSmallBasisSmem) return g;
+    return 0;
 }
 
 // ------------------------------------------------------------- cuSOLVER
@@ -362,16 +488,16 @@ ffdas_error_t get_solver(ffdas_context &ctx, solver_state **out) {
 
 // ------------------------------------------------------------------ driver
 
-constexpr size_t kSmallBasisSmem = 48 * 1024;
 constexpr size_t kGramPartialBytes = size_t(256) << 20;
 
 template <typename T, int RMAX>
 ffdas_error_t launch_small(ffdas_context &h, const T *x, int64_t sp, int64_t sq, int64_t p, int64_t q, const T *U,
-                           int r, int subtract, T *out) {
-    const int64_t blocks = (q + 255) / 256;
+                           int r, int groups, int subtract, T *out) {
+    const int64_t blocks = (q + 31) / 32;
     if (blocks > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
-    tr_project_small_kernel<T, RMAX><<<(unsigned)blocks, 256, (size_t)p * r * sizeof(T), h.stream>>>(
-        x, sp, sq, p, q, U, r, subtract, out);
+    const size_t smem = (size_t)(p * r + (int64_t)groups * r * 32) * sizeof(T);
+    tr_project_small_kernel<T, RMAX><<<(unsigned)blocks, 32 * groups, smem, h.stream>>>(x, sp, sq, p, q, U, r,
+                                                                                       subtract, out);
     return ffdas_launch_check(h.stream);
 }
 
@@ -403,7 +529,10 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
     // 1. Gram matrix, upper tiles, split over q
     const int64_t tiles = (p + kTrTile - 1) / kTrTile;
     const int64_t tri = tiles * (tiles + 1) / 2;
-    int64_t splits = (4 * (int64_t)h.sm_count + tri - 1) / tri;
+    // one wave: as many CTAs as the SMs hold at this kernel's occupancy
+    int per_sm = 0;
+    FFDAS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tr_gemm_kernel<T>, kTrThreads, 0));
+    int64_t splits = std::max<int64_t>(1, (int64_t)std::max(per_sm, 1) * h.sm_count / tri);
     splits = std::max<int64_t>(1, std::min<int64_t>(splits, (q + kTrTileK - 1) / kTrTileK));
     splits = std::max<int64_t>(1, std::min<int64_t>(splits, (int64_t)(kGramPartialBytes / ((size_t)p * p * sizeof(T)))));
     splits = std::min<int64_t>(splits, 65535);
@@ -424,9 +553,10 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
     g.M = p; g.N = p; g.K = q; g.kchunk = kchunk; g.upper = 1; g.sign = 1;
     FFDAS_TRY(launch_gemm(h, g, (int)splits));
     {
-        const int64_t blocks = (p * p + 255) / 256;
-        tr_gram_reduce_kernel<T><<<(unsigned)blocks, 256, 0, h.stream>>>(part.get<T>(), (int)splits, p,
-                                                                         1.0 / (double)q, gram.get<T>());
+        const int64_t blocks = (p * p + 31) / 32;
+        if (blocks > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
+        tr_gram_reduce_kernel<T><<<(unsigned)blocks, 32 * kReduceWarps, 0, h.stream>>>(
+            part.get<T>(), (int)splits, p, 1.0 / (double)q, gram.get<T>());
         FFDAS_TRY(ffdas_launch_check(h.stream));
     }
 
@@ -467,12 +597,13 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
         FFDAS_TRY(ffdas_launch_check(h.stream));
     }
     const int subtract = direct ? 0 : 1;
-    if (r <= 32 && (size_t)(p * r) * sizeof(T) <= kSmallBasisSmem) {
+    const int groups = small_groups<T>(p, r);
+    if (groups > 0) {
         const T *U = basis.get<T>();
-        if (r <= 4) FFDAS_TRY((launch_small<T, 4>(h, x, sp, sq, p, q, U, r, subtract, out)));
-        else if (r <= 8) FFDAS_TRY((launch_small<T, 8>(h, x, sp, sq, p, q, U, r, subtract, out)));
-        else if (r <= 16) FFDAS_TRY((launch_small<T, 16>(h, x, sp, sq, p, q, U, r, subtract, out)));
-        else FFDAS_TRY((launch_small<T, 32>(h, x, sp, sq, p, q, U, r, subtract, out)));
+        if (r <= 4) FFDAS_TRY((launch_small<T, 4>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
+        else if (r <= 8) FFDAS_TRY((launch_small<T, 8>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
+        else if (r <= 16) FFDAS_TRY((launch_small<T, 16>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
+        else FFDAS_TRY((launch_small<T, 32>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
     } else {
         workspace wbuf(h);
         FFDAS_TRY(wbuf.alloc((size_t)r * (size_t)q * sizeof(T)));
