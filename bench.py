@@ -623,25 +623,6 @@ def config_extras(args, impl: str) -> dict:
     return {"configs": out}
 
 
-def slow_time_ensemble(m: int, shape: tuple, dtype: torch.dtype, dev, seed: int) -> torch.Tensor:
-    """Seeded beamformed ensemble (m frames of `shape` voxels): 5 'tissue'
-    components, each 4x weaker than the previous, plus weak full-rank 'blood'."""
-    g = torch.Generator().manual_seed(seed)
-    n = int(np.prod(shape))
-    cplx = dtype.is_complex
-    rdt = torch.float64
-
-    def draw(*sz):
-        a = torch.randn(*sz, generator=g, dtype=rdt)
-        return torch.complex(a, torch.randn(*sz, generator=g, dtype=rdt)) if cplx else a
-
-    u = torch.linalg.qr(draw(m, 5))[0].to(dev)
-    v = (draw(n, 5) / np.sqrt(n)).to(dev)
-    s = (10.0 * np.sqrt(n)) * 4.0 ** -torch.arange(5, dtype=rdt, device=dev)
-    x = (u * s) @ v.conj().T + 1e-2 * draw(m, n).to(dev)
-    return x.to(dtype).reshape(m, *shape).contiguous()
-
-
 def rank_filter_extra(args, impl: str, dev, stream) -> dict:
     """The clutter filter that follows beamforming: truncate_rank with the 5
     leading (tissue) ranks removed, on a 200-frame 400x256 FP32 image
@@ -650,11 +631,12 @@ def rank_filter_extra(args, impl: str, dev, stream) -> dict:
     ffdas_truncate_rank; reference: its ffdas_truncate_rank built from its
     sources (cuBLAS GEMM, cuSOLVER syevd, SYRK + SYMM).  Both calls return
     with the stream drained (the solver status is read on the host)."""
+    from ffdas_b200 import workloads as W
     out = {}
     steps, warm = max(args.steps, 5), args.warmup
     for name, (m, shape, dtype, seed) in {"ensemble_f32": (200, (400, 256), torch.float32, 51),
                                           "volume_c64": (64, (64, 64, 64), torch.complex64, 52)}.items():
-        x = slow_time_ensemble(m, shape, dtype, dev, seed)
+        x = W.slow_time_ensemble(m, shape, dtype, dev, seed)
         if impl == "reference":
             from oracle import reference
             if not reference.available():

@@ -8,6 +8,11 @@ schedule to the device's library handle, calls das / das_sparse `--calls`
 times (the first calls warm the kernel attributes and the memory pool), and
 prints the last call's kernel info.  `--backward` runs ffdas_das_backward
 instead (random output gradient).
+
+    python -m ffdas_b200.profile_call rank_filter --calls 3
+
+runs truncate_rank(x, 5) on the seeded 200-frame 400x256 FP32 slow-time
+ensemble (workloads.slow_time_ensemble) instead.
 """
 from __future__ import annotations
 
@@ -23,7 +28,7 @@ from .library import get_library_handle
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=sorted(W.CONFIGS))
+    ap.add_argument("workload", choices=sorted(W.CONFIGS) + ["rank_filter"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--frames", type=int, default=None, help="ensemble: number of frames")
     ap.add_argument("--calls", type=int, default=4)
@@ -31,6 +36,14 @@ def main() -> int:
     ap.add_argument("--backward", action="store_true")
     args = ap.parse_args()
     dev = torch.device("cuda", torch.cuda.current_device())
+    if args.workload == "rank_filter":
+        from .truncate_rank import truncate_rank
+        x = W.slow_time_ensemble(args.frames or 200, (400, 256), torch.float32, dev)
+        for _ in range(args.calls):
+            y = truncate_rank(x, 5)
+        torch.cuda.synchronize()
+        print(json.dumps({"rank_filter": list(x.shape), "max_abs_out": float(y.abs().max())}))
+        return 0
     kw = {"frames": args.frames} if args.frames is not None else {}
     wl = W.CONFIGS[args.workload](device=dev, scale=args.scale, **kw)
     h = get_library_handle(dev)

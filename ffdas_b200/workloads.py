@@ -268,6 +268,30 @@ def _to(d: dict, device, **meta) -> dict:
     return out
 
 
+def slow_time_ensemble(m: int, shape: tuple, dtype=torch.float32, device="cpu", seed: int = 51,
+                       tissue: int = 5) -> torch.Tensor:
+    """Seeded beamformed ensemble for the clutter filter (truncate_rank): m
+    frames of `shape` voxels, `tissue` low-rank components each 4x weaker than
+    the previous, plus weak full-rank 'blood' (1e-2).  Complex dtypes draw
+    complex components (IQ images)."""
+    g = torch.Generator().manual_seed(seed)
+    n = 1
+    for d in shape:
+        n *= int(d)
+    cplx = dtype.is_complex
+    rdt = torch.float64
+
+    def draw(*sz):
+        a = torch.randn(*sz, generator=g, dtype=rdt)
+        return torch.complex(a, torch.randn(*sz, generator=g, dtype=rdt)) if cplx else a
+
+    u = torch.linalg.qr(draw(m, tissue))[0].to(device)
+    v = (draw(n, tissue) / math.sqrt(n)).to(device)
+    s = (10.0 * math.sqrt(n)) * 4.0 ** -torch.arange(tissue, dtype=rdt, device=device)
+    x = (u * s) @ v.conj().T + 1e-2 * draw(m, n).to(device)
+    return x.to(dtype).reshape(m, *shape).contiguous()
+
+
 CONFIGS = {
     "plane2d": plane2d,
     "diverging3d": diverging3d,
