@@ -17,10 +17,11 @@
 //     a fixed order in double.  The sum is therefore the same on every run.
 //     It is written as the column-major Hermitian matrix that the solver
 //     takes.  The reference forms the full product with one cuBLAS GEMM.
-//  2. Eigendecomposition of G with cuSOLVER's syevd, as the reference does.
-//     The library is loaded on first use, so the delay-and-sum path never
-//     depends on it.  Eigenvalues come back ascending, so singular rank s is
-//     eigenvector p-1-s.
+//  2. Eigendecomposition of G with cuSOLVER's syevd, as the reference does,
+//     or, when the basis of step 3 is one contiguous run of eigenvectors,
+//     syevdx over that index range only.  The library is loaded on first
+//     use, so the delay-and-sum path never depends on it.  Eigenvalues come
+//     back ascending, so singular rank s is eigenvector p-1-s.
 //  3. Projection with the smaller basis.  With k = stop-start kept vectors
 //     and c = p-k removed ones, out = U_k (U_k^H A) when k <= c, else
 //     out = A - U_c (U_c^H A).  Both are exact for an orthonormal
@@ -426,6 +427,8 @@ struct solver_api {
     decltype(&cusolverDnDestroyParams) destroy_params = nullptr;
     decltype(&cusolverDnXsyevd_bufferSize) buffer_size = nullptr;
     decltype(&cusolverDnXsyevd) syevd = nullptr;
+    decltype(&cusolverDnXsyevdx_bufferSize) buffer_size_x = nullptr;   // optional
+    decltype(&cusolverDnXsyevdx) syevdx = nullptr;                     // optional
     bool ok = false;
 };
 
@@ -442,6 +445,9 @@ const solver_api &solver() {
         s.destroy_params = reinterpret_cast<decltype(s.destroy_params)>(dlsym(lib, "cusolverDnDestroyParams"));
         s.buffer_size = reinterpret_cast<decltype(s.buffer_size)>(dlsym(lib, "cusolverDnXsyevd_bufferSize"));
         s.syevd = reinterpret_cast<decltype(s.syevd)>(dlsym(lib, "cusolverDnXsyevd"));
+        s.buffer_size_x = reinterpret_cast<decltype(s.buffer_size_x)>(dlsym(lib, "cusolverDnXsyevdx_bufferSize"));
+        s.syevdx = reinterpret_cast<decltype(s.syevdx)>(dlsym(lib, "cusolverDnXsyevdx"));
+        if (!s.buffer_size_x || !s.syevdx) s.buffer_size_x = nullptr, s.syevdx = nullptr;
         s.ok = s.create && s.destroy && s.set_stream && s.create_params && s.destroy_params && s.buffer_size &&
                s.syevd;
         return s;
@@ -560,12 +566,39 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
         FFDAS_TRY(ffdas_launch_check(h.stream));
     }
 
+    // 3's basis, chosen first: the smaller of the kept and the removed sets;
+    // eigenvector e = p-1-rank
+    const bool direct = keep <= drop;
+    const int r = (int)(direct ? keep : drop);
+    int64_t e0 = direct ? p - stop : 0;
+    int r0 = (int)(direct ? keep : p - stop);
+    const int64_t e1 = p - start;
+    // When the basis is one contiguous run of eigenvectors (always for the
+    // kept set; for the removed set when start = 0 or stop = p, as in the
+    // clutter filter), only those r are computed (syevdx, index range): the
+    // back-transform then handles r vectors instead of p.  They come back in
+    // columns 0..r-1.
+    int64_t lo = -1;
+    if (direct) lo = p - stop;
+    else if (stop == p) lo = p - start;
+    else if (start == 0) lo = 0;
+    const bool ranged = lo >= 0 && solver().syevdx != nullptr;
+
     // 2. eigendecomposition (truncate_rank_impl.cuh:481-500, 68-90)
     size_t dev_bytes = 0, host_bytes = 0;
-    if (solver().buffer_size(sv->h, sv->params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, p,
-                             tr_elem<T>::cuda, gram.get<T>(), p, tr_elem<T>::cuda_real, eig.get<real>(),
-                             tr_elem<T>::cuda, &dev_bytes, &host_bytes) != CUSOLVER_STATUS_SUCCESS)
-        return FFDAS_ERROR_CUSOLVER;
+    real vl = 0, vu = 0;
+    int64_t found = 0;
+    cusolverStatus_t st;
+    if (ranged)
+        st = solver().buffer_size_x(sv->h, sv->params, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I,
+                                    CUBLAS_FILL_MODE_UPPER, p, tr_elem<T>::cuda, gram.get<T>(), p, &vl, &vu, lo + 1,
+                                    lo + r, &found, tr_elem<T>::cuda_real, eig.get<real>(), tr_elem<T>::cuda,
+                                    &dev_bytes, &host_bytes);
+    else
+        st = solver().buffer_size(sv->h, sv->params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, p,
+                                  tr_elem<T>::cuda, gram.get<T>(), p, tr_elem<T>::cuda_real, eig.get<real>(),
+                                  tr_elem<T>::cuda, &dev_bytes, &host_bytes);
+    if (st != CUSOLVER_STATUS_SUCCESS) return FFDAS_ERROR_CUSOLVER;
     // The reference allocates p times the reported device workspace (its
     // note: the size is underestimated on some architectures); the same
     // margin here, bounded for large p.
@@ -576,18 +609,23 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
     workspace sdev(h);
     FFDAS_TRY(sdev.alloc(dev_alloc));
     std::vector<unsigned char> shost(std::max<size_t>(host_bytes, 1));
-    if (solver().syevd(sv->h, sv->params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, p, tr_elem<T>::cuda,
-                       gram.get<T>(), p, tr_elem<T>::cuda_real, eig.get<real>(), tr_elem<T>::cuda,
-                       sdev.get<void>(), dev_bytes, shost.data(), host_bytes,
-                       info.get<int>()) != CUSOLVER_STATUS_SUCCESS)
-        return FFDAS_ERROR_CUSOLVER;
+    if (ranged)
+        st = solver().syevdx(sv->h, sv->params, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I,
+                             CUBLAS_FILL_MODE_UPPER, p, tr_elem<T>::cuda, gram.get<T>(), p, &vl, &vu, lo + 1, lo + r,
+                             &found, tr_elem<T>::cuda_real, eig.get<real>(), tr_elem<T>::cuda, sdev.get<void>(),
+                             dev_bytes, shost.data(), host_bytes, info.get<int>());
+    else
+        st = solver().syevd(sv->h, sv->params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, p,
+                            tr_elem<T>::cuda, gram.get<T>(), p, tr_elem<T>::cuda_real, eig.get<real>(),
+                            tr_elem<T>::cuda, sdev.get<void>(), dev_bytes, shost.data(), host_bytes,
+                            info.get<int>());
+    if (st != CUSOLVER_STATUS_SUCCESS) return FFDAS_ERROR_CUSOLVER;
+    if (ranged) {
+        e0 = 0;           // the r vectors sit in columns 0..r-1
+        r0 = r;
+    }
 
-    // 3. projection with the smaller basis; eigenvector e = p-1-rank
-    const bool direct = keep <= drop;
-    const int r = (int)(direct ? keep : drop);
-    const int64_t e0 = direct ? p - stop : 0;
-    const int r0 = (int)(direct ? keep : p - stop);
-    const int64_t e1 = p - start;
+    // 3. projection
     workspace basis(h);
     FFDAS_TRY(basis.alloc((size_t)(p * r) * sizeof(T)));
     {
@@ -627,6 +665,7 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
     int h_info = 0;
     FFDAS_CUDA(cudaMemcpyAsync(&h_info, info.get<int>(), sizeof(int), cudaMemcpyDeviceToHost, h.stream));
     FFDAS_CUDA(cudaStreamSynchronize(h.stream));
+    if (ranged && found != r) return FFDAS_ERROR_CUSOLVER;
     return h_info == 0 ? FFDAS_SUCCESS : FFDAS_ERROR_CUSOLVER;
 }
 
