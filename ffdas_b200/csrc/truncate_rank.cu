@@ -17,9 +17,16 @@
 //     a fixed order in double.  The sum is therefore the same on every run.
 //     It is written as the column-major Hermitian matrix that the solver
 //     takes.  The reference forms the full product with one cuBLAS GEMM.
-//  2. Eigendecomposition of G with cuSOLVER's syevd, as the reference does,
-//     or, when the basis of step 3 is one contiguous run of eigenvectors,
-//     syevdx over that index range only.  The library is loaded on first
+//  2. The basis of step 3.  When it is the leading subspace (the clutter
+//     filter: remove ranks 0..start-1; or keep ranks 0..stop-1) and has at
+//     most 16 vectors, an orthogonal iteration in double on the device
+//     (G Q, Cholesky QR twice) runs first and is accepted at a backward-
+//     stable residual ||G Q - Q H|| <= 2 eps(FP32) max H_aa (45 eps for
+//     FP64): the subspace is then as accurate as a dense solver's for this G.
+//     Otherwise, or if it has not converged after 30 steps, the
+//     eigendecomposition of G runs in cuSOLVER's syevd, as in the reference,
+//     or syevdx over one index range when the basis is one contiguous run of
+//     eigenvectors.  The library is loaded on first
 //     use, so the delay-and-sum path never depends on it.  Eigenvalues come
 //     back ascending, so singular rank s is eigenvector p-1-s.
 //  3. Projection with the smaller basis.  With k = stop-start kept vectors
@@ -417,6 +424,191 @@ int small_groups(int64_t p, int r) {
     return 0;
 }
 
+// ------------------------------------------------- leading subspace (fast)
+
+// Double-precision helpers for the subspace iteration (real: double,
+// complex: double2).
+__device__ __forceinline__ double oi_conj(double a) { return a; }
+__device__ __forceinline__ double2 oi_conj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double oi_mul(double a, double b) { return a * b; }
+__device__ __forceinline__ double2 oi_mul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double oi_add(double a, double b) { return a + b; }
+__device__ __forceinline__ double2 oi_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double oi_sub(double a, double b) { return a - b; }
+__device__ __forceinline__ double2 oi_sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double oi_scale(double a, double s) { return a * s; }
+__device__ __forceinline__ double2 oi_scale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double oi_abs2(double a) { return a * a; }
+__device__ __forceinline__ double oi_abs2(double2 a) { return a.x * a.x + a.y * a.y; }
+__device__ __forceinline__ double oi_re(double a) { return a; }
+__device__ __forceinline__ double oi_re(double2 a) { return a.x; }
+__device__ __forceinline__ double oi_shfl(double a, int o) { return __shfl_xor_sync(0xffffffffu, a, o); }
+__device__ __forceinline__ double2 oi_shfl(double2 a, int o) {
+    return make_double2(__shfl_xor_sync(0xffffffffu, a.x, o), __shfl_xor_sync(0xffffffffu, a.y, o));
+}
+__device__ __forceinline__ double oi_from(float a) { return a; }
+__device__ __forceinline__ double oi_from(double a) { return a; }
+__device__ __forceinline__ double2 oi_from(float2 a) { return make_double2(a.x, a.y); }
+__device__ __forceinline__ double2 oi_from(double2 a) { return a; }
+__device__ __forceinline__ void oi_to(float &o, double a) { o = (float)a; }
+__device__ __forceinline__ void oi_to(double &o, double a) { o = a; }
+__device__ __forceinline__ void oi_to(float2 &o, double2 a) { o = make_float2((float)a.x, (float)a.y); }
+__device__ __forceinline__ void oi_to(double2 &o, double2 a) { o = a; }
+template <typename A> __device__ __forceinline__ A oi_real(double v);
+template <> __device__ __forceinline__ double oi_real<double>(double v) { return v; }
+template <> __device__ __forceinline__ double2 oi_real<double2>(double v) { return make_double2(v, 0.0); }
+template <typename A> __device__ __forceinline__ A oi_zero();
+template <> __device__ __forceinline__ double oi_zero<double>() { return 0.0; }
+template <> __device__ __forceinline__ double2 oi_zero<double2>() { return make_double2(0.0, 0.0); }
+// deterministic start vectors in [-1, 1)
+__device__ __forceinline__ double oi_hash(uint32_t k) {
+    k ^= k >> 16; k *= 0x7feb352du; k ^= k >> 15; k *= 0x846ca68bu; k ^= k >> 16;
+    return (double)k * (2.0 / 4294967296.0) - 1.0;
+}
+__device__ __forceinline__ void oi_start(double &a, uint32_t k) { a = oi_hash(2 * k + 1); }
+__device__ __forceinline__ void oi_start(double2 &a, uint32_t k) { a = make_double2(oi_hash(2 * k + 1), oi_hash(2 * k + 2)); }
+
+constexpr int kOiThreads = 512;
+constexpr int kOiMaxRank = 16;
+constexpr int kOiMaxIter = 30;
+// residual bound relative to the largest Rayleigh quotient: 2 eps for FP32
+// data, about 45 eps for FP64 (the rounding floor of G Q in double)
+template <typename T> constexpr double oi_tol() { return sizeof(typename tr_elem<T>::real) == 4 ? 2.4e-7 : 1e-14; }
+
+// M[a][b] = sum_i conj(X[i][a]) Z[i][b], a, b < r (row-major p x r inputs):
+// one warp per entry, lanes over rows, shuffle sums.  Ends with a barrier.
+template <typename A>
+__device__ void oi_inner(const A *X, const A *Z, int p, int r, A *M) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int e = warp; e < r * r; e += nw) {
+        const int a = e / r, b = e - a * r;
+        A s = oi_zero<A>();
+        for (int i = lane; i < p; i += 32) s = oi_add(s, oi_mul(oi_conj(X[i * r + a]), Z[i * r + b]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s = oi_add(s, oi_shfl(s, o));
+        if (lane == 0) M[e] = s;
+    }
+    __syncthreads();
+}
+
+// Q <- an orthonormal basis of span(Y) (p x r, row-major): columns scaled to
+// unit norm, then Cholesky QR twice (the second pass restores orthogonality
+// to rounding).  Returns false (on every thread) if a pivot is not positive.
+template <typename A>
+__device__ bool oi_orthonormalize(A *Y, A *Q, int p, int r, A *C, int *flag) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    oi_inner(Y, Y, p, r, C);
+    for (int e = tid; e < p * r; e += nt) {
+        const int b = e % r;
+        const double n2 = oi_re(C[b * r + b]);
+        Q[e] = n2 > 0.0 ? oi_scale(Y[e], rsqrt(n2)) : Y[e];
+    }
+    __syncthreads();
+    for (int pass = 0; pass < 2; pass++) {
+        oi_inner(Q, Q, p, r, C);
+        if (tid == 0) {
+            // C = L L^H in place (lower triangle)
+            int ok = 1;
+            for (int j = 0; j < r && ok; j++) {
+                double d = oi_re(C[j * r + j]);
+                for (int k = 0; k < j; k++) d -= oi_abs2(C[j * r + k]);
+                if (!(d > 0.0)) { ok = 0; break; }
+                const double ljj = sqrt(d);
+                C[j * r + j] = oi_real<A>(ljj);
+                for (int i = j + 1; i < r; i++) {
+                    A v = C[i * r + j];
+                    for (int k = 0; k < j; k++) v = oi_sub(v, oi_mul(C[i * r + k], oi_conj(C[j * r + k])));
+                    C[i * r + j] = oi_scale(v, 1.0 / ljj);
+                }
+            }
+            *flag = ok;
+        }
+        __syncthreads();
+        if (!*flag) return false;
+        // row-wise: z L^H = q  ->  z_b = (q_b - sum_{a<b} z_a conj(L[b][a])) / L[b][b]
+        for (int i = tid; i < p; i += nt) {
+            A *row = Q + (int64_t)i * r;
+            for (int b = 0; b < r; b++) {
+                A v = row[b];
+                for (int a = 0; a < b; a++) v = oi_sub(v, oi_mul(row[a], oi_conj(C[b * r + a])));
+                row[b] = oi_scale(v, 1.0 / oi_re(C[b * r + b]));
+            }
+        }
+        __syncthreads();
+    }
+    return true;
+}
+
+// Orthogonal iteration for the leading r-dimensional invariant subspace of
+// the Hermitian p x p matrix G (column-major, both triangles), in double:
+// Y = G Q, H = Q^H Y, stop when ||Y - Q H||_F <= tol * max_a H[a][a] (a
+// backward-stable residual: the subspace is then as good as a dense
+// eigensolver's for this G), else Q = orth(Y).  On convergence the basis is
+// written as T (row-major p x r) and *status = 1; otherwise *status = 0 and
+// the caller runs the dense eigensolver.  One CTA; every loop is bounded.
+template <typename T>
+__global__ void __launch_bounds__(kOiThreads) tr_leading_subspace_kernel(const T *__restrict__ G, int p, int r,
+                                                                        int max_iter, double tol,
+                                                                        T *__restrict__ basis,
+                                                                        int *__restrict__ status) {
+    using A = typename tr_elem<T>::acc;
+    extern __shared__ __align__(16) unsigned char oi_smem[];
+    A *Q = reinterpret_cast<A *>(oi_smem);
+    A *Y = Q + p * r;
+    A *H = Y + p * r;
+    A *C = H + r * r;
+    double *red = reinterpret_cast<double *>(C + r * r);
+    __shared__ int s_flag;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (tid == 0) *status = 0;
+    for (int e = tid; e < p * r; e += nt) oi_start(Y[e], (uint32_t)e);
+    __syncthreads();
+    if (!oi_orthonormalize(Y, Q, p, r, C, &s_flag)) return;
+    for (int it = 0; it < max_iter; it++) {
+        // Y = G Q: consecutive threads take consecutive rows i (coalesced G reads)
+        for (int e = tid; e < p * r; e += nt) {
+            const int j = e / p, i = e - j * p;
+            A s = oi_zero<A>();
+            for (int l = 0; l < p; l++) s = oi_add(s, oi_mul(oi_from(G[i + (int64_t)l * p]), Q[l * r + j]));
+            Y[i * r + j] = s;
+        }
+        __syncthreads();
+        oi_inner(Q, Y, p, r, H);
+        // residual ||Y - Q H||_F^2
+        double part = 0.0;
+        for (int e = tid; e < p * r; e += nt) {
+            const int i = e / r, b = e - i * r;
+            A v = Y[e];
+            for (int a = 0; a < r; a++) v = oi_sub(v, oi_mul(Q[i * r + a], H[a * r + b]));
+            part += oi_abs2(v);
+        }
+        red[tid] = part;
+        __syncthreads();
+        for (int w = nt / 2; w > 0; w >>= 1) {
+            if (tid < w) red[tid] += red[tid + w];
+            __syncthreads();
+        }
+        double scale = 0.0;
+        for (int a = 0; a < r; a++) scale = fmax(scale, oi_re(H[a * r + a]));
+        const bool done = sqrt(red[0]) <= tol * scale;
+        __syncthreads();
+        if (done) {
+            for (int e = tid; e < p * r; e += nt) oi_to(basis[e], Q[e]);
+            if (tid == 0) *status = 1;
+            return;
+        }
+        if (!oi_orthonormalize(Y, Q, p, r, C, &s_flag)) return;
+    }
+}
+
+// shared memory of the subspace kernel: Q, Y (p x r), H, C (r x r), the reduction
+template <typename T>
+size_t oi_smem_bytes(int64_t p, int r) {
+    return (size_t)(2 * p * r + 2 * (int64_t)r * r) * sizeof(typename tr_elem<T>::acc) + kOiThreads * sizeof(double);
+}
+
 // ------------------------------------------------------------- cuSOLVER
 
 struct solver_api {
@@ -515,6 +707,40 @@ ffdas_error_t launch_gemm(ffdas_context &h, const tr_gemm_args<T> &a, int splits
     return ffdas_launch_check(h.stream);
 }
 
+// out = U (U^H A), or A - U (U^H A) when subtract: the one-pass kernel for
+// bases of up to 32 vectors, else two tiled products through a (r, q)
+// workspace.
+template <typename T>
+ffdas_error_t project(ffdas_context &h, const T *x, int64_t sp, int64_t sq, int64_t p, int64_t q, const T *U, int r,
+                      int subtract, T *out) {
+    using real = typename tr_elem<T>::real;
+    const int groups = small_groups<T>(p, r);
+    if (groups > 0) {
+        if (r <= 4) FFDAS_TRY((launch_small<T, 4>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
+        else if (r <= 8) FFDAS_TRY((launch_small<T, 8>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
+        else if (r <= 16) FFDAS_TRY((launch_small<T, 16>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
+        else FFDAS_TRY((launch_small<T, 32>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
+    } else {
+        workspace wbuf(h);
+        FFDAS_TRY(wbuf.alloc((size_t)r * (size_t)q * sizeof(T)));
+        tr_gemm_args<T> w{};          // W = U^H A  (r x q)
+        w.L = U; w.li = 1; w.lk = r; w.conj_l = 1;
+        w.R = x; w.rk = sp; w.rj = sq;
+        w.C = wbuf.get<T>(); w.ci = q; w.cj = 1;
+        w.M = r; w.N = q; w.K = p; w.kchunk = (p + kTrTileK - 1) / kTrTileK * kTrTileK; w.sign = 1;
+        FFDAS_TRY(launch_gemm(h, w, 1));
+        tr_gemm_args<T> o{};          // out = U W, or A - U W
+        o.L = U; o.li = r; o.lk = 1;
+        o.R = wbuf.get<T>(); o.rk = q; o.rj = 1;
+        o.C = out; o.ci = sp; o.cj = sq;
+        o.base = subtract ? x : nullptr; o.sign = subtract ? (real)-1 : (real)1;
+        o.M = p; o.N = q; o.K = r; o.kchunk = ((int64_t)r + kTrTileK - 1) / kTrTileK * kTrTileK;
+        FFDAS_TRY(launch_gemm(h, o, 1));
+    }
+
+    return FFDAS_SUCCESS;
+}
+
 template <typename T>
 ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x, T *out, int64_t start,
                               int64_t stop) {
@@ -550,7 +776,7 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
     FFDAS_TRY(part.alloc((size_t)(splits * p * p) * sizeof(T)));
     FFDAS_TRY(gram.alloc((size_t)(p * p) * sizeof(T)));
     FFDAS_TRY(eig.alloc((size_t)p * sizeof(real)));
-    FFDAS_TRY(info.alloc(sizeof(int)));
+    FFDAS_TRY(info.alloc(2 * sizeof(int)));   // solver status, subspace-iteration status
 
     tr_gemm_args<T> g{};
     g.L = x; g.li = sp; g.lk = sq;
@@ -583,6 +809,26 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
     else if (stop == p) lo = p - start;
     else if (start == 0) lo = 0;
     const bool ranged = lo >= 0 && solver().syevdx != nullptr;
+    workspace basis(h);
+    FFDAS_TRY(basis.alloc((size_t)(p * r) * sizeof(T)));
+
+    // 2a. the basis is the leading subspace (kept ranks 0..stop-1, or removed
+    // ranks 0..start-1 with stop = p: the clutter filter) and small: try the
+    // orthogonal iteration first; the dense solver runs only if it does not
+    // reach its residual bound
+    const bool leading = direct ? start == 0 : stop == p;
+    if (leading && r <= kOiMaxRank && oi_smem_bytes<T>(p, r) <= kSmallBasisSmem) {
+        tr_leading_subspace_kernel<T><<<1, kOiThreads, oi_smem_bytes<T>(p, r), h.stream>>>(
+            gram.get<T>(), (int)p, r, kOiMaxIter, oi_tol<T>(), basis.get<T>(), info.get<int>() + 1);
+        FFDAS_TRY(ffdas_launch_check(h.stream));
+        int converged = 0;
+        FFDAS_CUDA(cudaMemcpyAsync(&converged, info.get<int>() + 1, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+        FFDAS_CUDA(cudaStreamSynchronize(h.stream));
+        if (converged == 1) {
+            FFDAS_TRY(project(h, x, sp, sq, p, q, basis.get<T>(), r, direct ? 0 : 1, out));
+            return FFDAS_SUCCESS;
+        }
+    }
 
     // 2. eigendecomposition (truncate_rank_impl.cuh:481-500, 68-90)
     size_t dev_bytes = 0, host_bytes = 0;
@@ -626,39 +872,13 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
     }
 
     // 3. projection
-    workspace basis(h);
-    FFDAS_TRY(basis.alloc((size_t)(p * r) * sizeof(T)));
     {
         const int64_t blocks = (p * r + 255) / 256;
         tr_gather_basis_kernel<T><<<(unsigned)blocks, 256, 0, h.stream>>>(gram.get<T>(), p, r, e0, r0, e1,
                                                                           basis.get<T>());
         FFDAS_TRY(ffdas_launch_check(h.stream));
     }
-    const int subtract = direct ? 0 : 1;
-    const int groups = small_groups<T>(p, r);
-    if (groups > 0) {
-        const T *U = basis.get<T>();
-        if (r <= 4) FFDAS_TRY((launch_small<T, 4>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
-        else if (r <= 8) FFDAS_TRY((launch_small<T, 8>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
-        else if (r <= 16) FFDAS_TRY((launch_small<T, 16>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
-        else FFDAS_TRY((launch_small<T, 32>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
-    } else {
-        workspace wbuf(h);
-        FFDAS_TRY(wbuf.alloc((size_t)r * (size_t)q * sizeof(T)));
-        tr_gemm_args<T> w{};          // W = U^H A  (r x q)
-        w.L = basis.get<T>(); w.li = 1; w.lk = r; w.conj_l = 1;
-        w.R = x; w.rk = sp; w.rj = sq;
-        w.C = wbuf.get<T>(); w.ci = q; w.cj = 1;
-        w.M = r; w.N = q; w.K = p; w.kchunk = (p + kTrTileK - 1) / kTrTileK * kTrTileK; w.sign = 1;
-        FFDAS_TRY(launch_gemm(h, w, 1));
-        tr_gemm_args<T> o{};          // out = U W, or A - U W
-        o.L = basis.get<T>(); o.li = r; o.lk = 1;
-        o.R = wbuf.get<T>(); o.rk = q; o.rj = 1;
-        o.C = out; o.ci = sp; o.cj = sq;
-        o.base = subtract ? x : nullptr; o.sign = subtract ? (real)-1 : (real)1;
-        o.M = p; o.N = q; o.K = r; o.kchunk = ((int64_t)r + kTrTileK - 1) / kTrTileK * kTrTileK;
-        FFDAS_TRY(launch_gemm(h, o, 1));
-    }
+    FFDAS_TRY(project(h, x, sp, sq, p, q, basis.get<T>(), r, direct ? 0 : 1, out));
 
     // The solver's status, read once everything is queued (the reference
     // reads it before the projection, truncate_rank_impl.cuh:92-97).

@@ -347,9 +347,12 @@ FFDAS_API ffdas_error_t ffdas_sparse_select(
  * x and out: 2-D, same dims, C-contiguous (else FFDAS_ERROR_NON_CONTIGUOUS),
  * same dtype in {R_32F, C_32F, R_64F, C_64F}; 0 <= start < stop <=
  * min(m, n), else FFDAS_ERROR_INVALID_ARGUMENT.  out may be x.  The
- * eigensolver (cuSOLVER syevd, loaded at the first call) reports through
- * FFDAS_ERROR_CUSOLVER; the call waits for its status, so it returns with
- * the handle's stream drained, as the reference's does. */
+ * leading-subspace case (start = 0, or stop = min(m, n)) is first tried
+ * with an orthogonal iteration on the device; otherwise, or if that does
+ * not converge, cuSOLVER's syevd/syevdx (loaded at the first call) solves
+ * the eigenproblem and reports through FFDAS_ERROR_CUSOLVER.  The call
+ * waits on the host for the eigen step's status, so, like the reference's,
+ * it cannot be captured in a CUDA graph. */
 FFDAS_API ffdas_error_t ffdas_truncate_rank(
     ffdas_handle_t handle,
     ffdas_tensor_desc_t x_desc,
