@@ -137,7 +137,7 @@ __device__ __forceinline__ void tr_store(double2 &o, double2 v, double s) { o = 
 // ---------------------------------------------------------- tiled product
 
 constexpr int kTrTile = 64;       // C tile edge
-constexpr int kTrTileK = 16;      // host-side k granularity (a multiple of every tr_tile_k)
+constexpr int kTrTileK = 32;      // host-side k granularity (a multiple of every tr_tile_k)
 constexpr int kTrThreads = 256;   // 16 x 16 threads, 4 x 4 outputs each (rows 4 ty + a, columns 4 tx + b)
 
 template <typename T>
@@ -159,9 +159,49 @@ struct tr_gemm_args {
 // four consecutive elements, read from shared memory as 16-byte vectors
 template <typename T> struct __align__(16) tr_quad { T v[4]; };
 
-// k depth staged per step: 16, or 8 for 16-byte elements (two stages of both
-// operand tiles stay within the 48 KB of static shared memory)
-template <typename T> constexpr int tr_tile_k() { return sizeof(T) > 8 ? 8 : 16; }
+// A thread's 4 x 4 accumulators.  For float they are held as pairs, so
+// that a step of the tile is 8 packed FMAs (the same operations and
+// rounding as 16 scalar ones, half the issue slots).
+template <typename T> struct tr_accum {
+    T c[4][4];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+            for (int y = 0; y < 4; y++) c[x][y] = tr_zero<T>();
+    }
+    __device__ __forceinline__ void mac(const tr_quad<T> &l, const tr_quad<T> &r) {
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+            for (int y = 0; y < 4; y++) tr_mac(c[x][y], l.v[x], r.v[y]);
+    }
+    __device__ __forceinline__ T get(int x, int y) const { return c[x][y]; }
+};
+template <> struct tr_accum<float> {
+    float2 c[4][2];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int x = 0; x < 4; x++) c[x][0] = c[x][1] = make_float2(0.f, 0.f);
+    }
+    __device__ __forceinline__ void mac(const tr_quad<float> &l, const tr_quad<float> &r) {
+        const float2 r01 = make_float2(r.v[0], r.v[1]), r23 = make_float2(r.v[2], r.v[3]);
+#pragma unroll
+        for (int x = 0; x < 4; x++) {
+            const float2 lx = make_float2(l.v[x], l.v[x]);
+            c[x][0] = __ffma2_rn(lx, r01, c[x][0]);
+            c[x][1] = __ffma2_rn(lx, r23, c[x][1]);
+        }
+    }
+    __device__ __forceinline__ float get(int x, int y) const { return (y & 1) ? c[x][y >> 1].y : c[x][y >> 1].x; }
+};
+
+// k depth staged per step: 32 for float, 16 for 8-byte and 8 for 16-byte
+// elements (two stages of both operand tiles, 34 KB, within the 48 KB of
+// static shared memory).  The step is deep so that each CTA keeps several KB
+// of loads in flight: with 16 floats per step the FP32 Gram was bound by the
+// latency of its loads (0.33 ms at 1.6 TB/s from L2 for 200 x 102400).
+template <typename T> constexpr int tr_tile_k() { return sizeof(T) > 8 ? 8 : (sizeof(T) == 4 ? 32 : 16); }
 
 // C = op(L) op(R) over a 64 x 64 tile of C per CTA.  Each operand tile is
 // loaded with consecutive threads on its unit-stride index, so the loads
@@ -187,11 +227,8 @@ __global__ void __launch_bounds__(kTrThreads, tr_min_blocks<T>()) tr_gemm_kernel
     const int64_t kbeg = (int64_t)blockIdx.z * a.kchunk;
     const int64_t kend = min(a.K, kbeg + a.kchunk);
     const bool l_kfast = a.lk == 1, r_kfast = a.rk == 1;
-    T acc[4][4];
-#pragma unroll
-    for (int x = 0; x < 4; x++)
-#pragma unroll
-        for (int y = 0; y < 4; y++) acc[x][y] = tr_zero<T>();
+    tr_accum<T> acc;
+    acc.zero();
 
     T rl[U], rr[U];
     auto fetch = [&](int64_t k0) {
@@ -240,10 +277,7 @@ __global__ void __launch_bounds__(kTrThreads, tr_min_blocks<T>()) tr_gemm_kernel
         for (int kk = 0; kk < BK; kk++) {
             const tr_quad<T> l = *reinterpret_cast<const tr_quad<T> *>(&sL[buf][kk][4 * ty]);
             const tr_quad<T> r = *reinterpret_cast<const tr_quad<T> *>(&sR[buf][kk][4 * tx]);
-#pragma unroll
-            for (int x = 0; x < 4; x++)
-#pragma unroll
-                for (int y = 0; y < 4; y++) tr_mac(acc[x][y], l.v[x], r.v[y]);
+            acc.mac(l, r);
         }
         // the other stage was last read before the previous barrier
         if (more) stage(buf ^ 1);
@@ -259,7 +293,7 @@ __global__ void __launch_bounds__(kTrThreads, tr_min_blocks<T>()) tr_gemm_kernel
         for (int y = 0; y < 4; y++) {
             const int64_t j = j0 + 4 * tx + y;
             if (j >= a.N) continue;
-            T v = acc[x][y];
+            T v = acc.get(x, y);
             if (a.base) v = tr_axpy(a.base[i * a.ci + j * a.cj], a.sign, v);
             C[i * a.ci + j * a.cj] = v;
         }
