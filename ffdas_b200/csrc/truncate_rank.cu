@@ -504,6 +504,11 @@ __device__ __forceinline__ double oi_hash(uint32_t k) {
 __device__ __forceinline__ void oi_start(double &a, uint32_t k) { a = oi_hash(2 * k + 1); }
 __device__ __forceinline__ void oi_start(double2 &a, uint32_t k) { a = make_double2(oi_hash(2 * k + 1), oi_hash(2 * k + 2)); }
 
+// eigen route of the last call, reported through ffdas_get_last_kernel_info
+// (variant): device orthogonal iteration, cuSOLVER syevd, syevdx over one
+// index range, or keep-all copy
+constexpr int kRouteSubspace = 10, kRouteSyevd = 11, kRouteSyevdx = 12, kRouteCopy = 13;
+
 constexpr int kOiThreads = 512;
 constexpr int kOiMaxRank = 16;
 constexpr int kOiMaxIter = 30;
@@ -784,6 +789,8 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
     const int64_t p = rows ? m : n, q = rows ? n : m;
     const int64_t sp = rows ? n : 1, sq = rows ? 1 : n;
     const int64_t keep = stop - start, drop = p - keep;
+    h.last = ffdas_kernel_info_t{};
+    h.last.variant = kRouteCopy;
     if (drop == 0) {
         if (out != x) FFDAS_CUDA(cudaMemcpyAsync(out, x, (size_t)(m * n) * sizeof(T), cudaMemcpyDeviceToDevice,
                                                  h.stream));
@@ -855,6 +862,9 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
         tr_leading_subspace_kernel<T><<<1, kOiThreads, oi_smem_bytes<T>(p, r), h.stream>>>(
             gram.get<T>(), (int)p, r, kOiMaxIter, oi_tol<T>(), basis.get<T>(), info.get<int>() + 1);
         FFDAS_TRY(ffdas_launch_check(h.stream));
+        h.last.variant = kRouteSubspace;
+        h.last.grid = tiles * tiles * splits;
+        h.last.kernels = 4;
         int converged = 0;
         FFDAS_CUDA(cudaMemcpyAsync(&converged, info.get<int>() + 1, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
         FFDAS_CUDA(cudaStreamSynchronize(h.stream));
@@ -900,6 +910,9 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
                             tr_elem<T>::cuda, sdev.get<void>(), dev_bytes, shost.data(), host_bytes,
                             info.get<int>());
     if (st != CUSOLVER_STATUS_SUCCESS) return FFDAS_ERROR_CUSOLVER;
+    h.last.variant = ranged ? kRouteSyevdx : kRouteSyevd;
+    h.last.grid = tiles * tiles * splits;
+    h.last.kernels = 4;
     if (ranged) {
         e0 = 0;           // the r vectors sit in columns 0..r-1
         r0 = r;

@@ -157,7 +157,10 @@ typedef struct {
     int32_t copy_engine;  /* staged kernels: 0 auto, 1 TMA tile loads, 2 per-thread cp.async copies */
 } ffdas_das_config_t;
 
-/* What the last das/das_sparse/backward call on a handle launched (new). */
+/* What the last das/das_sparse/backward call on a handle launched (new).
+ * After ffdas_truncate_rank, variant is its eigen route: 10 orthogonal
+ * iteration on the device, 11 cuSOLVER syevd, 12 syevdx over one index
+ * range, 13 keep-all copy; grid is the Gram kernel's CTA count. */
 typedef struct {
     int32_t variant;
     int32_t tile_x, tile_y, tile_z;

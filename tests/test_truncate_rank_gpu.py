@@ -216,3 +216,47 @@ def test_matches_reference_library(dtype, cplx, tol, m, n, start, stop):
     e_ref = np.abs(ref - orc).max() / scale
     assert e_ours <= max(tol, 2 * e_ref), (e_ours, e_ref)
     assert np.abs(ours - ref).max() / scale <= 2 * max(tol, e_ref)
+
+
+# ----------------------------------------------------------- eigen routes
+
+def _route():
+    # ffdas_get_last_kernel_info after truncate_rank: 10 device orthogonal
+    # iteration, 11 syevd, 12 syevdx over one index range, 13 keep-all copy
+    return get_library_handle(torch.device(DEV)).last_kernel_info()["variant"]
+
+
+def test_eigen_routes():
+    x = _cuda(tro.clutter_ensemble(64, 4000, rank=3, seed=5), torch.float32)
+    xs = x.cpu().numpy()
+    scale = np.abs(xs).max()
+    for (start, stop), route in [((3, None), 10), ((0, 3), 10), ((1, 3), 12), ((0, 64), 13)]:
+        res = ffdas_b200.truncate_rank(x, start, stop).cpu().numpy()
+        assert _route() == route, (start, stop, _route())
+        err = np.abs(res - tro.truncate_rank_f64(xs, start, stop)).max() / scale
+        assert err <= 2e-5, (start, stop, err)
+    # the removed set in two runs (ranks 0 and 6..7 of 8): the full syevd;
+    # both cuts sit at gaps of the spectrum (6 tissue ranks, 2x apart)
+    y = _cuda(tro.clutter_ensemble(8, 4000, rank=6, decay=2.0, blood=1e-4, seed=6), torch.float32)
+    ys = y.cpu().numpy()
+    res = ffdas_b200.truncate_rank(y, 1, 6).cpu().numpy()
+    assert _route() == 11, _route()
+    err = np.abs(res - tro.truncate_rank_f64(ys, 1, 6)).max() / np.abs(ys).max()
+    assert err <= 2e-5, err
+
+
+def test_iteration_falls_back_without_a_gap():
+    # singular values 10 -> 9 evenly over 48 ranks: the leading subspace is
+    # separated by about 0.4 % per rank, so 30 steps of the orthogonal
+    # iteration cannot reach the residual bound and the dense solver runs
+    rng = np.random.default_rng(9)
+    m, n = 48, 3000
+    u, _ = np.linalg.qr(rng.standard_normal((m, m)))
+    v, _ = np.linalg.qr(rng.standard_normal((n, m)))
+    s = np.linspace(10.0, 9.0, m)
+    x = _cuda((u * s) @ v.T, torch.float64)
+    for start, stop in [(4, None), (0, 4)]:
+        res = ffdas_b200.truncate_rank(x, start, stop).cpu().numpy()
+        assert _route() == 12, (start, stop, _route())
+        ref = tro.truncate_rank_f64(x.cpu().numpy(), start, stop)
+        assert np.abs(res - ref).max() / np.abs(x.cpu().numpy()).max() <= 1e-9
