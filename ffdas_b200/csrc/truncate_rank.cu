@@ -606,12 +606,25 @@ __global__ void __launch_bounds__(kOiThreads) tr_leading_subspace_kernel(const T
     __syncthreads();
     if (!oi_orthonormalize(Y, Q, p, r, C, &s_flag)) return;
     for (int it = 0; it < max_iter; it++) {
-        // Y = G Q: consecutive threads take consecutive rows i (coalesced G reads)
+        // Y = G Q: consecutive threads take consecutive rows i (coalesced G
+        // reads); 8 loads in flight per batch and two partial sums, so the
+        // column walk is not one dependent load-add chain
         for (int e = tid; e < p * r; e += nt) {
             const int j = e / p, i = e - j * p;
-            A s = oi_zero<A>();
-            for (int l = 0; l < p; l++) s = oi_add(s, oi_mul(oi_from(G[i + (int64_t)l * p]), Q[l * r + j]));
-            Y[i * r + j] = s;
+            A s0 = oi_zero<A>(), s1 = oi_zero<A>();
+            int l = 0;
+            for (; l + 8 <= p; l += 8) {
+                T gv[8];
+#pragma unroll
+                for (int b = 0; b < 8; b++) gv[b] = G[i + (int64_t)(l + b) * p];
+#pragma unroll
+                for (int b = 0; b < 8; b += 2) {
+                    s0 = oi_add(s0, oi_mul(oi_from(gv[b]), Q[(l + b) * r + j]));
+                    s1 = oi_add(s1, oi_mul(oi_from(gv[b + 1]), Q[(l + b + 1) * r + j]));
+                }
+            }
+            for (; l < p; l++) s0 = oi_add(s0, oi_mul(oi_from(G[i + (int64_t)l * p]), Q[l * r + j]));
+            Y[i * r + j] = oi_add(s0, s1);
         }
         __syncthreads();
         oi_inner(Q, Y, p, r, H);
