@@ -26,8 +26,8 @@
 //     Otherwise, or if it has not converged after 30 steps, the
 //     eigendecomposition of G runs in cuSOLVER's syevd, as in the reference,
 //     or syevdx over one index range when the basis is one contiguous run of
-//     eigenvectors.  The library is loaded on first
-//     use, so the delay-and-sum path never depends on it.  Eigenvalues come
+//     eigenvectors.  The library is loaded at the first call that needs
+//     it, so the delay-and-sum path and the iteration never depend on it.  Eigenvalues come
 //     back ascending, so singular rank s is eigenvector p-1-s.
 //  3. Projection with the smaller basis.  With k = stop-start kept vectors
 //     and c = p-k removed ones, out = U_k (U_k^H A) when k <= c, else
@@ -809,8 +809,6 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
                                                  h.stream));
         return FFDAS_SUCCESS;
     }
-    solver_state *sv = nullptr;
-    FFDAS_TRY(get_solver(h, &sv));
 
     // 1. Gram matrix, upper tiles, split over q
     const int64_t tiles = (p + kTrTile - 1) / kTrTile;
@@ -862,7 +860,7 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
     if (direct) lo = p - stop;
     else if (stop == p) lo = p - start;
     else if (start == 0) lo = 0;
-    const bool ranged = lo >= 0 && solver().syevdx != nullptr;
+    bool ranged = false;
     workspace basis(h);
     FFDAS_TRY(basis.alloc((size_t)(p * r) * sizeof(T)));
 
@@ -887,7 +885,12 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
         }
     }
 
-    // 2. eigendecomposition (truncate_rank_impl.cuh:481-500, 68-90)
+    // 2. eigendecomposition (truncate_rank_impl.cuh:481-500, 68-90).
+    // cuSOLVER is loaded here, at the first call that needs it; the device
+    // iteration above does not.
+    solver_state *sv = nullptr;
+    FFDAS_TRY(get_solver(h, &sv));
+    ranged = lo >= 0 && solver().syevdx != nullptr;
     size_t dev_bytes = 0, host_bytes = 0;
     real vl = 0, vu = 0;
     int64_t found = 0;

@@ -352,8 +352,8 @@ FFDAS_API ffdas_error_t ffdas_sparse_select(
  * min(m, n), else FFDAS_ERROR_INVALID_ARGUMENT.  out may be x.  The
  * leading-subspace case (start = 0, or stop = min(m, n)) is first tried
  * with an orthogonal iteration on the device; otherwise, or if that does
- * not converge, cuSOLVER's syevd/syevdx (loaded at the first call) solves
- * the eigenproblem and reports through FFDAS_ERROR_CUSOLVER.  The call
+ * not converge, cuSOLVER's syevd/syevdx (loaded at the first call that
+ * needs it) solves the eigenproblem and reports through FFDAS_ERROR_CUSOLVER.  The call
  * waits on the host for the eigen step's status, so, like the reference's,
  * it cannot be captured in a CUDA graph. */
 FFDAS_API ffdas_error_t ffdas_truncate_rank(
