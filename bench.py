@@ -18,7 +18,9 @@ Extra keys: `roofline` for the delay-and-sum kernel (FP32 work, 5 flop/unit,
 against the FP32 FMA peak measured on this GPU; the HBM figure beside it),
 `cpu_baseline` (the FP32 C/OpenMP loop of the same formula on a voxel subset,
 all host threads), `e2e` (through the public Python API with the channel data
-copied from pinned host memory and the image read back each step), `bf16` /
+copied from pinned host memory and the image read back each step, in series
+as the reference arm does; `e2e.pipelined` is the same with the copies
+overlapping compute through DASStream), `bf16` /
 `fp16` (reduced-precision pair storage: throughput, speed-up over FP32 and
 error against this library's FP64-pair pipeline), `bwd_fwd` (backward /
 forward time on the differentiable 128-channel, 8-plane-wave, batch-4
@@ -29,7 +31,9 @@ beamformed ensembles), `in_record_fraction` (share of the units
 whose tap lies inside the record) and `clocks` (SM clock and throttle reasons
 sampled through NVML during the timed region).
 `--impl reference` times the reference implementation (its CUDA das, built
-from its sources into oracle/_ref) on the same workloads and GPU.
+from its sources into oracle/_ref) on the same workloads and GPU; that arm
+never loads libffdas_b200.so (the workload generators are loaded from their
+file, not through the package).
 `--section bwd|configs` runs one part alone (for profiling).
 """
 from __future__ import annotations
@@ -153,6 +157,23 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ utils ---
+def workloads():
+    """The seeded workload generators, loaded from their file.
+
+    Importing them as `ffdas_b200.workloads` would run the package's
+    `__init__`, which loads libffdas_b200.so; the reference arm must not map
+    this library, so it loads the module on its own (it imports only numpy
+    and torch)."""
+    import importlib.util
+    mod = sys.modules.get("_ffdas_workloads")
+    if mod is None:
+        spec = importlib.util.spec_from_file_location("_ffdas_workloads", ROOT / "ffdas_b200" / "workloads.py")
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["_ffdas_workloads"] = mod
+        spec.loader.exec_module(mod)
+    return mod
+
+
 def peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -257,7 +278,7 @@ def cpu_baseline(wl, budget_s: float = 12.0) -> dict:
 
 # ------------------------------------------------------------ reference ---
 def run_reference(args, rank, world) -> dict:
-    from ffdas_b200 import workloads as W
+    W = workloads()
     from oracle import reference
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     wl = W.diverging3d(device=dev)
@@ -292,7 +313,8 @@ def run_reference(args, rank, world) -> dict:
                        "built for sm_100a from the reference sources, run on the same GPU"},
             "device": "gpu",
             "e2e": {"value": units / (ms_e2e * 1e-3) / 1e9, "unit": UNIT,
-                    "h2d_bytes_per_step": int(wl["x"].numel() * 4), "d2h_bytes_per_step": int(call.out.numel() * 4)},
+                    "h2d_bytes_per_step": int(wl["x"].numel() * 4), "d2h_bytes_per_step": int(call.out.numel() * 4),
+                    "api": "reference ffdas_das per step: pinned host copy in, call, copy out (serial)"},
             "clocks": ck}
     if cpu:
         line["cpu_baseline"] = cpu
@@ -403,11 +425,15 @@ def run_ours(args, rank, world) -> dict:
                        "l2": "inputs larger than L2 (no flush)", "schedule": info,
                        "autotune": {"best": tuned["config"], "top": tuned["table"][:5]}},
             "roofline": roofline,
-            "e2e": {"value": units * world / (ms_e2e * 1e-3) / 1e9, "unit": UNIT,
+            # e2e: the serial protocol the reference arm also uses (copy in,
+            # call, copy out, every step), so the two e2e values compare like
+            # for like; the pipelined figure (DASStream) is reported beside it
+            "e2e": {"value": units * world / (ms_e2e_serial * 1e-3) / 1e9, "unit": UNIT,
                     "h2d_bytes_per_step": int(x.numel() * 4), "d2h_bytes_per_step": int(out.numel() * 4),
-                    "api": "ffdas_b200.runner.DASStream (copies overlap compute)",
-                    "serial": {"value": units * world / (ms_e2e_serial * 1e-3) / 1e9,
-                               "api": "ffdas_b200.das per step: copy in, call, copy out"}},
+                    "api": "ffdas_b200.das per step: pinned host copy in, call, copy out (serial)",
+                    "pipelined": {"value": units * world / (ms_e2e * 1e-3) / 1e9,
+                                  "api": "ffdas_b200.runner.DASStream (the same copies overlapping compute "
+                                         "on separate streams)"}},
             "gpu_launches": 2 * args.steps,
             "in_record_fraction": in_record_fraction(wl),
             "clocks": ck}
@@ -570,12 +596,18 @@ def config_extras(args, impl: str) -> dict:
       pixels, FP32; ours replays a captured CUDA graph (DASRunner), the
       reference is called through its API; time per call in microseconds.
     ensemble: 200-frame FP16 ensemble, 128 ch, 11 plane waves, 1536 samples,
-      400x256 pixels (frames batched in one call).
+      400x256 pixels (frames batched in one call).  The reference arm times
+      both of its batched algorithms and reports the faster as the entry:
+      ALG1 with its 16-frame register tile (its default tile of 32 has no
+      float-output kernel, src/das/das_alg1.cu:219-239), and ALG2 on three
+      64-frame calls plus ALG1 on the last 8 frames -- ALG2 sums correctly
+      only when a call's batch equals its 64-frame batch block (see
+      `reference_alg2_ok`).
     sparse_focus: das_sparse, 64 focused transmits, 1..32 events per pixel
       (padding repeats an index with zero weight); units count real events.
     Parity of the two arms on these inputs is held by the test suite.
     """
-    from ffdas_b200 import workloads as W
+    W = workloads()
     dev = torch.device("cuda", torch.cuda.current_device())
     stream = torch.cuda.current_stream(dev)
     out = {}
@@ -601,6 +633,14 @@ def config_extras(args, impl: str) -> dict:
             ms = timed(fn, steps, warm, stream, 1) / reps
             call.close()
             kind = "reference ALG1 through ffdas_das" + ("_sparse" if idx is not None else "")
+            alg_table = {"alg1": ms}
+            if name == "ensemble":
+                ms2 = reference_alg2_ensemble(wl, steps, warm, stream)
+                if ms2 is not None:
+                    alg_table["alg2_64_frame_calls"] = ms2
+                    if ms2 < ms:
+                        ms = ms2
+                        kind = "reference ALG2 on 3 x 64 frames + ALG1 on the last 8 (the faster of its algorithms)"
         else:
             from ffdas_b200.runner import DASRunner
             run = DASRunner(*geo, sparse_indices=idx)
@@ -610,9 +650,12 @@ def config_extras(args, impl: str) -> dict:
                     run.replay()
             ms = timed(fn, steps, warm, stream, 1) / reps
             kind = f"ffdas_b200 CUDA graph replay, schedule {run.config}"
+            alg_table = None
             del run
         e = {"value": units / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_call": ms, "units_per_call": units,
              "x_dtype": str(wl["x"].dtype).replace("torch.", ""), "impl": kind}
+        if alg_table:
+            e["reference_ms_by_algorithm"] = alg_table
         if name == "plane2d":
             e["us_per_call"] = ms * 1e3
         out[name] = e
@@ -623,6 +666,52 @@ def config_extras(args, impl: str) -> dict:
     return {"configs": out}
 
 
+ALG2_FRAMES = 64
+
+
+def reference_alg2_ok(B: int) -> bool:
+    """Batch sizes on which the reference's ALG2 sums correctly.
+
+    Its launcher sets the frames per batch block to min(roundup(B, 16), 64)
+    (src/das/das_alg2.cu:405-408), while its kernel keeps (M * N) / 32
+    accumulators per thread (das_alg2_kernels.cuh:38, 77) and fills them over
+    n < N (:144) but writes them out over n < B (:169).  The two loops agree
+    only when B equals the block, 64 frames, for 4-byte and 2-byte samples
+    alike (with fewer frames the vector loads fill more accumulators than the
+    array holds; with more, each block writes frames of the other blocks from
+    accumulators it never filled).  The harness calls ALG2 only at B = 64."""
+    return B == ALG2_FRAMES
+
+
+def reference_alg2_ensemble(wl, steps: int, warm: int, stream):
+    """The 200-frame ensemble through the reference's ALG2: three calls of 64
+    frames and ALG1 (tile 8) on the last 8 frames, per call in ms; None when
+    ALG2 cannot be driven safely (a tap outside the record: ALG2 reads an
+    internal copy of x that cannot be guarded)."""
+    from oracle import reference
+    x = wl["x"]
+    B = x.shape[0]
+    geo = (wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"])
+    calls = []
+    try:
+        for b0 in range(0, B - B % ALG2_FRAMES, ALG2_FRAMES):
+            calls.append(reference.Prepared(x[b0:b0 + ALG2_FRAMES].contiguous(), *geo, alg=2))
+        if B % ALG2_FRAMES:
+            calls.append(reference.Prepared(x[B - B % ALG2_FRAMES:].contiguous(), *geo, alg=1, tile=8))
+    except ValueError:
+        for c in calls:
+            c.close()
+        return None
+
+    def fn():
+        for c in calls:
+            c()
+    ms = timed(fn, steps, warm, stream, 1)
+    for c in calls:
+        c.close()
+    return ms
+
+
 def rank_filter_extra(args, impl: str, dev, stream) -> dict:
     """The clutter filter that follows beamforming: truncate_rank with the 5
     leading (tissue) ranks removed, on a 200-frame 400x256 FP32 image
@@ -631,7 +720,7 @@ def rank_filter_extra(args, impl: str, dev, stream) -> dict:
     ffdas_truncate_rank; reference: its ffdas_truncate_rank built from its
     sources (cuBLAS GEMM, cuSOLVER syevd, SYRK + SYMM).  Both calls return
     with the stream drained (the solver status is read on the host)."""
-    from ffdas_b200 import workloads as W
+    W = workloads()
     out = {}
     steps, warm = max(args.steps, 5), args.warmup
     for name, (m, shape, dtype, seed) in {"ensemble_f32": (200, (400, 256), torch.float32, 51),
@@ -714,8 +803,8 @@ def main() -> int:
         if args.section != "all":
             if world > 1 or (args.impl == "reference" and args.section == "bwd"):
                 return 0
-            import ffdas_b200
             if args.section == "bwd":
+                import ffdas_b200
                 part = bwd_extras(args, ffdas_b200.get_library_handle(torch.device("cuda", 0)))
             else:
                 part = config_extras(args, args.impl)

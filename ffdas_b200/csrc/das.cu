@@ -7,6 +7,7 @@
 // (src/das/das_alg1.cu:172-178), sparse count (das_alg1.cu:267).
 // After validation every call runs: ingest (x -> pair rows) then the
 // forward kernel chosen by the planner or the handle's config.
+#include <cuda.h>
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -714,25 +715,94 @@ constexpr int kStaticMaxDevices = 64;
 static __device__ __align__(256) unsigned char g_static_pairs[kStaticPairBytes];
 
 std::mutex g_static_mu;
-void *g_static_addr[kStaticMaxDevices] = {};
 
-// Device address of g_static_pairs on the current device, looked up once per
-// device (host code may not use the symbol itself: its host-side name is a
-// stand-in, not a device address).
-ffdas_error_t static_pairs_address(void **ptr) {
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess) return FFDAS_ERROR_CUDA_RUNTIME;
-    if (dev < 0 || dev >= kStaticMaxDevices) return FFDAS_ERROR_INVALID_DEVICE;
-    std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_addr[dev]) {
+// Per-device set-up of the static entry: the array's device address and the
+// device properties the planner reads.  It is tied to the CUDA context it was
+// made in (by the context's unique id), so a context torn down and created
+// again -- cudaDeviceReset, a primary context released by another library --
+// gets a fresh lookup instead of a stale address.
+struct static_device_setup {
+    unsigned long long ctx_id = 0;   // 0: not set up
+    void *pairs = nullptr;
+    int sm_count = 0, arch_code = 0;
+    size_t smem_optin = 0;
+};
+static_device_setup g_static_setup[kStaticMaxDevices];
+
+using ctx_get_current_fn = CUresult (*)(CUcontext *);
+using ctx_get_id_fn = CUresult (*)(CUcontext, unsigned long long *);
+
+// Unique id of the calling thread's current context (driver entry points
+// fetched through the runtime, like the tensor-map encoder).
+ffdas_error_t current_context_id(unsigned long long *id) {
+    static ctx_get_current_fn get_current = nullptr;
+    static ctx_get_id_fn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
         void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_static_pairs) != cudaSuccess || !p) {
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<ctx_get_current_fn>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<ctx_get_id_fn>(p);
+        cudaGetLastError();
+    });
+    if (!get_current || !get_id) return FFDAS_ERROR_CUDA_DRIVER;
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return FFDAS_ERROR_CUDA_DRIVER;
+    if (get_id(ctx, id) != CUDA_SUCCESS) return FFDAS_ERROR_CUDA_DRIVER;
+    return FFDAS_SUCCESS;
+}
+
+// Set-up for the current device: looked up once per device and context
+// (host code may not use the symbol itself: its host-side name is a
+// stand-in, not a device address).  The queries allocate nothing.
+ffdas_error_t static_setup(int *device, static_device_setup *out) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return FFDAS_ERROR_CUDA_RUNTIME;
+    }
+    if (dev < 0 || dev >= kStaticMaxDevices) return FFDAS_ERROR_INVALID_DEVICE;
+    unsigned long long ctx_id = 0;
+    if (current_context_id(&ctx_id) != FFDAS_SUCCESS) {
+        // no current context yet on this thread: cudaSetDevice makes the
+        // device's primary context current (it allocates no device memory)
+        if (cudaSetDevice(dev) != cudaSuccess) {
             cudaGetLastError();
             return FFDAS_ERROR_CUDA_RUNTIME;
         }
-        g_static_addr[dev] = p;
+        FFDAS_TRY(current_context_id(&ctx_id));
     }
-    *ptr = g_static_addr[dev];
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    static_device_setup &st = g_static_setup[dev];
+    if (st.ctx_id != ctx_id) {
+        static_device_setup fresh;
+        if (cudaGetSymbolAddress(&fresh.pairs, g_static_pairs) != cudaSuccess || !fresh.pairs) {
+            cudaGetLastError();
+            return FFDAS_ERROR_CUDA_RUNTIME;
+        }
+        int major = 0, minor = 0, optin = 0;
+        if (cudaDeviceGetAttribute(&fresh.sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+            cudaGetLastError();
+            return FFDAS_ERROR_CUDA_RUNTIME;
+        }
+        // same rules and encoding as ffdas_create
+        if (major < 10) return FFDAS_ERROR_INSUFFICIENT_COMPUTE_CAPABILITY;
+        if (major != 10) return FFDAS_ERROR_DEVICE_NOT_SUPPORTED;
+        fresh.arch_code = major * 100 + minor * 10;
+        fresh.smem_optin = (size_t)optin;
+        fresh.ctx_id = ctx_id;
+        st = fresh;
+    }
+    *device = dev;
+    *out = st;
     return FFDAS_SUCCESS;
 }
 
@@ -769,14 +839,19 @@ extern "C" ffdas_error_t ffdas_das_static(uintptr_t stream, const float *srcpos,
     const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
     const size_t bytes = (size_t)std::max<int64_t>(rows, 1) * npad * storage_bytes(kind);
     if (bytes > kStaticPairBytes) return FFDAS_ERROR_DIMS_TOO_LARGE;
-    void *P = nullptr;
-    FFDAS_TRY(static_pairs_address(&P));
+    static_device_setup st;
+    int dev = -1;
+    FFDAS_TRY(static_setup(&dev, &st));
+    void *P = st.pairs;
 
-    // A handle-shaped view of the caller's stream: no pool, no status word, no
-    // events; the launch helpers below only read its stream.
+    // A handle-shaped view of the caller's stream and device: no pool, no
+    // status word, no events.
     ffdas_context ctx;
     ctx.stream = reinterpret_cast<cudaStream_t>(stream);
-    cudaGetDevice(&ctx.device_id);
+    ctx.device_id = dev;
+    ctx.sm_count = st.sm_count;
+    ctx.arch_code = st.arch_code;
+    ctx.smem_optin = st.smem_optin;
     // Every pair of every row is rewritten by the ingest pass, so nothing left
     // in the array by an earlier call needs clearing.
     FFDAS_TRY(launch_ingest(ctx, pb, xd.dtype, kind, x, npad, P));

@@ -301,7 +301,8 @@ FFDAS_API ffdas_error_t ffdas_das_backward(
  * 16-bit channel data) must not exceed 16 MiB, else FFDAS_ERROR_DIMS_TOO_LARGE.
  * Real channel data (float32, float16, bfloat16, int16) with float32 output only.
  * The first call on a device looks up the array's device address (once per
- * device); make that first call before any stream capture.  All calls share
+ * device and CUDA context: after cudaDeviceReset the next call looks it up
+ * again); make that first call before any stream capture.  All calls share
  * the one array: calls that overlap on the GPU (other streams, other host
  * threads) race and must be serialised by the caller. */
 FFDAS_API ffdas_error_t ffdas_das_static(

@@ -34,7 +34,7 @@ MAX_GUARD = 1 << 26   # elements
 _lib = None
 _handles = {}
 
-DT = {torch.float32: 0, torch.float16: 2, torch.float64: 16, torch.complex64: 4}
+DT = {torch.float32: 0, torch.float16: 2, torch.float64: 16, torch.complex64: 4, torch.complex32: 6}
 
 
 def available() -> bool:
@@ -95,10 +95,13 @@ def k_range(srcpos, dstpos, offsets) -> tuple[int, int]:
 
 
 def das(x: torch.Tensor, srcpos, dstpos, offsets, weights, *, sparse_indices=None, alg: int = 1,
-        tile: int | None = None) -> torch.Tensor:
+        tile: int | None = None, srcdir=None, wavenum: float = 0.0, beta: complex = 0.0,
+        out_init: torch.Tensor | None = None) -> torch.Tensor:
     """Reference das / das_sparse on a CUDA x (4-D, contiguous); returns (B, *spatial).
 
     x is copied into a guarded buffer first; the copy is outside any timing.
+    srcdir (C, 4), wavenum (complex data) and beta are passed through as the
+    reference's arguments; with beta != 0 the output starts from out_init.
     """
     assert x.is_cuda and x.ndim == 4
     dev = x.device
@@ -110,17 +113,27 @@ def das(x: torch.Tensor, srcpos, dstpos, offsets, weights, *, sparse_indices=Non
         raise ValueError("ALG2 reads an internal copy that cannot be guarded; every k must lie in the record")
     if guard > MAX_GUARD:
         raise ValueError(f"delay range needs {guard} guard elements; refusing to call the reference")
-    buf = torch.zeros(x.numel() + 2 * guard, dtype=x.dtype, device=dev)
-    xg = buf[guard:guard + x.numel()].view(x.shape)
-    xg.copy_(x)
+    if x.dtype == torch.complex32:   # complex half: a buffer of half pairs, viewed as complex32
+        buf = torch.zeros(2 * (x.numel() + 2 * guard), dtype=torch.float16, device=dev).view(torch.complex32)
+        xg = buf[guard:guard + x.numel()].view(x.shape)
+        xg.view(torch.float16).copy_(x.contiguous().view(torch.float16))
+    else:
+        buf = torch.zeros(x.numel() + 2 * guard, dtype=x.dtype, device=dev)
+        xg = buf[guard:guard + x.numel()].view(x.shape)
+        xg.copy_(x)
     f32 = lambda t: t.to(device=dev, dtype=torch.float32).contiguous()  # noqa: E731
     srcpos, dstpos, offsets, weights = f32(srcpos), f32(dstpos), f32(offsets), f32(weights)
+    sd = None if srcdir is None else f32(srcdir)
     spatial = tuple(dstpos.shape[:-1])
     out_dtype = torch.float64 if x.dtype == torch.float64 else (torch.complex64 if x.is_complex() else torch.float32)
     out = torch.zeros((B, *spatial), dtype=out_dtype, device=dev)
+    if out_init is not None:
+        out.copy_(out_init.reshape(out.shape))
     xd = _desc([B, C, S, N], DT[x.dtype])
     od = _desc([B, *spatial], DT[out_dtype])
-    beta = (ctypes.c_double * 2)() if out_dtype == torch.float64 else (ctypes.c_float * 2)()
+    bc = complex(beta)
+    beta = (ctypes.c_double * 2)(bc.real, bc.imag) if out_dtype == torch.float64 else \
+        (ctypes.c_float * 2)(bc.real, bc.imag)
     h = handle(dev.index)
     L = lib()
     L.ffdas_set_stream(h, torch.cuda.current_stream(dev).cuda_stream)
@@ -128,13 +141,14 @@ def das(x: torch.Tensor, srcpos, dstpos, offsets, weights, *, sparse_indices=Non
     if tile is not None:
         os.environ["FFDAS_ALG1_TILE_SIZE"] = str(tile)
     try:
+        sdp = None if sd is None else sd.data_ptr()
         if sparse_indices is None:
-            rc = L.ffdas_das(h, srcpos.data_ptr(), None, 0.0, xd, xg.data_ptr(), dstpos.data_ptr(),
+            rc = L.ffdas_das(h, srcpos.data_ptr(), sdp, float(wavenum), xd, xg.data_ptr(), dstpos.data_ptr(),
                              offsets.data_ptr(), weights.data_ptr(), ctypes.cast(beta, ctypes.c_void_p), od,
                              out.data_ptr(), 0, alg)
         else:
             idx = sparse_indices.to(device=dev, dtype=torch.int32).contiguous()
-            rc = L.ffdas_das_sparse(h, srcpos.data_ptr(), None, 0.0, xd, xg.data_ptr(), dstpos.data_ptr(),
+            rc = L.ffdas_das_sparse(h, srcpos.data_ptr(), sdp, float(wavenum), xd, xg.data_ptr(), dstpos.data_ptr(),
                                     offsets.data_ptr(), weights.data_ptr(), int(idx.shape[0]), idx.data_ptr(),
                                     ctypes.cast(beta, ctypes.c_void_p), od, out.data_ptr(), 0, alg)
     finally:

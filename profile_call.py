@@ -1,6 +1,6 @@
 """Run one delay-and-sum workload under a fixed schedule, for profilers.
 
-    python -m ffdas_b200.profile_call ensemble --frames 50 --calls 4 \\
+    python profile_call.py ensemble --frames 50 --calls 4 \\
         --schedule '{"variant": 2, "tile_x": 32, "tile_y": 8, "window": 64, "batch_tile": 8}'
 
 Builds the named synthetic workload (ffdas_b200.workloads.CONFIGS), applies the
@@ -9,7 +9,7 @@ times (the first calls warm the kernel attributes and the memory pool), and
 prints the last call's kernel info.  `--backward` runs ffdas_das_backward
 instead (random output gradient).
 
-    python -m ffdas_b200.profile_call rank_filter --calls 3
+    python profile_call.py rank_filter --calls 3
 
 runs truncate_rank(x, 5) on the seeded 200-frame 400x256 FP32 slow-time
 ensemble (workloads.slow_time_ensemble) instead.
@@ -21,9 +21,9 @@ import json
 
 import torch
 
-from . import workloads as W
-from .das import das, das_sparse
-from .library import get_library_handle
+from ffdas_b200 import workloads as W
+from ffdas_b200.das import das, das_sparse
+from ffdas_b200.library import get_library_handle
 
 
 def main() -> int:
@@ -37,7 +37,7 @@ def main() -> int:
     args = ap.parse_args()
     dev = torch.device("cuda", torch.cuda.current_device())
     if args.workload == "rank_filter":
-        from .truncate_rank import truncate_rank
+        from ffdas_b200.truncate_rank import truncate_rank
         x = W.slow_time_ensemble(args.frames or 200, (400, 256), torch.float32, dev)
         for _ in range(args.calls):
             y = truncate_rank(x, 5)

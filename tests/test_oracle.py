@@ -184,6 +184,9 @@ def test_oracle_matches_reference_outputs(path):
             kw[k] = z[k]
     wavenum = float(z["wavenum"]) if "wavenum" in z.files else 0.0
     q1 = bool(z["q1"]) if "q1" in z.files else False
+    if "beta" in z.files:   # out = beta * out_init + sum
+        kw["beta"] = complex(z["beta"])
+        kw["out"] = z["out_init"]
     ref_out = z["out"]
     got = oracle.das_f64(z["x"], z["srcpos"], z["dstpos"], z["offsets"], z["weights"], wavenum=wavenum,
                          q1=q1, **kw)

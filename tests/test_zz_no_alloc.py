@@ -5,10 +5,11 @@ that forbids allocation after start-up, or code that runs on a fixed memory
 budget without an ffdas handle (whose creation allocates a workspace pool).
 ffdas_das_static takes the caller's stream, inputs and output and keeps its
 interpolation-pair workspace in a fixed array inside the library.  This test
-calls it through the C-ABI and checks it against ffdas_das on two calls in a
-row with different problem sizes (the second call must not see the first
-call's leftovers), at the FP32 tolerance the forward tests use (2e-5 relative
-L2; both paths compute the same taps, so the match is much closer), and that
+calls it through the C-ABI and checks it against ffdas_das and against the
+FP64 oracle on two calls in a row with different problem sizes (the second
+call must not see the first call's leftovers), at the FP32 tolerance the
+forward tests use (2e-5 relative L2; both library paths compute the same taps,
+so their match is much closer), and that
 a problem larger than the array is refused with FFDAS_ERROR_DIMS_TOO_LARGE.
 
 This file is collected last so that a run stopping at the first failure has
@@ -56,6 +57,10 @@ def test_static_workspace_matches_das_on_consecutive_calls():
         ref = ffdas_b200.das(x, wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"])
         assert torch.isfinite(got).all()
         assert oracle.rel_l2(got.cpu().numpy(), ref.cpu().numpy()) < 2e-5
+        # and directly against the FP64 oracle, at the same bar
+        exact = oracle.das_f64(x.cpu().numpy(), wl["srcpos"].cpu().numpy(), wl["dstpos"].cpu().numpy(),
+                               wl["offsets"].cpu().numpy(), wl["weights"].cpu().numpy())
+        assert oracle.rel_l2(got.cpu().numpy(), exact) < 2e-5
 
 
 def test_static_workspace_refuses_oversized_problems():
