@@ -182,15 +182,20 @@ def peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def profile_traffic(name: str):
-    """Per-launch DRAM bytes of the kernel from the committed ncu summary, if any."""
+def profile_field(name: str, key: str):
+    """A figure of the committed ncu summary of the kernel (profiles/<name>.json), if any."""
     p = ROOT / "profiles" / f"{name}.json"
     if p.exists():
         try:
-            return json.loads(p.read_text()).get("dram_bytes_per_launch")
+            return json.loads(p.read_text()).get(key)
         except Exception:
             return None
     return None
+
+
+def profile_traffic(name: str):
+    """Per-launch DRAM bytes of the kernel from the committed ncu summary, if any."""
+    return profile_field(name, "dram_bytes_per_launch")
 
 
 def timed(fn, steps: int, warmup: int, stream, world: int):
@@ -358,12 +363,16 @@ def run_ours(args, rank, world) -> dict:
     for _ in range(max(3, args.steps)):
         step()
         kms.append(h.last_kernel_ms())
+    # units the kernel actually evaluated: it skips passes and stages whose
+    # every tap lies outside the record (they add exactly nothing)
+    units_eval = h.last_kernel_units()
     h.set_kernel_timing(False)
     info = h.last_kernel_info()
     kernel_ms = statistics.mean(kms[1:]) if len(kms) > 1 else kms[0]
     fp32_peak = h.measure_fp32_peak()
     pk = peaks()
-    achieved_tf = FLOP_PER_UNIT * units / (kernel_ms * 1e-3) / 1e12
+    work_units = units_eval if units_eval is not None else units
+    achieved_tf = FLOP_PER_UNIT * work_units / (kernel_ms * 1e-3) / 1e12
     bytes_alg = algorithmic_bytes(wl, 4)
     tile_voxels = info["tile_x"] * info["tile_y"] * info["tile_z"]
     if info["variant"] == 2 and tile_voxels == 512:
@@ -372,11 +381,31 @@ def run_ours(args, rank, world) -> dict:
         kname, pname = "das_staged_kernel<f32 pairs>", "das_staged_diverging3d"
     else:
         kname, pname = "das_gather_kernel<f32 pairs>", "das_gather_diverging3d"
+    # secondary ceilings of the same kernel, in units per second: the shared-
+    # memory data path (128 B per clock per SM; one 8-byte f32 pair per tap)
+    # and instruction issue (4 warp instructions per clock per SM, at the
+    # thread instructions per unit of the committed ncu summary)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    clk_hz = (ck.get("sm_mhz") or ck.get("sm_max_mhz") or 1965.0) * 1e6
+    ups = work_units / (kernel_ms * 1e-3)
+    smem_ceiling = sms * (128 / 8) * clk_hz
+    ceilings = {"smem_f32_pairs": {"units_per_s": smem_ceiling, "achieved_frac": ups / smem_ceiling,
+                                   "basis": f"{sms} SMs x 16 taps/clk (128 B/clk, 8-B pairs) x {clk_hz / 1e9:.3f} GHz"}}
+    ipu = profile_field(pname, "thread_instr_per_unit")
+    if ipu:
+        issue_ceiling = sms * 128 * clk_hz / ipu
+        ceilings["issue"] = {"units_per_s": issue_ceiling, "achieved_frac": ups / issue_ceiling,
+                             "basis": f"{sms} SMs x 128 thread-instr/clk / {ipu:.2f} instr per unit (ncu summary)"}
     roofline = {"bound": "fp32", "achieved": achieved_tf, "peak": fp32_peak, "unit": "TFLOP/s",
                 "frac": achieved_tf / fp32_peak, "traffic": profile_traffic(pname),
                 "kernel": kname, "kernel_ms": kernel_ms,
-                "peak_source": "FP32 FMA throughput measured on this GPU by ffdas_measure_fp32_peak",
+                "peak_source": "FP32 FMA throughput measured on this GPU by ffdas_measure_fp32_peak "
+                               "(faster of scalar FFMA and packed FFMA2)",
                 "flop_per_unit": FLOP_PER_UNIT, "units_per_launch": units,
+                "units_evaluated": work_units, "evaluated_fraction": work_units / units,
+                "achieved_basis": "5 flop x units the kernel evaluated / kernel time (out-of-record passes and "
+                                  "stages it skips are not counted as work)",
+                "ceilings": ceilings,
                 "hbm": {"algorithmic_bytes": bytes_alg, "achieved_gbs": bytes_alg / (kernel_ms * 1e-3) / 1e9,
                         "peak_gbs": pk["hbm_gbs"], "peak_source": pk["source"] + " (MEASURED_PEAKS.json hbm_gbs)"}}
 

@@ -76,6 +76,7 @@ class Error(enum.IntEnum):
     CUDA_LAUNCH_FAILED = 32
     CUDA_SYNC_FAILED = 33
     CUDA_MEMCPY_FAILED = 34
+    INVALID_STATE = 62
     INTERNAL = 100
     UNKNOWN = 101
 
@@ -136,6 +137,7 @@ SIGNATURES = {
     "ffdas_debug_fail_alloc_after": (None, [ctypes.c_int]),
     "ffdas_set_kernel_timing": (c_err, [c_handle, ctypes.c_int]),
     "ffdas_get_last_kernel_time": (c_err, [c_handle, ctypes.POINTER(ctypes.c_float)]),
+    "ffdas_get_last_kernel_units": (c_err, [c_handle, ctypes.POINTER(ctypes.c_longlong)]),
     "ffdas_measure_fp32_peak": (c_err, [c_handle, ctypes.POINTER(ctypes.c_double)]),
     "ffdas_get_device_status": (c_err, [c_handle, ctypes.POINTER(ctypes.c_int)]),
     "ffdas_debug_staged_drop_stage": (None, [ctypes.c_int]),
@@ -243,6 +245,15 @@ class Handle:
         ms = ctypes.c_float()
         check(load().ffdas_get_last_kernel_time(self.h, ctypes.byref(ms)))
         return float(ms.value)
+
+    def last_kernel_units(self):
+        """Units the last timed call's kernel evaluated, or None when it does not count them."""
+        u = ctypes.c_longlong()
+        rc = load().ffdas_get_last_kernel_units(self.h, ctypes.byref(u))
+        if rc == Error.INVALID_STATE:
+            return None
+        check(rc)
+        return int(u.value)
 
     def device_status(self) -> int:
         s = ctypes.c_int()

@@ -188,11 +188,14 @@ ffdas_error_t ffdas_create(ffdas_handle_t *handle) {
     pp.location.id = h->device_id;
     if (cudaMemPoolCreate(&h->pool, &pp) != cudaSuccess) { err = FFDAS_ERROR_CUDA_RUNTIME; goto fail; }
     cudaMemPoolSetAttribute(h->pool, cudaMemPoolAttrReleaseThreshold, &threshold);
-    if (cudaMalloc(reinterpret_cast<void **>(&h->status), sizeof(int)) != cudaSuccess ||
-        cudaMemset(h->status, 0, sizeof(int)) != cudaSuccess) {
+    // 16 device bytes: the status word, and at byte 8 the counter of units
+    // evaluated that kernel timing reads (ffdas_get_last_kernel_units)
+    if (cudaMalloc(reinterpret_cast<void **>(&h->status), 16) != cudaSuccess ||
+        cudaMemset(h->status, 0, 16) != cudaSuccess) {
         err = FFDAS_ERROR_ALLOCATION_FAILED;
         goto fail;
     }
+    h->unit_count = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(h->status) + 8);
     *handle = h;
     return FFDAS_SUCCESS;
 fail:

@@ -53,8 +53,10 @@ struct ffdas_context {
     ffdas_das_config_t config{};
     ffdas_kernel_info_t last{};
     int *status = nullptr;  // device word: bounded-wait timeouts of the staged kernels
+    unsigned long long *unit_count = nullptr;   // device counter: units the last timed kernel evaluated
     bool timing = false;
     bool timing_recorded = false;
+    bool units_recorded = false;   // the last timed kernel counted its units
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     // eigensolver state of ffdas_truncate_rank, created on its first call and
     // released with the handle

@@ -438,6 +438,10 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
     if (pb.C > 0 && !a.srcpos) return FFDAS_ERROR_NULL_POINTER;
     if ((int64_t)pb.B * pb.C * pb.S * pb.N > 0 && !a.x) return FFDAS_ERROR_NULL_POINTER;
     if (a.sparse && !a.sparse_indices) return FFDAS_ERROR_NULL_POINTER;
+    h.units_recorded = false;
+    // timed calls: the kernels that count the units they evaluate add into
+    // the handle's counter, cleared here, before the timed launch
+    if (h.timing && h.unit_count) FFDAS_CUDA(cudaMemsetAsync(h.unit_count, 0, sizeof(unsigned long long), h.stream));
 
     // ---- small problems: the whole call as one launch straight from x ----
     if (direct_supported(pb, xd.dtype, od.dtype, kind)) {

@@ -161,6 +161,7 @@ template <int K, int WB>
 static ffdas_error_t launch_fwd_sc(ffdas_context &h, const staged_params &sp, const CUtensorMap &map, int SC,
                                    dim3 grid) {
     if (sp.T0 * sp.T1 * sp.T2 == 2 * kStConsumers) {   // 512-voxel tiles: two voxels per thread
+        h.units_recorded = sp.units != nullptr;            // this kernel counts the units it evaluates
         // event chunks of 1, 4 (three CTAs per SM) or 8 (two CTAs per SM)
         switch (SC) {
             case 1: return launch_fwd2_t<K, 1, WB>(h, sp, map, grid);
@@ -213,6 +214,7 @@ static staged_params base_params(ffdas_context &h, const das_problem &pb, const 
     sp.beta_re = gp.beta_re; sp.beta_im = gp.beta_im; sp.beta_zero = gp.beta_zero;
     sp.wavenum = gp.wavenum;
     sp.status = h.status;
+    sp.units = h.timing ? h.unit_count : nullptr;
     sp.debug_drop_stage = ffdas_take_debug_drop_stage();
     sp.cchunk = gp.cchunk;
     return sp;

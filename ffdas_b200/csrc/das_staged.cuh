@@ -68,6 +68,7 @@ struct staged_params {
     const int *sparse_idx;
     int sparse_n;
     const int *gate;       // when set and *gate != 0 the kernel does nothing (a duplicate listed event)
+    unsigned long long *units;   // when set, the kernel adds the units it evaluated (512-voxel kernel)
     // adjoint only
     const float *gout;
     int64_t gout_bstride;
@@ -190,11 +191,32 @@ constexpr size_t kStMiscBytes = kStages * kStWin * 4      // meta
                                 + 32 * 4                   // abort flag (+pad)
                                 + kStWarps * 16 * 2 * 4    // reduction scratch
                                 + kStages * kStWin * 2 * 16   // channel table (position, normal)
-                                + kStages * kStWin * 2 * 16;  // channel positions as pairs (x,x,y,y), (z,z,0,0)
+                                + kStages * kStWin * 2 * 16   // channel positions as pairs (x,x,y,y), (z,z,0,0)
+                                + kStages * kStWin * 4        // window address biases (unclamped path)
+                                + kStages * 4                 // stage modes
+                                + 16 * 4;                     // channel box, pass flags
+
+// Stage modes written by the 512-voxel kernel's producer (sm.mode):
+//   kStageEmpty  no window of the stage holds data and none overflows: every
+//                tap of the stage reads zeros, the consumers skip it;
+//   kStageFast   every window of the stage is a real window or a zero window
+//                whose whole tap range fits one slot, so a tap address is
+//                bits(floor(tau) + 1.5 * 2^23) * pair_bytes + bias, no clamp.
+enum : int { kStageEmpty = 1, kStageFast = 2 };
+// Pass flags (sm.flags[2 + pass parity]), set by the consumers before a pass:
+//   kPassSkip    every tap of the pass lies outside the record for every
+//                voxel of the tile and every channel: the pass is skipped;
+//   kPassFast    every delay of the pass is present, finite and below 2^20 in
+//                magnitude, every voxel and channel position finite, the event
+//                chunk full and no directivity test: stages marked kStageFast
+//                may use the unclamped taps.
+enum : int { kPassSkip = 1, kPassFast = 2 };
+constexpr float kSaneRange = 1048576.0f;   // 2^20: tau, offsets and distances below it keep |rounding| < 1 sample
 
 template <int WB, int K>
 constexpr size_t staged_smem_bytes() {
-    return slot_geom<WB, K>::ring_bytes + kStMiscBytes + 128;
+    // ring, one zero slot (the target of zero windows on the unclamped path), misc
+    return slot_geom<WB, K>::ring_bytes + slot_geom<WB, K>::bytes + kStMiscBytes + 128;
 }
 
 // The adjoints keep two copies of their fixed-point gradient bins (cx.par
@@ -310,11 +332,17 @@ struct staged_smem {
     float *red;            // [warps][16][2]
     float4 *chan_pos, *chan_dir;  // [kStages][kStWin]
     float4 *chan_pair;            // [kStages][kStWin][2]: (x, x, y, y), (z, z, 0, 0)
+    unsigned char *zslot;  // one slot of zeros (zeroed once per CTA, never written by TMA)
+    uint32_t *bias;        // [kStages][kStWin]: tap address = bits(floor + magic) * pair_bytes + bias
+    int *mode;             // [kStages]: kStageEmpty / kStageFast
+    float *cbox;           // [6]: bounding box of this CTA's channels (min xyz, max xyz)
+    int *flags;            // [4]: -, voxel and channel positions finite, pass flags (by pass parity)
     unsigned char *extra;  // adjoint scratch
 
     __device__ explicit staged_smem(unsigned char *raw) {
         ring = raw;
-        meta = reinterpret_cast<uint32_t *>(ring + SG::ring_bytes);
+        zslot = ring + SG::ring_bytes;
+        meta = reinterpret_cast<uint32_t *>(zslot + SG::bytes);
         ovf = reinterpret_cast<int *>(meta + kStages * kStWin);
         full = reinterpret_cast<uint64_t *>(ovf + kStages);
         empty = full + kStages;
@@ -326,7 +354,11 @@ struct staged_smem {
         chan_pos = reinterpret_cast<float4 *>(red + kStWarps * 32);
         chan_dir = chan_pos + kStages * kStWin;
         chan_pair = chan_dir + kStages * kStWin;
-        extra = reinterpret_cast<unsigned char *>(chan_pair + kStages * kStWin * 2);
+        bias = reinterpret_cast<uint32_t *>(chan_pair + kStages * kStWin * 2);
+        mode = reinterpret_cast<int *>(bias + kStages * kStWin);
+        cbox = reinterpret_cast<float *>(mode + kStages);
+        flags = reinterpret_cast<int *>(cbox + 8);
+        extra = reinterpret_cast<unsigned char *>(flags + 8);
     }
 };
 
@@ -384,8 +416,13 @@ __device__ __forceinline__ staged_ctx staged_setup(const staged_params &p, stage
         const int g0 = t0 * p.T0 + i0, g1 = t1 * p.T1 + i1, g2 = t2 * p.T2 + i2;
         cx.par = (i0 + i1 + i2) & 1;
         cx.active = (g0 < p.D0 && g1 < p.D1 && g2 < p.D2);
-        if (cx.active) {
-            cx.v = ((int64_t)g2 * p.D1 + g1) * p.D0 + g0;
+        // 512-voxel tiles: a voxel past the grid stands in for the tile's
+        // first voxel (always inside the grid) -- same position and delays,
+        // weight 0, no output -- so every thread's taps stay inside the
+        // windows the producer bounds from the tile's voxels
+        const int64_t v_first = ((int64_t)(t2 * p.T2) * p.D1 + t1 * p.T1) * p.D0 + t0 * p.T0;
+        if (cx.active || vt == 2) {
+            cx.v = cx.active ? ((int64_t)g2 * p.D1 + g1) * p.D0 + g0 : v_first;
             cx.vx = __ldg(p.dstpos + 3 * cx.v);
             cx.vy = __ldg(p.dstpos + 3 * cx.v + 1);
             cx.vz = __ldg(p.dstpos + 3 * cx.v + 2);
@@ -395,12 +432,10 @@ __device__ __forceinline__ staged_ctx staged_setup(const staged_params &p, stage
             const int j0 = lt2 % p.T0, j1 = (lt2 / p.T0) % p.T1, j2 = lt2 / (p.T0 * p.T1);
             const int h0 = t0 * p.T0 + j0, h1 = t1 * p.T1 + j1, h2 = t2 * p.T2 + j2;
             cx.active2 = (h0 < p.D0 && h1 < p.D1 && h2 < p.D2);
-            if (cx.active2) {
-                cx.v2 = ((int64_t)h2 * p.D1 + h1) * p.D0 + h0;
-                cx.vx2 = __ldg(p.dstpos + 3 * cx.v2);
-                cx.vy2 = __ldg(p.dstpos + 3 * cx.v2 + 1);
-                cx.vz2 = __ldg(p.dstpos + 3 * cx.v2 + 2);
-            }
+            cx.v2 = cx.active2 ? ((int64_t)h2 * p.D1 + h1) * p.D0 + h0 : v_first;
+            cx.vx2 = __ldg(p.dstpos + 3 * cx.v2);
+            cx.vy2 = __ldg(p.dstpos + 3 * cx.v2 + 1);
+            cx.vz2 = __ldg(p.dstpos + 3 * cx.v2 + 2);
         }
     }
     if (cx.tid == 0) {
@@ -419,6 +454,7 @@ __device__ __forceinline__ staged_ctx staged_setup(const staged_params &p, stage
             const int slot = i / zwords, word = i - slot * zwords;
             reinterpret_cast<uint32_t *>(sm.ring + slot * SG::bytes + SG::data_bytes)[word] = 0u;
         }
+        for (int i = cx.tid; i < SG::bytes / 4; i += kStThreads) reinterpret_cast<uint32_t *>(sm.zslot)[i] = 0u;
     }
     if (!cx.producer) {
         float mn[3] = {cx.active ? cx.vx : INFINITY, cx.active ? cx.vy : INFINITY, cx.active ? cx.vz : INFINITY};
@@ -502,6 +538,93 @@ __device__ __forceinline__ void staged_pass_begin(const staged_params &p, staged
     __syncthreads();
 }
 
+// Channel bounding box of this CTA's channel slice (sm.cbox), whether every
+// voxel position of the tile and every channel position is finite
+// (sm.flags[1]), and the number of voxels of the tile inside the grid (the
+// return value, on every thread).  Called once after staged_setup.
+template <int K, int WB>
+__device__ __forceinline__ int staged_tile_bounds(const staged_params &p, staged_smem<K, WB> &sm,
+                                                  const staged_ctx &cx) {
+    bool fin = true;
+    if (!cx.producer) {
+        float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int c = chan_begin(p) + cx.tid; c < chan_end(p); c += kStConsumers) {
+            const float q[3] = {__ldg(p.srcpos + 3 * c), __ldg(p.srcpos + 3 * c + 1), __ldg(p.srcpos + 3 * c + 2)};
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                fin &= isfinite(q[a]);
+                mn[a] = fminf(mn[a], q[a]);
+                mx[a] = fmaxf(mx[a], q[a]);
+            }
+        }
+        fin &= isfinite(cx.vx) && isfinite(cx.vy) && isfinite(cx.vz) && isfinite(cx.vx2) && isfinite(cx.vy2) &&
+               isfinite(cx.vz2);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
+                mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
+            }
+        }
+        if (cx.lane == 0) {
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                sm.red[(cx.warp * 16 + a) * 2] = mn[a];
+                sm.red[(cx.warp * 16 + a) * 2 + 1] = mx[a];
+            }
+        }
+    }
+    const int all_fin = __syncthreads_and(fin);
+    const int n_active = __syncthreads_count(cx.active) + __syncthreads_count(cx.active2);
+    if (cx.tid < 3) {
+        float mn = INFINITY, mx = -INFINITY;
+        for (int w = 0; w < kStWarps; w++) {
+            mn = fminf(mn, sm.red[(w * 16 + cx.tid) * 2]);
+            mx = fmaxf(mx, sm.red[(w * 16 + cx.tid) * 2 + 1]);
+        }
+        sm.cbox[cx.tid] = mn;
+        sm.cbox[3 + cx.tid] = mx;
+    }
+    if (cx.tid == 0) sm.flags[1] = all_fin;
+    __syncthreads();
+    return n_active;
+}
+
+// Pass flags (kPassSkip, kPassFast) from the tile's per-event delay range, the
+// tile's box and the channel box.  A tap's sample index is floor(tau) with
+// tau = offset + |v - c|: the distance between the two boxes bounds |v - c|
+// from below and above, so when every event of the pass has offset + the
+// lower bound at or past N - 1 (or offset + the upper bound below 0), no tap
+// of the pass lies inside the record and the pass adds exactly nothing.  The
+// margin covers the FP32 rounding of tau, rsqrt included (< 1 sample below
+// 2^20).
+template <int K, int WB>
+__device__ __forceinline__ int pass_flags(const staged_params &p, const staged_smem<K, WB> &sm, int sc, int SC,
+                                          bool anybad) {
+    float gmin = 0.f, gmax = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float amin = sm.aabb[a], amax = sm.aabb[3 + a], cmin = sm.cbox[a], cmax = sm.cbox[3 + a];
+        const float gap = fmaxf(fmaxf(cmin - amax, amin - cmax), 0.f);
+        const float ext = fmaxf(fabsf(cmax - amin), fabsf(amax - cmin));
+        gmin += gap * gap;
+        gmax += ext * ext;
+    }
+    const float dmin = sqrtf(gmin), dmax = sqrtf(gmax);
+    const bool boxes_ok = sm.flags[1] != 0 && dmax == dmax && dmax <= kSaneRange;
+    bool skip = !anybad && boxes_ok;
+    bool fast = !anybad && boxes_ok && sc == SC && !p.sparse_idx && !p.srcdir;
+    for (int j = 0; j < sc; j++) {
+        const float lo = sm.ofs_lo[j], hi = sm.ofs_hi[j];
+        if (lo == INFINITY) { fast = false; continue; }   // no delay of this event is present
+        const float marg = 4.f + 1e-5f * (fabsf(lo) + fabsf(hi) + dmax);
+        skip &= (lo + dmin - marg >= (float)(p.N - 1)) || (hi + dmax + marg < 0.f);
+        fast &= fabsf(lo) <= kSaneRange && fabsf(hi) <= kSaneRange;
+    }
+    return (skip ? kPassSkip : 0) | (fast ? kPassFast : 0);
+}
+
 // staged_pass_begin for two voxels per thread: delays and weights as
 // (voxel 1, voxel 2) pairs; the per-event delay range covers both.
 template <int K, int WB, int SC>
@@ -518,20 +641,17 @@ __device__ __forceinline__ void staged_pass_begin2(const staged_params &p, stage
             w2[j] = make_float2(0.f, 0.f);
         }
         if (!p.sparse_idx) {
+            // a voxel past the grid stands in for the tile's first voxel
+            // (staged_setup): its delays, weight 0
 #pragma unroll
             for (int j = 0; j < SC; j++) {
                 if (j < sc) {
                     const int64_t base = (int64_t)(e0 + j) * p.V;
-                    if (cx.active) {
-                        ofs2[j].x = __ldg(p.offsets + base + cx.v);
-                        w2[j].x = __ldg(p.weights + base + cx.v);
-                        present |= 1u << (2 * j);
-                    }
-                    if (cx.active2) {
-                        ofs2[j].y = __ldg(p.offsets + base + cx.v2);
-                        w2[j].y = __ldg(p.weights + base + cx.v2);
-                        present |= 2u << (2 * j);
-                    }
+                    ofs2[j].x = __ldg(p.offsets + base + cx.v);
+                    w2[j].x = cx.active ? __ldg(p.weights + base + cx.v) : 0.f;
+                    ofs2[j].y = __ldg(p.offsets + base + cx.v2);
+                    w2[j].y = cx.active2 ? __ldg(p.weights + base + cx.v2) : 0.f;
+                    present |= 3u << (2 * j);
                 }
             }
         } else {
@@ -562,10 +682,13 @@ __device__ __forceinline__ void staged_pass_begin2(const staged_params &p, stage
                 }
             }
         }
+        bool bad = false;   // a present delay that is not finite (its tap is NaN)
 #pragma unroll
         for (int j = 0; j < SC; j++) {
-            const bool oka = ((present >> (2 * j)) & 1u) && isfinite(ofs2[j].x);
-            const bool okb = ((present >> (2 * j)) & 2u) && isfinite(ofs2[j].y);
+            const bool pa = (present >> (2 * j)) & 1u, pb = (present >> (2 * j)) & 2u;
+            const bool oka = pa && isfinite(ofs2[j].x);
+            const bool okb = pb && isfinite(ofs2[j].y);
+            bad |= (pa && !oka) || (pb && !okb);
             float lo = fminf(oka ? ofs2[j].x : INFINITY, okb ? ofs2[j].y : INFINITY);
             float hi = fmaxf(oka ? ofs2[j].x : -INFINITY, okb ? ofs2[j].y : -INFINITY);
 #pragma unroll
@@ -578,6 +701,8 @@ __device__ __forceinline__ void staged_pass_begin2(const staged_params &p, stage
                 sm.red[(cx.warp * 16 + j) * 2 + 1] = hi;
             }
         }
+        bad = __any_sync(0xffffffffu, bad);
+        if (cx.lane == 0) sm.red[(cx.warp * 16 + 15) * 2] = bad ? 1.f : 0.f;
         consumer_sync();
         if (cx.tid < SC) {
             float lo = INFINITY, hi = -INFINITY;
@@ -588,6 +713,14 @@ __device__ __forceinline__ void staged_pass_begin2(const staged_params &p, stage
             sm.ofs_lo[cx.tid] = lo;
             sm.ofs_hi[cx.tid] = hi;
         }
+        consumer_sync();
+        if (cx.tid == 0) {
+            bool anybad = false;
+            for (int ww = 0; ww < kStWarps; ww++) anybad |= sm.red[(ww * 16 + 15) * 2] != 0.f;
+            // two words by pass parity: a skipped pass has no barrier after
+            // its threads read the flags, so the next pass writes the other word
+            sm.flags[2 + ((e0 / SC) & 1)] = pass_flags(p, sm, sc, SC, anybad);
+        }
     }
     __syncthreads();
 }
@@ -595,7 +728,13 @@ __device__ __forceinline__ void staged_pass_begin2(const staged_params &p, stage
 // Producer warp: stage the windows of CC channels x SC events of one chunk.
 // Publishes, with the full barrier's arrival, the window metadata, the
 // overflow flag and the channel table of the stage.
-template <int K, int WB, int SC>
+//
+// With FAST (the 512-voxel kernel) it also publishes each window's address
+// bias and the stage's mode (kStageEmpty, kStageFast): a window whose whole
+// tap range -- [lo + 1, hi - 1] at most, see below -- fits its slot gets
+// bias = slot - pair_bytes * (bits(1.5 * 2^23) + k0); a zero window (no pair
+// row data in range) whose tap range fits one slot points at the zero slot.
+template <int K, int WB, int SC, bool FAST = false>
 __device__ __forceinline__ void staged_produce(const staged_params &p, const CUtensorMap *tmap,
                                                staged_smem<K, WB> &sm, const staged_ctx &cx, int stage,
                                                uint32_t phase, int e0, int sc, int c0, bool &dead,
@@ -612,8 +751,9 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
     // the consumers' bounded waits must expire.
     const bool drop = p.debug_drop_stage && e0 == 0 && c0 == 0;
     if (drop) dead = true;
-    bool issued = false, overflow = false;
+    bool issued = false, overflow = false, mappable = false;
     int k0w = 0;
+    uint32_t bias = 0u;
     if (!dead) {
         const int cl = lane / SC, j = lane % SC;
         const int c = c0 + cl;
@@ -644,6 +784,9 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
             const float rmax = sqrtf(ex * ex + ey * ey + ez * ez);
             const float lo = floorf(sm.ofs_lo[j] + rmin) - 2.f;
             const float hi = floorf(sm.ofs_hi[j] + rmax) + 2.f;
+            // Every tap's floor(tau) lies in [lo + 1, hi - 1] when the delays,
+            // distances and tau stay below 2^20 in magnitude (rounding < 1 sample).
+            const bool sane = fabsf(lo) <= kSaneRange && fabsf(hi) <= kSaneRange && rmax <= kSaneRange;
             // a window that misses the pair row entirely stays a zero window
             if (lo == lo && hi == hi && hi >= 0.f && lo < (float)p.npad) {
                 const int k0 = ((int)fmaxf(lo, -(float)WB)) & ~(staged_traits<K>::align_pairs - 1);
@@ -657,16 +800,28 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
                     k0w = k0;
                     m = kFloorMagicBits + (uint32_t)k0;
                     issued = true;
+                    if constexpr (FAST) {
+                        // the slot holds every tap only when neither end was clipped
+                        mappable = sane && (float)k0 <= lo && hi <= (float)(k0 + WB - 1);
+                        bias = smem_u32(stage_base + lane * SG::bytes) -
+                               (uint32_t)sizeof(st) * (kFloorMagicBits + (uint32_t)k0);
+                    }
                 } else {
                     m = kOvf;
                     overflow = true;
                 }
+            } else if (FAST && sane && hi - lo + 1.f <= (float)WB) {
+                // zero window: its taps read the zero slot
+                mappable = true;
+                bias = smem_u32(sm.zslot) - (uint32_t)sizeof(st) * (kFloorMagicBits + (uint32_t)(int)lo);
             }
         }
         sm.meta[stage * kStWin + lane] = m;
+        if constexpr (FAST) sm.bias[stage * kStWin + lane] = bias;
     }
     const unsigned issued_ballot = __ballot_sync(0xffffffffu, issued);
     const unsigned ovf_ballot = __ballot_sync(0xffffffffu, overflow);
+    const unsigned fast_ballot = __ballot_sync(0xffffffffu, mappable);
     if (p.copy_async && !drop) {
         // The warp copies the issued windows together, 16 bytes per lane per
         // copy: CPW lanes per window, 32 / CPW windows per round, coalesced
@@ -698,6 +853,9 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
     __syncwarp();
     if (lane == 0 && !drop) {
         sm.ovf[stage] = ovf_ballot != 0u;
+        if constexpr (FAST)
+            sm.mode[stage] = ((issued_ballot | ovf_ballot) == 0u ? kStageEmpty : 0) |
+                             (fast_ballot == 0xffffffffu ? kStageFast : 0);
         // the producer's arrival also publishes meta / ovf / channel table (release)
         if (p.copy_async)
             mbar_arrive(full_bar);
@@ -960,12 +1118,25 @@ __global__ void __launch_bounds__(kStThreads) das_staged_kernel(const staged_par
 // unit.  The packed FP32 lanes carry the two voxels (not two events): the
 // delay, floor split and fraction of one event for both voxels are one
 // instruction each, and both taps read the same window.
+//
+// Work that adds nothing is not done:
+//   * a pass (event chunk) whose taps all lie outside the record, for every
+//     voxel of the tile and every channel, is skipped by producer and
+//     consumers alike (pass_flags; deep tiles of a volume past the record);
+//   * a stage whose windows all miss the pair rows (kStageEmpty) is skipped
+//     by the consumers.
+// On stages whose windows each hold their whole tap range (kStageFast, with
+// the pass's kPassFast) a tap's shared address is one multiply-add of the
+// floor bits and the window's bias, with no clamp; other stages clamp the
+// index onto the slot's zero pair as before.  Every variant reads the same
+// pair for every tap, so the image is bit-identical across them.
 template <int K, int SC, int WB>
 __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kernel(const staged_params p,
                                                                   const __grid_constant__ CUtensorMap tmap) {
     using st = typename pair_traits<K>::storage;
     using SG = slot_geom<WB, K>;
     constexpr int CC = kStWin / SC;  // channels per stage
+    constexpr uint32_t PB = (uint32_t)sizeof(st);
     static_assert(kStWin % SC == 0, "SC must divide the stage");
 
     // a das_sparse call whose lists name an event twice runs on the gather
@@ -974,6 +1145,7 @@ __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kerne
     extern __shared__ __align__(128) unsigned char smem_raw[];
     staged_smem<K, WB> sm(smem_raw);
     const staged_ctx cx = staged_setup<K, WB>(p, sm, false, 2);
+    const int n_active = staged_tile_bounds<K, WB>(p, sm, cx);
     const int cbeg = chan_begin(p), cend = chan_end(p);   // this CTA's channel slice
 
     const st *__restrict__ Pg = static_cast<const st *>(p.P);
@@ -983,6 +1155,7 @@ __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kerne
     uint32_t phase = 0;
     bool dead = false;
     uint32_t issued_mask = 0;
+    unsigned long long units = 0ull;      // units evaluated (thread 0 counts)
 
     const uint32_t ring_u32 = smem_u32(sm.ring);
     const uint32_t chan_u32 = smem_u32(sm.chan_pos);
@@ -997,21 +1170,55 @@ __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kerne
         const int sc = min(SC, p.n_events - e0);
         float2 ofs2[SC], w2[SC];
         staged_pass_begin2<K, WB, SC>(p, sm, cx, e0, sc, ofs2, w2);
+        const int pflags = *(volatile int *)&sm.flags[2 + ((e0 / SC) & 1)];
+        if (pflags & kPassSkip) continue;   // uniform: the ring is left as it is
+        const bool pass_fast = (pflags & kPassFast) != 0;
 
         for (int c0 = cbeg; c0 < cend; c0 += CC) {
             if (cx.producer) {
-                staged_produce<K, WB, SC>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
+                staged_produce<K, WB, SC, true>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
             } else {
                 const uint32_t full_bar = smem_u32(&sm.full[stage]);
                 if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
-                if (!dead) {
+                const int mode = dead ? kStageEmpty : *(volatile int *)&sm.mode[stage];
+                if (!(mode & kStageEmpty)) {
+                    if (cx.tid == 0) units += (unsigned long long)min(CC, cend - c0) * sc * n_active;
                     const bool any_ovf = sm.ovf[stage] != 0;
                     const uint32_t stage_u32 = ring_u32 + stage * SG::stage_bytes;
-                    if (!any_ovf && !p.srcdir) {
-                        // Common case, no per-channel branch.  The channel table's
-                        // (x, x, y, y), (z, z, 0, 0) rows feed the packed geometry
-                        // directly: d = c - v, the exact negative of v - c, so rsq is
-                        // the same as receive_geometry's.  Channels past C carry a
+                    if (pass_fast && (mode & kStageFast)) {
+                        // Every window holds its whole tap range: address =
+                        // bits(floor + magic) * pair_bytes + bias, no clamp.
+#pragma unroll
+                        for (int cl = 0; cl < CC; cl++) {
+                            const float4 qa = lds_f4(pair_u32 + (stage * kStWin + cl) * 32);
+                            const float4 qb = lds_f4(pair_u32 + (stage * kStWin + cl) * 32 + 16);
+                            const float2 dx = __fadd2_rn(make_float2(qa.x, qa.y), nvx2);
+                            const float2 dy = __fadd2_rn(make_float2(qa.z, qa.w), nvy2);
+                            const float2 dz = __fadd2_rn(make_float2(qb.x, qb.y), nvz2);
+                            float2 r2 = __fmul2_rn(dx, dx);
+                            r2 = __ffma2_rn(dy, dy, r2);
+                            r2 = __ffma2_rn(dz, dz, r2);
+                            const float2 rsq2 = make_float2(fmaxf(r2.x, 1e-7f), fmaxf(r2.y, 1e-7f));
+                            const float2 rinv2 = make_float2(rsqrtf(rsq2.x), rsqrtf(rsq2.y));
+                            uint32_t bias[SC];
+                            load_meta<SC>(sm.bias, stage, cl, bias);
+#pragma unroll
+                            for (int j = 0; j < SC; j++) {
+                                const float2 tau2 = __ffma2_rn(rsq2, rinv2, ofs2[j]);
+                                const float2 mm2 = __fadd2_rd(tau2, magic2);
+                                const float2 nfl2 = __ffma2_rn(mm2, neg1, magic2);   // -(floor), exact
+                                const float2 t2 = __fadd2_rn(tau2, nfl2);
+                                const float ta = tap_at<K>(__float_as_uint(mm2.x) * PB + bias[j], t2.x);
+                                const float tb = tap_at<K>(__float_as_uint(mm2.y) * PB + bias[j], t2.y);
+                                acc2 = __ffma2_rn(w2[j], make_float2(ta, tb), acc2);
+                            }
+                        }
+                    } else if (!any_ovf && !p.srcdir) {
+                        // No per-channel branch; tap indices are clamped onto the
+                        // slot's zero pair.  The channel table's (x, x, y, y),
+                        // (z, z, 0, 0) rows feed the packed geometry directly:
+                        // d = c - v, the exact negative of v - c, so rsq is the
+                        // same as receive_geometry's.  Channels past C carry a
                         // zero window: their taps read the zero pair.
 #pragma unroll
                         for (int cl = 0; cl < CC; cl++) {
@@ -1125,6 +1332,7 @@ __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kerne
         return;
     }
     if (dead) return;
+    if (p.units && cx.tid == 0 && units) atomicAdd(p.units, units);
     float *o = static_cast<float *>(p.out) + (int64_t)cx.b * p.out_bstride;
     if (p.cchunk) {   // channel slices add into the prepared image
         if (cx.active) atomicAdd(o + cx.v, acc2.x);

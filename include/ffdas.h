@@ -384,8 +384,17 @@ FFDAS_API ffdas_error_t ffdas_get_last_kernel_info(ffdas_handle_t handle,
 FFDAS_API ffdas_error_t ffdas_set_kernel_timing(ffdas_handle_t handle, int enable);
 FFDAS_API ffdas_error_t ffdas_get_last_kernel_time(ffdas_handle_t handle, float *ms);
 
-/* New: measured FP32 FMA throughput of the current device (TFLOP/s), from a
- * short dependent-FMA kernel on the handle's stream (synchronous). */
+/* New: with kernel timing enabled, the number of voxel x channel x event x
+ * batch units the last call's main kernel actually evaluated (units of
+ * passes and stages it skipped because every tap lies outside the record
+ * are not counted).  Waits for the handle's stream.  FFDAS_ERROR_INVALID_STATE
+ * when timing is off or the last kernel does not count its units (only the
+ * 512-voxel TMA-staged forward does). */
+FFDAS_API ffdas_error_t ffdas_get_last_kernel_units(ffdas_handle_t handle, long long *units);
+
+/* New: measured FP32 FMA throughput of the current device (TFLOP/s): the
+ * faster of a scalar-FMA and a packed-f32x2-FMA kernel of independent chains
+ * on the handle's stream (synchronous). */
 FFDAS_API ffdas_error_t ffdas_measure_fp32_peak(ffdas_handle_t handle, double *tflops);
 
 /* New: device-side status of the handle's kernels since the last query
