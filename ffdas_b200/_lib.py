@@ -138,6 +138,7 @@ SIGNATURES = {
     "ffdas_set_kernel_timing": (c_err, [c_handle, ctypes.c_int]),
     "ffdas_get_last_kernel_time": (c_err, [c_handle, ctypes.POINTER(ctypes.c_float)]),
     "ffdas_get_last_kernel_units": (c_err, [c_handle, ctypes.POINTER(ctypes.c_longlong)]),
+    "ffdas_set_channel_scale": (c_err, [c_handle, c_ptr, ctypes.c_int64]),
     "ffdas_measure_fp32_peak": (c_err, [c_handle, ctypes.POINTER(ctypes.c_double)]),
     "ffdas_get_device_status": (c_err, [c_handle, ctypes.POINTER(ctypes.c_int)]),
     "ffdas_debug_staged_drop_stage": (None, [ctypes.c_int]),
@@ -245,6 +246,10 @@ class Handle:
         ms = ctypes.c_float()
         check(load().ffdas_get_last_kernel_time(self.h, ctypes.byref(ms)))
         return float(ms.value)
+
+    def set_channel_scale(self, scale_ptr, count: int) -> None:
+        """Per-channel scale applied by the ingest of the following calls (device pointer; None clears)."""
+        check(load().ffdas_set_channel_scale(self.h, scale_ptr, int(count) if scale_ptr else 0))
 
     def last_kernel_units(self):
         """Units the last timed call's kernel evaluated, or None when it does not count them."""

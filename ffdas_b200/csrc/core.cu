@@ -229,6 +229,14 @@ ffdas_error_t ffdas_destroy(ffdas_handle_t h) {
     return err;
 }
 
+ffdas_error_t ffdas_set_channel_scale(ffdas_handle_t h, const float *scale, int64_t count) {
+    if (!h) return FFDAS_ERROR_INVALID_HANDLE;
+    if (scale && count <= 0) return FFDAS_ERROR_INVALID_ARGUMENT;
+    h->chan_scale = scale;
+    h->chan_scale_count = scale ? count : 0;
+    return FFDAS_SUCCESS;
+}
+
 ffdas_error_t ffdas_set_stream(ffdas_handle_t h, uintptr_t stream) {
     if (!h) return FFDAS_ERROR_INVALID_HANDLE;
     h->stream = reinterpret_cast<cudaStream_t>(stream);

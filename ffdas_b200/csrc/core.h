@@ -57,6 +57,10 @@ struct ffdas_context {
     bool timing = false;
     bool timing_recorded = false;
     bool units_recorded = false;   // the last timed kernel counted its units
+    // per-channel gain applied by the ingest (ffdas_set_channel_scale): a
+    // caller-owned device array of chan_scale_count floats, or null
+    const float *chan_scale = nullptr;
+    int64_t chan_scale_count = 0;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     // eigensolver state of ffdas_truncate_rank, created on its first call and
     // released with the handle

@@ -141,7 +141,7 @@ static size_t storage_bytes(int kind) {
 // ---------------------------------------------------------------- ingest ---
 template <typename Tin, int K>
 static ffdas_error_t launch_ingest_t(ffdas_context &h, const das_problem &pb, const void *x,
-                                     int64_t npad, void *P) {
+                                     int64_t npad, void *P, const float *gain, int gain_bstride) {
     const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
     if (rows == 0) return FFDAS_SUCCESS;
     const int64_t bc = (int64_t)pb.B * pb.C;
@@ -151,52 +151,75 @@ static ffdas_error_t launch_ingest_t(ffdas_context &h, const das_problem &pb, co
               (unsigned)std::min<int64_t>(bc, 65535));
     ingest_pairs_kernel<Tin, K><<<grid, kIngestThreads, 0, h.stream>>>(
         static_cast<const Tin *>(x), pb.x_bstride, pb.x_cstride, pb.x_sstride, pb.C, pb.S, pb.N,
-        (int)bc, npad, static_cast<typename pair_traits<K>::storage *>(P));
+        (int)bc, npad, static_cast<typename pair_traits<K>::storage *>(P), gain, gain_bstride);
     return ffdas_launch_check(h.stream);
+}
+
+// Per-channel gain of the handle (ffdas_set_channel_scale) for a problem:
+// the pointer and its batch stride, or an error when its length fits neither
+// C nor B * C.
+static ffdas_error_t channel_gain(const ffdas_context &h, const das_problem &pb, const float **gain, int *bstride) {
+    *gain = nullptr;
+    *bstride = 0;
+    if (!h.chan_scale) return FFDAS_SUCCESS;
+    if (h.chan_scale_count == (int64_t)pb.C) {
+        *bstride = 0;
+    } else if (h.chan_scale_count == (int64_t)pb.B * pb.C) {
+        *bstride = pb.C;
+    } else {
+        return FFDAS_ERROR_INVALID_ARGUMENT;
+    }
+    *gain = h.chan_scale;
+    return FFDAS_SUCCESS;
 }
 
 static ffdas_error_t launch_ingest(ffdas_context &h, const das_problem &pb, ffdas_datatype_t xt,
                                    int kind, const void *x, int64_t npad, void *P) {
+    const float *gain = nullptr;
+    int gain_bstride = 0;
+    FFDAS_TRY(channel_gain(h, pb, &gain, &gain_bstride));
+#define FFDAS_INGEST(Tin, K) launch_ingest_t<Tin, K>(h, pb, x, npad, P, gain, gain_bstride)
     switch (xt) {
         case FFDAS_R_32F:
-            if (kind == ST_F32) return launch_ingest_t<float, ST_F32>(h, pb, x, npad, P);
-            if (kind == ST_F16) return launch_ingest_t<float, ST_F16>(h, pb, x, npad, P);
-            if (kind == ST_BF16) return launch_ingest_t<float, ST_BF16>(h, pb, x, npad, P);
+            if (kind == ST_F32) return FFDAS_INGEST(float, ST_F32);
+            if (kind == ST_F16) return FFDAS_INGEST(float, ST_F16);
+            if (kind == ST_BF16) return FFDAS_INGEST(float, ST_BF16);
             break;
         case FFDAS_R_16F:
-            if (kind == ST_F32) return launch_ingest_t<__half, ST_F32>(h, pb, x, npad, P);
-            if (kind == ST_F16) return launch_ingest_t<__half, ST_F16>(h, pb, x, npad, P);
-            if (kind == ST_BF16) return launch_ingest_t<__half, ST_BF16>(h, pb, x, npad, P);
+            if (kind == ST_F32) return FFDAS_INGEST(__half, ST_F32);
+            if (kind == ST_F16) return FFDAS_INGEST(__half, ST_F16);
+            if (kind == ST_BF16) return FFDAS_INGEST(__half, ST_BF16);
             break;
         case FFDAS_R_16I:
-            if (kind == ST_F32) return launch_ingest_t<int16_t, ST_F32>(h, pb, x, npad, P);
-            if (kind == ST_F16) return launch_ingest_t<int16_t, ST_F16>(h, pb, x, npad, P);
-            if (kind == ST_BF16) return launch_ingest_t<int16_t, ST_BF16>(h, pb, x, npad, P);
+            if (kind == ST_F32) return FFDAS_INGEST(int16_t, ST_F32);
+            if (kind == ST_F16) return FFDAS_INGEST(int16_t, ST_F16);
+            if (kind == ST_BF16) return FFDAS_INGEST(int16_t, ST_BF16);
             break;
         case FFDAS_R_16BF:
-            if (kind == ST_F32) return launch_ingest_t<__nv_bfloat16, ST_F32>(h, pb, x, npad, P);
-            if (kind == ST_BF16) return launch_ingest_t<__nv_bfloat16, ST_BF16>(h, pb, x, npad, P);
-            if (kind == ST_F16) return launch_ingest_t<__nv_bfloat16, ST_F16>(h, pb, x, npad, P);
+            if (kind == ST_F32) return FFDAS_INGEST(__nv_bfloat16, ST_F32);
+            if (kind == ST_BF16) return FFDAS_INGEST(__nv_bfloat16, ST_BF16);
+            if (kind == ST_F16) return FFDAS_INGEST(__nv_bfloat16, ST_F16);
             break;
         case FFDAS_R_64F:
-            if (kind == ST_F64) return launch_ingest_t<double, ST_F64>(h, pb, x, npad, P);
-            if (kind == ST_F32) return launch_ingest_t<double, ST_F32>(h, pb, x, npad, P);
+            if (kind == ST_F64) return FFDAS_INGEST(double, ST_F64);
+            if (kind == ST_F32) return FFDAS_INGEST(double, ST_F32);
             break;
         case FFDAS_C_32F:
-            if (kind == ST_C32) return launch_ingest_t<float2, ST_C32>(h, pb, x, npad, P);
-            if (kind == ST_C16) return launch_ingest_t<float2, ST_C16>(h, pb, x, npad, P);
+            if (kind == ST_C32) return FFDAS_INGEST(float2, ST_C32);
+            if (kind == ST_C16) return FFDAS_INGEST(float2, ST_C16);
             break;
         case FFDAS_C_16F:
-            if (kind == ST_C16) return launch_ingest_t<__half2, ST_C16>(h, pb, x, npad, P);
+            if (kind == ST_C16) return FFDAS_INGEST(__half2, ST_C16);
             break;
         case FFDAS_C_64F:
-            if (kind == ST_C64) return launch_ingest_t<double2, ST_C64>(h, pb, x, npad, P);
-            if (kind == ST_C32) return launch_ingest_t<double2, ST_C32>(h, pb, x, npad, P);
+            if (kind == ST_C64) return FFDAS_INGEST(double2, ST_C64);
+            if (kind == ST_C32) return FFDAS_INGEST(double2, ST_C32);
             break;
         default:
             break;
     }
     return FFDAS_ERROR_INTERNAL;
+#undef FFDAS_INGEST
 }
 
 ffdas_error_t ingest_for_backward(ffdas_context &h, const das_problem &pb, ffdas_datatype_t xt, int kind,
@@ -443,8 +466,16 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
     // the handle's counter, cleared here, before the timed launch
     if (h.timing && h.unit_count) FFDAS_CUDA(cudaMemsetAsync(h.unit_count, 0, sizeof(unsigned long long), h.stream));
 
+    // a channel scale of the wrong length fails before anything is launched
+    {
+        const float *g = nullptr;
+        int gb = 0;
+        FFDAS_TRY(channel_gain(h, pb, &g, &gb));
+    }
+
     // ---- small problems: the whole call as one launch straight from x ----
-    if (direct_supported(pb, xd.dtype, od.dtype, kind)) {
+    // (it reads x in place, so not with a channel scale, which the ingest applies)
+    if (!h.chan_scale && direct_supported(pb, xd.dtype, od.dtype, kind)) {
         const bool asked = h.has_config && h.config.variant == 5;
         const bool planner = !h.has_config || h.config.variant == 0;
         const int64_t units = pb.V * pb.C * (int64_t)pb.S * pb.B;

@@ -278,6 +278,8 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
                            const void *gout, float *gx, float *goff, float *gw, float *gdst, float *gsrc) {
     const ffdas_tensor_desc &xd = *a.x_desc;
     if (a.srcdir != nullptr || a.wavenum != 0.f) return FFDAS_ERROR_INVALID_ARGUMENT;
+    // the adjoint of a channel-scaled forward is not provided: clear the scale
+    if (h.chan_scale) return FFDAS_ERROR_INVALID_ARGUMENT;
     if (gd.dtype != FFDAS_R_32F) return FFDAS_ERROR_UNSUPPORTED_TYPE;
     const int kind = select_storage(xd.dtype, FFDAS_R_32F, a.compute_type, xd.ndim == 4 ? (int)xd.dims[0] : 1);
     if (kind != ST_F32 && kind != ST_F16 && kind != ST_BF16) return FFDAS_ERROR_UNSUPPORTED_TYPE;

@@ -142,6 +142,13 @@ template <> struct sample_io<float2> { using w = float2; __device__ static w loa
 template <> struct sample_io<double2> { using w = double2; __device__ static w load(const double2 *p) { return __ldg(p); } };
 template <> struct sample_io<__half2> { using w = float2; __device__ static w load(const __half2 *p) { return __half22float2(*p); } };
 
+// per-channel gain of the ingest, applied to a working scalar in its own
+// precision (FP32, or FP64 for FP64 data; both components of complex samples)
+__device__ __forceinline__ float scaled(float v, float g) { return v * g; }
+__device__ __forceinline__ double scaled(double v, float g) { return v * (double)g; }
+__device__ __forceinline__ float2 scaled(float2 v, float g) { return make_float2(v.x * g, v.y * g); }
+__device__ __forceinline__ double2 scaled(double2 v, float g) { return make_double2(v.x * (double)g, v.y * (double)g); }
+
 // conversion of a working scalar to the storage kind's make() argument type
 __device__ __forceinline__ float2 to_c32(float2 v) { return v; }
 __device__ __forceinline__ float2 to_c32(double2 v) { return make_float2((float)v.x, (float)v.y); }
@@ -187,12 +194,16 @@ struct alignas(sizeof(S) * kIngestVec >= 16 ? 16 : sizeof(S) * kIngestVec) pair_
     S v[kIngestVec];
 };
 
+// With `gain` set, sample k of row (b, c, s) enters as gain[b * gain_bstride + c]
+// times its value (a per-channel scale: ADC gains, or 1 / peak to normalise
+// each channel before 16-bit storage).
 template <typename Tin, int K>
 __global__ void __launch_bounds__(kIngestThreads) ingest_pairs_kernel(
     const Tin *__restrict__ x, int64_t bstride, int64_t cstride, int64_t sstride,
     int C, int S, int N, int BC, int64_t Npad,
-    typename pair_traits<K>::storage *__restrict__ P) {
+    typename pair_traits<K>::storage *__restrict__ P, const float *__restrict__ gain, int gain_bstride) {
     using st = typename pair_traits<K>::storage;
+    using W = typename sample_io<Tin>::w;
     static_assert(sizeof(pair_quad<st>) == kIngestVec * sizeof(st), "pair_quad packing");
     const int64_t k0 = ((int64_t)blockIdx.x * kIngestThreads + threadIdx.x) * kIngestVec;
     if (k0 >= Npad) return;   // Npad is a multiple of kIngestVec
@@ -200,21 +211,30 @@ __global__ void __launch_bounds__(kIngestThreads) ingest_pairs_kernel(
         for (int bc = blockIdx.z; bc < BC; bc += gridDim.z) {
             const int c = bc % C, b = bc / C;
             const Tin *xr = x + (int64_t)b * bstride + (int64_t)c * cstride + (int64_t)s * sstride;
+            const float g = gain ? __ldg(gain + (int64_t)b * gain_bstride + c) : 1.f;
             pair_quad<st> q;
             if (k0 + kIngestVec < (int64_t)N) {   // every pair of the quad inside the record
-                typename sample_io<Tin>::w v[kIngestVec + 1];
+                W v[kIngestVec + 1];
 #pragma unroll
                 for (int i = 0; i <= kIngestVec; i++) v[i] = sample_io<Tin>::load(xr + k0 + i);
+                if (gain) {
 #pragma unroll
-                for (int i = 0; i < kIngestVec; i++) q.v[i] = make_pair<K, typename sample_io<Tin>::w>::go(v[i], v[i + 1]);
+                    for (int i = 0; i <= kIngestVec; i++) v[i] = scaled(v[i], g);
+                }
+#pragma unroll
+                for (int i = 0; i < kIngestVec; i++) q.v[i] = make_pair<K, W>::go(v[i], v[i + 1]);
             } else {
 #pragma unroll
                 for (int i = 0; i < kIngestVec; i++) {
                     const int64_t k = k0 + i;
                     if (k < (int64_t)N - 1) {
-                        auto a = sample_io<Tin>::load(xr + k);
-                        auto bb = sample_io<Tin>::load(xr + k + 1);
-                        q.v[i] = make_pair<K, decltype(a)>::go(a, bb);
+                        W a = sample_io<Tin>::load(xr + k);
+                        W bb = sample_io<Tin>::load(xr + k + 1);
+                        if (gain) {
+                            a = scaled(a, g);
+                            bb = scaled(bb, g);
+                        }
+                        q.v[i] = make_pair<K, W>::go(a, bb);
                     } else {
                         memset(&q.v[i], 0, sizeof(st));
                     }

@@ -865,6 +865,159 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
     if (!dead) issued_mask |= (1u << stage);
 }
 
+// Producer warp of the 512-voxel kernel: all stages of one pass.  Per stage
+// the same windows, metadata, address biases and modes as staged_produce<FAST>,
+// but the work that needs no ring slot is done before waiting for the slot:
+// the channel positions are loaded one stage ahead, and each lane's window
+// bounds (its event's delay range and the tile box are pass constants held in
+// registers) are computed from them; only the stores, the copies and the
+// arrival wait for the consumers to release the slot.  The distance bounds
+// use x * rsqrt(x) (relative error a few 1e-7, far inside the windows'
+// two-sample margins).
+template <int K, int WB, int SC>
+__device__ __forceinline__ void staged_produce_pass2(const staged_params &p, const CUtensorMap *tmap,
+                                                     staged_smem<K, WB> &sm, const staged_ctx &cx, int &stage,
+                                                     uint32_t &phase, int e0, int sc, bool &dead,
+                                                     uint32_t &issued_mask) {
+    using SG = slot_geom<WB, K>;
+    using st = typename pair_traits<K>::storage;
+    constexpr int CC = kStWin / SC;
+    constexpr uint32_t PB = (uint32_t)sizeof(st);
+    const int cbeg = chan_begin(p), cend = chan_end(p);
+    const int lane = cx.lane, cl = lane / SC, j = lane % SC;
+    const bool jv = j < sc;
+    const float olo = sm.ofs_lo[j], ohi = sm.ofs_hi[j];
+    const float ax0 = sm.aabb[0], ay0 = sm.aabb[1], az0 = sm.aabb[2];
+    const float ax1 = sm.aabb[3], ay1 = sm.aabb[4], az1 = sm.aabb[5];
+    const uint32_t zslot_u32 = smem_u32(sm.zslot);
+    int c = cbeg + cl;
+    float px = 0.f, py = 0.f, pz = 0.f;
+    if (c < cend) {
+        px = __ldg(p.srcpos + 3 * c);
+        py = __ldg(p.srcpos + 3 * c + 1);
+        pz = __ldg(p.srcpos + 3 * c + 2);
+    }
+    for (int c0 = cbeg; c0 < cend; c0 += CC) {
+        // the next stage's channel position, in flight while this stage is built
+        const int cn = c + CC;
+        float qx = 0.f, qy = 0.f, qz = 0.f;
+        if (cn < cend) {
+            qx = __ldg(p.srcpos + 3 * cn);
+            qy = __ldg(p.srcpos + 3 * cn + 1);
+            qz = __ldg(p.srcpos + 3 * cn + 2);
+        }
+        // this lane's window of (channel c, event e0 + j): registers only
+        uint32_t m = kZeroWindow;   // every tap index clamps to the zero pair
+        bool issue = false, overflow = false, mappable = false, zero_map = false;
+        int k0 = 0;
+        if (c < cend && jv) {
+            const float dx = fmaxf(fmaxf(ax0 - px, px - ax1), 0.f);
+            const float dy = fmaxf(fmaxf(ay0 - py, py - ay1), 0.f);
+            const float dz = fmaxf(fmaxf(az0 - pz, pz - az1), 0.f);
+            const float ex = fmaxf(fabsf(px - ax0), fabsf(px - ax1));
+            const float ey = fmaxf(fabsf(py - ay0), fabsf(py - ay1));
+            const float ez = fmaxf(fabsf(pz - az0), fabsf(pz - az1));
+            const float n2 = dx * dx + dy * dy + dz * dz, x2 = ex * ex + ey * ey + ez * ez;
+            const float rmin = n2 > 0.f ? n2 * rsqrtf(n2) : 0.f;
+            const float rmax = x2 > 0.f ? x2 * rsqrtf(x2) : 0.f;
+            const float lo = floorf(olo + rmin) - 2.f;
+            const float hi = floorf(ohi + rmax) + 2.f;
+            // Every tap's floor(tau) lies in [lo + 1, hi - 1] when the delays,
+            // distances and tau stay below 2^20 in magnitude (rounding < 1 sample).
+            const bool sane = fabsf(lo) <= kSaneRange && fabsf(hi) <= kSaneRange && rmax <= kSaneRange;
+            if (lo == lo && hi == hi && hi >= 0.f && lo < (float)p.npad) {   // the window meets the pair row
+                k0 = ((int)fmaxf(lo, -(float)WB)) & ~(staged_traits<K>::align_pairs - 1);
+                const int k1 = (int)fminf(hi, (float)p.npad + WB);
+                if (k1 - k0 + 1 <= WB) {
+                    issue = true;
+                    m = kFloorMagicBits + (uint32_t)k0;
+                    // the slot holds every tap only when neither end was clipped
+                    mappable = sane && (float)k0 <= lo && hi <= (float)(k0 + WB - 1);
+                } else {
+                    m = kOvf;
+                    overflow = true;
+                }
+            } else if (sane && hi - lo + 1.f <= (float)WB) {
+                // zero window: its taps read the zero slot
+                mappable = zero_map = true;
+                k0 = (int)lo;
+            }
+        }
+
+        const uint32_t full_bar = smem_u32(&sm.full[stage]);
+        const uint32_t empty_bar = smem_u32(&sm.empty[stage]);
+        unsigned char *stage_base = sm.ring + stage * SG::stage_bytes;
+        if (!dead && !bounded_wait(empty_bar, phase ^ 1u, sm.abort_flag, p.status)) dead = true;
+        // Test hook: leave the very first stage unfilled (no copy, no arrival) so
+        // the consumers' bounded waits must expire.
+        const bool drop = p.debug_drop_stage && e0 == 0 && c0 == 0;
+        if (drop) dead = true;
+        if (dead) issue = overflow = mappable = false;
+        if (!dead) {
+            if (j == 0) {
+                sm.chan_pos[stage * kStWin + cl] = make_float4(px, py, pz, 0.f);
+                sm.chan_pair[(stage * kStWin + cl) * 2] = make_float4(px, px, py, py);
+                sm.chan_pair[(stage * kStWin + cl) * 2 + 1] = make_float4(pz, pz, 0.f, 0.f);
+                if (p.srcdir)
+                    sm.chan_dir[stage * kStWin + cl] = (c < cend) ? __ldg(p.srcdir + c) : make_float4(0, 0, 0, 2.f);
+            }
+            const uint32_t slot_u32 = smem_u32(stage_base + lane * SG::bytes);
+            if (issue && !p.copy_async) {
+                const int row = (cx.b * p.C + c) * p.S + (e0 + j);
+                tma_load_row(slot_u32, tmap, k0 * staged_traits<K>::tma_units, row, full_bar);
+            }
+            sm.meta[stage * kStWin + lane] = m;
+            sm.bias[stage * kStWin + lane] = (zero_map ? zslot_u32 : slot_u32) - PB * (kFloorMagicBits + (uint32_t)k0);
+        }
+        const unsigned issued_ballot = __ballot_sync(0xffffffffu, issue);
+        const unsigned ovf_ballot = __ballot_sync(0xffffffffu, overflow);
+        const unsigned fast_ballot = __ballot_sync(0xffffffffu, mappable);
+        if (p.copy_async && !drop) {
+            // The warp copies the issued windows together, 16 bytes per lane per
+            // copy (as in staged_produce).
+            constexpr int PBY = (int)sizeof(st);
+            constexpr int CPW = WB * PBY / 16;
+            constexpr int WPR = 32 / CPW;
+            constexpr int PPC = 16 / PBY;
+            static_assert(CPW >= 1 && CPW <= 32 && 32 % CPW == 0, "window must split into lane chunks");
+            const uint32_t stage_u32 = smem_u32(stage_base);
+            const char *Pb = static_cast<const char *>(p.P);
+            const int q = lane % CPW;
+#pragma unroll 1
+            for (int it = 0; it < CPW; it++) {
+                const int w = it * WPR + lane / CPW;
+                const int kw = __shfl_sync(0xffffffffu, k0, w);
+                if ((issued_ballot >> w) & 1u) {
+                    const int64_t row = ((int64_t)cx.b * p.C + c0 + w / SC) * p.S + e0 + w % SC;
+                    const int kp = kw + q * PPC;
+                    const bool in_row = kp >= 0 && (int64_t)kp < p.npad;
+                    const char *src = Pb + (row * p.npad + (in_row ? kp : 0)) * PBY;
+                    cp_async16(stage_u32 + w * SG::bytes + q * 16, src, in_row ? 16u : 0u);
+                }
+            }
+            cp_async_arrive(full_bar);
+        }
+        __syncwarp();
+        if (lane == 0 && !drop) {
+            sm.ovf[stage] = ovf_ballot != 0u;
+            sm.mode[stage] = ((issued_ballot | ovf_ballot) == 0u ? kStageEmpty : 0) |
+                             (fast_ballot == 0xffffffffu ? kStageFast : 0);
+            // the producer's arrival also publishes meta / ovf / channel table (release)
+            if (p.copy_async)
+                mbar_arrive(full_bar);
+            else
+                mbar_arrive_expect_tx(full_bar, (uint32_t)__popc(issued_ballot) * (uint32_t)(WB * sizeof(st)));
+        }
+        if (!dead) issued_mask |= (1u << stage);
+        if (++stage == kStages) {
+            stage = 0;
+            phase ^= 1u;
+        }
+        c = cn;
+        px = qx; py = qy; pz = qz;
+    }
+}
+
 // After an abort the producer waits (bounded, ignoring the abort flag) until
 // every copy its CTA issued has landed, so no TMA write outlives the CTA.
 template <int K, int WB>
@@ -1174,10 +1327,11 @@ __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kerne
         if (pflags & kPassSkip) continue;   // uniform: the ring is left as it is
         const bool pass_fast = (pflags & kPassFast) != 0;
 
+        if (cx.producer) {
+            staged_produce_pass2<K, WB, SC>(p, &tmap, sm, cx, stage, phase, e0, sc, dead, issued_mask);
+        } else {
         for (int c0 = cbeg; c0 < cend; c0 += CC) {
-            if (cx.producer) {
-                staged_produce<K, WB, SC, true>(p, &tmap, sm, cx, stage, phase, e0, sc, c0, dead, issued_mask);
-            } else {
+            {
                 const uint32_t full_bar = smem_u32(&sm.full[stage]);
                 if (!dead && !bounded_wait(full_bar, phase, sm.abort_flag, p.status)) dead = true;
                 const int mode = dead ? kStageEmpty : *(volatile int *)&sm.mode[stage];
@@ -1323,6 +1477,7 @@ __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kerne
                 stage = 0;
                 phase ^= 1u;
             }
+        }
         }
         __syncthreads();
     }

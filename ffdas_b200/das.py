@@ -157,7 +157,7 @@ def _needs_grad(*ts) -> bool:
 
 
 def _run(x, srcpos, dstpos, offsets, weights, sparse_indices, *, srcdir, wavenum, algorithm,
-         use_fp16, use_bf16, channels_trailing, out):
+         use_fp16, use_bf16, channels_trailing, out, channel_scale=None):
     spatial = _check_spatial(dstpos, offsets, weights, sparse_indices)
     xt = _to_torch(x)
     if xt.ndim not in (3, 4):
@@ -192,15 +192,28 @@ def _run(x, srcpos, dstpos, offsets, weights, sparse_indices, *, srcdir, wavenum
                              _FFDAS_DTYPE.get(out_t.dtype, DataType.R_32F))
     L = _lib.load()
     ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
-    if idx_t is None:
-        code = L.ffdas_das(handle.h, ptr(srcpos_t), ptr(srcdir_t), float(wavenum), x_desc.desc, ptr(xt),
-                           ptr(dstpos_t), ptr(offsets_t), ptr(weights_t), ctypes.cast(beta, ctypes.c_void_p),
-                           o_desc.desc, ptr(out_t), int(ctype), int(algorithm))
-    else:
-        code = L.ffdas_das_sparse(handle.h, ptr(srcpos_t), ptr(srcdir_t), float(wavenum), x_desc.desc, ptr(xt),
-                                  ptr(dstpos_t), ptr(offsets_t), ptr(weights_t), int(idx_t.shape[0]), ptr(idx_t),
-                                  ctypes.cast(beta, ctypes.c_void_p), o_desc.desc, ptr(out_t), int(ctype),
-                                  int(algorithm))
+    scale_t = None
+    if channel_scale is not None:
+        scale_t = _astype(channel_scale, torch.float32, dev, "channel_scale")
+        C = xt.shape[-2] if channels_trailing else xt.shape[-3]
+        B = xt.shape[0] if xt.ndim == 4 else 1
+        if scale_t.numel() not in (C, B * C):
+            raise ValueError(f"channel_scale must hold {C} (per channel) or {B * C} (per item and channel) "
+                             f"values, got shape {tuple(scale_t.shape)}")
+        handle.set_channel_scale(scale_t.data_ptr(), scale_t.numel())
+    try:
+        if idx_t is None:
+            code = L.ffdas_das(handle.h, ptr(srcpos_t), ptr(srcdir_t), float(wavenum), x_desc.desc, ptr(xt),
+                               ptr(dstpos_t), ptr(offsets_t), ptr(weights_t), ctypes.cast(beta, ctypes.c_void_p),
+                               o_desc.desc, ptr(out_t), int(ctype), int(algorithm))
+        else:
+            code = L.ffdas_das_sparse(handle.h, ptr(srcpos_t), ptr(srcdir_t), float(wavenum), x_desc.desc,
+                                      ptr(xt), ptr(dstpos_t), ptr(offsets_t), ptr(weights_t), int(idx_t.shape[0]),
+                                      ptr(idx_t), ctypes.cast(beta, ctypes.c_void_p), o_desc.desc, ptr(out_t),
+                                      int(ctype), int(algorithm))
+    finally:
+        if scale_t is not None:
+            handle.set_channel_scale(None, 0)
     _lib.check(code)
     if out is not None:
         return out
@@ -209,7 +222,7 @@ def _run(x, srcpos, dstpos, offsets, weights, sparse_indices, *, srcdir, wavenum
 
 def das(x, srcpos, dstpos, offsets, weights, *, srcdir=None, wavenum: float = 0.0,
         algorithm: Algorithm = Algorithm.DEFAULT, use_fp16: bool = False, use_bf16: bool = False,
-        channels_trailing: bool = False, out=None):
+        channels_trailing: bool = False, out=None, channel_scale=None):
     """Delay-and-sum beamforming, compounding over the sequence dimension.
 
     For each target v:  out[b, v] = sum_s sum_c weights[s, v] *
@@ -230,31 +243,40 @@ def das(x, srcpos, dstpos, offsets, weights, *, srcdir=None, wavenum: float = 0.
         use_bf16: store channel data as bf16 pairs (fp32 interpolation and accumulation).
         channels_trailing: x is ([batch,] sequence, channels, samples).
         out: optional preallocated output.
+        channel_scale: optional per-channel scale, (channels,) or (batch, channels), applied
+            to the channel data as it is stored (ffdas_set_channel_scale): e.g. 1 / peak to
+            normalise each channel before fp16/bf16 storage, or ADC gains of int16 data.
+            Not differentiable.
     """
     if _needs_grad(x, srcpos, dstpos, offsets, weights):
+        if channel_scale is not None:
+            raise NotImplementedError("channel_scale has no backward; apply the scale to x instead")
         from .autograd import das_autograd
         return das_autograd(x, srcpos, dstpos, offsets, weights, None, srcdir=srcdir, wavenum=wavenum,
                             use_fp16=use_fp16, use_bf16=use_bf16, channels_trailing=channels_trailing)
     return _run(x, srcpos, dstpos, offsets, weights, None, srcdir=srcdir, wavenum=wavenum, algorithm=algorithm,
-                use_fp16=use_fp16, use_bf16=use_bf16, channels_trailing=channels_trailing, out=out)
+                use_fp16=use_fp16, use_bf16=use_bf16, channels_trailing=channels_trailing, out=out,
+                channel_scale=channel_scale)
 
 
 def das_sparse(x, srcpos, dstpos, offsets, weights, sparse_indices, *, srcdir=None, wavenum: float = 0.0,
                algorithm: Algorithm = Algorithm.DEFAULT, use_fp16: bool = False, use_bf16: bool = False,
-               channels_trailing: bool = False, out=None):
+               channels_trailing: bool = False, out=None, channel_scale=None):
     """Sparse compounding: each target sums the n events named by sparse_indices (n, ...).
 
     Entries with weight exactly 0 are skipped, so per-target subsets of uneven
     length can be padded with weight 0.  Other arguments as in `das`.
     """
     if _needs_grad(x, srcpos, dstpos, offsets, weights):
+        if channel_scale is not None:
+            raise NotImplementedError("channel_scale has no backward; apply the scale to x instead")
         from .autograd import das_autograd
         return das_autograd(x, srcpos, dstpos, offsets, weights, sparse_indices, srcdir=srcdir,
                             wavenum=wavenum, use_fp16=use_fp16, use_bf16=use_bf16,
                             channels_trailing=channels_trailing)
     return _run(x, srcpos, dstpos, offsets, weights, sparse_indices, srcdir=srcdir, wavenum=wavenum,
                 algorithm=algorithm, use_fp16=use_fp16, use_bf16=use_bf16, channels_trailing=channels_trailing,
-                out=out)
+                out=out, channel_scale=channel_scale)
 
 
 def sparse_select(weights, k: int, offsets=None):

@@ -290,6 +290,21 @@ FFDAS_API ffdas_error_t ffdas_das_backward(
     float *grad_srcpos
 );
 
+/* New: per-channel scale of the channel data, applied by the ingest of every
+ * following ffdas_das / ffdas_das_sparse call on this handle (it replaces the
+ * reference's caller-side cast/copy, src/tensor_ops/contiguous_copy_impl.cuh:
+ * 17-57, with a scaled one): sample k of row (b, c, s) enters as
+ * scale[c] * x[b,c,s,k] when count == C, or scale[b * C + c] * x[b,c,s,k]
+ * when count == B * C, formed in FP32 (FP64 for FP64 data, both parts of
+ * complex samples) and then rounded into the pair storage -- so FP32 or int16
+ * data can be normalised per channel (scale = 1 / peak) before FP16/BF16
+ * storage, or raw ADC samples given their channel gains.  `scale` is a
+ * device array the caller keeps alive while it is set; NULL clears it.  A
+ * call whose C or B * C does not match `count` returns
+ * FFDAS_ERROR_INVALID_ARGUMENT; ffdas_das_backward returns the same while a
+ * scale is set (its adjoint is not provided). */
+FFDAS_API ffdas_error_t ffdas_set_channel_scale(ffdas_handle_t handle, const float *scale, int64_t count);
+
 /* New, no counterpart in the reference: the forward delay-and-sum for callers
  * that cannot allocate device memory (a real-time or embedded host where
  * cudaMalloc is forbidden, a memory budget fixed before the first frame, or a

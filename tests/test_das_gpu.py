@@ -531,3 +531,81 @@ def test_int16_channel_data_gradients():
     ffdas_b200.das(xf, wl["srcpos"], wl["dstpos"], *leavesf).square().sum().backward()
     for a, b in zip(leaves16, leavesf):
         assert oracle.rel_l2(_np(a.grad), _np(b.grad)) < 1e-6
+
+
+# ----------------------------------------------------------- channel scale ---
+# ffdas_set_channel_scale: the ingest multiplies channel c (of item b) by its
+# scale before storing the pairs, so the image is that of scale * x.
+
+@pytest.mark.parametrize("cfg", [None, dict(variant=1), dict(variant=2, tile_x=16, tile_y=16, window=32)],
+                         ids=["planner", "gather", "staged"])
+@pytest.mark.parametrize("per_item", [False, True])
+def test_channel_scale_fp32(cfg, per_item):
+    from ffdas_b200.tune import schedule
+    rng = np.random.default_rng(21)
+    x, src, dst, offs, w = _small(rng, B=3, C=40, S=4, N=128, V=(24, 30))
+    B, C = x.shape[0], x.shape[1]
+    scale = torch.from_numpy(rng.uniform(0.2, 3.0, (B, C) if per_item else (C,)).astype(np.float32)).to(DEV)
+    with schedule(cfg, DEV):
+        got = ffdas_b200.das(x, src, dst, offs, w, channel_scale=scale)
+    xs = _np(x).astype(np.float64) * (_np(scale).astype(np.float64).reshape(B if per_item else 1, C, 1, 1))
+    ref = oracle.das_f64(xs, _np(src), _np(dst), _np(offs), _np(w))
+    assert oracle.rel_l2(_np(got), ref) < TOL[torch.float32]
+    # the setting does not outlive the call
+    plain = ffdas_b200.das(x, src, dst, offs, w)
+    assert oracle.rel_l2(_np(plain), oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w))) < 2e-5
+
+
+def test_channel_scale_int16_gains_and_sparse():
+    # raw ADC samples with per-channel gains, dense and das_sparse
+    wl = W.diverging3d(device=DEV, scale=0.125)
+    g = torch.Generator().manual_seed(5)
+    x16 = (wl["x"].cpu() * 8000).round().clamp(-32768, 32767).to(torch.int16).to(DEV)
+    C = x16.shape[1]
+    gains = (torch.rand(C, generator=g) * 2 + 0.5).float().to(DEV)
+    got = ffdas_b200.das(x16, wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"], channel_scale=gains)
+    xs = _np(x16).astype(np.float64) * _np(gains).astype(np.float64).reshape(1, C, 1, 1)
+    geo = [_np(t) for t in (wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"])]
+    assert oracle.rel_l2(_np(got), oracle.das_f64(xs, *geo)) < TOL[torch.float32]
+    S = x16.shape[2]
+    V = wl["dstpos"].shape[:-1]
+    idx = torch.argsort(torch.rand((S, *V), generator=g), dim=0)[: max(1, S // 2)].int().to(DEV)
+    ofs_s = torch.gather(wl["offsets"], 0, idx.long())
+    w_s = torch.gather(wl["weights"], 0, idx.long())
+    got_s = ffdas_b200.das_sparse(x16, wl["srcpos"], wl["dstpos"], ofs_s, w_s, idx, channel_scale=gains)
+    ref_s = oracle.das_f64(xs, geo[0], geo[1], _np(ofs_s), _np(w_s), sparse_indices=_np(idx))
+    assert oracle.rel_l2(_np(got_s), ref_s) < TOL[torch.float32]
+
+
+@pytest.mark.parametrize("flag,tol", [("use_bf16", TOL[torch.bfloat16]), ("use_fp16", TOL[torch.float16])])
+def test_channel_scale_normalises_before_16bit_storage(flag, tol):
+    # FP32 data normalised per channel (scale = 1 / peak) inside the ingest and
+    # stored as 16-bit pairs: the image of the normalised data, as if the
+    # caller had normalised it
+    wl = W.diverging3d(device=DEV, scale=0.125)
+    x = wl["x"] * 1e4   # far outside FP16's comfortable range before scaling
+    peak = x.abs().amax(dim=(0, 2, 3)).clamp_min(1e-30)
+    got = ffdas_b200.das(x, wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"], channel_scale=1.0 / peak,
+                         **{flag: True})
+    xn = _np(x).astype(np.float64) / _np(peak).astype(np.float64).reshape(1, -1, 1, 1)
+    ref = oracle.das_f64(xn, *[_np(t) for t in (wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"])])
+    assert oracle.rel_l2(_np(got), ref) < tol
+
+
+def test_channel_scale_is_checked():
+    rng = np.random.default_rng(2)
+    x, src, dst, offs, w = _small(rng, B=2, C=6)
+    with pytest.raises(ValueError):
+        ffdas_b200.das(x, src, dst, offs, w, channel_scale=torch.ones(5, device=DEV))
+    xg = x.clone().requires_grad_(True)
+    with pytest.raises(NotImplementedError):
+        ffdas_b200.das(xg, src, dst, offs, w, channel_scale=torch.ones(6, device=DEV))
+    # through the C-ABI a wrong length is INVALID_ARGUMENT, and the backward refuses
+    h = ffdas_b200.get_library_handle(DEV)
+    bad = torch.ones(7, device=DEV)
+    h.set_channel_scale(bad.data_ptr(), 7)
+    try:
+        with pytest.raises(RuntimeError):
+            ffdas_b200.das(x, src, dst, offs, w)
+    finally:
+        h.set_channel_scale(None, 0)

@@ -15,9 +15,14 @@ Two questions are asked of each channel-data dtype:
   itself is held to 1e-5 elsewhere).  The 16-bit pair formats must not add to
   it beyond the 1e-3 target.
 * storage error -- the image of the 16-bit data against the FP64 oracle of the
-  original FP32 data: quantising the channel data itself.  Rounding
-  peak-normalised 1024-channel data to bf16 (8-bit mantissa) costs about
-  1e-3 on these planes by itself, fp16 (11 bits) about 1.5e-4.
+  original FP32 data: quantising the channel data itself.  Measured on B200
+  (this library; the FP64 oracle of the quantised data alone in brackets):
+  bf16 (8-bit mantissa) 1.04e-3 (1.02e-3) on these four planes and 1.72e-3
+  (1.70e-3) on eight; fp16 (11 bits) 1.6e-4 (1.2e-4) and 3.7e-4 (3.2e-4).
+  The 1e-3 bar therefore holds for fp16 storage and, for bf16, only against
+  the oracle of the same bf16 data (the compute error above): rounding the
+  data to 8 bits already costs 1.0-1.7e-3, whatever the kernel does.  The
+  bf16 storage check stays at 2e-3 for that reason.
 """
 import numpy as np
 import pytest
