@@ -515,7 +515,8 @@ def extras(args, wl, ms_fp32, h) -> dict:
     out = torch.empty((1, *dstpos.shape[:-1]), device=dev)
 
     def measure(x, **kw):
-        cfg = autotune(x, srcpos, dstpos, offs, w, reps=2, use_cache=False, **kw)["config"]
+        tkw = {k: v for k, v in kw.items() if k != "channel_scale"}
+        cfg = autotune(x, srcpos, dstpos, offs, w, reps=2, use_cache=False, **tkw)["config"]
         h.set_config(cfg)
         ms = timed(lambda: ffdas_b200.das(x, srcpos, dstpos, offs, w, out=out, **kw), args.steps, args.warmup,
                    stream, 1)
@@ -552,6 +553,16 @@ def extras(args, wl, ms_fp32, h) -> dict:
         res[name + "_pairs"] = {"value": units / (msp * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": msp,
                                 "speedup_vs_fp32": ms32 / msp, "error_vs_fp64_pairs": errp, "schedule": cfgp,
                                 "input": f"FP32 channel data stored as {name} pairs ({flag}), half the workspace"}
+        # the same with the per-channel normalisation done by the library's
+        # ingest (ffdas_set_channel_scale, scale = 1 / peak) on the raw data
+        xr = wl["x"]
+        inv_peak = 1.0 / xr.abs().amax(dim=(0, 2, 3)).clamp_min(1e-30)
+        mss, errs, cfgs = measure(xr, **{flag: True, "channel_scale": inv_peak})
+        res[name + "_pairs_channel_scale"] = {
+            "value": units / (mss * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": mss, "speedup_vs_fp32": ms32 / mss,
+            "error_vs_fp64_pairs": errs, "schedule": cfgs,
+            "input": f"raw FP32 channel data, normalised per channel (1 / peak) and stored as {name} pairs "
+                     f"by the ingest (channel_scale)"}
     h.set_config(None)
     return res
 

@@ -259,7 +259,7 @@ ffdas_error_t ffdas_das_set_config(ffdas_handle_t h, const ffdas_das_config_t *c
     }
     const ffdas_das_config_t &c = *config;
     auto pow2_or_zero = [](int v, int hi) { return v == 0 || (v > 0 && v <= hi && (v & (v - 1)) == 0); };
-    if (c.variant < 0 || c.variant > 5 || c.variant == 4) return FFDAS_ERROR_INVALID_ARGUMENT;
+    if (c.variant < 0 || c.variant > 6 || c.variant == 4) return FFDAS_ERROR_INVALID_ARGUMENT;
     if (!pow2_or_zero(c.tile_x, 256) || !pow2_or_zero(c.tile_y, 256) || !pow2_or_zero(c.tile_z, 256))
         return FFDAS_ERROR_INVALID_ARGUMENT;
     if (!pow2_or_zero(c.batch_tile, 16)) return FFDAS_ERROR_INVALID_ARGUMENT;

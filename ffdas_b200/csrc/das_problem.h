@@ -97,4 +97,15 @@ ffdas_error_t launch_staged_sparse(ffdas_context &h, const das_problem &pb, int 
 ffdas_error_t launch_staged_bwd(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,
                                 const staged_grads &gr, int SC, int WB, int BT, int copy, dim3 grid);
 
+// das_sparse as one persistent launch over (tile, channel slice) work items,
+// longest tiles first (csrc/das_sparse_items.cuh): real pair storage, f32
+// output, lists of at most 64 entries.  gp holds 256-voxel tiles and the
+// channel slice (cchunk); ws is sparse_items_workspace() bytes; *gate is
+// zeroed, set for a list naming an event twice (the kernel then does nothing
+// and the caller's gated gather kernel runs).
+bool sparse_items_supported(const das_problem &pb, int kind);
+size_t sparse_items_workspace(const das_problem &pb, int n_tiles, int SC);
+ffdas_error_t launch_sparse_items(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,
+                                  int SC, int WB, int copy, void *ws, int *gate);
+
 }  // namespace ffdas

@@ -16,6 +16,7 @@
 #include "core.h"
 #include "das_problem.h"
 #include "das_staged.cuh"
+#include "das_sparse_items.cuh"
 
 namespace ffdas {
 
@@ -355,6 +356,112 @@ ffdas_error_t launch_staged_sparse(ffdas_context &h, const das_problem &pb, int 
             return WB == 64 ? launch_fwd_sc<ST_F16, 64>(h, sp, map, SC, grid) : launch_fwd_sc<ST_F16, 32>(h, sp, map, SC, grid);
         default:
             return WB == 64 ? launch_fwd_sc<ST_BF16, 64>(h, sp, map, SC, grid) : launch_fwd_sc<ST_BF16, 32>(h, sp, map, SC, grid);
+    }
+}
+
+// ------------------------------------------------------ das_sparse items ---
+bool sparse_items_supported(const das_problem &pb, int kind) {
+    return (kind == ST_F32 || kind == ST_F16 || kind == ST_BF16) && pb.sparse && pb.n_events <= kItemsMaxList &&
+           pair_row_length(pb.N) >= 64 && (int64_t)pb.B * pb.C * pb.S < INT32_MAX && pb.B <= 64 &&
+           (pb.S + 3) / 4 < 255;
+}
+
+size_t sparse_items_workspace(const das_problem &pb, int n_tiles, int SC) {
+    const int passes = (pb.S + SC - 1) / SC;
+    size_t b = ((size_t)pb.n_events * pb.V * 12 + 255) & ~size_t(255);   // sorted lists
+    b += ((size_t)(passes + 1) * pb.V + 255) & ~size_t(255);             // pass starts
+    b += ((size_t)n_tiles * 8 + 255) & ~size_t(255);                     // tile work, order
+    b += 256;                                                             // queues (one per batch item)
+    return b;
+}
+
+template <int K, int SC, int WB>
+static ffdas_error_t launch_items_t(ffdas_context &h, const staged_params &sp, const items_params &ip,
+                                    const CUtensorMap &map, int batch) {
+    constexpr size_t smem = items_smem_bytes<K, WB>();
+    FFDAS_TRY((prepare_once<das_sparse_items_kernel<K, SC, WB>>(smem)));
+    int per_sm = 0;
+    FFDAS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, das_sparse_items_kernel<K, SC, WB>, kStThreads,
+                                                             smem));
+    per_sm = std::max(per_sm, 1);
+    // a persistent grid: as many CTAs as the GPU holds at once (split over the
+    // batch items, each of which pulls from its own queue)
+    const int64_t items = (int64_t)ip.tiles * ip.slices;
+    const int64_t resident = std::max<int64_t>(1, (int64_t)std::max(h.sm_count, 1) * per_sm / std::max(batch, 1));
+    const int grid = (int)std::min(items, resident);
+    h.last.grid = (int64_t)grid * batch;
+    das_sparse_items_kernel<K, SC, WB><<<dim3((unsigned)grid, (unsigned)batch), kStThreads, smem, h.stream>>>(sp, ip, map);
+    return ffdas_launch_check(h.stream);
+}
+
+ffdas_error_t launch_sparse_items(ffdas_context &h, const das_problem &pb, int kind, const gather_params &gp,
+                                  int SC, int WB, int copy, void *ws, int *gate) {
+    if (gp.T0 * gp.T1 * gp.T2 != kItemsTile || !gp.sparse_idx || !sparse_items_supported(pb, kind))
+        return FFDAS_ERROR_INTERNAL;
+    SC = SC <= 4 ? 4 : 8;
+    const int tiles = gp.n0 * gp.n1 * ((pb.D2 + gp.T2 - 1) / gp.T2);
+    const int passes = (pb.S + SC - 1) / SC;
+    char *w = static_cast<char *>(ws);
+    int *bs = reinterpret_cast<int *>(w);
+    float *bo = reinterpret_cast<float *>(bs + (size_t)pb.n_events * pb.V);
+    float *bw = bo + (size_t)pb.n_events * pb.V;
+    w += ((size_t)pb.n_events * pb.V * 12 + 255) & ~size_t(255);
+    uint8_t *pstart = reinterpret_cast<uint8_t *>(w);
+    w += ((size_t)(passes + 1) * pb.V + 255) & ~size_t(255);
+    int *tile_work = reinterpret_cast<int *>(w);
+    int *order = tile_work + tiles;
+    w += ((size_t)tiles * 8 + 255) & ~size_t(255);
+    int *queue = reinterpret_cast<int *>(w);
+
+    FFDAS_CUDA(cudaMemsetAsync(gate, 0, sizeof(int), h.stream));
+    FFDAS_CUDA(cudaMemsetAsync(tile_work, 0, (size_t)tiles * 4, h.stream));
+    FFDAS_CUDA(cudaMemsetAsync(queue, 0, 256, h.stream));
+    bucket_params bp;
+    bp.idx = gp.sparse_idx; bp.ofs = gp.offsets; bp.w = gp.weights;
+    bp.n = pb.n_events; bp.S = pb.S; bp.SC = SC; bp.passes = passes; bp.V = pb.V;
+    bp.D0 = pb.D0; bp.D1 = pb.D1; bp.T0 = gp.T0; bp.T1 = gp.T1; bp.T2 = gp.T2; bp.n0 = gp.n0; bp.n1 = gp.n1;
+    bp.bs = bs; bp.bo = bo; bp.bw = bw; bp.pstart = pstart; bp.tile_work = tile_work; bp.gate = gate;
+    const int64_t vb = (pb.V + 127) / 128;
+    if (vb > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
+    sparse_bucket_kernel<<<(unsigned)vb, 128, 0, h.stream>>>(bp);
+    FFDAS_TRY(ffdas_launch_check(h.stream));
+    sparse_order_kernel<<<1, 1024, 0, h.stream>>>(tile_work, tiles, order);
+    FFDAS_TRY(ffdas_launch_check(h.stream));
+    if (gp.cchunk) {   // channel slices add into the image: prepare it unless the call falls back
+        dim3 sg((unsigned)((pb.V + 255) / 256), (unsigned)std::min(pb.B, 65535));
+        scale_image_kernel<<<sg, 256, 0, h.stream>>>(static_cast<float *>(gp.out), pb.out_bstride, pb.V, pb.B,
+                                                     (float)gp.beta_re, gp.beta_zero, gate);
+        FFDAS_TRY(ffdas_launch_check(h.stream));
+    }
+    copy = resolve_copy(copy);
+    CUtensorMap map;
+    std::memset(&map, 0, sizeof(map));
+    if (copy == 1) FFDAS_TRY(pair_row_map(map, gp.P, gp.npad, (int64_t)pb.B * pb.C * pb.S, kind, WB));
+    staged_params sp = base_params(h, pb, gp);
+    sp.copy_async = copy == 2;
+    sp.gate = gate;
+    h.last.copy_engine = copy;
+    items_params ip;
+    ip.bs = bs; ip.bo = bo; ip.bw = bw; ip.pstart = pstart; ip.n = pb.n_events; ip.order = order;
+    ip.tiles = tiles;
+    ip.slices = gp.cchunk ? (pb.C + gp.cchunk - 1) / gp.cchunk : 1;
+    ip.queue = queue;
+    switch (kind) {
+        case ST_F32:
+            if (WB == 64) return SC <= 4 ? launch_items_t<ST_F32, 4, 64>(h, sp, ip, map, pb.B)
+                                         : launch_items_t<ST_F32, 8, 64>(h, sp, ip, map, pb.B);
+            return SC <= 4 ? launch_items_t<ST_F32, 4, 32>(h, sp, ip, map, pb.B)
+                           : launch_items_t<ST_F32, 8, 32>(h, sp, ip, map, pb.B);
+        case ST_F16:
+            if (WB == 64) return SC <= 4 ? launch_items_t<ST_F16, 4, 64>(h, sp, ip, map, pb.B)
+                                         : launch_items_t<ST_F16, 8, 64>(h, sp, ip, map, pb.B);
+            return SC <= 4 ? launch_items_t<ST_F16, 4, 32>(h, sp, ip, map, pb.B)
+                           : launch_items_t<ST_F16, 8, 32>(h, sp, ip, map, pb.B);
+        default:
+            if (WB == 64) return SC <= 4 ? launch_items_t<ST_BF16, 4, 64>(h, sp, ip, map, pb.B)
+                                         : launch_items_t<ST_BF16, 8, 64>(h, sp, ip, map, pb.B);
+            return SC <= 4 ? launch_items_t<ST_BF16, 4, 32>(h, sp, ip, map, pb.B)
+                           : launch_items_t<ST_BF16, 8, 32>(h, sp, ip, map, pb.B);
     }
 }
 

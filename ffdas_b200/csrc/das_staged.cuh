@@ -599,9 +599,11 @@ __device__ __forceinline__ int staged_tile_bounds(const staged_params &p, staged
 // of the pass lies inside the record and the pass adds exactly nothing.  The
 // margin covers the FP32 rounding of tau, rsqrt included (< 1 sample below
 // 2^20).
+// `items`: the delays are the per-voxel list entries of the sparse item
+// kernel, all present, so the fast path is open to them.
 template <int K, int WB>
 __device__ __forceinline__ int pass_flags(const staged_params &p, const staged_smem<K, WB> &sm, int sc, int SC,
-                                          bool anybad) {
+                                          bool anybad, bool items = false) {
     float gmin = 0.f, gmax = 0.f;
 #pragma unroll
     for (int a = 0; a < 3; a++) {
@@ -614,10 +616,13 @@ __device__ __forceinline__ int pass_flags(const staged_params &p, const staged_s
     const float dmin = sqrtf(gmin), dmax = sqrtf(gmax);
     const bool boxes_ok = sm.flags[1] != 0 && dmax == dmax && dmax <= kSaneRange;
     bool skip = !anybad && boxes_ok;
-    bool fast = !anybad && boxes_ok && sc == SC && !p.sparse_idx && !p.srcdir;
+    bool fast = !anybad && boxes_ok && (items || (sc == SC && !p.sparse_idx)) && !p.srcdir;
     for (int j = 0; j < sc; j++) {
         const float lo = sm.ofs_lo[j], hi = sm.ofs_hi[j];
-        if (lo == INFINITY) { fast = false; continue; }   // no delay of this event is present
+        if (lo == INFINITY) {   // no delay of this event is present
+            if (!items) fast = false;   // (item taps never name such an event)
+            continue;
+        }
         const float marg = 4.f + 1e-5f * (fabsf(lo) + fabsf(hi) + dmax);
         skip &= (lo + dmin - marg >= (float)(p.N - 1)) || (hi + dmax + marg < 0.f);
         fast &= fabsf(lo) <= kSaneRange && fabsf(hi) <= kSaneRange;
@@ -874,16 +879,19 @@ __device__ __forceinline__ void staged_produce(const staged_params &p, const CUt
 // arrival wait for the consumers to release the slot.  The distance bounds
 // use x * rsqrt(x) (relative error a few 1e-7, far inside the windows'
 // two-sample margins).
-template <int K, int WB, int SC>
+// The channel range is [cbeg, cend), the batch item cx.b.  With ITEMS (the
+// sparse item kernel) a window no tap can read -- an event with no list
+// entry in the tile, an event past the chunk, a channel past the slice, which
+// that kernel's consumers skip -- does not hold the stage off the unclamped path.
+template <int K, int WB, int SC, bool ITEMS = false>
 __device__ __forceinline__ void staged_produce_pass2(const staged_params &p, const CUtensorMap *tmap,
                                                      staged_smem<K, WB> &sm, const staged_ctx &cx, int &stage,
                                                      uint32_t &phase, int e0, int sc, bool &dead,
-                                                     uint32_t &issued_mask) {
+                                                     uint32_t &issued_mask, int cbeg, int cend) {
     using SG = slot_geom<WB, K>;
     using st = typename pair_traits<K>::storage;
     constexpr int CC = kStWin / SC;
     constexpr uint32_t PB = (uint32_t)sizeof(st);
-    const int cbeg = chan_begin(p), cend = chan_end(p);
     const int lane = cx.lane, cl = lane / SC, j = lane % SC;
     const bool jv = j < sc;
     const float olo = sm.ofs_lo[j], ohi = sm.ofs_hi[j];
@@ -910,7 +918,8 @@ __device__ __forceinline__ void staged_produce_pass2(const staged_params &p, con
         uint32_t m = kZeroWindow;   // every tap index clamps to the zero pair
         bool issue = false, overflow = false, mappable = false, zero_map = false;
         int k0 = 0;
-        if (c < cend && jv) {
+        if (ITEMS && !(c < cend && jv && olo != INFINITY)) mappable = true;   // never read
+        if (c < cend && jv && !(ITEMS && olo == INFINITY)) {
             const float dx = fmaxf(fmaxf(ax0 - px, px - ax1), 0.f);
             const float dy = fmaxf(fmaxf(ay0 - py, py - ay1), 0.f);
             const float dz = fmaxf(fmaxf(az0 - pz, pz - az1), 0.f);
@@ -1328,7 +1337,7 @@ __global__ void __launch_bounds__(kStThreads, SC >= 8 ? 2 : 3) das_staged2_kerne
         const bool pass_fast = (pflags & kPassFast) != 0;
 
         if (cx.producer) {
-            staged_produce_pass2<K, WB, SC>(p, &tmap, sm, cx, stage, phase, e0, sc, dead, issued_mask);
+            staged_produce_pass2<K, WB, SC>(p, &tmap, sm, cx, stage, phase, e0, sc, dead, issued_mask, cbeg, cend);
         } else {
         for (int c0 = cbeg; c0 < cend; c0 += CC) {
             {

@@ -97,6 +97,12 @@ def candidates(x, dstpos, offsets, sparse_indices=None) -> list[dict]:
                         if lanes <= C:
                             out.append(dict(variant=5, batch_tile=bt, tile_x=lanes))
     if real and sparse_indices is not None and x.dtype != torch.float64:
+        # das_sparse as one persistent launch over bucketed lists (256-voxel tiles)
+        for t0, t1 in tiles:
+            for wb in (32, 64):
+                for ec in (4, 8):
+                    for mb in (4, 8, 16):   # channel slicing: about mb work items per SM
+                        out.append(dict(variant=6, tile_x=t0, tile_y=t1, window=wb, event_chunk=ec, min_blocks=mb))
         # das_sparse on the staged kernel: 512-voxel tiles, passes over x's events
         S = x.shape[-2]
         for t0 in (128, 64, 32, 16, 8):

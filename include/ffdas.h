@@ -143,7 +143,11 @@ typedef struct {
     int32_t variant;      /* 0 auto, 1 L1 gather kernel, 2 TMA-staged kernel (forward and adjoint),
                              3 gather adjoint in ffdas_das_backward (forward as 0),
                              5 direct kernel: one launch, no workspace, for small real problems
-                               (forward; the adjoint as 0) */
+                               (forward; the adjoint as 0),
+                             6 das_sparse: persistent staged kernel over bucketed lists, tiles
+                               longest first (real data, lists of up to 64 entries;
+                               min_blocks sets the channel slicing, about that many work
+                               items per SM) */
     int32_t tile_x;       /* voxels per CTA along the innermost spatial dim
                              (variant 5: lanes per voxel, 1..32, 0 = from the occupancy) */
     int32_t tile_y;       /* ... along the middle spatial dim */

@@ -609,3 +609,107 @@ def test_channel_scale_is_checked():
             ffdas_b200.das(x, src, dst, offs, w)
     finally:
         h.set_channel_scale(None, 0)
+
+
+# --------------------------------------------- das_sparse, persistent items ---
+# das_sparse schedule variant 6: lists bucketed by event, tiles pulled from a
+# queue longest first by a persistent grid, voxels of a pass ordered by their
+# entry count, windows staged by TMA.
+
+def _distinct_lists(g, S, n, V, p_zero=0.0):
+    """Per voxel a list of up to n distinct events of S (random order), uneven
+    lengths 0..n padded with zero weight and a repeated index."""
+    perm = torch.argsort(torch.rand((S, *V), generator=g), dim=0)[:n].int()
+    length = torch.randint(0, n + 1, V, generator=g)
+    ofs_s = (torch.rand((n, *V), generator=g) * 60 - 10).float()
+    w_s = (torch.rand((n, *V), generator=g) + 0.1).float()
+    pad = torch.arange(n).reshape(n, *([1] * len(V))) >= length[None]
+    w_s[pad] = 0.0
+    perm[pad] = perm[0:1].expand_as(perm)[pad]
+    if p_zero:
+        w_s[torch.rand((n, *V), generator=g) < p_zero] = 0.0
+    return perm, ofs_s, w_s
+
+
+@pytest.mark.parametrize("cfg", [dict(variant=6), dict(variant=6, event_chunk=4), dict(variant=6, window=32)],
+                         ids=["default", "chunk4", "window32"])
+@pytest.mark.parametrize("B", [1, 3])
+def test_sparse_items_uneven_lists(rng, cfg, B):
+    from ffdas_b200.tune import schedule
+    x, src, dst, offs, w = _small(rng, B=B, C=12, S=13, N=180, V=(37, 29))
+    g = torch.Generator().manual_seed(31 + B)
+    V = dst.shape[:-1]
+    idx, ofs_s, w_s = _distinct_lists(g, 13, 9, V, p_zero=0.1)
+    idx, ofs_s, w_s = idx.to(DEV), ofs_s.to(DEV), w_s.to(DEV)
+    h = ffdas_b200.get_library_handle(DEV)
+    with schedule(cfg, DEV):
+        got = ffdas_b200.das_sparse(x, src, dst, ofs_s, w_s, idx)
+        info = h.last_kernel_info()
+    assert info["variant"] == 6
+    with schedule(dict(variant=1), DEV):
+        gat = ffdas_b200.das_sparse(x, src, dst, ofs_s, w_s, idx)
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(ofs_s), _np(w_s), sparse_indices=_np(idx))
+    assert oracle.rel_l2(_np(got), ref) < TOL[torch.float32]
+    assert oracle.rel_l2(_np(got), _np(gat)) < 1e-6
+
+
+@pytest.mark.parametrize("dup", [False, True], ids=["items", "fallback"])
+def test_sparse_items_channel_slices_with_beta(dup):
+    # 128 channels over a small grid: the work items split the channels, each
+    # slice adding into an image prepared with beta; a doubly named event
+    # falls back to the gated gather kernel, which applies beta itself
+    import ctypes
+    from ffdas_b200 import _lib
+    from ffdas_b200._lib import DataType
+    rng = np.random.default_rng(8)
+    x, src, dst, offs, w = _small(rng, C=128, S=10, N=160, V=(24, 20))
+    V = dst.shape[:-1]
+    g = torch.Generator().manual_seed(12)
+    idx, ofs_s, w_s = _distinct_lists(g, 10, 6, V)
+    if dup:
+        idx[1, 3, 3] = idx[0, 3, 3]
+        w_s[0, 3, 3] = w_s[1, 3, 3] = 0.7
+    idx, ofs_s, w_s = idx.to(DEV), ofs_s.to(DEV), w_s.to(DEV)
+    h = ffdas_b200.get_library_handle(DEV)
+    h.set_config(dict(variant=6))
+    L = _lib.load()
+    prev = torch.randn((1, *V), device=DEV)
+    out = prev.clone()
+    xd = _lib.TensorDesc(list(x.shape), None, DataType.R_32F)
+    od = _lib.TensorDesc(list(out.shape), None, DataType.R_32F)
+    beta = (ctypes.c_float * 2)(0.5, 0.0)
+    h.set_stream(torch.cuda.current_stream().cuda_stream)
+    _lib.check(L.ffdas_das_sparse(h.h, src.data_ptr(), None, 0.0, xd.desc, x.data_ptr(), dst.data_ptr(),
+                                  ofs_s.data_ptr(), w_s.data_ptr(), idx.shape[0], idx.data_ptr(),
+                                  ctypes.cast(beta, ctypes.c_void_p), od.desc, out.data_ptr(), 0, 0))
+    info = h.last_kernel_info()
+    h.set_config(None)
+    torch.cuda.synchronize()
+    assert info["variant"] == 6 and info["kernels"] == 6   # ingest, buckets, order, image prep, items, gather
+    ref = 0.5 * _np(prev) + oracle.das_f64(_np(x), _np(src), _np(dst), _np(ofs_s), _np(w_s),
+                                          sparse_indices=_np(idx))
+    assert oracle.rel_l2(_np(out), ref) < TOL[torch.float32]
+
+
+def test_sparse_items_3d_volume_and_16bit_storage():
+    # a 3-D volume with half its transmits per voxel, FP32 and BF16 pair storage
+    wl = W.diverging3d(device=DEV, scale=0.25)
+    S = wl["x"].shape[2]
+    V = wl["dstpos"].shape[:-1]
+    g = torch.Generator().manual_seed(40)
+    idx, _, w_s = _distinct_lists(g, S, max(1, S // 2), V)
+    idx = idx.to(DEV)
+    ofs_s = torch.gather(wl["offsets"], 0, idx.long())
+    w_s = w_s.to(DEV) * torch.gather(wl["weights"], 0, idx.long())
+    h = ffdas_b200.get_library_handle(DEV)
+    geo = [_np(t) for t in (wl["srcpos"], wl["dstpos"])]
+    ref = oracle.das_f64(_np(wl["x"]), *geo, _np(ofs_s), _np(w_s), sparse_indices=_np(idx))
+    from ffdas_b200.tune import schedule
+    with schedule(dict(variant=6), DEV):
+        got = ffdas_b200.das_sparse(wl["x"], wl["srcpos"], wl["dstpos"], ofs_s, w_s, idx)
+        assert h.last_kernel_info()["variant"] == 6
+        xb = wl["x"].to(torch.bfloat16)
+        gotb = ffdas_b200.das_sparse(xb, wl["srcpos"], wl["dstpos"], ofs_s, w_s, idx, use_bf16=True)
+    assert oracle.rel_l2(_np(got), ref) < TOL[torch.float32]
+    refb = oracle.das_f64(_np(xb.float()), *geo, _np(ofs_s), _np(w_s), sparse_indices=_np(idx))
+    assert oracle.rel_l2(_np(gotb), refb) < TOL[torch.bfloat16]
