@@ -586,9 +586,16 @@ def bwd_extras(args, h) -> dict:
     gout = torch.randn((xa.shape[0], *af["dstpos"].shape[:-1]), device=dev)
     fcfg = autotune(xa, *args_f, reps=2, use_cache=False)["config"]
     h.set_config(fcfg)
+    xdsc = _lib.TensorDesc(list(xa.shape), list(xa.stride()), DataType.R_32F)
+    # as in the autograd forward: the pair rows go into a buffer that the
+    # backward then reads instead of building them again
+    nbytes = _lib.pair_bytes(xdsc, 0)
+    pairs = torch.empty(nbytes, dtype=torch.uint8, device=dev)
 
     def fwd():
+        h.set_pair_buffer(pairs.data_ptr(), nbytes)
         ffdas_b200.das(xa, *args_f)
+        h.set_pair_buffer(None, 0)
 
     msf = timed(fwd, args.steps, args.warmup, stream, 1)
     finfo = h.last_kernel_info()
@@ -598,16 +605,19 @@ def bwd_extras(args, h) -> dict:
     gw = torch.empty_like(af["weights"])
     gd = torch.empty_like(af["dstpos"])
     gs = torch.empty_like(af["srcpos"])
-    xdsc = _lib.TensorDesc(list(xa.shape), list(xa.stride()), DataType.R_32F)
     gdsc = _lib.TensorDesc(list(gout.shape), None, DataType.R_32F)
     L = _lib.load()
+    reuse = [True]
 
     def bwd():
         h.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+        if reuse[0]:
+            h.set_pair_buffer(pairs.data_ptr(), nbytes)
         _lib.check(L.ffdas_das_backward(h.h, af["srcpos"].data_ptr(), None, 0.0, xdsc.desc, xa.data_ptr(),
                                         af["dstpos"].data_ptr(), af["offsets"].data_ptr(), af["weights"].data_ptr(),
                                         0, None, gdsc.desc, gout.data_ptr(), gx.data_ptr(), go.data_ptr(),
                                         gw.data_ptr(), gd.data_ptr(), gs.data_ptr()))
+        h.set_pair_buffer(None, 0)
 
     table = []
     bcands = [None] + [dict(variant=2, tile_x=tx, tile_y=256 // tx, window=wb)
@@ -620,8 +630,16 @@ def bwd_extras(args, h) -> dict:
         table.append((ms, cfg, h.last_kernel_info()))
     table.sort(key=lambda t: t[0])
     msb, bcfg, binfo = table[0]
+    # the same backward building its own pair rows (a backward without the
+    # forward's buffer, e.g. called on its own through the C-ABI)
+    reuse[0] = False
+    h.set_config(bcfg)
+    msb_own = timed(bwd, args.steps, args.warmup, stream, 1)
     h.set_config(None)
     return {"bwd_fwd": {"ratio": msb / msf, "fwd_ms": msf, "bwd_ms": msb,
+                        "bwd_ms_own_pairs": msb_own, "ratio_own_pairs": msb_own / msf,
+                        "pairs": "the backward reads the pair rows the forward built (ffdas_set_pair_buffer), as "
+                                 "the autograd function does; ratio_own_pairs: it builds them itself",
                         "fwd_schedule": finfo, "bwd_schedule": binfo, "bwd_config": bcfg,
                         "bwd_table": [[m, c, i["variant"]] for m, c, i in table],
                         "workload": "autofocus: 128 ch, 8 plane waves, batch 4, 2048 samples, 256x256 voxels; "

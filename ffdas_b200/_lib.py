@@ -139,6 +139,8 @@ SIGNATURES = {
     "ffdas_get_last_kernel_time": (c_err, [c_handle, ctypes.POINTER(ctypes.c_float)]),
     "ffdas_get_last_kernel_units": (c_err, [c_handle, ctypes.POINTER(ctypes.c_longlong)]),
     "ffdas_set_channel_scale": (c_err, [c_handle, c_ptr, ctypes.c_int64]),
+    "ffdas_set_pair_buffer": (c_err, [c_handle, c_ptr, ctypes.c_size_t]),
+    "ffdas_das_pair_bytes": (c_err, [c_desc, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "ffdas_measure_fp32_peak": (c_err, [c_handle, ctypes.POINTER(ctypes.c_double)]),
     "ffdas_get_device_status": (c_err, [c_handle, ctypes.POINTER(ctypes.c_int)]),
     "ffdas_debug_staged_drop_stage": (None, [ctypes.c_int]),
@@ -251,6 +253,10 @@ class Handle:
         """Per-channel scale applied by the ingest of the following calls (device pointer; None clears)."""
         check(load().ffdas_set_channel_scale(self.h, scale_ptr, int(count) if scale_ptr else 0))
 
+    def set_pair_buffer(self, ptr, nbytes: int) -> None:
+        """Caller-owned buffer for the pair rows of the next calls (None clears)."""
+        check(load().ffdas_set_pair_buffer(self.h, ptr, int(nbytes) if ptr else 0))
+
     def last_kernel_units(self):
         """Units the last timed call's kernel evaluated, or None when it does not count them."""
         u = ctypes.c_longlong()
@@ -296,6 +302,13 @@ def device_count() -> int:
     d = ctypes.c_int()
     check(load().ffdas_device_count(ctypes.byref(d)))
     return d.value
+
+
+def pair_bytes(desc: "TensorDesc", compute_type: int) -> int:
+    """Bytes of a pair buffer for a forward call on x (ffdas_das_pair_bytes)."""
+    n = ctypes.c_size_t()
+    check(load().ffdas_das_pair_bytes(desc.desc, int(compute_type), ctypes.byref(n)))
+    return int(n.value)
 
 
 def event_create() -> int:

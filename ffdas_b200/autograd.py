@@ -15,7 +15,7 @@ import torch
 
 from . import _lib
 from ._lib import DataType
-from .das import _FFDAS_DTYPE, _astype, _check_spatial, _run, _to_torch
+from .das import _FFDAS_DTYPE, _astype, _check_spatial, _compute_type, _run, _to_torch, _x_desc
 from .library import get_library_handle
 
 
@@ -23,10 +23,26 @@ class DASFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, srcpos, dstpos, offsets, weights, sparse_indices, opts: dict):
         ctx.opts = opts
-        out = _run(x.detach(), srcpos.detach(), dstpos.detach(), offsets.detach(), weights.detach(),
-                   sparse_indices, srcdir=opts["srcdir"], wavenum=opts["wavenum"], algorithm=0,
-                   use_fp16=opts["use_fp16"], use_bf16=opts["use_bf16"],
-                   channels_trailing=opts["channels_trailing"], out=None)
+        ctx.pairs = None
+        xt = x.detach()
+        handle = get_library_handle(xt.device)
+        # The forward builds its interpolation-pair rows into a buffer kept for
+        # the backward (ffdas_set_pair_buffer), which then skips building them
+        # again; only where the backward can run (real data, no directivity).
+        keep = (opts["srcdir"] is None and opts["wavenum"] == 0.0 and not xt.is_complex()
+                and xt.dtype in _FFDAS_DTYPE)
+        if keep:
+            nbytes = _lib.pair_bytes(_x_desc(xt, opts["channels_trailing"]), _compute_type(xt, False, False))
+            ctx.pairs = torch.empty(nbytes, dtype=torch.uint8, device=xt.device)
+            handle.set_pair_buffer(ctx.pairs.data_ptr(), nbytes)
+        try:
+            out = _run(xt, srcpos.detach(), dstpos.detach(), offsets.detach(), weights.detach(),
+                       sparse_indices, srcdir=opts["srcdir"], wavenum=opts["wavenum"], algorithm=0,
+                       use_fp16=opts["use_fp16"], use_bf16=opts["use_bf16"],
+                       channels_trailing=opts["channels_trailing"], out=None)
+        finally:
+            if keep:
+                handle.set_pair_buffer(None, 0)
         ctx.save_for_backward(x, srcpos, dstpos, offsets, weights,
                               sparse_indices if sparse_indices is not None else torch.empty(0))
         ctx.has_sparse = sparse_indices is not None
@@ -67,10 +83,17 @@ class DASFunction(torch.autograd.Function):
         handle = get_library_handle(dev)
         handle.set_stream(torch.cuda.current_stream(dev).cuda_stream)
         ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
-        _lib.check(_lib.load().ffdas_das_backward(
-            handle.h, ptr(srcpos_t), None, 0.0, x_desc.desc, ptr(xt), ptr(dstpos_t), ptr(offsets_t),
-            ptr(weights_t), int(idx_t.shape[0]) if idx_t is not None else 0, ptr(idx_t), g_desc.desc,
-            ptr(gout), ptr(gx), ptr(goff), ptr(gw), ptr(gdst), ptr(gsrc)))
+        if ctx.pairs is not None:   # the forward's pair rows, read instead of rebuilt when they match
+            handle.set_pair_buffer(ctx.pairs.data_ptr(), ctx.pairs.numel())
+        try:
+            _lib.check(_lib.load().ffdas_das_backward(
+                handle.h, ptr(srcpos_t), None, 0.0, x_desc.desc, ptr(xt), ptr(dstpos_t), ptr(offsets_t),
+                ptr(weights_t), int(idx_t.shape[0]) if idx_t is not None else 0, ptr(idx_t), g_desc.desc,
+                ptr(gout), ptr(gx), ptr(goff), ptr(gw), ptr(gdst), ptr(gsrc)))
+        finally:
+            if ctx.pairs is not None:
+                handle.set_pair_buffer(None, 0)
+        ctx.pairs = None
         if gx is not None:
             if opts["channels_trailing"]:
                 gx = gx.transpose(1, 2)

@@ -61,6 +61,19 @@ struct ffdas_context {
     // caller-owned device array of chan_scale_count floats, or null
     const float *chan_scale = nullptr;
     int64_t chan_scale_count = 0;
+    // caller-owned buffer for the pair rows (ffdas_set_pair_buffer) and what
+    // the last forward call on this handle wrote into it
+    void *pair_buf = nullptr;
+    size_t pair_buf_bytes = 0;
+    struct pair_signature {
+        const void *buf = nullptr;     // null: the last forward wrote no buffer
+        const void *x = nullptr;
+        ffdas_tensor_desc desc{};
+        int kind = -1;
+        const float *scale = nullptr;
+        int64_t scale_count = 0;
+    } pair_sig;
+    bool last_pairs_reused = false;   // the last ffdas_das_backward read the pair buffer
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     // eigensolver state of ffdas_truncate_rank, created on its first call and
     // released with the handle

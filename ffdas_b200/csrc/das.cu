@@ -222,6 +222,39 @@ static ffdas_error_t launch_ingest(ffdas_context &h, const das_problem &pb, ffda
 #undef FFDAS_INGEST
 }
 
+// Bytes a pair buffer needs for a forward call on x (the pair rows and one
+// 256-byte control block), for the default output dtype of x.
+ffdas_error_t pair_buffer_bytes(const ffdas_tensor_desc &xd, ffdas_compute_type_t ct, size_t *bytes) {
+    ffdas_datatype_t od;
+    switch (xd.dtype) {
+        case FFDAS_R_64F: od = FFDAS_R_64F; break;
+        case FFDAS_C_16F: case FFDAS_C_32F: od = FFDAS_C_32F; break;
+        case FFDAS_C_64F: od = FFDAS_C_64F; break;
+        default: od = FFDAS_R_32F; break;
+    }
+    if (xd.ndim != 3 && xd.ndim != 4) return FFDAS_ERROR_INVALID_DIMS;
+    const int kind = select_storage(xd.dtype, od, ct, xd.ndim == 4 ? (int)xd.dims[0] : 1);
+    if (kind < 0) return FFDAS_ERROR_UNSUPPORTED_TYPE;
+    const int o = xd.ndim == 4 ? 1 : 0;
+    const int64_t B = xd.ndim == 4 ? xd.dims[0] : 1;
+    const int64_t rows = B * xd.dims[o] * xd.dims[o + 1];
+    const int64_t npad = pair_row_length((int)xd.dims[o + 2]);
+    *bytes = ((((size_t)std::max<int64_t>(rows, 1) * npad * storage_bytes(kind)) + 255) & ~size_t(255)) + 256;
+    return FFDAS_SUCCESS;
+}
+
+// The pair rows a forward call left in the handle's pair buffer, if they are
+// those of this x (same pointer, descriptor, storage and channel scale).
+void *reusable_pairs(const ffdas_context &h, const ffdas_tensor_desc &xd, const void *x, int kind) {
+    const auto &g = h.pair_sig;
+    if (!h.pair_buf || g.buf != h.pair_buf || g.x != x || g.kind != kind || g.scale != h.chan_scale ||
+        g.scale_count != h.chan_scale_count || g.desc.ndim != xd.ndim || g.desc.dtype != xd.dtype)
+        return nullptr;
+    for (int64_t i = 0; i < xd.ndim; i++)
+        if (g.desc.dims[i] != xd.dims[i] || g.desc.strides[i] != xd.strides[i]) return nullptr;
+    return h.pair_buf;
+}
+
 ffdas_error_t ingest_for_backward(ffdas_context &h, const das_problem &pb, ffdas_datatype_t xt, int kind,
                                   const void *x, int64_t npad, void *P) {
     return launch_ingest(h, pb, xt, kind, x, npad, P);
@@ -462,6 +495,7 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
     if ((int64_t)pb.B * pb.C * pb.S * pb.N > 0 && !a.x) return FFDAS_ERROR_NULL_POINTER;
     if (a.sparse && !a.sparse_indices) return FFDAS_ERROR_NULL_POINTER;
     h.units_recorded = false;
+    h.pair_sig = ffdas_context::pair_signature{};   // set again below if this call fills the pair buffer
     // timed calls: the kernels that count the units they evaluate add into
     // the handle's counter, cleared here, before the timed launch
     if (h.timing && h.unit_count) FFDAS_CUDA(cudaMemsetAsync(h.unit_count, 0, sizeof(unsigned long long), h.stream));
@@ -494,15 +528,31 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
     const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
     workspace P(h);
     const size_t pair_bytes = ((size_t)std::max<int64_t>(rows, 1) * npad * storage_bytes(kind) + 255) & ~size_t(255);
-    FFDAS_TRY(P.alloc(pair_bytes + (a.sparse ? 256 : 0)));   // das_sparse: a gate word after the pairs
-    FFDAS_TRY(launch_ingest(h, pb, xd.dtype, kind, a.x, npad, P.get<void>()));
+    // the caller's pair buffer when one is set and large enough (the pair
+    // rows then outlive the call, for ffdas_das_backward), else workspace
+    void *Pbase = nullptr;
+    if (h.pair_buf && h.pair_buf_bytes >= pair_bytes + 256) {
+        Pbase = h.pair_buf;
+    } else {
+        FFDAS_TRY(P.alloc(pair_bytes + (a.sparse ? 256 : 0)));   // das_sparse: a gate word after the pairs
+        Pbase = P.get<void>();
+    }
+    FFDAS_TRY(launch_ingest(h, pb, xd.dtype, kind, a.x, npad, Pbase));
+    if (Pbase == h.pair_buf) {
+        h.pair_sig.buf = h.pair_buf;
+        h.pair_sig.x = a.x;
+        h.pair_sig.desc = xd;
+        h.pair_sig.kind = kind;
+        h.pair_sig.scale = h.chan_scale;
+        h.pair_sig.scale_count = h.chan_scale_count;
+    }
 
     // ---- forward kernel ----
     const bool staged_ok = staged_supported(pb, kind) && od.dtype == FFDAS_R_32F;
     const schedule s = plan_schedule(h, pb, kind, staged_ok);
     gather_params gp;
     std::memset(&gp, 0, sizeof(gp));
-    gp.P = P.get<void>();
+    gp.P = Pbase;
     gp.npad = npad;
     gp.C = pb.C;
     gp.S = pb.S;
@@ -625,7 +675,7 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
             }
             workspace IW(h);
             FFDAS_TRY(IW.alloc(sparse_items_workspace(pb, (int)tiles, SCi)));
-            int *gate = reinterpret_cast<int *>(static_cast<char *>(P.get<void>()) + pair_bytes);
+            int *gate = reinterpret_cast<int *>(static_cast<char *>(Pbase) + pair_bytes);
             h.last.variant = 6;
             h.last.batch_tile = 1;
             h.last.event_chunk = SCi;
@@ -691,7 +741,7 @@ ffdas_error_t das_forward(ffdas_context &h, const das_call &a) {
         const int WBs = (c && c->window > 32) ? 64 : 32;
         const int copy = c ? c->copy_engine : 0;
         if (stiles <= INT32_MAX && pb.B <= 65535) {
-            int *gate = reinterpret_cast<int *>(static_cast<char *>(P.get<void>()) + pair_bytes);
+            int *gate = reinterpret_cast<int *>(static_cast<char *>(Pbase) + pair_bytes);
             h.last.variant = 2;
             h.last.tile_x = T0; h.last.tile_y = T1; h.last.tile_z = 1;
             h.last.batch_tile = 1;
@@ -754,6 +804,19 @@ static ffdas_error_t das_entry(ffdas_handle_t handle, das_call &a) {
 }
 
 extern "C" {
+
+ffdas_error_t ffdas_das_pair_bytes(ffdas_tensor_desc_t x_desc, ffdas_compute_type_t compute_type, size_t *bytes) {
+    if (!x_desc || !bytes) return FFDAS_ERROR_NULL_POINTER;
+    return pair_buffer_bytes(*x_desc, compute_type, bytes);
+}
+
+ffdas_error_t ffdas_set_pair_buffer(ffdas_handle_t handle, void *buffer, size_t bytes) {
+    if (!handle) return FFDAS_ERROR_INVALID_HANDLE;
+    if (buffer && bytes == 0) return FFDAS_ERROR_INVALID_ARGUMENT;
+    handle->pair_buf = buffer;
+    handle->pair_buf_bytes = buffer ? bytes : 0;
+    return FFDAS_SUCCESS;
+}
 
 ffdas_error_t ffdas_das(ffdas_handle_t handle, const float *srcpos, const float *srcdir,
                         float wavenum, ffdas_tensor_desc_t x_desc, const void *x,

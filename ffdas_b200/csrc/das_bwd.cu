@@ -273,6 +273,7 @@ static ffdas_error_t launch_bwd_k(ffdas_context &h, const bwd_params &bp, int BT
 // defined in das.cu
 ffdas_error_t ingest_for_backward(ffdas_context &h, const das_problem &pb, ffdas_datatype_t xt, int kind,
                                   const void *x, int64_t npad, void *P);
+void *reusable_pairs(const ffdas_context &h, const ffdas_tensor_desc &xd, const void *x, int kind);
 
 ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tensor_desc &gd,
                            const void *gout, float *gx, float *goff, float *gw, float *gdst, float *gsrc) {
@@ -301,13 +302,20 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
     const int64_t npad = pair_row_length(pb.N);
     const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
     const size_t sb = (kind == ST_F32) ? 8 : 4;
+    // the pair rows of the forward call on this x when it left them in the
+    // handle's pair buffer, else built again
     workspace P(h);
-    FFDAS_TRY(P.alloc((size_t)std::max<int64_t>(rows, 1) * npad * sb));
-    FFDAS_TRY(ingest_for_backward(h, pb, xd.dtype, kind, a.x, npad, P.get<void>()));
+    void *Pbase = reusable_pairs(h, xd, a.x, kind);
+    h.last_pairs_reused = Pbase != nullptr;
+    if (!Pbase) {
+        FFDAS_TRY(P.alloc((size_t)std::max<int64_t>(rows, 1) * npad * sb));
+        FFDAS_TRY(ingest_for_backward(h, pb, xd.dtype, kind, a.x, npad, P.get<void>()));
+        Pbase = P.get<void>();
+    }
 
     bwd_params bp;
     std::memset(&bp, 0, sizeof(bp));
-    bp.P = P.get<void>();
+    bp.P = Pbase;
     bp.npad = npad;
     bp.C = pb.C; bp.S = pb.S; bp.N = pb.N; bp.n_events = pb.n_events; bp.B = pb.B; bp.V = pb.V;
     bp.D0 = pb.D0; bp.D1 = pb.D1; bp.D2 = pb.D2;
@@ -387,7 +395,7 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
         if (gsrc) FFDAS_CUDA(cudaMemsetAsync(gsrc, 0, (size_t)pb.C * 3 * sizeof(float), h.stream));
         gather_params gp;
         std::memset(&gp, 0, sizeof(gp));
-        gp.P = P.get<void>();
+        gp.P = Pbase;
         gp.npad = npad;
         gp.C = pb.C; gp.S = pb.S; gp.n_events = pb.n_events; gp.B = pb.B; gp.V = pb.V;
         gp.D0 = pb.D0; gp.D1 = pb.D1; gp.D2 = pb.D2;
@@ -400,7 +408,7 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
         h.last.variant = 4;
         h.last.tile_x = bp.T0; h.last.tile_y = bp.T1; h.last.tile_z = bp.T2;
         h.last.batch_tile = BT; h.last.event_chunk = SC; h.last.storage = kind;
-        h.last.kernels = 2; h.last.grid = stiles * bchunks_st * csplit;
+        h.last.kernels = h.last_pairs_reused ? 1 : 2;   // (ingest,) adjoint h.last.grid = stiles * bchunks_st * csplit;
         if (bchunks_st > 65535) return FFDAS_ERROR_DIMS_TOO_LARGE;
         h.mark_start();
         const ffdas_error_t err = launch_staged_bwd(h, pb, kind, gp, gr, SC, WB, BT, copy,
@@ -427,7 +435,7 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
     h.last.variant = 3;
     h.last.tile_x = bp.T0; h.last.tile_y = bp.T1; h.last.tile_z = bp.T2;
     h.last.batch_tile = BT; h.last.event_chunk = 8; h.last.storage = kind;
-    h.last.kernels = 2; h.last.grid = tiles * bchunks;
+    h.last.kernels = h.last_pairs_reused ? 1 : 2;   // (ingest,) adjoint h.last.grid = tiles * bchunks;
     const bool sp = a.sparse;
     ffdas_error_t err;
     h.mark_start();

@@ -294,6 +294,18 @@ FFDAS_API ffdas_error_t ffdas_das_backward(
     float *grad_srcpos
 );
 
+/* New: a caller-owned device buffer for the interpolation-pair rows.  While
+ * one is set (and holds ffdas_das_pair_bytes for the call), a forward call
+ * builds its pair rows there instead of in workspace, and
+ * ffdas_das_backward on the same x -- same pointer, descriptor, pair storage
+ * and channel scale as the last forward call on this handle -- reads them
+ * instead of building them again (the adjoint then launches one kernel
+ * fewer).  The caller keeps the buffer and x unchanged in between (an
+ * autograd forward saves both for its backward).  NULL clears the buffer. */
+FFDAS_API ffdas_error_t ffdas_set_pair_buffer(ffdas_handle_t handle, void *buffer, size_t bytes);
+FFDAS_API ffdas_error_t ffdas_das_pair_bytes(ffdas_tensor_desc_t x_desc, ffdas_compute_type_t compute_type,
+                                             size_t *bytes);
+
 /* New: per-channel scale of the channel data, applied by the ingest of every
  * following ffdas_das / ffdas_das_sparse call on this handle (it replaces the
  * reference's caller-side cast/copy, src/tensor_ops/contiguous_copy_impl.cuh:

@@ -193,3 +193,36 @@ def test_channel_sliced_adjoint(B):
         assert oracle.rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-5, name
     for i in (0, 4):
         assert oracle.rel_l2(grads[0][i].cpu().numpy(), ref[i].grad.numpy()) < 2e-4
+
+
+def test_backward_reads_the_forward_pair_rows():
+    # the autograd forward builds its pair rows into a buffer kept for the
+    # backward (ffdas_set_pair_buffer); the backward then launches only the
+    # adjoint kernel, and its gradients equal those of a backward that builds
+    # the rows again
+    from ffdas_b200 import _lib
+    from ffdas_b200._lib import DataType
+    wl = W.autofocus(device=DEV, scale=0.25)
+    h = ffdas_b200.get_library_handle(DEV)
+    leaves = [t.clone().requires_grad_(True) for t in (wl["x"], wl["offsets"], wl["weights"])]
+    out = ffdas_b200.das(leaves[0], wl["srcpos"], wl["dstpos"], leaves[1], leaves[2])
+    out.square().sum().backward()
+    assert h.last_kernel_info()["kernels"] == 1
+    grads = [t.grad.clone() for t in leaves]
+    # the same backward through the C-ABI without the buffer: ingest + adjoint
+    x = wl["x"]
+    gout = 2 * out.detach()
+    gx = torch.zeros_like(x)
+    go = torch.empty_like(wl["offsets"])
+    gw = torch.empty_like(wl["weights"])
+    xd = _lib.TensorDesc(list(x.shape), list(x.stride()), DataType.R_32F)
+    gd = _lib.TensorDesc(list(gout.shape), None, DataType.R_32F)
+    h.set_stream(torch.cuda.current_stream().cuda_stream)
+    _lib.check(_lib.load().ffdas_das_backward(h.h, wl["srcpos"].data_ptr(), None, 0.0, xd.desc, x.data_ptr(),
+                                              wl["dstpos"].data_ptr(), wl["offsets"].data_ptr(),
+                                              wl["weights"].data_ptr(), 0, None, gd.desc, gout.data_ptr(),
+                                              gx.data_ptr(), go.data_ptr(), gw.data_ptr(), None, None))
+    assert h.last_kernel_info()["kernels"] == 2
+    torch.cuda.synchronize()
+    for a, b in zip(grads, (gx, go, gw)):
+        assert torch.equal(a, b)
