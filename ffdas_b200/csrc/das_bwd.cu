@@ -408,7 +408,8 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
         h.last.variant = 4;
         h.last.tile_x = bp.T0; h.last.tile_y = bp.T1; h.last.tile_z = bp.T2;
         h.last.batch_tile = BT; h.last.event_chunk = SC; h.last.storage = kind;
-        h.last.kernels = h.last_pairs_reused ? 1 : 2;   // (ingest,) adjoint h.last.grid = stiles * bchunks_st * csplit;
+        h.last.kernels = h.last_pairs_reused ? 1 : 2;   // (ingest,) adjoint
+        h.last.grid = stiles * bchunks_st * csplit;
         if (bchunks_st > 65535) return FFDAS_ERROR_DIMS_TOO_LARGE;
         h.mark_start();
         const ffdas_error_t err = launch_staged_bwd(h, pb, kind, gp, gr, SC, WB, BT, copy,
@@ -435,7 +436,8 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
     h.last.variant = 3;
     h.last.tile_x = bp.T0; h.last.tile_y = bp.T1; h.last.tile_z = bp.T2;
     h.last.batch_tile = BT; h.last.event_chunk = 8; h.last.storage = kind;
-    h.last.kernels = h.last_pairs_reused ? 1 : 2;   // (ingest,) adjoint h.last.grid = tiles * bchunks;
+    h.last.kernels = h.last_pairs_reused ? 1 : 2;   // (ingest,) adjoint
+    h.last.grid = tiles * bchunks;
     const bool sp = a.sparse;
     ffdas_error_t err;
     h.mark_start();

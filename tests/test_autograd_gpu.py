@@ -198,7 +198,7 @@ def test_channel_sliced_adjoint(B):
 def test_backward_reads_the_forward_pair_rows():
     # the autograd forward builds its pair rows into a buffer kept for the
     # backward (ffdas_set_pair_buffer); the backward then launches only the
-    # adjoint kernel, and its gradients equal those of a backward that builds
+    # adjoint kernel, and its gradients match those of a backward that builds
     # the rows again
     from ffdas_b200 import _lib
     from ffdas_b200._lib import DataType
@@ -224,5 +224,6 @@ def test_backward_reads_the_forward_pair_rows():
                                               gx.data_ptr(), go.data_ptr(), gw.data_ptr(), None, None))
     assert h.last_kernel_info()["kernels"] == 2
     torch.cuda.synchronize()
+    # equal up to the order of the float atomics that add the tiles' gradients
     for a, b in zip(grads, (gx, go, gw)):
-        assert torch.equal(a, b)
+        assert oracle.rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-6
