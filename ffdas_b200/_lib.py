@@ -139,6 +139,7 @@ SIGNATURES = {
     "ffdas_get_last_kernel_time": (c_err, [c_handle, ctypes.POINTER(ctypes.c_float)]),
     "ffdas_get_last_kernel_units": (c_err, [c_handle, ctypes.POINTER(ctypes.c_longlong)]),
     "ffdas_set_channel_scale": (c_err, [c_handle, c_ptr, ctypes.c_int64]),
+    "ffdas_set_gram_engine": (c_err, [c_handle, ctypes.c_int32]),
     "ffdas_set_pair_buffer": (c_err, [c_handle, c_ptr, ctypes.c_size_t]),
     "ffdas_das_pair_bytes": (c_err, [c_desc, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "ffdas_measure_fp32_peak": (c_err, [c_handle, ctypes.POINTER(ctypes.c_double)]),
@@ -252,6 +253,10 @@ class Handle:
     def set_channel_scale(self, scale_ptr, count: int) -> None:
         """Per-channel scale applied by the ingest of the following calls (device pointer; None clears)."""
         check(load().ffdas_set_channel_scale(self.h, scale_ptr, int(count) if scale_ptr else 0))
+
+    def set_gram_engine(self, engine: int) -> None:
+        """truncate_rank's Gram engine: 0 auto, 1 FP32 FMA kernel, 2 tensor cores where the input qualifies."""
+        check(load().ffdas_set_gram_engine(self.h, int(engine)))
 
     def set_pair_buffer(self, ptr, nbytes: int) -> None:
         """Caller-owned buffer for the pair rows of the next calls (None clears)."""

@@ -237,6 +237,13 @@ ffdas_error_t ffdas_set_channel_scale(ffdas_handle_t h, const float *scale, int6
     return FFDAS_SUCCESS;
 }
 
+ffdas_error_t ffdas_set_gram_engine(ffdas_handle_t h, int32_t engine) {
+    if (!h) return FFDAS_ERROR_INVALID_HANDLE;
+    if (engine < 0 || engine > 2) return FFDAS_ERROR_INVALID_ARGUMENT;
+    h->gram_engine = engine;
+    return FFDAS_SUCCESS;
+}
+
 ffdas_error_t ffdas_set_stream(ffdas_handle_t h, uintptr_t stream) {
     if (!h) return FFDAS_ERROR_INVALID_HANDLE;
     h->stream = reinterpret_cast<cudaStream_t>(stream);

@@ -74,6 +74,7 @@ struct ffdas_context {
         int64_t scale_count = 0;
     } pair_sig;
     bool last_pairs_reused = false;   // the last ffdas_das_backward read the pair buffer
+    int gram_engine = 0;              // ffdas_set_gram_engine: 0 auto, 1 FP32 FMA, 2 tensor cores
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     // eigensolver state of ffdas_truncate_rank, created on its first call and
     // released with the handle

@@ -22,7 +22,8 @@ namespace ffdas {
 
 constexpr int kDefaultCopy = 1;   // TMA tile loads
 
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+// Shared with the tensor-core Gram of truncate_rank (gram_tc.cuh).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static std::once_flag once;
     std::call_once(once, [] {

@@ -44,6 +44,7 @@
 // the filter subtracts a dominant component.  A TF32 product carries errors
 // of about 1e-3 of |x|, which is the size of the signal that remains.
 #include "core.h"
+#include "gram_tc.cuh"
 
 #include <cusolverDn.h>
 #include <dlfcn.h>
@@ -751,6 +752,68 @@ ffdas_error_t launch_small(ffdas_context &h, const T *x, int64_t sp, int64_t sq,
     return ffdas_launch_check(h.stream);
 }
 
+// Tensor-core Gram (gram_tc.cuh): FP32 rows (A = x, m <= n) of at most 256,
+// rows 16-byte aligned for the tensor map.  Engine 0 keeps small problems on
+// the FMA kernel.
+template <typename T>
+bool gram_tc_usable(const ffdas_context &, const T *, bool, int64_t, int64_t, int64_t) { return false; }
+template <>
+bool gram_tc_usable<float>(const ffdas_context &h, const float *x, bool rows, int64_t p, int64_t q, int64_t n) {
+    if (h.gram_engine == 1 || h.arch_code != 1000) return false;
+    if (!rows || p < 1 || p > 256 || q < gram_tc::kChunk || q > INT32_MAX || n % 4 != 0) return false;
+    if (reinterpret_cast<uintptr_t>(x) % 16 != 0) return false;
+    if (h.gram_engine == 0 && p * q < (int64_t(1) << 20)) return false;
+    return tensor_map_encoder() != nullptr;
+}
+
+template <int NB>
+ffdas_error_t launch_gram_tc(ffdas_context &h, const CUtensorMap &map, const gram_tc::params &a, int64_t splits) {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(gram_tc::gram_tc_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)gram_tc::smem_bytes<NB>());
+    });
+    if (attr != cudaSuccess) return FFDAS_ERROR_CUDA_RUNTIME;
+    gram_tc::gram_tc_kernel<NB><<<(unsigned)splits, gram_tc::kThreads, gram_tc::smem_bytes<NB>(), h.stream>>>(map, a);
+    return ffdas_launch_check(h.stream);
+}
+
+// Partials of G = A A^T over `splits` column ranges, about one CTA per SM;
+// `ok` false when the tensor map cannot be encoded (the caller then uses the
+// FMA kernel).
+ffdas_error_t gram_tc_partials(ffdas_context &h, const float *x, int64_t p, int64_t q, int64_t n, workspace &part,
+                               int64_t &splits, bool &ok) {
+    using namespace gram_tc;
+    ok = false;
+    splits = std::min<int64_t>(h.sm_count, (q + kChunk - 1) / kChunk);
+    int64_t kchunk = (q + splits - 1) / splits;
+    kchunk = (kchunk + kChunk - 1) / kChunk * kChunk;
+    splits = (q + kchunk - 1) / kchunk;
+    const int NB = p > 128 ? 2 : 1;
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {(cuuint64_t)q, (cuuint64_t)p};
+    const cuuint64_t strides[1] = {(cuuint64_t)n * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)kChunk, (cuuint32_t)(128 * NB)};
+    const cuuint32_t estr[2] = {1u, 1u};
+    if (tensor_map_encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(x), dims, strides, box,
+                             estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return FFDAS_SUCCESS;
+    ok = true;
+    FFDAS_TRY(part.alloc((size_t)(splits * p * p) * sizeof(float)));
+    params a{};
+    a.p = (int)p;
+    a.q = q;
+    a.kchunk = kchunk;
+    const auto up16 = [](int64_t v) { return (int)((v + 15) / 16 * 16); };
+    a.n0 = up16(p);
+    a.n1 = NB == 2 ? up16(p - 128) : 16;
+    a.part = part.get<float>();
+    a.status = h.status;
+    return NB == 2 ? launch_gram_tc<2>(h, map, a, splits) : launch_gram_tc<1>(h, map, a, splits);
+}
+
 template <typename T>
 ffdas_error_t launch_gemm(ffdas_context &h, const tr_gemm_args<T> &a, int splits) {
     const int64_t gx = (a.N + kTrTile - 1) / kTrTile, gy = (a.M + kTrTile - 1) / kTrTile;
@@ -810,32 +873,41 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
         return FFDAS_SUCCESS;
     }
 
-    // 1. Gram matrix, upper tiles, split over q
-    const int64_t tiles = (p + kTrTile - 1) / kTrTile;
-    const int64_t tri = tiles * (tiles + 1) / 2;
-    // one wave: as many CTAs as the SMs hold at this kernel's occupancy
-    int per_sm = 0;
-    FFDAS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tr_gemm_kernel<T>, kTrThreads, 0));
-    int64_t splits = std::max<int64_t>(1, (int64_t)std::max(per_sm, 1) * h.sm_count / tri);
-    splits = std::max<int64_t>(1, std::min<int64_t>(splits, (q + kTrTileK - 1) / kTrTileK));
-    splits = std::max<int64_t>(1, std::min<int64_t>(splits, (int64_t)(kGramPartialBytes / ((size_t)p * p * sizeof(T)))));
-    splits = std::min<int64_t>(splits, 65535);
-    int64_t kchunk = (q + splits - 1) / splits;
-    kchunk = (kchunk + kTrTileK - 1) / kTrTileK * kTrTileK;
-    splits = (q + kchunk - 1) / kchunk;
-
+    // 1. Gram matrix split over q: on the tensor cores (FP32 rows up to 256),
+    // else the FMA kernel over the upper tiles
     workspace part(h), gram(h), eig(h), info(h);
-    FFDAS_TRY(part.alloc((size_t)(splits * p * p) * sizeof(T)));
+    int64_t splits = 0, gram_grid = 0;
+    bool tensor = false;
+    if (gram_tc_usable<T>(h, x, rows, p, q, n)) {
+        FFDAS_TRY(gram_tc_partials(h, reinterpret_cast<const float *>(x), p, q, n, part, splits, tensor));
+        gram_grid = splits;
+    }
+    if (!tensor) {
+        const int64_t tiles = (p + kTrTile - 1) / kTrTile;
+        const int64_t tri = tiles * (tiles + 1) / 2;
+        // one wave: as many CTAs as the SMs hold at this kernel's occupancy
+        int per_sm = 0;
+        FFDAS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tr_gemm_kernel<T>, kTrThreads, 0));
+        splits = std::max<int64_t>(1, (int64_t)std::max(per_sm, 1) * h.sm_count / tri);
+        splits = std::max<int64_t>(1, std::min<int64_t>(splits, (q + kTrTileK - 1) / kTrTileK));
+        splits = std::max<int64_t>(1, std::min<int64_t>(splits, (int64_t)(kGramPartialBytes / ((size_t)p * p * sizeof(T)))));
+        splits = std::min<int64_t>(splits, 65535);
+        int64_t kchunk = (q + splits - 1) / splits;
+        kchunk = (kchunk + kTrTileK - 1) / kTrTileK * kTrTileK;
+        splits = (q + kchunk - 1) / kchunk;
+        FFDAS_TRY(part.alloc((size_t)(splits * p * p) * sizeof(T)));
+        tr_gemm_args<T> g{};
+        g.L = x; g.li = sp; g.lk = sq;
+        g.R = x; g.rk = sq; g.rj = sp; g.conj_r = 1;
+        g.C = part.get<T>(); g.ci = p; g.cj = 1; g.zstride = p * p;
+        g.M = p; g.N = p; g.K = q; g.kchunk = kchunk; g.upper = 1; g.sign = 1;
+        FFDAS_TRY(launch_gemm(h, g, (int)splits));
+        gram_grid = tiles * tiles * splits;
+    }
     FFDAS_TRY(gram.alloc((size_t)(p * p) * sizeof(T)));
     FFDAS_TRY(eig.alloc((size_t)p * sizeof(real)));
     FFDAS_TRY(info.alloc(2 * sizeof(int)));   // solver status, subspace-iteration status
-
-    tr_gemm_args<T> g{};
-    g.L = x; g.li = sp; g.lk = sq;
-    g.R = x; g.rk = sq; g.rj = sp; g.conj_r = 1;
-    g.C = part.get<T>(); g.ci = p; g.cj = 1; g.zstride = p * p;
-    g.M = p; g.N = p; g.K = q; g.kchunk = kchunk; g.upper = 1; g.sign = 1;
-    FFDAS_TRY(launch_gemm(h, g, (int)splits));
+    h.last.copy_engine = tensor ? 2 : 1;
     {
         const int64_t blocks = (p * p + 31) / 32;
         if (blocks > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
@@ -874,7 +946,7 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
             gram.get<T>(), (int)p, r, kOiMaxIter, oi_tol<T>(), basis.get<T>(), info.get<int>() + 1);
         FFDAS_TRY(ffdas_launch_check(h.stream));
         h.last.variant = kRouteSubspace;
-        h.last.grid = tiles * tiles * splits;
+        h.last.grid = gram_grid;
         h.last.kernels = 4;
         int converged = 0;
         FFDAS_CUDA(cudaMemcpyAsync(&converged, info.get<int>() + 1, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
@@ -927,7 +999,7 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
                             info.get<int>());
     if (st != CUSOLVER_STATUS_SUCCESS) return FFDAS_ERROR_CUSOLVER;
     h.last.variant = ranged ? kRouteSyevdx : kRouteSyevd;
-    h.last.grid = tiles * tiles * splits;
+    h.last.grid = gram_grid;
     h.last.kernels = 4;
     if (ranged) {
         e0 = 0;           // the r vectors sit in columns 0..r-1

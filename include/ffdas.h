@@ -17,6 +17,15 @@
  *   - ffdas_das_set_config / ffdas_das_get_config: kernel schedule override
  *     used by the autotuner.
  *   - ffdas_get_last_kernel_info: which kernel the last call launched.
+ *   - ffdas_set_pair_buffer / ffdas_das_pair_bytes: interpolation pairs kept
+ *     from a forward call for the backward on the same data.
+ *   - ffdas_set_channel_scale: per-channel gain applied at the ingest.
+ *   - ffdas_das_static: forward without device allocation or handle.
+ *   - ffdas_sparse_select: das_sparse index lists selected on the device.
+ *   - ffdas_set_gram_engine: tensor-core or FP32-FMA Gram in truncate_rank.
+ *   - ffdas_set_kernel_timing / ffdas_get_last_kernel_time /
+ *     ffdas_get_last_kernel_units / ffdas_measure_fp32_peak /
+ *     ffdas_get_device_status: measurement and bounded-wait status.
  *
  * Conventions (unchanged from the reference):
  *   - dims and strides are in ELEMENTS; strides == NULL means C-contiguous.
@@ -164,7 +173,8 @@ typedef struct {
 /* What the last das/das_sparse/backward call on a handle launched (new).
  * After ffdas_truncate_rank, variant is its eigen route: 10 orthogonal
  * iteration on the device, 11 cuSOLVER syevd, 12 syevdx over one index
- * range, 13 keep-all copy; grid is the Gram kernel's CTA count. */
+ * range, 13 keep-all copy; grid is the Gram kernel's CTA count and
+ * copy_engine the Gram engine (1 FP32 FMA, 2 tensor cores). */
 typedef struct {
     int32_t variant;
     int32_t tile_x, tile_y, tile_z;
@@ -387,7 +397,11 @@ FFDAS_API ffdas_error_t ffdas_sparse_select(
  * not converge, cuSOLVER's syevd/syevdx (loaded at the first call that
  * needs it) solves the eigenproblem and reports through FFDAS_ERROR_CUSOLVER.  The call
  * waits on the host for the eigen step's status, so, like the reference's,
- * it cannot be captured in a CUDA graph. */
+ * it cannot be captured in a CUDA graph.  The Gram matrix of the smaller
+ * side is formed on the tensor cores (tcgen05, FP32 split into two TF32
+ * parts, three products) for float32 with m <= n, m <= 256, n a multiple
+ * of 4 and x 16-byte aligned, else with FP32 FMAs; see
+ * ffdas_set_gram_engine. */
 FFDAS_API ffdas_error_t ffdas_truncate_rank(
     ffdas_handle_t handle,
     ffdas_tensor_desc_t x_desc,
@@ -397,6 +411,18 @@ FFDAS_API ffdas_error_t ffdas_truncate_rank(
     ffdas_tensor_desc_t out_desc,
     void *out
 );
+
+/* New: engine of ffdas_truncate_rank's Gram matrix on this handle.
+ * 0 (default): tensor cores where the input qualifies (see above) and
+ * m * n >= 2^20, else the FP32 FMA kernel; 1: always the FP32 FMA kernel
+ * (every product and sum in FP32, as the reference's cuBLAS SGEMM);
+ * 2: tensor cores wherever the input qualifies.  Tensor-core Gram entries
+ * carry about 2^-21 relative error per product (the dropped lo*lo term and
+ * TF32 rounding of the low part) against FP32's 2^-24; both sum in FP32
+ * within a CTA and in double across CTAs.  After the call,
+ * ffdas_get_last_kernel_info's copy_engine is the engine used (1 FMA,
+ * 2 tensor cores).  Other values: FFDAS_ERROR_INVALID_ARGUMENT. */
+FFDAS_API ffdas_error_t ffdas_set_gram_engine(ffdas_handle_t handle, int32_t engine);
 
 /* New: schedule override for the following calls on this handle
  * (NULL restores the planner default). */

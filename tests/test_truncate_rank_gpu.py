@@ -260,3 +260,79 @@ def test_iteration_falls_back_without_a_gap():
         assert _route() == 12, (start, stop, _route())
         ref = tro.truncate_rank_f64(x.cpu().numpy(), start, stop)
         assert np.abs(res - ref).max() / np.abs(x.cpu().numpy()).max() <= 1e-9
+
+
+# ------------------------------------------ tensor-core (tcgen05) Gram
+
+def _engine_call(engine, x, start, stop=None):
+    h = get_library_handle(torch.device(DEV))
+    h.set_gram_engine(engine)
+    try:
+        res = ffdas_b200.truncate_rank(x, start, stop)
+        info = h.last_kernel_info()
+    finally:
+        h.set_gram_engine(0)
+    return res, info
+
+
+@pytest.mark.parametrize("m, n", [(2, 64), (16, 4096), (100, 1000), (128, 3000), (129, 3000),
+                                  (144, 2048), (250, 256), (256, 2052), (200, 102400)])
+def test_tensor_core_gram(m, n):
+    # one and two 128-row blocks, product widths that are not a multiple of
+    # 16 rows, column counts that are not a multiple of the 32-column stage
+    # (the last stage reads zeros past n), fewer columns than CTAs, and the
+    # 200 x 102400 ensemble; against the float64 oracle at the FP32 bar and
+    # against the FP32 FMA Gram
+    rank = min(3, m - 1)
+    x = _cuda(tro.clutter_ensemble(m, n, rank=rank, seed=m + 3 * n).astype(np.float32))
+    xs = x.cpu().numpy()
+    scale = np.abs(xs).max()
+    orc = tro.truncate_rank_f64(xs, rank)
+    tc, info = _engine_call(2, x, rank)
+    assert info["copy_engine"] == 2, info
+    fma, info1 = _engine_call(1, x, rank)
+    assert info1["copy_engine"] == 1, info1
+    e_tc = np.abs(tc.cpu().numpy() - orc).max() / scale
+    e_fma = np.abs(fma.cpu().numpy() - orc).max() / scale
+    assert e_tc <= 2e-5, (e_tc, e_fma)
+    assert e_tc <= max(2 * e_fma, 2e-6), (e_tc, e_fma)
+    # the kept window too: the leading ranks themselves
+    tc_keep, _ = _engine_call(2, x, 0, rank)
+    assert np.abs(tc_keep.cpu().numpy() - tro.truncate_rank_f64(xs, 0, rank)).max() / scale <= 2e-5
+    assert get_library_handle(torch.device(DEV)).device_status() == 0
+
+
+def test_tensor_core_gram_deterministic_and_default():
+    x = _cuda(tro.clutter_ensemble(200, 20480, rank=5, seed=4).astype(np.float32))
+    a, info = _engine_call(0, x, 5)
+    assert info["copy_engine"] == 2, info          # 200 x 20480 >= 2^20 elements: tensor cores by default
+    b, _ = _engine_call(0, x, 5)
+    assert torch.equal(a, b)                        # fixed split ranges and reduction order
+    small = _cuda(tro.clutter_ensemble(16, 4096, rank=2, seed=4).astype(np.float32))
+    _, info = _engine_call(0, small, 2)
+    assert info["copy_engine"] == 1, info           # small: the FMA kernel
+
+
+@pytest.mark.parametrize("case", ["odd_row_stride", "transposed", "float64", "complex64", "p_over_256"])
+def test_tensor_core_gram_not_eligible(case):
+    # inputs the tensor-core Gram does not take run the FMA kernel even when
+    # it is requested
+    shape, dtype, cplx = {"odd_row_stride": ((64, 4098), torch.float32, False),
+                          "transposed": ((4096, 64), torch.float32, False),
+                          "float64": ((64, 4096), torch.float64, False),
+                          "complex64": ((64, 4096), torch.complex64, True),
+                          "p_over_256": ((260, 4096), torch.float32, False)}[case]
+    x = _cuda(tro.clutter_ensemble(*shape, rank=3, complex_=cplx, seed=2), dtype)
+    res, info = _engine_call(2, x, 3)
+    assert info["copy_engine"] == 1, info
+    ref = tro.truncate_rank_f64(x.cpu().numpy(), 3)
+    tol = 1e-9 if dtype == torch.float64 else 2e-5
+    assert np.abs(res.cpu().numpy() - ref).max() / np.abs(x.cpu().numpy()).max() <= tol
+
+
+def test_gram_engine_rejects_unknown_values():
+    h = get_library_handle(torch.device(DEV))
+    for bad in (-1, 3):
+        with pytest.raises(Exception):
+            h.set_gram_engine(bad)
+    h.set_gram_engine(0)
