@@ -12,11 +12,14 @@
 // with V the right singular vectors, the same result).
 //
 // Steps on the device:
-//  1. G = A A^H / q, p x p: a tiled SIMT product over the upper-triangle
-//     tiles only, split over q into partial sums that a second kernel adds in
-//     a fixed order in double.  The sum is therefore the same on every run.
-//     It is written as the column-major Hermitian matrix that the solver
-//     takes.  The reference forms the full product with one cuBLAS GEMM.
+//  1. G = A A^H / q, p x p, split over q into partial sums that a second
+//     kernel adds in a fixed order in double.  The sum is therefore the same
+//     on every run.  It is written as the column-major Hermitian matrix that
+//     the solver takes.  The reference forms the full product with one
+//     cuBLAS GEMM.  FP32 rows (A = x, p <= 256) run on the tensor cores
+//     (gram_tc.cuh: tcgen05, each element split into two TF32 parts, three
+//     products); every other case, or ffdas_set_gram_engine(1), runs a tiled
+//     SIMT product over the upper-triangle tiles only.
 //  2. The basis of step 3.  When it is the leading subspace (the clutter
 //     filter: remove ranks 0..start-1; or keep ranks 0..stop-1) and has at
 //     most 16 vectors, an orthogonal iteration in double on the device
@@ -40,9 +43,10 @@
 //     bases run as two tiled products through a (r, q) workspace.
 //  With k = p (keep everything) out is x, copied.
 //
-// The tensor cores are not used.  The reference computes in FP32/FP64, and
-// the filter subtracts a dominant component.  A TF32 product carries errors
-// of about 1e-3 of |x|, which is the size of the signal that remains.
+// A single TF32 product would not do: the filter subtracts a dominant
+// component, and TF32 carries errors of about 1e-3 of |x|, the size of the
+// signal that remains.  The three-product split keeps each Gram term within
+// about 2^-21 of |a|^2, and the projection stays in FP32 FMAs.
 #include "core.h"
 #include "gram_tc.cuh"
 
