@@ -4,14 +4,19 @@
 // The reference forms G = A A^T with one cuBLAS GEMM in FP32
 // (src/truncate_rank/truncate_rank_impl.cuh:64-90, 451-480).  Here A is p x q,
 // p <= 256, each row contiguous (K-major), and every CTA (one per SM) sums the
-// columns [z * kchunk, (z + 1) * kchunk) into a p x p row-major FP32 partial;
-// tr_gram_reduce_kernel adds the partials in double in a fixed order.
+// columns [z * kchunk, (z + 1) * kchunk) into a p x p FP32 partial, stored
+// column-major (entry (i, j) at j * p + i: a warp's 32 rows of one column are
+// one 128-byte store); tr_gram_reduce_kernel adds the partials in double in a
+// fixed order.
 //
 // Per CTA, a ring of S stages each holds 32 columns of all 128 * NB rows:
 //  * warp 0 (one lane) loads a stage with one TMA box {32 columns, 128 * NB
 //    rows} and the 128-byte swizzle, which is the K-major layout the MMA
-//    reads (8-row groups 1024 bytes apart); rows past p read as zeros;
-//  * warps 2-5 split each element a into hi = tf32(a), written in place, and
+//    reads (8-row groups 1024 bytes apart); rows past p read as zeros.  A
+//    stage is p row segments of 128 bytes, each in its own DRAM page, so the
+//    same lane also prefetches the boxes kPrefetch chunks ahead into L2: the
+//    stage loads then wait on L2, not on DRAM;
+//  * warps 2-9 split each element a into hi = tf32(a), written in place, and
 //    lo = tf32(a - hi), written to the stage's second buffer at the same
 //    offset (the split is elementwise, so the swizzle is kept), then make the
 //    writes visible to the tensor core's proxy and arrive on the stage;
@@ -25,9 +30,9 @@
 //    with NB = 2, row block 1 against rows 128..128+n1-1 a second one into
 //    columns 256..; the lower-left block, which the symmetric reduce never
 //    reads, is not formed;
-//  * after the last stage warps 2-5 read the accumulators back (warp w reads
-//    tensor-memory lanes 32 (w % 4) .. +31, one row of D per thread) and
-//    store rows and columns below p.
+//  * after the last stage warps 2-9 read the accumulators back (warp w reads
+//    tensor-memory lanes 32 (w % 4) .. +31, one row of D per thread, and
+//    every other 16-column block) and store rows and columns below p.
 // Every wait is bounded (about two seconds of clock): on expiry the CTA
 // records FFDAS device status 1, stops issuing, waits (bounded) for its own
 // copies and products in flight, releases its tensor memory and returns.
@@ -47,12 +52,14 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 namespace gram_tc {
 
 constexpr int kChunk = 32;           // columns per stage: one 128-byte row of FP32
-constexpr int kThreads = 192;        // warp 0 loads, warp 1 issues products, warps 2-5 split and store
-constexpr int kSplitters = 128;      // threads of warps 2-5
+constexpr int kThreads = 320;        // warp 0 loads, warp 1 issues products, warps 2-9 split and store
+constexpr int kSplitters = 256;      // threads of warps 2-9: two per SM sub-partition, so that one
+                                     // hides the other's shared-memory latency
 constexpr int kRowBytes = kChunk * 4;
 constexpr long long kWaitCycles = 4000000000LL;   // ~2 s at 2 GHz
 constexpr int kStatusTimeout = 1;
 constexpr uint32_t kBlock1Col = 256;             // tensor-memory column of row block 1's accumulator
+constexpr int kPrefetch = 8;                     // chunks prefetched into L2 ahead of the stage loads
 
 template <int NB> constexpr int stages() { return NB == 1 ? 6 : 3; }
 template <int NB> constexpr uint32_t stage_bytes() { return (uint32_t)(128 * NB * kRowBytes); }
@@ -68,7 +75,7 @@ struct params {
     int64_t q;          // columns of A
     int64_t kchunk;     // columns per CTA, a multiple of kChunk
     int n0, n1;         // product widths (multiples of 16): rows 0..n0-1 against block 0, 128..128+n1-1 against block 1
-    float *part;        // gridDim.x partials of p x p, row-major
+    float *part;        // gridDim.x partials of p x p, column-major
     int *status;        // device status word
 };
 
@@ -112,6 +119,10 @@ __device__ __forceinline__ void settle(uint32_t bar, uint32_t parity) {
     while (!bar_test(bar, parity) && clock64() - t0 < kWaitCycles) __nanosleep(64);
 }
 
+__device__ __forceinline__ void tma_prefetch(const CUtensorMap *map, int x, int y) {
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];"
+                 ::"l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y) : "memory");
+}
 __device__ __forceinline__ void tma_load(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
@@ -152,21 +163,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&v)[16]) {
 __device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// a = hi + lo + O(2^-22 |a|): both parts TF32 values (round to nearest, ties away)
+// Nearest TF32 value, ties away from zero: add half of the 13 dropped
+// significand bits to the magnitude and clear them (integer ops at full rate;
+// a carry into the exponent gives the next binade, infinities stay).
+__device__ __forceinline__ float round_tf32(float a) {
+    return __uint_as_float((__float_as_uint(a) + 0x1000u) & 0xFFFFE000u);
+}
+// a = hi + lo + O(2^-22 |a|), both parts TF32 values
 __device__ __forceinline__ void split_tf32(float a, float &hi, float &lo) {
-    uint32_t h, l;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(a));
-    hi = __uint_as_float(h);
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(a - hi));
-    lo = __uint_as_float(l);
+    hi = round_tf32(a);
+    lo = round_tf32(a - hi);
 }
 
-// Rows r0..r0+127 of D (one per thread of warps 2-5) from the accumulator at
-// tensor-memory column `col`, columns c0..c0+n-1, into the partial.
-__device__ __forceinline__ void store_block(uint32_t tmem, int quarter, int lane, int r0, int c0, int n, int p,
-                                            bool zero, float *part) {
+// Rows r0..r0+127 of D (one per thread, warp quarter w % 4) from the
+// accumulator at tensor-memory address `tmem`, 16-column blocks `half`,
+// half + 2, ... of the n columns, into columns c0.. of the partial.
+__device__ __forceinline__ void store_block(uint32_t tmem, int quarter, int half, int lane, int r0, int c0, int n,
+                                            int p, bool zero, float *part) {
     const int i = r0 + quarter * 32 + lane;
-    for (int c = 0; c < n; c += 16) {
+    for (int c = 16 * half; c < n; c += 32) {
         uint32_t v[16];
         __syncwarp();    // the load below is warp-collective
         if (!zero) tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c, v);
@@ -174,7 +189,7 @@ __device__ __forceinline__ void store_block(uint32_t tmem, int quarter, int lane
 #pragma unroll
             for (int t = 0; t < 16; t++) {
                 const int j = c0 + c + t;
-                if (j < p) part[(int64_t)i * p + j] = zero ? 0.f : __uint_as_float(v[t]);
+                if (j < p) part[(int64_t)j * p + i] = zero ? 0.f : __uint_as_float(v[t]);
             }
         }
     }
@@ -234,8 +249,11 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(const __grid_const
     if (warp == 0) {
         if (lane == 0) {
             int issued = 0;
+            for (int c = 0; c < nchunks && c < kPrefetch; c++)
+                tma_prefetch(&map, (int)(kbeg + (int64_t)c * kChunk), 0);
             for (int c = 0; c < nchunks; c++) {
                 const int s = c % S;
+                if (c + kPrefetch < nchunks) tma_prefetch(&map, (int)(kbeg + (int64_t)(c + kPrefetch) * kChunk), 0);
                 if (c >= S && !wait(su32(&bars[2 * S + s]), ((c / S) - 1) & 1, abort, a.status)) break;
                 bar_expect(su32(&bars[s]), SB);
                 tma_load(hi0 + s * SB, &map, (int)(kbeg + (int64_t)c * kChunk), 0, su32(&bars[s]));
@@ -296,11 +314,11 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(const __grid_const
         }
         if (wait(done, 0, abort, a.status)) {
             fence_after_sync();
-            const int quarter = warp & 3;
+            const int quarter = warp & 3, half = (warp - 2) >> 2;
             float *part = a.part + (int64_t)blockIdx.x * a.p * a.p;
             const bool zero = nchunks == 0;
-            store_block(tmem, quarter, lane, 0, 0, a.n0, a.p, zero, part);
-            if (NB == 2) store_block(tmem + kBlock1Col, quarter, lane, 128, 128, a.n1, a.p, zero, part);
+            store_block(tmem, quarter, half, lane, 0, 0, a.n0, a.p, zero, part);
+            if (NB == 2) store_block(tmem + kBlock1Col, quarter, half, lane, 128, 128, a.n1, a.p, zero, part);
         }
     }
 

@@ -306,21 +306,23 @@ __global__ void __launch_bounds__(kTrThreads, tr_min_blocks<T>()) tr_gemm_kernel
 }
 
 // G (column-major, p x p, both triangles) = scale * sum over the splits of
-// the row-major partials, in double and in a fixed order: a CTA takes 32
-// consecutive elements, warp w adds splits w, w+8, ..., and the eight warp
-// sums are added in warp order.  Only i <= j is read: every upper-triangle
+// the partials, in double and in a fixed order: a CTA takes 32 consecutive
+// elements, warp w adds splits w, w+8, ..., and the eight warp sums are added
+// in warp order.  The partials are row-major (FMA kernel) or column-major
+// (tensor-core kernel, `cm`); only i <= j is read: every upper-triangle
 // element lies in a computed tile.
 constexpr int kReduceWarps = 8;
 
 template <typename T>
 __global__ void __launch_bounds__(32 * kReduceWarps) tr_gram_reduce_kernel(const T *__restrict__ part, int splits,
-                                                                          int64_t p, double scale,
+                                                                          int64_t p, double scale, int cm,
                                                                           T *__restrict__ G) {
     using acc_t = typename tr_elem<T>::acc;
     __shared__ acc_t red[kReduceWarps][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t e = (int64_t)blockIdx.x * 32 + lane;
-    const int64_t i = e / p, j = e - i * p;
+    const int64_t major = e / p, minor = e - major * p;
+    const int64_t i = cm ? minor : major, j = cm ? major : minor;
     const bool use = e < p * p && i <= j;
     acc_t s = tr_acc_zero<T>();
     if (use) {
@@ -916,7 +918,7 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
         const int64_t blocks = (p * p + 31) / 32;
         if (blocks > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
         tr_gram_reduce_kernel<T><<<(unsigned)blocks, 32 * kReduceWarps, 0, h.stream>>>(
-            part.get<T>(), (int)splits, p, 1.0 / (double)q, gram.get<T>());
+            part.get<T>(), (int)splits, p, 1.0 / (double)q, tensor ? 1 : 0, gram.get<T>());
         FFDAS_TRY(ffdas_launch_check(h.stream));
     }
 
