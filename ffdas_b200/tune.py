@@ -140,6 +140,36 @@ def schedule(cfg: dict | None, device=None):
 
 _MIN_TIMED_MS = 2.0      # a timed run of a small call repeats it until about this much device time
 _MAX_REPS = 256
+_GRAPH_BELOW_MS = 0.1    # calls shorter than this are timed as CUDA graph replays
+
+
+def _time_graph(fn, n: int) -> float:
+    """Per-call milliseconds of `n` calls captured into one CUDA graph (the
+    device time of the call itself: no host launch overhead between calls)."""
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        fn()
+    s.synchronize()
+    with torch.cuda.graph(g, stream=s):
+        for _ in range(n):
+            fn()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+
+    def run():
+        with torch.cuda.stream(s):
+            a.record(s)
+            g.replay()
+            b.record(s)
+        b.synchronize()
+        return a.elapsed_time(b) / n
+
+    run()
+    best = min(run(), run(), run())
+    del g
+    return best
 
 
 def _time(fn, reps: int) -> float:
@@ -147,7 +177,10 @@ def _time(fn, reps: int) -> float:
 
     Calls of a few microseconds are repeated until a run holds about 2 ms of
     device time, so that launch jitter does not decide between schedules whose
-    difference is a few percent."""
+    difference is a few percent.  Calls under 0.1 ms are timed as replays of a
+    CUDA graph holding the repeated calls: issued one by one from Python they
+    are bound by the host, and every schedule would time the same; under a
+    graph (the way `DASRunner` runs them) the device time decides."""
     fn()
     torch.cuda.synchronize()
     a = torch.cuda.Event(enable_timing=True)
@@ -165,6 +198,11 @@ def _time(fn, reps: int) -> float:
     n = reps
     if first * reps < _MIN_TIMED_MS:
         n = min(_MAX_REPS, max(reps, int(_MIN_TIMED_MS / max(first, 1e-3))))
+    if first < _GRAPH_BELOW_MS:
+        try:
+            return _time_graph(fn, n)
+        except RuntimeError:
+            torch.cuda.synchronize()
     return min(first if n == reps else run(n), run(n), run(n))
 
 
