@@ -109,3 +109,86 @@ def test_fp16_input_against_reference_and_oracle():
     e_ref = oracle.rel_l2(ref.cpu().numpy(), exact)
     # our fp16 path interpolates in fp32; the reference interpolates in fp16
     assert e_ours <= e_ref * 1.01 + 1e-6, (e_ours, e_ref)
+
+
+# ------------------------------------------- error codes, against the library
+
+def _codes(L, h, make_desc, x_dims, x_dtype, out_dims, out_dtype, *, x_strides=None, compute=0, alg=0,
+           sparse=None):
+    """One das / das_sparse call on tiny zero-filled buffers through library L
+    (positions, offsets and weights all zero, so every tap reads x[0], x[1])."""
+    import ctypes
+    nx = int(np.prod(x_dims))
+    x = torch.zeros(nx * 4, dtype=torch.float32, device=DEV)
+    out = torch.zeros(max(int(np.prod(out_dims)), 1) * 4, dtype=torch.float32, device=DEV)
+    buf = torch.zeros(1 << 16, dtype=torch.float32, device=DEV)
+    xd = make_desc(x_dims, x_dtype, x_strides)
+    od = make_desc(out_dims, out_dtype, None)
+    beta = (ctypes.c_double * 2)()
+    p = buf.data_ptr()
+    if sparse is None:
+        rc = L.ffdas_das(h, p, None, 0.0, xd, x.data_ptr(), p, p, p, ctypes.cast(beta, ctypes.c_void_p), od,
+                         out.data_ptr(), compute, alg)
+    else:
+        rc = L.ffdas_das_sparse(h, p, None, 0.0, xd, x.data_ptr(), p, p, p, sparse, p,
+                                ctypes.cast(beta, ctypes.c_void_p), od, out.data_ptr(), compute, alg)
+    torch.cuda.synchronize()
+    return rc
+
+
+def test_rejections_match_reference_library():
+    # Every invalid call that the reference rejects before it launches
+    # anything, made on both libraries with their own descriptors: the codes
+    # must be equal (and nonzero).  Cases where the libraries differ by design
+    # (int16 data, null pointers, size-1 dims with huge strides) are held in
+    # tests/test_capi.py.
+    import ctypes
+    from ffdas_b200 import _lib
+    from ffdas_b200._lib import DataType
+    ours_h = ffdas_b200.get_library_handle(DEV)
+    ours_h.set_stream(torch.cuda.current_stream().cuda_stream)
+    keep = []
+
+    def ours_desc(dims, dtype, strides):
+        d = _lib.TensorDesc(list(dims), list(strides) if strides else None, dtype)
+        keep.append(d)
+        return d.desc
+
+    RL = reference.lib()
+
+    def ref_desc(dims, dtype, strides):
+        d = ctypes.c_void_p()
+        arr = (ctypes.c_int64 * len(dims))(*dims)
+        st = (ctypes.c_int64 * len(dims))(*strides) if strides else None
+        assert RL.ffdas_create_tensor_desc(ctypes.byref(d), len(dims), arr, st, int(dtype)) == 0
+        keep.append(d)
+        return d
+
+    R32, R16, C32, R64 = DataType.R_32F, DataType.R_16F, DataType.C_32F, DataType.R_64F
+    ok = ([1, 2, 2, 16], R32, [1, 4], R32)
+    cases = [
+        ("out dtype", ([1, 2, 2, 16], R32, [1, 4], C32), {}),
+        ("x dtype int32", ([1, 2, 2, 16], DataType.R_32I, [1, 4], R32), {}),
+        ("x 2-D", ([2, 16], R32, [4], R32), {}),
+        ("x 5-D", ([1, 1, 2, 2, 16], R32, [1, 4], R32), {}),
+        ("batch mismatch", ([2, 2, 2, 16], R32, [3, 4], R32), {}),
+        ("sample stride 2", ([1, 2, 2, 16], R32, [1, 4], R32), dict(x_strides=[64, 32, 16, 2])),
+        ("int32 indexing", ([2, 2, 2, 16], R32, [2, 4], R32), dict(x_strides=[1 << 31, 32, 16, 1])),
+        ("ALG3", ok, dict(alg=3)),
+        ("FP64 with ALG2", ([1, 2, 2, 16], R64, [1, 4], R64), dict(alg=2)),
+        ("half data, half compute", ([1, 2, 2, 16], R16, [1, 4], R32), dict(compute=1)),
+        ("sparse count 0", ok, dict(sparse=0)),
+        ("sparse with ALG2", ok, dict(sparse=2, alg=2)),
+    ]
+    rh = reference.handle(0)
+    RL.ffdas_set_stream(rh, torch.cuda.current_stream().cuda_stream)
+    for name, args, kw in cases:
+        a = _codes(_lib.load(), ours_h.h, ours_desc, *args, **kw)
+        b = _codes(RL, rh, ref_desc, *args, **kw)
+        assert a == b and a != 0, (name, a, b)
+    # and the same valid call succeeds on both
+    assert _codes(_lib.load(), ours_h.h, ours_desc, *ok) == 0
+    assert _codes(RL, rh, ref_desc, *ok) == 0
+    for d in keep:
+        if isinstance(d, ctypes.c_void_p):
+            RL.ffdas_destroy_tensor_desc(d)
