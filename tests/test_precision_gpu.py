@@ -15,14 +15,17 @@ Two questions are asked of each channel-data dtype:
   itself is held to 1e-5 elsewhere).  The 16-bit pair formats must not add to
   it beyond the 1e-3 target.
 * storage error -- the image of the 16-bit data against the FP64 oracle of the
-  original FP32 data: quantising the channel data itself.  Measured on B200
-  (this library; the FP64 oracle of the quantised data alone in brackets):
-  bf16 (8-bit mantissa) 1.04e-3 (1.02e-3) on these four planes and 1.72e-3
-  (1.70e-3) on eight; fp16 (11 bits) 1.6e-4 (1.2e-4) and 3.7e-4 (3.2e-4).
-  The 1e-3 bar therefore holds for fp16 storage and, for bf16, only against
-  the oracle of the same bf16 data (the compute error above): rounding the
-  data to 8 bits already costs 1.0-1.7e-3, whatever the kernel does.  The
-  bf16 storage check stays at 2e-3 for that reason.
+  original FP32 data: quantising the channel data itself.  Over the whole
+  image it is far inside the 1e-3 bar: the FP64 oracle of the bf16 data
+  against that of the FP32 data gives 3.1e-5 relative L2 over all 128 depth
+  planes (fp16: 2.6e-6), and 1.4-5.4e-5 over every 2nd, 4th, 8th or 16th
+  plane, so the 16 planes 0, 8, ..., 120 stand for the volume here and are
+  held to 1e-3.  Planes 66-127 lie past the end of the 4096-sample record
+  and image to zero.  Plane by plane the relative error is larger where
+  little signal is left: on the four planes below (two of them empty) bf16
+  measured 1.04e-3 (the oracle of the bf16 data alone: 1.02e-3) and on eight
+  1.72e-3 (1.70e-3); fp16 1.6e-4 and 3.7e-4.  Those four-plane checks stay
+  at 2e-3 (bf16) and 1e-3 (fp16).
 """
 import numpy as np
 import pytest
@@ -71,3 +74,28 @@ def test_storage_error_vs_fp64_oracle_of_fp32_data(volume, dtype, tol):
     xn, geo, ref = volume
     img = ffdas_b200.das(xn.to(dtype), *geo)
     assert oracle.rel_l2(img.cpu().numpy(), ref(torch.float32)) < tol
+
+
+@pytest.fixture(scope="module")
+def volume16():
+    # depth planes 0, 8, ..., 120 of the same volume
+    wl = W.diverging3d(device=DEV)
+    xn = W.normalize_channels(wl["x"])
+    sel = torch.arange(0, 128, 8, device=DEV)
+    geo = (wl["srcpos"], wl["dstpos"][sel].contiguous(), wl["offsets"][:, sel].contiguous(),
+           wl["weights"][:, sel].contiguous())
+    ref = oracle.das_f64(xn.double().cpu().numpy(), *[t.cpu().numpy() for t in geo])
+    return xn, geo, ref
+
+
+@pytest.mark.parametrize("dtype", [torch.bfloat16, torch.float16])
+def test_storage_error_over_the_volume(volume16, dtype):
+    # the 16-bit image against the FP64 oracle of the FP32 data over 16
+    # planes spread through the volume: the 1e-3 bar
+    xn, geo, ref = volume16
+    img = ffdas_b200.das(xn.to(dtype), *geo)
+    err = oracle.rel_l2(img.cpu().numpy(), ref)
+    assert err < 1e-3, err
+    # the FP32 / FP16 pair storage of FP32 data on the same planes, same bar
+    img_p = ffdas_b200.das(xn, *geo, **({"use_bf16": True} if dtype == torch.bfloat16 else {"use_fp16": True}))
+    assert oracle.rel_l2(img_p.cpu().numpy(), ref) < 1e-3
