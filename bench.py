@@ -608,15 +608,20 @@ def bwd_extras(args, h) -> dict:
     gdsc = _lib.TensorDesc(list(gout.shape), None, DataType.R_32F)
     L = _lib.load()
     reuse = [True]
+    every_grad = [True]
 
     def bwd():
         h.set_stream(torch.cuda.current_stream(dev).cuda_stream)
         if reuse[0]:
             h.set_pair_buffer(pairs.data_ptr(), nbytes)
+        # every_grad False: the gradients an autofocus step takes (the delays
+        # and both position sets scale with the sound speed; x and the
+        # weights do not), as the autograd function passes them
+        gxp, gwp = (gx.data_ptr(), gw.data_ptr()) if every_grad[0] else (None, None)
         _lib.check(L.ffdas_das_backward(h.h, af["srcpos"].data_ptr(), None, 0.0, xdsc.desc, xa.data_ptr(),
                                         af["dstpos"].data_ptr(), af["offsets"].data_ptr(), af["weights"].data_ptr(),
-                                        0, None, gdsc.desc, gout.data_ptr(), gx.data_ptr(), go.data_ptr(),
-                                        gw.data_ptr(), gd.data_ptr(), gs.data_ptr()))
+                                        0, None, gdsc.desc, gout.data_ptr(), gxp, go.data_ptr(),
+                                        gwp, gd.data_ptr(), gs.data_ptr()))
         h.set_pair_buffer(None, 0)
 
     table = []
@@ -635,11 +640,17 @@ def bwd_extras(args, h) -> dict:
     reuse[0] = False
     h.set_config(bcfg)
     msb_own = timed(bwd, args.steps, args.warmup, stream, 1)
+    reuse[0], every_grad[0] = True, False
+    msb_af = timed(bwd, args.steps, args.warmup, stream, 1)
     h.set_config(None)
     return {"bwd_fwd": {"ratio": msb / msf, "fwd_ms": msf, "bwd_ms": msb,
                         "bwd_ms_own_pairs": msb_own, "ratio_own_pairs": msb_own / msf,
                         "pairs": "the backward reads the pair rows the forward built (ffdas_set_pair_buffer), as "
                                  "the autograd function does; ratio_own_pairs: it builds them itself",
+                        "bwd_ms_autofocus_grads": msb_af, "ratio_autofocus_grads": msb_af / msf,
+                        "autofocus_grads": "the gradients an autofocus step takes: delays, voxel and channel "
+                                           "positions (x and the weights do not depend on the sound speed, so "
+                                           "the autograd function passes no buffers for them)",
                         "fwd_schedule": finfo, "bwd_schedule": binfo, "bwd_config": bcfg,
                         "bwd_table": [[m, c, i["variant"]] for m, c, i in table],
                         "workload": "autofocus: 128 ch, 8 plane waves, batch 4, 2048 samples, 256x256 voxels; "

@@ -60,6 +60,26 @@ def test_gradients_match_float64_reference(B):
         assert err < 2e-4, (name, err)
 
 
+@pytest.mark.parametrize("B", [1, 4])
+def test_autofocus_gradient_subset_matches_float64_reference(B):
+    # the gradients an autofocus step takes (delays, voxel and channel
+    # positions; x and the weights hold no grad), which the backward computes
+    # without the channel-data scatter
+    cpu = _problem(4, B=B)
+    need = [False, True, True, True, False]
+    gpu = [t.to(DEV).requires_grad_(n) for t, n in zip(cpu, need)]
+    ref = [t.double().requires_grad_(n) for t, n in zip(cpu, need)]
+    g = torch.randn((B, *cpu[2].shape[:-1]), generator=torch.Generator().manual_seed(5))
+    das_autograd(*gpu).backward(g.to(DEV))
+    das_ref(*ref).backward(g.double())
+    for name, a, b, n in zip(["x", "srcpos", "dstpos", "offsets", "weights"], gpu, ref, need):
+        if not n:
+            assert a.grad is None, name
+            continue
+        err = oracle.rel_l2(a.grad.cpu().numpy(), b.grad.numpy())
+        assert err < 2e-4, (name, err)
+
+
 def test_sparse_gradients_match_reference():
     x, src, dst, offs, w = _problem(4, B=2, S=5)
     idx = torch.randint(0, 5, (3, *dst.shape[:-1]), generator=torch.Generator().manual_seed(5)).int()
