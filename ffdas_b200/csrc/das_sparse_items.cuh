@@ -188,7 +188,6 @@ __global__ void __launch_bounds__(kStThreads, 2) das_sparse_items_kernel(const s
     const st *__restrict__ Pg = static_cast<const st *>(p.P);
     const uint32_t kmax_pair = (uint32_t)(p.npad - 1);
     const uint32_t ring_u32 = smem_u32(sm.ring);
-    const int passes = (p.S + SC - 1) / SC;
     int stage = 0;
     uint32_t phase = 0;
     bool dead = false;
