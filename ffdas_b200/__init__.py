@@ -11,7 +11,7 @@ loads the compiled library and fails if it is missing.
 from . import _lib
 from ._lib import Algorithm, ComputeType, DataType, DasConfig, FFDASError
 from .library import get_cuda_device, set_cuda_device, get_library_handle
-from .das import das, das_sparse, sparse_select, DowncastWarning
+from .das import das, das_from_host, das_sparse, sparse_select, DowncastWarning
 from .timing import Timer
 from .truncate_rank import truncate_rank
 
@@ -20,6 +20,6 @@ _lib.load()
 __version__ = "0.1.0"
 
 __all__ = [
-    "das", "das_sparse", "sparse_select", "truncate_rank", "Algorithm", "ComputeType", "DataType", "DasConfig", "FFDASError",
+    "das", "das_from_host", "das_sparse", "sparse_select", "truncate_rank", "Algorithm", "ComputeType", "DataType", "DasConfig", "FFDASError",
     "DowncastWarning", "get_cuda_device", "set_cuda_device", "get_library_handle", "Timer",
 ]

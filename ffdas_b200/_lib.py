@@ -140,6 +140,8 @@ SIGNATURES = {
     "ffdas_get_last_kernel_units": (c_err, [c_handle, ctypes.POINTER(ctypes.c_longlong)]),
     "ffdas_set_channel_scale": (c_err, [c_handle, c_ptr, ctypes.c_int64]),
     "ffdas_set_gram_engine": (c_err, [c_handle, ctypes.c_int32]),
+    "ffdas_das_from_host": (c_err, [c_handle, c_ptr, c_ptr, ctypes.c_float, c_desc, c_ptr, c_ptr, c_ptr, c_ptr,
+                                    c_ptr, c_desc, c_ptr, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "ffdas_set_pair_buffer": (c_err, [c_handle, c_ptr, ctypes.c_size_t]),
     "ffdas_das_pair_bytes": (c_err, [c_desc, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "ffdas_measure_fp32_peak": (c_err, [c_handle, ctypes.POINTER(ctypes.c_double)]),

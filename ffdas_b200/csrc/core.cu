@@ -222,6 +222,12 @@ ffdas_error_t ffdas_destroy(ffdas_handle_t h) {
     }
     if (h->ev_start) cudaEventDestroy(h->ev_start);
     if (h->ev_stop) cudaEventDestroy(h->ev_stop);
+    for (cudaEvent_t e : h->upload_ev)
+        if (e) cudaEventDestroy(e);
+    if (h->upload_stream) {
+        cudaStreamSynchronize(h->upload_stream);
+        cudaStreamDestroy(h->upload_stream);
+    }
     if (h->status) cudaFree(h->status);
     if (h->solver && h->solver_release) h->solver_release(h->solver);
     cudaGetLastError();

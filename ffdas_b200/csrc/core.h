@@ -75,6 +75,11 @@ struct ffdas_context {
     } pair_sig;
     bool last_pairs_reused = false;   // the last ffdas_das_backward read the pair buffer
     int gram_engine = 0;              // ffdas_set_gram_engine: 0 auto, 1 FP32 FMA, 2 tensor cores
+    // ffdas_das_from_host: the stream that uploads channel chunks, and one
+    // event per chunk plus one for the start (created at the first call)
+    static constexpr int kUploadEvents = 17;
+    cudaStream_t upload_stream = nullptr;
+    cudaEvent_t upload_ev[kUploadEvents] = {};
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     // eigensolver state of ffdas_truncate_rank, created on its first call and
     // released with the handle

@@ -803,7 +803,152 @@ static ffdas_error_t das_entry(ffdas_handle_t handle, das_call &a) {
     return das_forward(*handle, a);
 }
 
+// ------------------------------------------- host-resident channel data ---
+// ffdas_das_from_host: ffdas_das on channel data in host memory.  The
+// channels are cut into K chunks; the handle's upload stream copies chunk
+// k + 1 (one cudaMemcpyAsync per batch item) while the handle's stream runs
+// chunk k's ingest and delay-and-sum, which waits only for its own chunk's
+// event; chunk 0 applies the caller's beta and every later chunk adds into
+// the image (beta = 1).  So the upload of all but the first chunk hides behind
+// the beamforming, where a copy followed by ffdas_das pays for both.
+namespace {
+
+constexpr int kHostChunksMax = ffdas_context::kUploadEvents - 1;
+
+ffdas_error_t upload_resources(ffdas_context &h) {
+    if (!h.upload_stream) FFDAS_CUDA(cudaStreamCreateWithFlags(&h.upload_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t &e : h.upload_ev)
+        if (!e) FFDAS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return FFDAS_SUCCESS;
+}
+
+// Channels per chunk: about C / 8 when there are 1024 channels, never under
+// 128 channels, rounded to the 8 channels of one staged-kernel stage.
+int host_chunk_channels(int64_t C, int chunks) {
+    int64_t k = chunks > 0 ? chunks : std::max<int64_t>(1, std::min<int64_t>(8, C / 128));
+    k = std::min<int64_t>(std::min<int64_t>(k, kHostChunksMax), std::max<int64_t>(C, 1));
+    int64_t cc = (C + k - 1) / k;
+    if (k > 1) cc = (cc + 7) / 8 * 8;
+    return (int)std::max<int64_t>(cc, 1);
+}
+
+ffdas_error_t das_from_host(ffdas_context &h, const das_call &a0, int chunks) {
+    const ffdas_tensor_desc &xd = *a0.x_desc;
+    if (xd.ndim != 3 && xd.ndim != 4) return FFDAS_ERROR_INVALID_DIMS;
+    const size_t esz = ffdas_type_size(xd.dtype);
+    if (esz == 0) return FFDAS_ERROR_UNSUPPORTED_TYPE;
+    int64_t expect = 1;
+    for (int i = (int)xd.ndim - 1; i >= 0; i--) {   // C-contiguous: chunks are runs of whole channels
+        if (xd.dims[i] > 1 && xd.strides[i] != expect) return FFDAS_ERROR_NON_CONTIGUOUS;
+        expect *= xd.dims[i];
+    }
+    const int cdim = (int)xd.ndim - 3;
+    const int64_t B = xd.ndim == 4 ? xd.dims[0] : 1, C = xd.dims[cdim];
+    const int64_t row = xd.dims[cdim + 1] * xd.dims[cdim + 2];          // S * N elements per channel
+    const int64_t total = B * C * row;
+    if (total > 0 && !a0.x) return FFDAS_ERROR_NULL_POINTER;
+    if (C > 0 && !a0.srcpos) return FFDAS_ERROR_NULL_POINTER;
+    // a per-item channel scale (B x C values) does not split by channel
+    const bool item_scale = h.chan_scale && h.chan_scale_count != C;
+    const int cc = item_scale ? (int)std::max<int64_t>(C, 1) : host_chunk_channels(C, chunks);
+    const int K = (int)std::max<int64_t>(1, (C + cc - 1) / cc);
+
+    FFDAS_TRY(upload_resources(h));
+    workspace X(h);
+    FFDAS_TRY(X.alloc((size_t)std::max<int64_t>(total, 1) * esz));
+    unsigned char *xdev = X.get<unsigned char>();
+    const unsigned char *xh = static_cast<const unsigned char *>(a0.x);
+    // the uploads start after the work already queued on the handle's stream
+    // (the staging buffer's allocation among it)
+    FFDAS_CUDA(cudaEventRecord(h.upload_ev[kHostChunksMax], h.stream));
+    FFDAS_CUDA(cudaStreamWaitEvent(h.upload_stream, h.upload_ev[kHostChunksMax], 0));
+    ffdas_error_t cerr = FFDAS_SUCCESS;
+    for (int k = 0; k < K && cerr == FFDAS_SUCCESS; k++) {
+        const int64_t c0 = (int64_t)k * cc, c1 = std::min<int64_t>(C, c0 + cc);
+        for (int64_t b = 0; b < B && cerr == FFDAS_SUCCESS; b++) {
+            const size_t off = (size_t)((b * C + c0) * row) * esz;
+            if (cudaMemcpyAsync(xdev + off, xh + off, (size_t)((c1 - c0) * row) * esz, cudaMemcpyHostToDevice,
+                                h.upload_stream) != cudaSuccess)
+                cerr = FFDAS_ERROR_CUDA_MEMCPY_FAILED;
+        }
+        if (cerr == FFDAS_SUCCESS && cudaEventRecord(h.upload_ev[k], h.upload_stream) != cudaSuccess)
+            cerr = FFDAS_ERROR_CUDA_RUNTIME;
+    }
+    // The end of this call's uploads, recorded whatever happened above: the
+    // handle's stream waits for it before the staging buffer is released.
+    const cudaEvent_t uploads_done = h.upload_ev[kHostChunksMax];
+    cudaEventRecord(uploads_done, h.upload_stream);
+    if (cerr != FFDAS_SUCCESS) {
+        cudaStreamWaitEvent(h.stream, uploads_done, 0);
+        return cerr;
+    }
+
+    // beta = 1 of the output type, for the chunks after the first
+    const float one_f[2] = {1.f, 0.f};
+    const double one_d[2] = {1.0, 0.0};
+    const ffdas_datatype_t ot = a0.out_desc->dtype;
+    const void *one = (ot == FFDAS_R_64F || ot == FFDAS_C_64F) ? static_cast<const void *>(one_d)
+                                                                : static_cast<const void *>(one_f);
+    // chunks neither fill nor read the caller's pair buffer
+    void *const saved_buf = h.pair_buf;
+    const size_t saved_bytes = h.pair_buf_bytes;
+    const float *const saved_scale = h.chan_scale;
+    const int64_t saved_count = h.chan_scale_count;
+    h.pair_buf = nullptr;
+    h.pair_buf_bytes = 0;
+    ffdas_error_t err = FFDAS_SUCCESS;
+    int kernels = 0;
+    for (int k = 0; k < K && err == FFDAS_SUCCESS; k++) {
+        const int64_t c0 = (int64_t)k * cc, c1 = std::min<int64_t>(C, c0 + cc);
+        ffdas_tensor_desc dk = xd;
+        dk.dims[cdim] = c1 - c0;
+        das_call a = a0;
+        a.x_desc = &dk;
+        a.x = xdev + (size_t)(c0 * row) * esz;
+        a.srcpos = a0.srcpos + 3 * c0;
+        a.srcdir = a0.srcdir ? a0.srcdir + 4 * c0 : nullptr;
+        a.beta = k == 0 ? a0.beta : one;
+        if (saved_scale && !item_scale) {
+            h.chan_scale = saved_scale + c0;
+            h.chan_scale_count = c1 - c0;
+        }
+        err = cudaStreamWaitEvent(h.stream, h.upload_ev[k], 0) == cudaSuccess ? FFDAS_SUCCESS
+                                                                                : FFDAS_ERROR_CUDA_RUNTIME;
+        if (err == FFDAS_SUCCESS) err = das_forward(h, a);
+        kernels += h.last.kernels;
+    }
+    h.pair_buf = saved_buf;
+    h.pair_buf_bytes = saved_bytes;
+    h.chan_scale = saved_scale;
+    h.chan_scale_count = saved_count;
+    h.last.kernels = kernels;
+    // every upload lands before the staging buffer is released on the
+    // handle's stream, whatever happened above
+    if (cudaStreamWaitEvent(h.stream, uploads_done, 0) != cudaSuccess && err == FFDAS_SUCCESS)
+        err = FFDAS_ERROR_CUDA_RUNTIME;
+    return err;
+}
+
+}  // namespace
+
 extern "C" {
+
+ffdas_error_t ffdas_das_from_host(ffdas_handle_t handle, const float *srcpos, const float *srcdir, float wavenum,
+                                  ffdas_tensor_desc_t x_desc, const void *x_host, const float *dstpos,
+                                  const float *offsets, const float *weights, const void *beta,
+                                  ffdas_tensor_desc_t out_desc, void *out, ffdas_compute_type_t compute_type,
+                                  ffdas_alg_t alg, int chunks) {
+    if (!handle) return FFDAS_ERROR_INVALID_HANDLE;
+    FFDAS_TRY(handle->check_device());
+    if (!x_desc || !out_desc) return FFDAS_ERROR_NULL_POINTER;
+    if (chunks < 0) return FFDAS_ERROR_INVALID_ARGUMENT;
+    das_call a;
+    a.srcpos = srcpos; a.srcdir = srcdir; a.wavenum = wavenum;
+    a.x_desc = x_desc; a.x = x_host; a.dstpos = dstpos; a.offsets = offsets; a.weights = weights;
+    a.beta = beta; a.out_desc = out_desc; a.out = out;
+    a.compute_type = compute_type; a.alg = alg; a.sparse = false;
+    return das_from_host(*handle, a, chunks);
+}
 
 ffdas_error_t ffdas_das_pair_bytes(ffdas_tensor_desc_t x_desc, ffdas_compute_type_t compute_type, size_t *bytes) {
     if (!x_desc || !bytes) return FFDAS_ERROR_NULL_POINTER;

@@ -157,16 +157,25 @@ def _needs_grad(*ts) -> bool:
 
 
 def _run(x, srcpos, dstpos, offsets, weights, sparse_indices, *, srcdir, wavenum, algorithm,
-         use_fp16, use_bf16, channels_trailing, out, channel_scale=None):
+         use_fp16, use_bf16, channels_trailing, out, channel_scale=None, host_chunks=None):
     spatial = _check_spatial(dstpos, offsets, weights, sparse_indices)
     xt = _to_torch(x)
     if xt.ndim not in (3, 4):
         raise ValueError("x must have dimensions ([batch,] channels, sequence, samples)")
-    if not xt.is_cuda:
-        raise ValueError("x must be a CUDA tensor")
+    if host_chunks is None:
+        if not xt.is_cuda:
+            raise ValueError("x must be a CUDA tensor")
+        dev = xt.device
+    else:
+        if xt.is_cuda:
+            raise ValueError("das_from_host takes x in host memory; use das for CUDA tensors")
+        sp = _to_torch(srcpos)
+        if not (torch.is_tensor(sp) and sp.is_cuda):
+            raise ValueError("das_from_host needs srcpos, dstpos, offsets and weights on the GPU")
+        dev = sp.device
+        xt = xt.contiguous()
     if xt.dtype not in _FFDAS_DTYPE:
         raise TypeError(f"unsupported channel data dtype {xt.dtype}")
-    dev = xt.device
     srcpos_t = _astype(srcpos, torch.float32, dev, "srcpos")
     dstpos_t = _astype(dstpos, torch.float32, dev, "dstpos")
     offsets_t = _astype(offsets, torch.float32, dev, "offsets")
@@ -202,7 +211,12 @@ def _run(x, srcpos, dstpos, offsets, weights, sparse_indices, *, srcdir, wavenum
                              f"values, got shape {tuple(scale_t.shape)}")
         handle.set_channel_scale(scale_t.data_ptr(), scale_t.numel())
     try:
-        if idx_t is None:
+        if host_chunks is not None:
+            code = L.ffdas_das_from_host(handle.h, ptr(srcpos_t), ptr(srcdir_t), float(wavenum), x_desc.desc,
+                                         ptr(xt), ptr(dstpos_t), ptr(offsets_t), ptr(weights_t),
+                                         ctypes.cast(beta, ctypes.c_void_p), o_desc.desc, ptr(out_t), int(ctype),
+                                         int(algorithm), int(host_chunks))
+        elif idx_t is None:
             code = L.ffdas_das(handle.h, ptr(srcpos_t), ptr(srcdir_t), float(wavenum), x_desc.desc, ptr(xt),
                                ptr(dstpos_t), ptr(offsets_t), ptr(weights_t), ctypes.cast(beta, ctypes.c_void_p),
                                o_desc.desc, ptr(out_t), int(ctype), int(algorithm))
@@ -218,6 +232,30 @@ def _run(x, srcpos, dstpos, offsets, weights, sparse_indices, *, srcdir, wavenum
     if out is not None:
         return out
     return _from_torch_like(out_t, x)
+
+
+def das_from_host(x, srcpos, dstpos, offsets, weights, *, srcdir=None, wavenum: float = 0.0,
+                  algorithm: Algorithm = Algorithm.DEFAULT, use_fp16: bool = False, use_bf16: bool = False,
+                  out=None, channel_scale=None, chunks: int = 0):
+    """`das` on channel data in host memory (ffdas_das_from_host).
+
+    x is a CPU tensor (or array), ([batch,] channels, sequence, samples), best
+    in page-locked memory (`tensor.pin_memory()`) so that its upload overlaps
+    the beamforming; every other tensor and the output are on the GPU.  The
+    channels are uploaded in `chunks` runs (0: about channels / 128, at most
+    8), each beamformed as soon as it has landed and added into the image, so
+    only the first run's copy is not hidden.  The call returns once the work
+    is queued on torch's current stream; x must stay unchanged until then.
+    Same result as `das` up to the rounding of the sum over channels.  No
+    autograd.
+    """
+    if _needs_grad(srcpos, dstpos, offsets, weights) or (torch.is_tensor(x) and x.requires_grad):
+        raise NotImplementedError("das_from_host has no backward; use das on device data")
+    if int(chunks) < 0:
+        raise ValueError("chunks must be >= 0")
+    return _run(x, srcpos, dstpos, offsets, weights, None, srcdir=srcdir, wavenum=wavenum, algorithm=algorithm,
+                use_fp16=use_fp16, use_bf16=use_bf16, channels_trailing=False, out=out,
+                channel_scale=channel_scale, host_chunks=int(chunks))
 
 
 def das(x, srcpos, dstpos, offsets, weights, *, srcdir=None, wavenum: float = 0.0,

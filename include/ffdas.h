@@ -21,6 +21,8 @@
  *     from a forward call for the backward on the same data.
  *   - ffdas_set_channel_scale: per-channel gain applied at the ingest.
  *   - ffdas_das_static: forward without device allocation or handle.
+ *   - ffdas_das_from_host: forward on host-resident channel data, uploads
+ *     overlapped with the beamforming.
  *   - ffdas_sparse_select: das_sparse index lists selected on the device.
  *   - ffdas_set_gram_engine: tensor-core or FP32-FMA Gram in truncate_rank.
  *   - ffdas_set_kernel_timing / ffdas_get_last_kernel_time /
@@ -315,6 +317,26 @@ FFDAS_API ffdas_error_t ffdas_das_backward(
 FFDAS_API ffdas_error_t ffdas_set_pair_buffer(ffdas_handle_t handle, void *buffer, size_t bytes);
 FFDAS_API ffdas_error_t ffdas_das_pair_bytes(ffdas_tensor_desc_t x_desc, ffdas_compute_type_t compute_type,
                                              size_t *bytes);
+
+/* New: ffdas_das on channel data in host memory (page-locked for the copies
+ * to overlap; pageable memory works, serially).  Same arguments as ffdas_das
+ * except that x_host is a host pointer to C-contiguous x, plus `chunks`: the
+ * channels are cut into that many runs (0: about C / 128, at most 8; at most
+ * 16).  The handle's own upload stream copies run k + 1 while the handle's
+ * stream beamforms run k, which waits only for its own run; run 0 applies
+ * beta and every later run adds into out (beta = 1), so only the first run's
+ * upload is not hidden behind the beamforming.  The output, positions,
+ * delays and weights are device buffers as for ffdas_das.  A per-item
+ * channel scale (B * C values) keeps the whole call in one run.  The sum
+ * over channels is grouped by run, so the image differs from ffdas_das's in
+ * rounding only.  Not for ffdas_das_backward's pair reuse (the runs do not
+ * fill the pair buffer).  x_host must stay valid and unchanged until the
+ * call's work on the handle's stream has completed. */
+FFDAS_API ffdas_error_t ffdas_das_from_host(ffdas_handle_t handle, const float *srcpos, const float *srcdir,
+                                            float wavenum, ffdas_tensor_desc_t x_desc, const void *x_host,
+                                            const float *dstpos, const float *offsets, const float *weights,
+                                            const void *beta, ffdas_tensor_desc_t out_desc, void *out,
+                                            ffdas_compute_type_t compute_type, ffdas_alg_t alg, int chunks);
 
 /* New: per-channel scale of the channel data, applied by the ingest of every
  * following ffdas_das / ffdas_das_sparse call on this handle (it replaces the

@@ -713,3 +713,92 @@ def test_sparse_items_3d_volume_and_16bit_storage():
     assert oracle.rel_l2(_np(got), ref) < TOL[torch.float32]
     refb = oracle.das_f64(_np(xb.float()), *geo, _np(ofs_s), _np(w_s), sparse_indices=_np(idx))
     assert oracle.rel_l2(_np(gotb), refb) < TOL[torch.bfloat16]
+
+
+# -------------------------------------------- host-resident channel data ---
+# ffdas_das_from_host: x in host memory, uploaded in channel runs on the
+# handle's upload stream while earlier runs are beamformed.
+
+@pytest.mark.parametrize("B, chunks", [(1, 0), (1, 3), (2, 4), (3, 1), (1, 16)])
+def test_das_from_host_matches_das(rng, B, chunks):
+    x, src, dst, offs, w = _small(rng, B=B, C=40, S=3, N=200, V=(33, 27))
+    xh = x.cpu().pin_memory()
+    got = ffdas_b200.das_from_host(xh, src, dst, offs, w, chunks=chunks)
+    assert got.is_cuda and got.shape == (B, 33, 27)
+    dev = ffdas_b200.das(x, src, dst, offs, w)
+    assert oracle.rel_l2(_np(got), _np(dev)) < 1e-6
+    ref = oracle.das_f64(_np(x), _np(src), _np(dst), _np(offs), _np(w))
+    assert oracle.rel_l2(_np(got), ref) < TOL[torch.float32]
+
+
+def test_das_from_host_staged_volume_beta_and_pageable_memory():
+    # a volume large enough for the staged kernel, run in 8 channel runs:
+    # beta applies once (the first run), the later runs add; pageable host
+    # memory gives the same image
+    import ctypes
+    from ffdas_b200 import _lib
+    from ffdas_b200._lib import DataType
+    wl = W.diverging3d(device=DEV, scale=0.5)          # 256 channels, 64^3 voxels: the staged kernel
+    x = wl["x"]
+    geo = (wl["srcpos"], wl["dstpos"], wl["offsets"], wl["weights"])
+    xh = x.cpu().pin_memory()
+    h = ffdas_b200.get_library_handle(DEV)
+    L = _lib.load()
+    prev = torch.randn((x.shape[0], *wl["dstpos"].shape[:-1]), device=DEV)
+    out = prev.clone()
+    xd = _lib.TensorDesc(list(x.shape), None, DataType.R_32F)
+    od = _lib.TensorDesc(list(out.shape), None, DataType.R_32F)
+    beta = (ctypes.c_float * 2)(0.25, 0.0)
+    h.set_stream(torch.cuda.current_stream().cuda_stream)
+    _lib.check(L.ffdas_das_from_host(h.h, geo[0].data_ptr(), None, 0.0, xd.desc, xh.data_ptr(), geo[1].data_ptr(),
+                                     geo[2].data_ptr(), geo[3].data_ptr(), ctypes.cast(beta, ctypes.c_void_p),
+                                     od.desc, out.data_ptr(), 0, 0, 8))
+    torch.cuda.synchronize()
+    assert h.last_kernel_info()["kernels"] >= 16          # ingest + kernel per run
+    dev = ffdas_b200.das(x, *geo)
+    assert oracle.rel_l2(_np(out), _np(0.25 * prev + dev)) < 1e-6
+    got_pageable = ffdas_b200.das_from_host(x.cpu(), *geo)
+    assert oracle.rel_l2(_np(got_pageable), _np(dev)) < 1e-6
+
+
+def test_das_from_host_channel_scale_and_16bit():
+    # per-channel scale is offset to each run; FP16 host data
+    rng = np.random.default_rng(17)
+    x, src, dst, offs, w = _small(rng, C=48, S=2, N=160, V=(20, 18))
+    scale = torch.linspace(0.5, 2.0, 48, device=DEV)
+    got = ffdas_b200.das_from_host(x.cpu().pin_memory(), src, dst, offs, w, chunks=3, channel_scale=scale)
+    dev = ffdas_b200.das(x, src, dst, offs, w, channel_scale=scale)
+    assert oracle.rel_l2(_np(got), _np(dev)) < 1e-6
+    xh16 = x.half().cpu().pin_memory()
+    got16 = ffdas_b200.das_from_host(xh16, src, dst, offs, w, chunks=3)
+    dev16 = ffdas_b200.das(x.half(), src, dst, offs, w)
+    assert oracle.rel_l2(_np(got16), _np(dev16)) < 1e-6
+
+
+def test_das_from_host_rejections():
+    import ctypes
+    from ffdas_b200 import _lib
+    from ffdas_b200._lib import DataType, Error
+    rng = np.random.default_rng(18)
+    x, src, dst, offs, w = _small(rng, C=8, S=2, N=64, V=(6, 5))
+    with pytest.raises(ValueError, match="host memory"):
+        ffdas_b200.das_from_host(x, src, dst, offs, w)                   # x already on the GPU
+    with pytest.raises(ValueError, match="on the GPU"):
+        ffdas_b200.das_from_host(x.cpu(), src.cpu(), dst, offs, w)       # geometry on the host
+    with pytest.raises(ValueError):
+        ffdas_b200.das_from_host(x.cpu(), src, dst, offs, w, chunks=-1)
+    h = ffdas_b200.get_library_handle(DEV)
+    L = _lib.load()
+    xh = x.cpu()
+    out = torch.empty((1, 6, 5), device=DEV)
+    od = _lib.TensorDesc(list(out.shape), None, DataType.R_32F)
+    beta = (ctypes.c_float * 2)()
+    strided = _lib.TensorDesc([1, 8, 2, 32], [1024, 128, 64, 2], DataType.R_32F)   # every other sample
+    rc = L.ffdas_das_from_host(h.h, src.data_ptr(), None, 0.0, strided.desc, xh.data_ptr(), dst.data_ptr(),
+                               offs.data_ptr(), w.data_ptr(), ctypes.cast(beta, ctypes.c_void_p), od.desc,
+                               out.data_ptr(), 0, 0, 0)
+    assert rc == Error.NON_CONTIGUOUS
+    xdsc = _lib.TensorDesc(list(xh.shape), None, DataType.R_32F)
+    rc = L.ffdas_das_from_host(h.h, src.data_ptr(), None, 0.0, xdsc.desc, None, dst.data_ptr(), offs.data_ptr(),
+                               w.data_ptr(), ctypes.cast(beta, ctypes.c_void_p), od.desc, out.data_ptr(), 0, 0, 0)
+    assert rc == Error.NULL_POINTER
