@@ -822,11 +822,13 @@ ffdas_error_t upload_resources(ffdas_context &h) {
     return FFDAS_SUCCESS;
 }
 
-// Channels per chunk: about C / 8 when there are 1024 channels, never under
-// 128 channels, rounded to the 8 channels of one staged-kernel stage.
+// Channels per run: about C / 8 when there are 1024 channels, runs of at
+// least 128 channels, rounded to the 8 channels of one staged-kernel stage.
 int host_chunk_channels(int64_t C, int chunks) {
     int64_t k = chunks > 0 ? chunks : std::max<int64_t>(1, std::min<int64_t>(8, C / 128));
-    k = std::min<int64_t>(std::min<int64_t>(k, kHostChunksMax), std::max<int64_t>(C, 1));
+    // at most kHostChunksMax - 1 full runs: with the half-width first run the
+    // runs then fit the kHostChunksMax per-run events
+    k = std::min<int64_t>(std::min<int64_t>(k, kHostChunksMax - 1), std::max<int64_t>(C, 1));
     int64_t cc = (C + k - 1) / k;
     if (k > 1) cc = (cc + 7) / 8 * 8;
     return (int)std::max<int64_t>(cc, 1);
@@ -851,7 +853,13 @@ ffdas_error_t das_from_host(ffdas_context &h, const das_call &a0, int chunks) {
     // a per-item channel scale (B x C values) does not split by channel
     const bool item_scale = h.chan_scale && h.chan_scale_count != C;
     const int cc = item_scale ? (int)std::max<int64_t>(C, 1) : host_chunk_channels(C, chunks);
-    const int K = (int)std::max<int64_t>(1, (C + cc - 1) / cc);
+    // Run k covers channels [run_lo(k), run_lo(k + 1)).  The first run's
+    // upload is the one copy nothing hides, so it is half a run (whole
+    // stages of 8 channels) when there are several runs.
+    const int64_t first = (cc >= C) ? C : std::min<int64_t>(C, std::max<int64_t>(8, (cc / 2 + 7) / 8 * 8));
+    const int K = (int)(first >= C ? 1 : 1 + (C - first + cc - 1) / cc);
+    auto run_lo = [&](int k) -> int64_t { return k == 0 ? 0 : std::min<int64_t>(C, first + (int64_t)(k - 1) * cc); };
+    if (K > kHostChunksMax) return FFDAS_ERROR_INTERNAL;
 
     FFDAS_TRY(upload_resources(h));
     workspace X(h);
@@ -864,7 +872,7 @@ ffdas_error_t das_from_host(ffdas_context &h, const das_call &a0, int chunks) {
     FFDAS_CUDA(cudaStreamWaitEvent(h.upload_stream, h.upload_ev[kHostChunksMax], 0));
     ffdas_error_t cerr = FFDAS_SUCCESS;
     for (int k = 0; k < K && cerr == FFDAS_SUCCESS; k++) {
-        const int64_t c0 = (int64_t)k * cc, c1 = std::min<int64_t>(C, c0 + cc);
+        const int64_t c0 = run_lo(k), c1 = run_lo(k + 1);
         for (int64_t b = 0; b < B && cerr == FFDAS_SUCCESS; b++) {
             const size_t off = (size_t)((b * C + c0) * row) * esz;
             if (cudaMemcpyAsync(xdev + off, xh + off, (size_t)((c1 - c0) * row) * esz, cudaMemcpyHostToDevice,
@@ -899,7 +907,7 @@ ffdas_error_t das_from_host(ffdas_context &h, const das_call &a0, int chunks) {
     ffdas_error_t err = FFDAS_SUCCESS;
     int kernels = 0;
     for (int k = 0; k < K && err == FFDAS_SUCCESS; k++) {
-        const int64_t c0 = (int64_t)k * cc, c1 = std::min<int64_t>(C, c0 + cc);
+        const int64_t c0 = run_lo(k), c1 = run_lo(k + 1);
         ffdas_tensor_desc dk = xd;
         dk.dims[cdim] = c1 - c0;
         das_call a = a0;

@@ -321,11 +321,12 @@ FFDAS_API ffdas_error_t ffdas_das_pair_bytes(ffdas_tensor_desc_t x_desc, ffdas_c
 /* New: ffdas_das on channel data in host memory (page-locked for the copies
  * to overlap; pageable memory works, serially).  Same arguments as ffdas_das
  * except that x_host is a host pointer to C-contiguous x, plus `chunks`: the
- * channels are cut into that many runs (0: about C / 128, at most 8; at most
- * 16).  The handle's own upload stream copies run k + 1 while the handle's
- * stream beamforms run k, which waits only for its own run; run 0 applies
- * beta and every later run adds into out (beta = 1), so only the first run's
- * upload is not hidden behind the beamforming.  The output, positions,
+ * channels are cut into about that many runs (0: about C / 128, at most 8;
+ * at most 15), the first of half the width.  The handle's own upload stream
+ * copies run k + 1 while the handle's stream beamforms run k, which waits
+ * only for its own run; run 0 applies beta and every later run adds into out
+ * (beta = 1), so only the first run's upload is not hidden behind the
+ * beamforming.  The output, positions,
  * delays and weights are device buffers as for ffdas_das.  A per-item
  * channel scale (B * C values) keeps the whole call in one run.  The sum
  * over channels is grouped by run, so the image differs from ffdas_das's in
