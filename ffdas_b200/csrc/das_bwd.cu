@@ -36,6 +36,7 @@ struct bwd_params {
     int64_t gout_bstride;
     float *gx;                  // (B, C, S, N) contiguous
     float *goff, *gw, *gdst, *gsrc;
+    int cchunk;                 // channels per blockIdx.z slice (0: no split)
 };
 
 constexpr int kBwdThreads = 256;
@@ -52,16 +53,35 @@ __global__ void __launch_bounds__(kBwdThreads) das_bwd_kernel(const bwd_params p
     const int lane = tid & 31;
     const int tile = blockIdx.x;
     const int t0 = tile % p.n0, t1 = (tile / p.n0) % p.n1, t2 = tile / (p.n0 * p.n1);
-    const int i0 = tid % p.T0, i1 = (tid / p.T0) % p.T1, i2 = tid / (p.T0 * p.T1);
+    // das_sparse without the weight gradient: the CTA orders its voxels by
+    // list length (as the forward gather does) and each warp runs its events
+    // only up to its longest real list.  Padding entries (zero weight) add
+    // nothing to the other gradients; they do have a weight gradient (the
+    // tap they would read), so with gw the walk covers every entry.
+    int pos = tid, n_ev = p.n_events;
+    if constexpr (SPARSE) {
+        if (p.gw == nullptr) {
+            __shared__ int Ls[kBwdThreads];
+            int L;
+            const int me = sparse_balance(p, tid, t0, t1, t2, L);
+            Ls[tid] = L;
+            __syncthreads();
+            pos = me;
+            n_ev = (int)__reduce_max_sync(0xffffffffu, (unsigned)Ls[me]);
+        }
+    }
+    const int i0 = pos % p.T0, i1 = (pos / p.T0) % p.T1, i2 = pos / (p.T0 * p.T1);
     const int g0 = t0 * p.T0 + i0, g1 = t1 * p.T1 + i1, g2 = t2 * p.T2 + i2;
     const bool active = (g0 < p.D0 && g1 < p.D1 && g2 < p.D2);
     const int64_t v = active ? ((int64_t)g2 * p.D1 + g1) * p.D0 + g0 : 0;
     const int b0 = blockIdx.y * BT;
     const bool do_gx = p.gx != nullptr;
-    // A CTA that owns several batch chunks writes the voxel-side gradients
-    // only from chunk 0 after reducing across chunks with atomics; with one
-    // chunk it stores them directly.
-    const bool multi_chunk = gridDim.y > 1;
+    // When several CTAs share a voxel (batch chunks, channel slices) they add
+    // the voxel-side gradients with atomics into zeroed outputs; a single CTA
+    // stores them directly.
+    const bool multi_chunk = gridDim.y > 1 || gridDim.z > 1;
+    const int cbeg = p.cchunk ? (int)blockIdx.z * p.cchunk : 0;
+    const int cend = p.cchunk ? min(p.C, cbeg + p.cchunk) : p.C;
 
     for (int i = tid; i < SC * BT * kBwdWin; i += kBwdThreads) (&win[0][0][0])[i] = 0.f;
     if (tid < SC) { kmin_s[tid] = INT_MAX; kmax_s[tid] = INT_MIN; }
@@ -81,8 +101,8 @@ __global__ void __launch_bounds__(kBwdThreads) das_bwd_kernel(const bwd_params p
     const int64_t row_b = (int64_t)p.C * p.S * p.npad;
     float gpx = 0.f, gpy = 0.f, gpz = 0.f;
 
-    for (int e0 = 0; e0 < p.n_events; e0 += SC) {
-        const int sc = min(SC, p.n_events - e0);
+    for (int e0 = 0; e0 < n_ev; e0 += SC) {
+        const int sc = min(SC, n_ev - e0);
         float ofs[SC], w[SC], gwa[SC], goa[SC];
         int srow[SC];
 #pragma unroll
@@ -103,7 +123,7 @@ __global__ void __launch_bounds__(kBwdThreads) das_bwd_kernel(const bwd_params p
             }
         }
 
-        for (int c = 0; c < p.C; c++) {
+        for (int c = cbeg; c < cend; c++) {
             const float cx = __ldg(p.srcpos + 3 * c), cy = __ldg(p.srcpos + 3 * c + 1),
                         cz = __ldg(p.srcpos + 3 * c + 2);
             const recv_geom gm = receive_geometry(vx, vy, vz, cx, cy, cz);
@@ -422,22 +442,39 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
     const int bchunks = (pb.B + BT - 1) / BT;
     const int64_t tiles = (int64_t)bp.n0 * bp.n1 * n2;
     if (tiles > INT32_MAX || bchunks > 65535) return FFDAS_ERROR_DIMS_TOO_LARGE;
-    // outputs reduced with atomics must start at zero
+    // Channel slices over blockIdx.z (32+ channels each) until there are about
+    // min_blocks (default 16) CTAs per SM: at 97 registers two CTAs fit an
+    // SM, and a few hundred tiles leave the last wave half empty.
+    int csplit = 1;
+    {
+        const int per_sm = (h.has_config && h.config.min_blocks) ? h.config.min_blocks : 16;
+        const int64_t want = (int64_t)std::max(h.sm_count, 1) * per_sm;
+        while (tiles * bchunks * csplit * 2 <= want && pb.C >= 64 * csplit && csplit < 64) csplit *= 2;
+    }
+    if (csplit > 1) {
+        const int chunk = (pb.C + csplit - 1) / csplit;
+        csplit = (pb.C + chunk - 1) / chunk;
+        bp.cchunk = csplit > 1 ? chunk : 0;
+    }
+    // outputs reduced with atomics must start at zero; the balanced das_sparse
+    // walk (no weight gradient) stores no delay gradient for the entries past
+    // a warp's longest list, which are padding: zero them too
     const size_t ve = (size_t)pb.n_events * pb.V * sizeof(float);
-    if (bchunks > 1) {
+    const bool shared_voxels = bchunks > 1 || csplit > 1;
+    if (shared_voxels || (a.sparse && !gw)) {
         if (gw) FFDAS_CUDA(cudaMemsetAsync(gw, 0, ve, h.stream));
         if (goff) FFDAS_CUDA(cudaMemsetAsync(goff, 0, ve, h.stream));
-        if (gdst) FFDAS_CUDA(cudaMemsetAsync(gdst, 0, (size_t)pb.V * 3 * sizeof(float), h.stream));
     }
+    if (shared_voxels && gdst) FFDAS_CUDA(cudaMemsetAsync(gdst, 0, (size_t)pb.V * 3 * sizeof(float), h.stream));
     if (gsrc) FFDAS_CUDA(cudaMemsetAsync(gsrc, 0, (size_t)pb.C * 3 * sizeof(float), h.stream));
 
-    dim3 grid((unsigned)tiles, (unsigned)bchunks);
+    dim3 grid((unsigned)tiles, (unsigned)bchunks, (unsigned)csplit);
     h.last = ffdas_kernel_info_t{};
     h.last.variant = 3;
     h.last.tile_x = bp.T0; h.last.tile_y = bp.T1; h.last.tile_z = bp.T2;
     h.last.batch_tile = BT; h.last.event_chunk = 8; h.last.storage = kind;
     h.last.kernels = h.last_pairs_reused ? 1 : 2;   // (ingest,) adjoint
-    h.last.grid = tiles * bchunks;
+    h.last.grid = tiles * bchunks * csplit;
     const bool sp = a.sparse;
     ffdas_error_t err;
     h.mark_start();

@@ -114,8 +114,8 @@ template <> __device__ __forceinline__ void store_out<double2>(double2 *o, doubl
 // of sparse_count.  Returns the tile position this thread takes; L_out is the
 // L of the thread's original position (the caller exchanges them through
 // shared memory).
-__device__ __forceinline__ int sparse_balance(const gather_params &p, int tid, int t0, int t1, int t2,
-                                              int &L_out) {
+template <typename Params>   // gather_params, or the adjoint's parameters (same field names)
+__device__ __forceinline__ int sparse_balance(const Params &p, int tid, int t0, int t1, int t2, int &L_out) {
     __shared__ int hist[64], base[64];
     __shared__ short order[256];
     const int i0 = tid % p.T0, i1 = (tid / p.T0) % p.T1, i2 = tid / (p.T0 * p.T1);

@@ -6,8 +6,10 @@
 Builds the named synthetic workload (ffdas_b200.workloads.CONFIGS), applies the
 schedule to the device's library handle, calls das / das_sparse `--calls`
 times (the first calls warm the kernel attributes and the memory pool), and
-prints the last call's kernel info.  `--backward` runs ffdas_das_backward
-instead (random output gradient).
+prints the last call's kernel info.  `--backward` runs the forward with
+autograd and its backward (output gradient of ones): ffdas_das_backward for
+the gradient of x (and, for das_sparse workloads, of the delays and
+weights).
 
     python profile_call.py rank_filter --calls 3
 
@@ -53,7 +55,12 @@ def main() -> int:
     for _ in range(args.calls):
         if args.backward:
             xg = x.float().requires_grad_(True)
-            out = das(xg, *geo)
+            if "sparse_indices" in wl:   # adjoint of das_sparse: grads of x, delays and weights
+                og = wl["offsets"].clone().requires_grad_(True)
+                wg = wl["weights"].clone().requires_grad_(True)
+                out = das_sparse(xg, wl["srcpos"], wl["dstpos"], og, wg, wl["sparse_indices"])
+            else:
+                out = das(xg, *geo)
             out.backward(torch.ones_like(out))
         elif "sparse_indices" in wl:
             das_sparse(x, *geo, wl["sparse_indices"])

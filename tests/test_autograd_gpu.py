@@ -93,6 +93,38 @@ def test_sparse_gradients_match_reference():
         assert oracle.rel_l2(a.grad.cpu().numpy(), b.grad.numpy()) < 2e-4, name
 
 
+@pytest.mark.parametrize("C", [6, 128], ids=["one_slice", "channel_slices"])
+@pytest.mark.parametrize("weights_grad", [True, False], ids=["all", "no_weight_grad"])
+def test_sparse_gradients_uneven_lists(C, weights_grad):
+    # uneven lists padded with zero weights; 128 channels split over CTAs
+    # whose voxel-side gradients add atomically; without the weight gradient
+    # each warp walks only up to its longest real list
+    g = torch.Generator().manual_seed(11 + C)
+    x, src, dst, offs, w = _problem(8, B=2, C=C, S=7, N=140)
+    V = dst.shape[:-1]
+    n = 5
+    idx = torch.randint(0, 7, (n, *V), generator=g).int()
+    length = torch.randint(0, n + 1, V, generator=g)
+    pad = torch.arange(n).reshape(n, 1, 1) >= length[None]
+    ofs_s = (torch.rand((n, *V), generator=g) * 30 + 5).float()
+    w_s = (torch.rand((n, *V), generator=g) + 0.2).float()
+    w_s[pad] = 0.0
+    need = [True, True, True, True, weights_grad]
+    gpu = [t.to(DEV).requires_grad_(r) for t, r in zip((x, src, dst, ofs_s, w_s), need)]
+    ref = [t.double().requires_grad_(r) for t, r in zip((x, src, dst, ofs_s, w_s), need)]
+    gy = torch.randn((2, *V), generator=g)
+    ffdas_b200.das_sparse(*gpu, idx.to(DEV)).backward(gy.to(DEV))
+    das_ref(*ref, sparse_indices=idx).backward(gy.double())
+    for name, a, b, r in zip(["x", "srcpos", "dstpos", "offsets", "weights"], gpu, ref, need):
+        if not r:
+            continue
+        assert oracle.rel_l2(a.grad.cpu().numpy(), b.grad.numpy()) < 2e-4, name
+    info = ffdas_b200.get_library_handle(DEV).last_kernel_info()
+    assert info["variant"] == 3
+    # 2 tiles of 4 x 64 voxels, one batch chunk of 2 items; 128 channels: 4 slices of 32
+    assert info["grid"] == (8 if C == 128 else 2), info
+
+
 def test_central_finite_differences_fp64():
     x, src, dst, offs, w = _problem(6, B=2)
     loss_ref = lambda o, ww: -(das_ref(x.double(), src.double(), dst.double(), o, ww) ** 4).sum()  # noqa: E731
