@@ -658,6 +658,32 @@ def bwd_extras(args, h) -> dict:
     reuse[0], every_grad[0] = True, False
     msb_af = timed(bwd, args.steps, args.warmup, stream, 1)
     h.set_config(None)
+
+    # das_sparse: the focused 64-transmit frame (uneven lists of 1..32
+    # transmits), planner schedules, the adjoint of every input and without
+    # the weight gradient (padding entries then need no work)
+    sf = W.sparse_focus(device=dev)
+    xs, idx_s = sf["x"], sf["sparse_indices"]
+    geo_s = (sf["srcpos"], sf["dstpos"], sf["offsets"], sf["weights"])
+    msf_s = timed(lambda: ffdas_b200.das_sparse(xs, *geo_s, idx_s), args.steps, args.warmup, stream, 1)
+    gout_s = torch.randn((1, *sf["dstpos"].shape[:-1]), device=dev)
+    gxs, gos, gws = torch.zeros_like(xs), torch.empty_like(sf["offsets"]), torch.empty_like(sf["weights"])
+    gds, gss = torch.empty_like(sf["dstpos"]), torch.empty_like(sf["srcpos"])
+    xdsc_s = _lib.TensorDesc(list(xs.shape), None, DataType.R_32F)
+    gdsc_s = _lib.TensorDesc(list(gout_s.shape), None, DataType.R_32F)
+    with_w = [True]
+
+    def bwd_s():
+        h.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+        _lib.check(L.ffdas_das_backward(h.h, sf["srcpos"].data_ptr(), None, 0.0, xdsc_s.desc, xs.data_ptr(),
+                                        sf["dstpos"].data_ptr(), sf["offsets"].data_ptr(),
+                                        sf["weights"].data_ptr(), int(idx_s.shape[0]), idx_s.data_ptr(),
+                                        gdsc_s.desc, gout_s.data_ptr(), gxs.data_ptr(), gos.data_ptr(),
+                                        gws.data_ptr() if with_w[0] else None, gds.data_ptr(), gss.data_ptr()))
+    msb_s = timed(bwd_s, args.steps, args.warmup, stream, 1)
+    binfo_s = h.last_kernel_info()
+    with_w[0] = False
+    msb_s_nw = timed(bwd_s, args.steps, args.warmup, stream, 1)
     return {"bwd_fwd": {"ratio": msb / msf, "fwd_ms": msf, "bwd_ms": msb,
                         "bwd_ms_own_pairs": msb_own, "ratio_own_pairs": msb_own / msf,
                         "pairs": "the backward reads the pair rows the forward built (ffdas_set_pair_buffer), as "
@@ -669,7 +695,14 @@ def bwd_extras(args, h) -> dict:
                         "fwd_schedule": finfo, "bwd_schedule": binfo, "bwd_config": bcfg,
                         "bwd_table": [[m, c, i["variant"]] for m, c, i in table],
                         "workload": "autofocus: 128 ch, 8 plane waves, batch 4, 2048 samples, 256x256 voxels; "
-                                    "backward = grads of x, offsets, weights, voxel and channel positions"}}
+                                    "backward = grads of x, offsets, weights, voxel and channel positions"},
+            "bwd_fwd_sparse": {"ratio": msb_s / msf_s, "fwd_ms": msf_s, "bwd_ms": msb_s,
+                               "bwd_ms_without_weight_grad": msb_s_nw, "ratio_without_weight_grad": msb_s_nw / msf_s,
+                               "bwd_kernel": binfo_s,
+                               "workload": "das_sparse, 128 ch, 64 focused transmits, 1536 samples, 400x256 "
+                                           "pixels, lists of 1..32 transmits padded to 32; backward = grads of x, "
+                                           "offsets, weights, voxel and channel positions (and the same "
+                                           "without the weight gradient)"}}
 
 
 

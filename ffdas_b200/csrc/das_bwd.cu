@@ -290,6 +290,254 @@ static ffdas_error_t launch_bwd_k(ffdas_context &h, const bwd_params &bp, int BT
     }
 }
 
+// ---------------------------------------- das_sparse adjoint, sorted lists ---
+// The gather adjoint above gives each lane a voxel and walks its list, so at
+// a list slot the lanes of a warp name different events and the two-tap
+// scatter of the channel-data gradient goes to up to 32 pair rows per warp
+// reduction.  Here a lane takes one list entry instead: the CTA (a tile of
+// up to 128 voxels) counts its entries per event in a shared histogram,
+// scans the counts and places every entry in its event's bucket, so the
+// lanes of a warp mostly share the event and their reductions land on one
+// row at nearby samples.  No lane works on a padding entry (zero weight)
+// unless the weight gradient is asked for, where its tap is the gradient.
+// Per entry the lane sums over the channels, as the gather adjoint does per
+// voxel: the weight gradient g L, the delay gradient g w d and the voxel
+// position gradient g w d (v - c) / r; the channel positions take the warp's
+// sum per channel.  The position gradients of a voxel's entries meet in
+// shared memory.
+constexpr int kBwsThreads = 256;
+constexpr int kBwsMaxEvents = 4096;     // events of x (shared histogram)
+constexpr int kBwsMaxSlots = 8192;      // tile voxels x list length (16-bit entry codes)
+constexpr int kBwsMaxTile = 128;
+constexpr size_t kBwsMaxSmem = 200 * 1024;   // dynamic shared memory the kernel may be launched with
+
+constexpr int kBwsGroup = 8;                 // channels whose position gradients a warp sums at once
+constexpr int kBwsRed = 3 * kBwsGroup * 33;   // floats of a warp's staging tile (rows padded to 33)
+
+size_t bws_smem_bytes(int TV, int L, int S, int CS) {   // CS: channels of one CTA
+    return (size_t)TV * 16 + (size_t)TV * 4 * 2 + (size_t)TV * 12 + (size_t)(kBwsThreads / 32) * kBwsRed * 4 +
+           (size_t)S * 4 + (size_t)CS * 12 + (size_t)TV * L * 2;
+}
+
+template <int K, bool POS>   // POS: voxel or channel position gradients wanted
+__global__ void __launch_bounds__(kBwsThreads) das_bwd_sorted_kernel(const bwd_params p, int L) {
+    using tr = pair_traits<K>;
+    using st = typename tr::storage;
+    extern __shared__ __align__(16) unsigned char bws_smem[];
+    __shared__ int total;
+    const int TV = p.T0 * p.T1 * p.T2;
+    const int NE = TV * L;                                          // slot q = j * TV + vl
+    float4 *vpos = reinterpret_cast<float4 *>(bws_smem);            // [TV] position, w = 1 on the grid
+    int *vidx = reinterpret_cast<int *>(vpos + TV);                 // [TV] voxel index
+    float *gvox = reinterpret_cast<float *>(vidx + TV);             // [TV] output gradient of the voxel
+    float *gpos = gvox + TV;                                        // [TV][3] voxel position gradients
+    float *gred = gpos + 3 * TV;                                    // [warps][kBwsRed] channel-gradient staging
+    int *cnt = reinterpret_cast<int *>(gred + (kBwsThreads / 32) * kBwsRed);   // [S] counts, then cursors
+    float *gch = reinterpret_cast<float *>(cnt + p.S);              // [CTA's channels][3] position gradients
+    const int cbeg = p.cchunk ? (int)blockIdx.z * p.cchunk : 0;
+    const int cend = p.cchunk ? min(p.C, cbeg + p.cchunk) : p.C;
+    uint16_t *code = reinterpret_cast<uint16_t *>(gch + 3 * (cend - cbeg));   // [NE] sorted position -> slot
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int b = blockIdx.y;
+    const bool multi_chunk = gridDim.y > 1 || gridDim.z > 1;
+    const bool all_entries = p.gw != nullptr;   // padding entries have a weight gradient
+
+    const int tile = blockIdx.x;
+    const int t0 = tile % p.n0, t1 = (tile / p.n0) % p.n1, t2 = tile / (p.n0 * p.n1);
+    for (int vl = tid; vl < TV; vl += kBwsThreads) {
+        const int i0 = vl % p.T0, i1 = (vl / p.T0) % p.T1, i2 = vl / (p.T0 * p.T1);
+        const int g0 = t0 * p.T0 + i0, g1 = t1 * p.T1 + i1, g2 = t2 * p.T2 + i2;
+        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+        int v = 0;
+        float gv = 0.f;
+        if (g0 < p.D0 && g1 < p.D1 && g2 < p.D2) {
+            v = (g2 * p.D1 + g1) * p.D0 + g0;
+            q = make_float4(__ldg(p.dstpos + 3 * (int64_t)v), __ldg(p.dstpos + 3 * (int64_t)v + 1),
+                            __ldg(p.dstpos + 3 * (int64_t)v + 2), 1.f);
+            gv = __ldg(p.gout + (int64_t)b * p.gout_bstride + v);
+        }
+        vpos[vl] = q;
+        vidx[vl] = v;
+        gvox[vl] = gv;
+        gpos[3 * vl] = gpos[3 * vl + 1] = gpos[3 * vl + 2] = 0.f;
+    }
+    for (int e = tid; e < p.S; e += kBwsThreads) cnt[e] = 0;
+    if (POS)
+        for (int i = tid; i < 3 * (cend - cbeg); i += kBwsThreads) gch[i] = 0.f;
+    __syncthreads();
+
+    // entries that can have a gradient: on the grid, event in [0, S), and a
+    // nonzero weight unless the weight gradient is wanted (an entry with an
+    // event outside [0, S) reads the zero pair: every gradient is 0, which
+    // the zeroed outputs already hold)
+    auto entry = [&](int q, int &s) -> bool {
+        const int j = q / TV, vl = q - j * TV;
+        if (vpos[vl].w == 0.f) return false;
+        const int64_t idx = (int64_t)j * p.V + vidx[vl];
+        s = __ldg(p.sparse_idx + idx);
+        return (unsigned)s < (unsigned)p.S && (all_entries || __ldg(p.weights + idx) != 0.f);
+    };
+    for (int q = tid; q < NE; q += kBwsThreads) {
+        int s;
+        if (entry(q, s)) atomicAdd(&cnt[s], 1);
+    }
+    __syncthreads();
+    if (warp == 0) {   // bucket starts: each lane scans a contiguous run of events
+        const int per = (p.S + 31) / 32;
+        const int s0 = min(lane * per, p.S), s1 = min(s0 + per, p.S);
+        int sum = 0;
+        for (int e = s0; e < s1; e++) sum += cnt[e];
+        int incl = sum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += y;
+        }
+        int run = incl - sum;
+        for (int e = s0; e < s1; e++) {
+            const int c = cnt[e];
+            cnt[e] = run;
+            run += c;
+        }
+        if (lane == 31) total = incl;
+    }
+    __syncthreads();
+    for (int q = tid; q < NE; q += kBwsThreads) {
+        int s;
+        if (entry(q, s)) code[atomicAdd(&cnt[s], 1)] = (uint16_t)q;
+    }
+    __syncthreads();
+
+    const int E = total;
+    const st *Pb = static_cast<const st *>(p.P) + (int64_t)b * p.C * p.S * p.npad;   // < 2^31 pairs per item
+    const uint32_t kmax = (uint32_t)(p.npad - 1);
+    const uint32_t cstride = (uint32_t)(p.S * p.npad);
+    for (int e0 = warp * 32; e0 < E; e0 += kBwsThreads) {   // uniform per warp: lanes past E stay for the shuffles
+        const int e = e0 + lane;
+        const bool act = e < E;
+        int vl = 0, s = 0;
+        int64_t idx = 0;
+        float ofs = 1e30f, w = 0.f, g = 0.f;
+        float4 vp = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (act) {
+            const int q = code[e];
+            const int j = q / TV;
+            vl = q - j * TV;
+            idx = (int64_t)j * p.V + vidx[vl];
+            ofs = __ldg(p.offsets + idx);
+            w = __ldg(p.weights + idx);
+            s = __ldg(p.sparse_idx + idx);
+            g = gvox[vl];
+            vp = vpos[vl];
+        }
+        const uint32_t row = (uint32_t)s * (uint32_t)p.npad;
+        float *gxr = p.gx ? p.gx + ((int64_t)b * p.C * p.S + s) * p.N : nullptr;   // + (c S) N + k
+        const float a = g * w;
+        float gwa = 0.f, goa = 0.f, ex = 0.f, ey = 0.f, ez = 0.f;
+        for (int c = cbeg; c < cend; c++) {
+            const float cx = __ldg(p.srcpos + 3 * c), cy = __ldg(p.srcpos + 3 * c + 1),
+                        cz = __ldg(p.srcpos + 3 * c + 2);
+            const recv_geom gm = receive_geometry(vp.x, vp.y, vp.z, cx, cy, cz);
+            const tau_split ts = split_tau(__fmaf_rn(gm.rsq, gm.rinv, ofs));
+            const st pr = Pb[row + (uint32_t)c * cstride + min(ts.k, kmax)];
+            const float Lt = tr::tap(pr, ts.t);
+            const float gd = g * tr::slope(pr);
+            gwa = __fmaf_rn(g, Lt, gwa);
+            goa = __fmaf_rn(w, gd, goa);
+            if (POS) {
+            const float qr = w * gd * gm.rinv;
+            const float dx = (vp.x - cx) * qr, dy = (vp.y - cy) * qr, dz = (vp.z - cz) * qr;
+            ex += dx; ey += dy; ez += dz;
+            if (p.gsrc) {
+                // channel position gradients, summed over the warp's entries
+                // through a staging tile: each lane writes its three terms of
+                // up to 8 channels, then lane r sums row r (channel r / 3,
+                // component r % 3) and adds it to the CTA's sum
+                float *rw = gred + warp * kBwsRed;
+                const int slot = (c - cbeg) % kBwsGroup;
+                rw[(3 * slot) * 33 + lane] = -dx;
+                rw[(3 * slot + 1) * 33 + lane] = -dy;
+                rw[(3 * slot + 2) * 33 + lane] = -dz;
+                if (slot == kBwsGroup - 1 || c == cend - 1) {   // uniform over the warp
+                    __syncwarp();
+                    if (lane < 3 * (slot + 1)) {
+                        float sum = 0.f;
+#pragma unroll 8
+                        for (int i = 0; i < 32; i++) sum += rw[lane * 33 + i];
+                        if (sum != 0.f) atomicAdd(gch + 3 * (c - slot - cbeg) + lane, sum);
+                    }
+                    __syncwarp();
+                }
+            }
+            }
+            // two-tap scatter of the channel-data gradient: the warp's lanes
+            // mostly share the event, so these land in one row
+            if (gxr && a != 0.f && ts.k < (uint32_t)(p.N - 1)) {
+                float *gr = gxr + (int64_t)c * p.S * p.N + ts.k;
+                const float a1 = a * ts.t;
+                atomicAdd(gr, a - a1);
+                atomicAdd(gr + 1, a1);
+            }
+        }
+        if (act) {
+            if (multi_chunk) {
+                if (p.gw) atomicAdd(p.gw + idx, gwa);
+                if (p.goff) atomicAdd(p.goff + idx, goa);
+            } else {
+                if (p.gw) p.gw[idx] = gwa;
+                if (p.goff) p.goff[idx] = goa;
+            }
+            if (POS && p.gdst) {
+                atomicAdd(&gpos[3 * vl], ex);
+                atomicAdd(&gpos[3 * vl + 1], ey);
+                atomicAdd(&gpos[3 * vl + 2], ez);
+            }
+        }
+    }
+    if (POS) __syncthreads();
+    if (POS && p.gsrc) {   // one global add per channel and component from each CTA
+        for (int i = tid; i < 3 * (cend - cbeg); i += kBwsThreads)
+            if (gch[i] != 0.f) atomicAdd(p.gsrc + 3 * cbeg + i, gch[i]);
+    }
+    if (POS && p.gdst) {
+        for (int vl = tid; vl < TV; vl += kBwsThreads) {
+            if (vpos[vl].w == 0.f) continue;
+            float *o = p.gdst + 3 * (int64_t)vidx[vl];
+            if (multi_chunk) {
+                atomicAdd(o, gpos[3 * vl]); atomicAdd(o + 1, gpos[3 * vl + 1]); atomicAdd(o + 2, gpos[3 * vl + 2]);
+            } else {
+                o[0] = gpos[3 * vl]; o[1] = gpos[3 * vl + 1]; o[2] = gpos[3 * vl + 2];
+            }
+        }
+    }
+}
+
+bool bws_supported(const das_problem &pb, int kind) {
+    if (kind != ST_F32 && kind != ST_F16 && kind != ST_BF16) return false;
+    const int64_t item_pairs = (int64_t)pb.C * pb.S * pair_row_length(pb.N);
+    return pb.n_events >= 1 && pb.n_events <= kBwsMaxSlots / 32 && pb.S >= 1 && pb.S <= kBwsMaxEvents &&
+           pb.V <= INT_MAX && (int64_t)pb.D0 * pb.D1 * pb.D2 <= INT_MAX && pb.B <= 65535 && item_pairs < INT_MAX;
+}
+
+template <int K, bool POS>
+ffdas_error_t launch_bws_pos(ffdas_context &h, const bwd_params &bp, int L, dim3 grid, size_t smem) {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(das_bwd_sorted_kernel<K, POS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kBwsMaxSmem);
+    });
+    if (attr != cudaSuccess) return FFDAS_ERROR_CUDA_RUNTIME;
+    das_bwd_sorted_kernel<K, POS><<<grid, kBwsThreads, smem, h.stream>>>(bp, L);
+    return ffdas_launch_check(h.stream);
+}
+
+template <int K>
+ffdas_error_t launch_bws_t(ffdas_context &h, const bwd_params &bp, int L, dim3 grid, size_t smem) {
+    return (bp.gdst || bp.gsrc) ? launch_bws_pos<K, true>(h, bp, L, grid, smem)
+                                : launch_bws_pos<K, false>(h, bp, L, grid, smem);
+}
+
 // defined in das.cu
 ffdas_error_t ingest_for_backward(ffdas_context &h, const das_problem &pb, ffdas_datatype_t xt, int kind,
                                   const void *x, int64_t npad, void *P);
@@ -436,6 +684,66 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
                                                     dim3((unsigned)stiles, (unsigned)bchunks_st, (unsigned)csplit));
         h.mark_stop();
         return err;
+    }
+
+    // das_sparse: the sorted-list adjoint (a lane per list entry) unless the
+    // schedule asks for the gather adjoint (variant 3) or the CTA's tables
+    // would not fit shared memory
+    if (a.sparse && bws_supported(pb, kind) && !(h.has_config && h.config.variant == 3)) {
+        bwd_params sp = bp;
+        const int Ls = pb.n_events;
+        int TV = kBwsMaxTile;
+        while (TV > 32 && TV * Ls > kBwsMaxSlots) TV >>= 1;
+        auto fit = [](int want, int dim) {   // power of two up to want, not past the first one >= dim
+            int t = 1;
+            while (t * 2 <= want && t < dim) t *= 2;
+            return t;
+        };
+        sp.T0 = fit(std::min(TV, 16), pb.D0);
+        sp.T1 = fit(TV / sp.T0, pb.D1);
+        sp.T2 = fit(TV / (sp.T0 * sp.T1), pb.D2);
+        sp.T0 = TV / (sp.T1 * sp.T2);
+        sp.n0 = (pb.D0 + sp.T0 - 1) / sp.T0;
+        sp.n1 = (pb.D1 + sp.T1 - 1) / sp.T1;
+        const int64_t stiles = (int64_t)sp.n0 * sp.n1 * ((pb.D2 + sp.T2 - 1) / sp.T2);
+        int csplit = 1;
+        {
+            const int per_sm = (h.has_config && h.config.min_blocks) ? h.config.min_blocks : 16;
+            const int64_t want = (int64_t)std::max(h.sm_count, 1) * per_sm;
+            while (stiles * pb.B * csplit * 2 <= want && pb.C >= 64 * csplit && csplit < 64) csplit *= 2;
+        }
+        sp.cchunk = 0;
+        if (csplit > 1) {
+            const int chunk = (pb.C + csplit - 1) / csplit;
+            csplit = (pb.C + chunk - 1) / chunk;
+            sp.cchunk = csplit > 1 ? chunk : 0;
+        }
+        const size_t smem = bws_smem_bytes(TV, Ls, pb.S, sp.cchunk ? sp.cchunk : pb.C);
+        if (stiles <= INT32_MAX && smem <= kBwsMaxSmem) {
+            // entries the kernel does not place have no gradient: zeroed outputs
+            const size_t ves = (size_t)pb.n_events * pb.V * sizeof(float);
+            if (gw) FFDAS_CUDA(cudaMemsetAsync(gw, 0, ves, h.stream));
+            if (goff) FFDAS_CUDA(cudaMemsetAsync(goff, 0, ves, h.stream));
+            if (gdst && (pb.B > 1 || csplit > 1))
+                FFDAS_CUDA(cudaMemsetAsync(gdst, 0, (size_t)pb.V * 3 * sizeof(float), h.stream));
+            if (gsrc) FFDAS_CUDA(cudaMemsetAsync(gsrc, 0, (size_t)pb.C * 3 * sizeof(float), h.stream));
+            h.last = ffdas_kernel_info_t{};
+            h.last.variant = 7;
+            h.last.tile_x = sp.T0; h.last.tile_y = sp.T1; h.last.tile_z = sp.T2;
+            h.last.batch_tile = 1; h.last.event_chunk = 0; h.last.storage = kind;
+            h.last.kernels = h.last_pairs_reused ? 1 : 2;   // (ingest,) adjoint
+            h.last.grid = stiles * pb.B * csplit;
+            const dim3 grid((unsigned)stiles, (unsigned)pb.B, (unsigned)csplit);
+            ffdas_error_t err;
+            h.mark_start();
+            switch (kind) {
+                case ST_F32: err = launch_bws_t<ST_F32>(h, sp, Ls, grid, smem); break;
+                case ST_F16: err = launch_bws_t<ST_F16>(h, sp, Ls, grid, smem); break;
+                default: err = launch_bws_t<ST_BF16>(h, sp, Ls, grid, smem); break;
+            }
+            h.mark_stop();
+            return err;
+        }
     }
 
     const int BT = pb.B >= 4 ? 4 : (pb.B >= 2 ? 2 : 1);

@@ -93,12 +93,15 @@ def test_sparse_gradients_match_reference():
         assert oracle.rel_l2(a.grad.cpu().numpy(), b.grad.numpy()) < 2e-4, name
 
 
+@pytest.mark.parametrize("kernel", ["sorted", "gather"])
 @pytest.mark.parametrize("C", [6, 128], ids=["one_slice", "channel_slices"])
 @pytest.mark.parametrize("weights_grad", [True, False], ids=["all", "no_weight_grad"])
-def test_sparse_gradients_uneven_lists(C, weights_grad):
-    # uneven lists padded with zero weights; 128 channels split over CTAs
-    # whose voxel-side gradients add atomically; without the weight gradient
-    # each warp walks only up to its longest real list
+def test_sparse_gradients_uneven_lists(kernel, C, weights_grad):
+    # uneven lists padded with zero weights, on the sorted-list adjoint (the
+    # default: a lane per list entry) and the gather adjoint (variant 3);
+    # 128 channels split over CTAs whose voxel-side gradients add
+    # atomically; without the weight gradient the padding is skipped
+    from ffdas_b200.tune import schedule
     g = torch.Generator().manual_seed(11 + C)
     x, src, dst, offs, w = _problem(8, B=2, C=C, S=7, N=140)
     V = dst.shape[:-1]
@@ -113,16 +116,22 @@ def test_sparse_gradients_uneven_lists(C, weights_grad):
     gpu = [t.to(DEV).requires_grad_(r) for t, r in zip((x, src, dst, ofs_s, w_s), need)]
     ref = [t.double().requires_grad_(r) for t, r in zip((x, src, dst, ofs_s, w_s), need)]
     gy = torch.randn((2, *V), generator=g)
-    ffdas_b200.das_sparse(*gpu, idx.to(DEV)).backward(gy.to(DEV))
+    with schedule(dict(variant=3) if kernel == "gather" else None, DEV):
+        ffdas_b200.das_sparse(*gpu, idx.to(DEV)).backward(gy.to(DEV))
+        info = ffdas_b200.get_library_handle(DEV).last_kernel_info()
     das_ref(*ref, sparse_indices=idx).backward(gy.double())
     for name, a, b, r in zip(["x", "srcpos", "dstpos", "offsets", "weights"], gpu, ref, need):
         if not r:
             continue
         assert oracle.rel_l2(a.grad.cpu().numpy(), b.grad.numpy()) < 2e-4, name
-    info = ffdas_b200.get_library_handle(DEV).last_kernel_info()
-    assert info["variant"] == 3
-    # 2 tiles of 4 x 64 voxels, one batch chunk of 2 items; 128 channels: 4 slices of 32
-    assert info["grid"] == (8 if C == 128 else 2), info
+    if kernel == "gather":
+        assert info["variant"] == 3
+        # 2 tiles of 4 x 64 voxels, one batch chunk of 2 items; 128 channels: 4 slices of 32
+        assert info["grid"] == (8 if C == 128 else 2), info
+    else:
+        assert info["variant"] == 7
+        # one 8 x 16 tile (7 x 9 voxels) per batch item; 128 channels: 4 slices of 32
+        assert info["grid"] == (8 if C == 128 else 2), info
 
 
 def test_central_finite_differences_fp64():
