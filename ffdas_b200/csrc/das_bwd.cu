@@ -312,6 +312,7 @@ constexpr int kBwsMaxTile = 128;
 constexpr size_t kBwsMaxSmem = 200 * 1024;   // dynamic shared memory the kernel may be launched with
 
 constexpr int kBwsGroup = 8;                 // channels whose position gradients a warp sums at once
+constexpr int kBwsUnroll = 4;                // channels whose pair loads are in flight together
 constexpr int kBwsRed = 3 * kBwsGroup * 33;   // floats of a warp's staging tile (rows padded to 33)
 
 size_t bws_smem_bytes(int TV, int L, int S, int CS) {   // CS: channels of one CTA
@@ -434,18 +435,14 @@ __global__ void __launch_bounds__(kBwsThreads) das_bwd_sorted_kernel(const bwd_p
         float *gxr = p.gx ? p.gx + ((int64_t)b * p.C * p.S + s) * p.N : nullptr;   // + (c S) N + k
         const float a = g * w;
         float gwa = 0.f, goa = 0.f, ex = 0.f, ey = 0.f, ez = 0.f;
-        for (int c = cbeg; c < cend; c++) {
-            const float cx = __ldg(p.srcpos + 3 * c), cy = __ldg(p.srcpos + 3 * c + 1),
-                        cz = __ldg(p.srcpos + 3 * c + 2);
-            const recv_geom gm = receive_geometry(vp.x, vp.y, vp.z, cx, cy, cz);
-            const tau_split ts = split_tau(__fmaf_rn(gm.rsq, gm.rinv, ofs));
-            const st pr = Pb[row + (uint32_t)c * cstride + min(ts.k, kmax)];
+        // the gradients of one channel from its pair, once loaded
+        auto channel = [&](int c, float cx, float cy, float cz, float rinv, const tau_split &ts, const st &pr) {
             const float Lt = tr::tap(pr, ts.t);
             const float gd = g * tr::slope(pr);
             gwa = __fmaf_rn(g, Lt, gwa);
             goa = __fmaf_rn(w, gd, goa);
             if (POS) {
-            const float qr = w * gd * gm.rinv;
+            const float qr = w * gd * rinv;
             const float dx = (vp.x - cx) * qr, dy = (vp.y - cy) * qr, dz = (vp.z - cz) * qr;
             ex += dx; ey += dy; ez += dz;
             if (p.gsrc) {
@@ -478,6 +475,32 @@ __global__ void __launch_bounds__(kBwsThreads) das_bwd_sorted_kernel(const bwd_p
                 atomicAdd(gr, a - a1);
                 atomicAdd(gr + 1, a1);
             }
+        };
+        // kBwsUnroll channels at a time: their pair loads are in flight together
+        int c = cbeg;
+        for (; c + kBwsUnroll <= cend; c += kBwsUnroll) {
+            float cx[kBwsUnroll], cy[kBwsUnroll], cz[kBwsUnroll], ri[kBwsUnroll];
+            tau_split ts[kBwsUnroll];
+            st pr[kBwsUnroll];
+#pragma unroll
+            for (int u = 0; u < kBwsUnroll; u++) {
+                cx[u] = __ldg(p.srcpos + 3 * (c + u));
+                cy[u] = __ldg(p.srcpos + 3 * (c + u) + 1);
+                cz[u] = __ldg(p.srcpos + 3 * (c + u) + 2);
+                const recv_geom gm = receive_geometry(vp.x, vp.y, vp.z, cx[u], cy[u], cz[u]);
+                ri[u] = gm.rinv;
+                ts[u] = split_tau(__fmaf_rn(gm.rsq, gm.rinv, ofs));
+                pr[u] = Pb[row + (uint32_t)(c + u) * cstride + min(ts[u].k, kmax)];
+            }
+#pragma unroll
+            for (int u = 0; u < kBwsUnroll; u++) channel(c + u, cx[u], cy[u], cz[u], ri[u], ts[u], pr[u]);
+        }
+        for (; c < cend; c++) {
+            const float cx = __ldg(p.srcpos + 3 * c), cy = __ldg(p.srcpos + 3 * c + 1),
+                        cz = __ldg(p.srcpos + 3 * c + 2);
+            const recv_geom gm = receive_geometry(vp.x, vp.y, vp.z, cx, cy, cz);
+            const tau_split ts = split_tau(__fmaf_rn(gm.rsq, gm.rinv, ofs));
+            channel(c, cx, cy, cz, gm.rinv, ts, Pb[row + (uint32_t)c * cstride + min(ts.k, kmax)]);
         }
         if (act) {
             if (multi_chunk) {
