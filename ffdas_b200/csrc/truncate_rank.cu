@@ -598,10 +598,13 @@ template <typename T>
 __global__ void __launch_bounds__(kOiThreads) tr_leading_subspace_kernel(const T *__restrict__ G, int p, int r,
                                                                         int max_iter, double tol,
                                                                         T *__restrict__ basis,
-                                                                        int *__restrict__ status) {
+                                                                        int *__restrict__ status, int g_shared) {
     using A = typename tr_elem<T>::acc;
     extern __shared__ __align__(16) unsigned char oi_smem[];
-    A *Q = reinterpret_cast<A *>(oi_smem);
+    // g_shared: G is copied into shared memory once (it is read p times per
+    // step: from L2 each step was a chain of dependent load batches)
+    const size_t g_bytes = g_shared ? ((size_t)p * p * sizeof(T) + 15) / 16 * 16 : 0;
+    A *Q = reinterpret_cast<A *>(oi_smem + g_bytes);
     A *Y = Q + p * r;
     A *H = Y + p * r;
     A *C = H + r * r;
@@ -609,6 +612,13 @@ __global__ void __launch_bounds__(kOiThreads) tr_leading_subspace_kernel(const T
     __shared__ int s_flag;
     const int tid = threadIdx.x, nt = blockDim.x;
     if (tid == 0) *status = 0;
+    // the copy of G the steps read: shared memory (generic loads) or G itself
+    const T *Gm = G;
+    if (g_shared) {
+        T *Gs = reinterpret_cast<T *>(oi_smem);
+        for (int64_t e = tid; e < (int64_t)p * p; e += nt) Gs[e] = G[e];
+        Gm = Gs;
+    }
     for (int e = tid; e < p * r; e += nt) oi_start(Y[e], (uint32_t)e);
     __syncthreads();
     if (!oi_orthonormalize(Y, Q, p, r, C, &s_flag)) return;
@@ -623,14 +633,14 @@ __global__ void __launch_bounds__(kOiThreads) tr_leading_subspace_kernel(const T
             for (; l + 8 <= p; l += 8) {
                 T gv[8];
 #pragma unroll
-                for (int b = 0; b < 8; b++) gv[b] = G[i + (int64_t)(l + b) * p];
+                for (int b = 0; b < 8; b++) gv[b] = Gm[i + (int64_t)(l + b) * p];
 #pragma unroll
                 for (int b = 0; b < 8; b += 2) {
                     s0 = oi_add(s0, oi_mul(oi_from(gv[b]), Q[(l + b) * r + j]));
                     s1 = oi_add(s1, oi_mul(oi_from(gv[b + 1]), Q[(l + b + 1) * r + j]));
                 }
             }
-            for (; l < p; l++) s0 = oi_add(s0, oi_mul(oi_from(G[i + (int64_t)l * p]), Q[l * r + j]));
+            for (; l < p; l++) s0 = oi_add(s0, oi_mul(oi_from(Gm[i + (int64_t)l * p]), Q[l * r + j]));
             Y[i * r + j] = oi_add(s0, s1);
         }
         __syncthreads();
@@ -948,8 +958,26 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
     // reach its residual bound
     const bool leading = direct ? start == 0 : stop == p;
     if (leading && r <= kOiMaxRank && oi_smem_bytes<T>(p, r) <= kSmallBasisSmem) {
-        tr_leading_subspace_kernel<T><<<1, kOiThreads, oi_smem_bytes<T>(p, r), h.stream>>>(
-            gram.get<T>(), (int)p, r, kOiMaxIter, oi_tol<T>(), basis.get<T>(), info.get<int>() + 1);
+        // G in shared memory too when it fits the device's opt-in limit
+        // (the dynamic limit is the device's opt-in size less the kernel's static shared memory)
+        static std::once_flag once;
+        static size_t dyn_max = 0;
+        std::call_once(once, [&] {
+            cudaFuncAttributes fa{};
+            if (cudaFuncGetAttributes(&fa, tr_leading_subspace_kernel<T>) == cudaSuccess &&
+                h.smem_optin > fa.sharedSizeBytes) {
+                const size_t want = h.smem_optin - fa.sharedSizeBytes;
+                if (cudaFuncSetAttribute(tr_leading_subspace_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)want) == cudaSuccess)
+                    dyn_max = want;
+            }
+            cudaGetLastError();
+        });
+        const size_t g_bytes = ((size_t)p * p * sizeof(T) + 15) / 16 * 16;
+        const int g_shared = oi_smem_bytes<T>(p, r) + g_bytes <= dyn_max ? 1 : 0;
+        const size_t oi_smem = oi_smem_bytes<T>(p, r) + (g_shared ? g_bytes : 0);
+        tr_leading_subspace_kernel<T><<<1, kOiThreads, oi_smem, h.stream>>>(
+            gram.get<T>(), (int)p, r, kOiMaxIter, oi_tol<T>(), basis.get<T>(), info.get<int>() + 1, g_shared);
         FFDAS_TRY(ffdas_launch_check(h.stream));
         h.last.variant = kRouteSubspace;
         h.last.grid = gram_grid;
