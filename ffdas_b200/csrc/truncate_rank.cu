@@ -451,6 +451,95 @@ __global__ void __launch_bounds__(32 * kProjMaxGroups) tr_project_small_kernel(
     }
 }
 
+// The same pass for FP32 with unit column stride (A = x's rows), q a
+// multiple of 4 and x, out and the row stride 16-byte aligned: a lane takes
+// four adjacent columns and reads each row's four values as one 16-byte load
+// (a warp's row read is 512 bytes), and a warp's ragged last batch of rows
+// is read together with the rest of its batch, under a predicate.  Per
+// column the operations and their order are those of the kernel above.
+__device__ __forceinline__ void mac4(float4 &c, float a, const float4 &b) {
+    c.x = fmaf(a, b.x, c.x); c.y = fmaf(a, b.y, c.y); c.z = fmaf(a, b.z, c.z); c.w = fmaf(a, b.w, c.w);
+}
+
+template <int RMAX>
+__global__ void __launch_bounds__(32 * kProjMaxGroups) tr_project_small4_kernel(
+    const float *x, int64_t sp, int64_t p, int64_t q, const float *__restrict__ U, int r, int subtract,
+    float *out) {
+    constexpr int B = RMAX <= 8 ? 8 : 4;   // rows a warp reads at once
+    extern __shared__ __align__(16) unsigned char tr_smem[];
+    float *sU = reinterpret_cast<float *>(tr_smem);                                 // p x r
+    float4 *red = reinterpret_cast<float4 *>(sU + ((p * r + 3) & ~int64_t(3)));     // [groups][r][32]
+    const int groups = blockDim.x >> 5, g = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int64_t e = threadIdx.x; e < p * r; e += blockDim.x) sU[e] = U[e];
+    __syncthreads();
+    const int64_t j = ((int64_t)blockIdx.x * 32 + lane) * 4;
+    const bool ok = j < q;
+    const int64_t rows = (p + groups - 1) / groups;
+    const int64_t l0 = min(p, g * rows), l1 = min(p, l0 + rows);
+    const float *col = x + (ok ? j : 0);
+    float4 w[RMAX];
+#pragma unroll
+    for (int t = 0; t < RMAX; t++) w[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (ok) {
+        for (int64_t l = l0; l < l1; l += B) {
+            float4 v[B];
+#pragma unroll
+            for (int b = 0; b < B; b++)
+                if (l + b < l1) v[b] = *reinterpret_cast<const float4 *>(col + (l + b) * sp);
+#pragma unroll
+            for (int b = 0; b < B; b++) {
+                if (l + b >= l1) continue;
+                const float *u = sU + (l + b) * r;
+#pragma unroll
+                for (int t = 0; t < RMAX; t++)
+                    if (t < r) mac4(w[t], u[t], v[b]);
+            }
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < RMAX; t++)
+        if (t < r) red[((int64_t)g * r + t) * 32 + lane] = w[t];
+    __syncthreads();
+    if (!ok) return;
+#pragma unroll
+    for (int t = 0; t < RMAX; t++) {
+        if (t >= r) continue;
+        float4 s4 = red[(int64_t)t * 32 + lane];
+        for (int k = 1; k < groups; k++) {
+            const float4 c = red[((int64_t)k * r + t) * 32 + lane];
+            s4.x = fmaf(1.f, c.x, s4.x); s4.y = fmaf(1.f, c.y, s4.y);
+            s4.z = fmaf(1.f, c.z, s4.z); s4.w = fmaf(1.f, c.w, s4.w);
+        }
+        w[t] = s4;
+    }
+    float *oc = out + j;
+    for (int64_t l = l0; l < l1; l += B) {
+        float4 v[B];
+        if (subtract) {
+#pragma unroll
+            for (int b = 0; b < B; b++)
+                if (l + b < l1) v[b] = *reinterpret_cast<const float4 *>(col + (l + b) * sp);
+        }
+#pragma unroll
+        for (int b = 0; b < B; b++) {
+            if (l + b >= l1) continue;
+            const float *u = sU + (l + b) * r;
+            float4 s4 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int t = 0; t < RMAX; t++)
+                if (t < r) {
+                    s4.x = fmaf(u[t], w[t].x, s4.x); s4.y = fmaf(u[t], w[t].y, s4.y);
+                    s4.z = fmaf(u[t], w[t].z, s4.z); s4.w = fmaf(u[t], w[t].w, s4.w);
+                }
+            float4 o = s4;
+            if (subtract)
+                o = make_float4(fmaf(-1.f, s4.x, v[b].x), fmaf(-1.f, s4.y, v[b].y), fmaf(-1.f, s4.z, v[b].z),
+                                fmaf(-1.f, s4.w, v[b].w));
+            *reinterpret_cast<float4 *>(oc + (l + b) * sp) = o;
+        }
+    }
+}
+
 // Row groups (warps) per CTA of the one-pass projection: at least 32 rows
 // per warp (fewer leaves each warp too little work for the basis load and
 // the barrier), at most 8, and shared memory (basis + partials) within the
@@ -757,9 +846,43 @@ ffdas_error_t get_solver(ffdas_context &ctx, solver_state **out) {
 
 constexpr size_t kGramPartialBytes = size_t(256) << 20;
 
+// Row groups of the four-column FP32 pass (0: it does not apply): unit
+// column stride, q and the row stride multiples of 4, x and out 16-byte
+// aligned, and the basis and float4 partials of the one-column pass's group
+// count within the static limit.  The group count sets the order of the
+// sums, so it is never changed: aligned or not, the bits are the same.
+template <typename T>
+int small4_groups(const T *, int64_t, int64_t, int64_t, int64_t, int, int, const T *) { return 0; }
+template <>
+int small4_groups<float>(const float *x, int64_t sp, int64_t sq, int64_t p, int64_t q, int r, int groups,
+                         const float *out) {
+    if (sq != 1 || q % 4 != 0 || sp % 4 != 0 || reinterpret_cast<uintptr_t>(x) % 16 != 0 ||
+        reinterpret_cast<uintptr_t>(out) % 16 != 0)
+        return 0;
+    const size_t smem = (size_t)(((p * r + 3) & ~int64_t(3)) + (int64_t)groups * r * 32 * 4) * sizeof(float);
+    return smem <= kSmallBasisSmem ? groups : 0;
+}
+
+template <int RMAX, typename T>
+ffdas_error_t launch_small4(ffdas_context &, const T *, int64_t, int64_t, int64_t, const T *, int, int, int, T *) {
+    return FFDAS_ERROR_INTERNAL;
+}
+template <int RMAX>
+ffdas_error_t launch_small4(ffdas_context &h, const float *x, int64_t sp, int64_t p, int64_t q, const float *U, int r,
+                            int groups, int subtract, float *out) {
+    const int64_t blocks = (q / 4 + 31) / 32;
+    if (blocks > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
+    const size_t smem = (size_t)(((p * r + 3) & ~int64_t(3)) + (int64_t)groups * r * 32 * 4) * sizeof(float);
+    tr_project_small4_kernel<RMAX><<<(unsigned)blocks, 32 * groups, smem, h.stream>>>(x, sp, p, q, U, r, subtract,
+                                                                                     out);
+    return ffdas_launch_check(h.stream);
+}
+
 template <typename T, int RMAX>
 ffdas_error_t launch_small(ffdas_context &h, const T *x, int64_t sp, int64_t sq, int64_t p, int64_t q, const T *U,
                            int r, int groups, int subtract, T *out) {
+    if (const int g4 = small4_groups<T>(x, sp, sq, p, q, r, groups, out))
+        return launch_small4<RMAX>(h, x, sp, p, q, U, r, g4, subtract, out);
     const int64_t blocks = (q + 31) / 32;
     if (blocks > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
     const size_t smem = (size_t)(p * r + (int64_t)groups * r * 32) * sizeof(T);

@@ -330,6 +330,28 @@ def test_tensor_core_gram_not_eligible(case):
     assert np.abs(res.cpu().numpy() - ref).max() / np.abs(x.cpu().numpy()).max() <= tol
 
 
+@pytest.mark.parametrize("m, n, start, stop", [(200, 8192, 5, None), (37, 1024, 3, None), (64, 2048, 0, 3),
+                                                 (96, 4096, 12, None), (130, 1028, 20, None), (9, 64, 1, 2)])
+def test_four_column_projection_matches_one_column(m, n, start, stop):
+    # FP32 rows with a column count that is a multiple of 4, 16-byte aligned:
+    # the projection reads four columns per lane (where its partials fit in
+    # the shared memory the one-column kernel uses; 130 x 20 does not); the
+    # same matrix stored one element off the 16-byte boundary takes the
+    # one-column kernel.  Both run the same operations in the same order per
+    # column: the same bits.  The FMA Gram runs in both calls so that the
+    # bases are the same.
+    x = _cuda(tro.clutter_ensemble(m, n, rank=max(start, stop or 0), seed=m + n).astype(np.float32))
+    shifted = torch.empty(m * n + 1, device=DEV)[1:].view(m, n)
+    shifted.copy_(x)
+    assert shifted.data_ptr() % 16 != 0 and x.data_ptr() % 16 == 0
+    a, _ = _engine_call(1, x, start, stop)
+    b, _ = _engine_call(1, shifted, start, stop)
+    assert torch.equal(a, b)
+    if max(start, stop or 0) <= 5:             # deeper cuts fall inside the noise: ill conditioned
+        ref = tro.truncate_rank_f64(x.cpu().numpy(), start, stop)
+        assert np.abs(a.cpu().numpy() - ref).max() / np.abs(x.cpu().numpy()).max() <= 2e-5
+
+
 def test_gram_engine_rejects_unknown_values():
     h = get_library_handle(torch.device(DEV))
     for bad in (-1, 3):
