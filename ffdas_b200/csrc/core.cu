@@ -7,6 +7,8 @@
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
 #include <atomic>
+#include <map>
+#include <mutex>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -28,6 +30,22 @@ extern "C" FFDAS_API void ffdas_debug_staged_drop_stage(int enable) {
 
 int ffdas_take_debug_drop_stage() {
     return g_drop_stage.exchange(0);
+}
+
+cudaError_t ffdas_raise_smem_limit(const void *func, int device, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> raised;
+    std::lock_guard<std::mutex> lock(mu);
+    const auto key = std::make_pair(func, device);
+    const auto it = raised.find(key);
+    if (it != raised.end() && it->second >= bytes) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return e;
+    }
+    raised[key] = bytes;
+    return cudaSuccess;
 }
 
 ffdas_error_t ffdas_launch_check(cudaStream_t stream) {

@@ -129,3 +129,8 @@ private:
 // handle creation (then the stream is synchronised after every launch, as the
 // reference's CUDA_LAUNCH_CHECK does under FFDAS_DEBUG, error_checking.h:115).
 ffdas_error_t ffdas_launch_check(cudaStream_t stream);
+
+// Raises the dynamic shared memory limit of kernel `func` to `bytes` on
+// `device` (the current device; the attribute belongs to the device's
+// context), once per kernel, device and size.
+cudaError_t ffdas_raise_smem_limit(const void *func, int device, size_t bytes);

@@ -544,13 +544,9 @@ bool bws_supported(const das_problem &pb, int kind) {
 
 template <int K, bool POS>
 ffdas_error_t launch_bws_pos(ffdas_context &h, const bwd_params &bp, int L, dim3 grid, size_t smem) {
-    static std::once_flag once;
-    static cudaError_t attr = cudaSuccess;
-    std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(das_bwd_sorted_kernel<K, POS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)kBwsMaxSmem);
-    });
-    if (attr != cudaSuccess) return FFDAS_ERROR_CUDA_RUNTIME;
+    if (ffdas_raise_smem_limit(reinterpret_cast<const void *>(das_bwd_sorted_kernel<K, POS>), h.device_id,
+                               kBwsMaxSmem) != cudaSuccess)
+        return FFDAS_ERROR_CUDA_RUNTIME;
     das_bwd_sorted_kernel<K, POS><<<grid, kBwsThreads, smem, h.stream>>>(bp, L);
     return ffdas_launch_check(h.stream);
 }

@@ -372,7 +372,8 @@ constexpr size_t kSmallBasisSmem = 48 * 1024;   // dynamic shared memory without
 template <typename T, int RMAX>
 __global__ void __launch_bounds__(32 * kProjMaxGroups) tr_project_small_kernel(
     const T *x, int64_t sp, int64_t sq, int64_t p, int64_t q, const T *__restrict__ U, int r, int subtract,
-    T *out) {
+    T *out, const int *gate) {
+    if (gate && *gate != 1) return;
     extern __shared__ __align__(16) unsigned char tr_smem[];
     T *sU = reinterpret_cast<T *>(tr_smem);      // p x r
     T *red = sU + p * r;                          // [groups][r][32]
@@ -464,7 +465,8 @@ __device__ __forceinline__ void mac4(float4 &c, float a, const float4 &b) {
 template <int RMAX>
 __global__ void __launch_bounds__(32 * kProjMaxGroups) tr_project_small4_kernel(
     const float *x, int64_t sp, int64_t p, int64_t q, const float *__restrict__ U, int r, int subtract,
-    float *out) {
+    float *out, const int *gate) {
+    if (gate && *gate != 1) return;
     constexpr int B = RMAX <= 8 ? 8 : 4;   // rows a warp reads at once
     extern __shared__ __align__(16) unsigned char tr_smem[];
     float *sU = reinterpret_cast<float *>(tr_smem);                                 // p x r
@@ -578,8 +580,6 @@ __device__ __forceinline__ double oi_shfl(double a, int o) { return __shfl_xor_s
 __device__ __forceinline__ double2 oi_shfl(double2 a, int o) {
     return make_double2(__shfl_xor_sync(0xffffffffu, a.x, o), __shfl_xor_sync(0xffffffffu, a.y, o));
 }
-__device__ __forceinline__ double oi_from(float a) { return a; }
-__device__ __forceinline__ double oi_from(double a) { return a; }
 __device__ __forceinline__ double2 oi_from(float2 a) { return make_double2(a.x, a.y); }
 __device__ __forceinline__ double2 oi_from(double2 a) { return a; }
 __device__ __forceinline__ void oi_to(float &o, double a) { o = (float)a; }
@@ -608,72 +608,246 @@ constexpr int kRouteSubspace = 10, kRouteSyevd = 11, kRouteSyevdx = 12, kRouteCo
 constexpr int kOiThreads = 512;
 constexpr int kOiMaxRank = 16;
 constexpr int kOiMaxIter = 30;
+constexpr int kOiMaxSlices = 8;
 // residual bound relative to the largest Rayleigh quotient: 2 eps for FP32
 // data, about 45 eps for FP64 (the rounding floor of G Q in double)
 template <typename T> constexpr double oi_tol() { return sizeof(typename tr_elem<T>::real) == 4 ? 2.4e-7 : 1e-14; }
 
-// M[a][b] = sum_i conj(X[i][a]) Z[i][b], a, b < r (row-major p x r inputs):
-// one warp per entry, lanes over rows, shuffle sums.  Ends with a barrier.
+// (a, b), a <= b, of the e-th entry of an r x r upper triangle, row by row
+__device__ __forceinline__ void oi_upper(int e, int r, int &a, int &b) {
+    a = 0;
+    while (e >= r - a && a < r) e -= r - a, a++;
+    b = a + e;
+}
+
+// Hermitian products of p x r row-major matrices, M = X^H Z, and M2 =
+// X2^H Z2 when X2 is given (the products this iteration forms are Q^H Y,
+// Y^H Y and Q^H Q, Hermitian in exact arithmetic): the upper triangles, one
+// warp per entry, lanes over rows and a shuffle sum, mirrored into the lower
+// triangles.  Ends with a barrier.
 template <typename A>
-__device__ void oi_inner(const A *X, const A *Z, int p, int r, A *M) {
+__device__ void oi_hermitian(const A *X, const A *Z, A *M, const A *X2, const A *Z2, A *M2, int p, int r) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int e = warp; e < r * r; e += nw) {
-        const int a = e / r, b = e - a * r;
+    const int ne = r * (r + 1) / 2, total = X2 ? 2 * ne : ne;
+    for (int e = warp; e < total; e += nw) {
+        const bool second = e >= ne;
+        const A *x = second ? X2 : X;
+        const A *z = second ? Z2 : Z;
+        A *m = second ? M2 : M;
+        int a, b;
+        oi_upper(second ? e - ne : e, r, a, b);
         A s = oi_zero<A>();
-        for (int i = lane; i < p; i += 32) s = oi_add(s, oi_mul(oi_conj(X[i * r + a]), Z[i * r + b]));
+        for (int i = lane; i < p; i += 32) s = oi_add(s, oi_mul(oi_conj(x[i * r + a]), z[i * r + b]));
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s = oi_add(s, oi_shfl(s, o));
-        if (lane == 0) M[e] = s;
+        if (lane == 0) {
+            m[a * r + b] = s;
+            if (a != b) m[b * r + a] = oi_conj(s);
+        }
     }
     __syncthreads();
 }
 
-// Q <- an orthonormal basis of span(Y) (p x r, row-major): columns scaled to
-// unit norm, then Cholesky QR twice (the second pass restores orthogonality
-// to rounding).  Returns false (on every thread) if a pivot is not positive.
+// Cholesky factor of the r x r Hermitian C (full storage), C = L L^H, in
+// place (L in the lower triangle), by one warp: per column the pivot, then
+// a lane per row of the trailing lower triangle.  With `cs`, of
+// D C D for D = diag(C)^-1/2 (the Gram matrix of the columns scaled to unit
+// norm; a zero column keeps scale 1), the scales stored to cs.  1 / L[j][j]
+// goes to invd; *flag = 0 when a pivot is not positive.  Called by warp 0.
 template <typename A>
-__device__ bool oi_orthonormalize(A *Y, A *Q, int p, int r, A *C, int *flag) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    oi_inner(Y, Y, p, r, C);
-    for (int e = tid; e < p * r; e += nt) {
-        const int b = e % r;
-        const double n2 = oi_re(C[b * r + b]);
-        Q[e] = n2 > 0.0 ? oi_scale(Y[e], rsqrt(n2)) : Y[e];
+__device__ void oi_cholesky_warp(A *C, int r, double *invd, double *cs, int *flag) {
+    const int lane = threadIdx.x & 31;
+    if (cs) {
+        if (lane < r) {
+            const double n2 = oi_re(C[lane * r + lane]);
+            cs[lane] = n2 > 0.0 ? rsqrt(n2) : 1.0;
+        }
+        __syncwarp();
+        if (lane < r)
+            for (int k = 0; k < r; k++) C[lane * r + k] = oi_scale(C[lane * r + k], cs[lane] * cs[k]);
+        __syncwarp();
     }
+    int ok = 1;
+    for (int j = 0; j < r; j++) {
+        const double d = oi_re(C[j * r + j]);
+        if (!(d > 0.0)) {
+            ok = 0;
+            break;
+        }
+        const double inv = rsqrt(d);
+        if (lane == j) C[j * r + j] = oi_real<A>(d * inv);
+        else if (lane > j && lane < r) C[lane * r + j] = oi_scale(C[lane * r + j], inv);
+        if (lane == 0) invd[j] = inv;
+        __syncwarp();
+        if (lane > j && lane < r) {   // row `lane` of the trailing lower triangle
+            const A lij = C[lane * r + j];
+            for (int k = j + 1; k <= lane; k++)
+                C[lane * r + k] = oi_sub(C[lane * r + k], oi_mul(lij, oi_conj(C[k * r + j])));
+        }
+        __syncwarp();
+    }
+    if (lane == 0) *flag = ok;
+}
+
+// Rows of Q = (Y D) L^-H (D = diag(cs), or none): per row the forward
+// substitution z_b = ((y D)_b - sum_{a<b} z_a conj(L[b][a])) / L[b][b], in
+// registers.  Y and Q may be the same array.
+template <typename A, int RM>
+__device__ void oi_solve_rows(const A *Y, A *Q, int p, int r, const A *Lm, const double *invd, const double *cs) {
+    for (int i = threadIdx.x; i < p; i += blockDim.x) {
+        A z[RM];
+#pragma unroll
+        for (int b = 0; b < RM; b++) {
+            if (b >= r) break;
+            A v = Y[i * r + b];
+            if (cs) v = oi_scale(v, cs[b]);
+#pragma unroll
+            for (int a = 0; a < b; a++) v = oi_sub(v, oi_mul(z[a], oi_conj(Lm[b * r + a])));
+            z[b] = oi_scale(v, invd[b]);
+        }
+#pragma unroll
+        for (int b = 0; b < RM; b++)
+            if (b < r) Q[i * r + b] = z[b];
+    }
+}
+
+// shared memory the subspace kernel addresses past G
+template <typename A>
+struct oi_layout {
+    A *Q, *Y, *H, *C, *P;
+    double *red, *invd, *cs;
+    __device__ oi_layout(unsigned char *base, int p, int r, int ks) {
+        Q = reinterpret_cast<A *>(base);
+        Y = Q + p * r;
+        H = Y + p * r;
+        C = H + r * r;
+        P = C + r * r;
+        red = reinterpret_cast<double *>(P + (ks - 1) * p * r);
+        invd = red + 32;
+        cs = invd + kOiMaxRank;
+    }
+};
+
+// Q <- an orthonormal basis of span(Y), given C = Y^H Y: Cholesky QR of the
+// unit-norm columns, then once more on the result unless Q^H Q is already
+// within `orth` of the identity in every entry (the second pass restores
+// orthogonality to rounding; one pass loses about cond(Y)^2 eps).  False (on
+// every thread) when a pivot is not positive.
+template <typename A, int RM>
+__device__ bool oi_orthonormalize(const oi_layout<A> &s, int p, int r, int *flag, double orth) {
+    const int warp = threadIdx.x >> 5;
+    if (warp == 0) oi_cholesky_warp<A>(s.C, r, s.invd, s.cs, flag);
     __syncthreads();
-    for (int pass = 0; pass < 2; pass++) {
-        oi_inner(Q, Q, p, r, C);
-        if (tid == 0) {
-            // C = L L^H in place (lower triangle)
-            int ok = 1;
-            for (int j = 0; j < r && ok; j++) {
-                double d = oi_re(C[j * r + j]);
-                for (int k = 0; k < j; k++) d -= oi_abs2(C[j * r + k]);
-                if (!(d > 0.0)) { ok = 0; break; }
-                const double ljj = sqrt(d);
-                C[j * r + j] = oi_real<A>(ljj);
-                for (int i = j + 1; i < r; i++) {
-                    A v = C[i * r + j];
-                    for (int k = 0; k < j; k++) v = oi_sub(v, oi_mul(C[i * r + k], oi_conj(C[j * r + k])));
-                    C[i * r + j] = oi_scale(v, 1.0 / ljj);
-                }
-            }
-            *flag = ok;
+    if (!*flag) return false;
+    oi_solve_rows<A, RM>(s.Y, s.Q, p, r, s.C, s.invd, s.cs);
+    __syncthreads();
+    oi_hermitian<A>(s.Q, s.Q, s.C, nullptr, nullptr, nullptr, p, r);
+    double dev2 = 0.0;   // largest squared deviation from I
+    for (int a = 0; a < r; a++)
+        for (int b = 0; b < r; b++) {
+            const A c = s.C[a * r + b];
+            dev2 = fmax(dev2, oi_abs2(a == b ? oi_sub(c, oi_real<A>(1.0)) : c));
         }
-        __syncthreads();
-        if (!*flag) return false;
-        // row-wise: z L^H = q  ->  z_b = (q_b - sum_{a<b} z_a conj(L[b][a])) / L[b][b]
-        for (int i = tid; i < p; i += nt) {
-            A *row = Q + (int64_t)i * r;
-            for (int b = 0; b < r; b++) {
-                A v = row[b];
-                for (int a = 0; a < b; a++) v = oi_sub(v, oi_mul(row[a], oi_conj(C[b * r + a])));
-                row[b] = oi_scale(v, 1.0 / oi_re(C[b * r + b]));
-            }
-        }
-        __syncthreads();
-    }
+    if (dev2 <= orth * orth) return true;
+    if (warp == 0) oi_cholesky_warp<A>(s.C, r, s.invd, nullptr, flag);
+    __syncthreads();
+    if (!*flag) return false;
+    oi_solve_rows<A, RM>(s.Q, s.Q, p, r, s.C, s.invd, nullptr);
+    __syncthreads();
     return true;
+}
+
+// Asynchronous copy of G's p columns (p elements each) into shared memory
+// with leading dimension ld, issued before the start basis is built and
+// waited for before the first product: 16-byte pieces when the column and
+// ld byte sizes allow, else one element per copy (4, 8 or 16 bytes).
+template <int BYTES>
+__device__ __forceinline__ void oi_cp_async(uint32_t dst, const char *src) {
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dst), "l"(src), "n"(BYTES) : "memory");
+}
+template <typename T>
+__device__ void oi_copy_async(unsigned char *dst, const T *G, int p, int ld) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    const char *g = reinterpret_cast<const char *>(G);
+    // (the copy fits shared memory: every offset fits 32 bits)
+    const uint32_t col = (uint32_t)p * sizeof(T), dcol = (uint32_t)ld * sizeof(T);
+    if (col % 16 == 0 && dcol % 16 == 0) {
+        const uint32_t per = col / 16;
+        for (uint32_t e = threadIdx.x; e < per * (uint32_t)p; e += blockDim.x) {
+            const uint32_t k = e / per, o = (e - k * per) * 16;
+            oi_cp_async<16>(d + k * dcol + o, g + (size_t)k * col + o);
+        }
+    } else {
+        for (uint32_t e = threadIdx.x; e < (uint32_t)(p * p); e += blockDim.x) {
+            const uint32_t k = e / (uint32_t)p, o = (e - k * (uint32_t)p) * (uint32_t)sizeof(T);
+            oi_cp_async<sizeof(T)>(d + k * dcol + o, g + (size_t)k * col + o);
+        }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void oi_copy_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Y = G Q for real data on the FP64 tensor cores (mma.m8n8k4 .f64; each of
+// its products and sums is an FP64 operation).  A task is an 8-row tile of
+// Y, an 8-column tile of Q and one of `parts` ranges of the inner dimension
+// (steps of 4); a warp runs up to kOiTasks tasks at once, so that their
+// fragment loads and products overlap (the product's latency is about six
+// times its issue interval).  Part 0 goes to Y, part k to P + (k-1) p r.
+// Fragments (PTX ISA, mma.m8n8k4 .f64): lane l holds A[l/4][l%4],
+// B[l%4][l/4] and D[l/4][2(l%4) + 0..1].  G column-major with leading
+// dimension ld; Q, Y row-major p x r.
+constexpr int kOiTasks = 4;
+__device__ __forceinline__ double oi_widen(float f) { return f; }
+__device__ __forceinline__ double oi_widen(double d) { return d; }
+template <typename T>
+__device__ void oi_gq_dmma(const T *G, int ld, const double *Q, double *Y, double *P, int p, int r, int parts) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int mt = (p + 7) / 8, tiles = mt * ((r + 7) / 8), kt = (p + 3) / 4, steps = (kt + parts - 1) / parts;
+    const int tasks = tiles * parts;
+    const int g = lane >> 2, t4 = lane & 3;
+    for (int base = 0; base < tasks; base += kOiTasks * nw) {
+        int row[kOiTasks], col[kOiTasks], k0[kOiTasks], part[kOiTasks];
+        bool on[kOiTasks];
+#pragma unroll
+        for (int u = 0; u < kOiTasks; u++) {
+            const int task = base + warp + u * nw;
+            on[u] = task < tasks;
+            const int tile = on[u] ? task % tiles : 0;
+            part[u] = on[u] ? task / tiles : 0;
+            row[u] = (tile % mt) * 8;
+            col[u] = (tile / mt) * 8;
+            k0[u] = part[u] * steps * 4 + t4;
+        }
+        double c0[kOiTasks], c1[kOiTasks];
+#pragma unroll
+        for (int u = 0; u < kOiTasks; u++) c0[u] = c1[u] = 0.0;
+        // every slot multiplies (an idle one zeros): no branch around the
+        // warp-wide instruction
+        for (int s = 0; s < steps; s++) {
+            double a[kOiTasks], b[kOiTasks];
+#pragma unroll
+            for (int u = 0; u < kOiTasks; u++) {
+                const int k = k0[u] + 4 * s, i = row[u] + g, n = col[u] + g;
+                a[u] = on[u] && i < p && k < p ? oi_widen(G[i + (int64_t)k * ld]) : 0.0;
+                b[u] = on[u] && n < r && k < p ? Q[k * r + n] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kOiTasks; u++)
+                asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                    : "+d"(c0[u]), "+d"(c1[u]) : "d"(a[u]), "d"(b[u]));
+        }
+#pragma unroll
+        for (int u = 0; u < kOiTasks; u++) {
+            if (!on[u]) continue;
+            double *dst = part[u] == 0 ? Y : P + (int64_t)(part[u] - 1) * p * r;
+            const int i = row[u] + g, n = col[u] + 2 * t4;
+            if (i < p && n < r) dst[i * r + n] = c0[u];
+            if (i < p && n + 1 < r) dst[i * r + n + 1] = c1[u];
+        }
+    }
 }
 
 // Orthogonal iteration for the leading r-dimensional invariant subspace of
@@ -683,88 +857,120 @@ __device__ bool oi_orthonormalize(A *Y, A *Q, int p, int r, A *C, int *flag) {
 // eigensolver's for this G), else Q = orth(Y).  On convergence the basis is
 // written as T (row-major p x r) and *status = 1; otherwise *status = 0 and
 // the caller runs the dense eigensolver.  One CTA; every loop is bounded.
-template <typename T>
+// g_ld > 0: G is copied into shared memory with that leading dimension
+// (padded so that the tensor-core fragments' loads meet no bank conflicts).
+// Real data: G Q on the FP64 tensor cores.  Complex data: G Q split over ks
+// slices of its inner dimension, so that more threads than rows share the
+// product (each G element is read and widened to double once per step).
+template <typename T, int RM>
 __global__ void __launch_bounds__(kOiThreads) tr_leading_subspace_kernel(const T *__restrict__ G, int p, int r,
                                                                         int max_iter, double tol,
                                                                         T *__restrict__ basis,
-                                                                        int *__restrict__ status, int g_shared) {
+                                                                        int *__restrict__ status, int g_ld,
+                                                                        int ks) {
     using A = typename tr_elem<T>::acc;
+    constexpr bool kReal = sizeof(A) == sizeof(double);
     extern __shared__ __align__(16) unsigned char oi_smem[];
-    // g_shared: G is copied into shared memory once (it is read p times per
-    // step: from L2 each step was a chain of dependent load batches)
-    const size_t g_bytes = g_shared ? ((size_t)p * p * sizeof(T) + 15) / 16 * 16 : 0;
-    A *Q = reinterpret_cast<A *>(oi_smem + g_bytes);
-    A *Y = Q + p * r;
-    A *H = Y + p * r;
-    A *C = H + r * r;
-    double *red = reinterpret_cast<double *>(C + r * r);
+    const size_t g_bytes = g_ld ? ((size_t)p * g_ld * sizeof(T) + 15) / 16 * 16 : 0;
+    const oi_layout<A> s(oi_smem + g_bytes, p, r, ks);
     __shared__ int s_flag;
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     if (tid == 0) *status = 0;
-    // the copy of G the steps read: shared memory (generic loads) or G itself
-    const T *Gm = G;
-    if (g_shared) {
-        T *Gs = reinterpret_cast<T *>(oi_smem);
-        for (int64_t e = tid; e < (int64_t)p * p; e += nt) Gs[e] = G[e];
-        Gm = Gs;
-    }
-    for (int e = tid; e < p * r; e += nt) oi_start(Y[e], (uint32_t)e);
+    const T *Gs = reinterpret_cast<const T *>(oi_smem);
+    if (g_ld) oi_copy_async<T>(oi_smem, G, p, g_ld);
+    for (int e = tid; e < p * r; e += nt) oi_start(s.Y[e], (uint32_t)e);
     __syncthreads();
-    if (!oi_orthonormalize(Y, Q, p, r, C, &s_flag)) return;
+    oi_hermitian<A>(s.Y, s.Y, s.C, nullptr, nullptr, nullptr, p, r);
+    // one pass leaving Q^H Q within tol / 16 of I keeps the residual test and
+    // the basis at the bound
+    const double orth = tol / 16;
+    const bool ok0 = oi_orthonormalize<A, RM>(s, p, r, &s_flag, orth);
+    oi_copy_wait();
+    __syncthreads();
+    if (!ok0) return;
+    const int len = (p + ks - 1) / ks;
     for (int it = 0; it < max_iter; it++) {
-        // Y = G Q: consecutive threads take consecutive rows i (coalesced G
-        // reads); 8 loads in flight per batch and two partial sums, so the
-        // column walk is not one dependent load-add chain
-        for (int e = tid; e < p * r; e += nt) {
-            const int j = e / p, i = e - j * p;
-            A s0 = oi_zero<A>(), s1 = oi_zero<A>();
-            int l = 0;
-            for (; l + 8 <= p; l += 8) {
-                T gv[8];
+        if constexpr (kReal) {
+            const double *Qd = reinterpret_cast<const double *>(s.Q);
+            double *Yd = reinterpret_cast<double *>(s.Y), *Pd = reinterpret_cast<double *>(s.P);
+            if (g_ld) oi_gq_dmma<T>(Gs, g_ld, Qd, Yd, Pd, p, r, ks);
+            else oi_gq_dmma<T>(G, p, Qd, Yd, Pd, p, r, ks);
+        } else {
+            // Y = G Q: thread (slice, row i) sums its slice of l for all r
+            // columns; consecutive threads take consecutive rows (coalesced G)
+            const T *Gm = g_ld ? Gs : G;
+            const int ld = g_ld ? g_ld : p;
+            for (int t = tid; t < p * ks; t += nt) {
+                const int sl = t / p, i = t - sl * p;
+                const int l0 = min(p, sl * len), l1 = min(p, l0 + len);
+                A acc[RM];
 #pragma unroll
-                for (int b = 0; b < 8; b++) gv[b] = Gm[i + (int64_t)(l + b) * p];
+                for (int j = 0; j < RM; j++) acc[j] = oi_zero<A>();
+                for (int l = l0; l < l1; l++) {
+                    const A g = oi_from(Gm[i + (int64_t)l * ld]);
+                    const A *qr = s.Q + l * r;
 #pragma unroll
-                for (int b = 0; b < 8; b += 2) {
-                    s0 = oi_add(s0, oi_mul(oi_from(gv[b]), Q[(l + b) * r + j]));
-                    s1 = oi_add(s1, oi_mul(oi_from(gv[b + 1]), Q[(l + b + 1) * r + j]));
+                    for (int j = 0; j < RM; j++)
+                        if (j < r) acc[j] = oi_add(acc[j], oi_mul(g, qr[j]));
                 }
+                A *dst = sl == 0 ? s.Y : s.P + (sl - 1) * p * r;
+#pragma unroll
+                for (int j = 0; j < RM; j++)
+                    if (j < r) dst[i * r + j] = acc[j];
             }
-            for (; l < p; l++) s0 = oi_add(s0, oi_mul(oi_from(Gm[i + (int64_t)l * p]), Q[l * r + j]));
-            Y[i * r + j] = oi_add(s0, s1);
         }
         __syncthreads();
-        oi_inner(Q, Y, p, r, H);
-        // residual ||Y - Q H||_F^2
-        double part = 0.0;
-        for (int e = tid; e < p * r; e += nt) {
-            const int i = e / r, b = e - i * r;
-            A v = Y[e];
-            for (int a = 0; a < r; a++) v = oi_sub(v, oi_mul(Q[i * r + a], H[a * r + b]));
-            part += oi_abs2(v);
-        }
-        red[tid] = part;
-        __syncthreads();
-        for (int w = nt / 2; w > 0; w >>= 1) {
-            if (tid < w) red[tid] += red[tid + w];
+        if (ks > 1) {   // the parts in order
+            for (int e = tid; e < p * r; e += nt) {
+                A v = s.Y[e];
+                for (int k = 1; k < ks; k++) v = oi_add(v, s.P[(k - 1) * p * r + e]);
+                s.Y[e] = v;
+            }
             __syncthreads();
         }
-        double scale = 0.0;
-        for (int a = 0; a < r; a++) scale = fmax(scale, oi_re(H[a * r + a]));
-        const bool done = sqrt(red[0]) <= tol * scale;
+        // H = Q^H Y and C = Y^H Y together
+        oi_hermitian<A>(s.Q, s.Y, s.H, s.Y, s.Y, s.C, p, r);
+        // residual ||Y - Q H||_F^2: a row per thread, warp sums, then every
+        // thread adds the warp sums in the same order (the same decision)
+        double part = 0.0;
+        for (int i = tid; i < p; i += nt) {
+            A qi[RM];
+#pragma unroll
+            for (int a = 0; a < RM; a++) qi[a] = a < r ? s.Q[i * r + a] : oi_zero<A>();
+#pragma unroll
+            for (int b = 0; b < RM; b++) {
+                if (b >= r) break;
+                A v = s.Y[i * r + b];
+#pragma unroll
+                for (int a = 0; a < RM; a++)
+                    if (a < r) v = oi_sub(v, oi_mul(qi[a], s.H[a * r + b]));
+                part += oi_abs2(v);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (lane == 0) s.red[warp] = part;
         __syncthreads();
-        if (done) {
-            for (int e = tid; e < p * r; e += nt) oi_to(basis[e], Q[e]);
+        double res2 = 0.0;
+        for (int w = 0; w < nw; w++) res2 += s.red[w];
+        double scale = 0.0;
+        for (int a = 0; a < r; a++) scale = fmax(scale, oi_re(s.H[a * r + a]));
+        if (sqrt(res2) <= tol * scale) {
+            for (int e = tid; e < p * r; e += nt) oi_to(basis[e], s.Q[e]);
             if (tid == 0) *status = 1;
             return;
         }
-        if (!oi_orthonormalize(Y, Q, p, r, C, &s_flag)) return;
+        if (!oi_orthonormalize<A, RM>(s, p, r, &s_flag, orth)) return;
     }
 }
 
-// shared memory of the subspace kernel: Q, Y (p x r), H, C (r x r), the reduction
+// shared memory of the subspace kernel past G: Q, Y (p x r), H, C (r x r),
+// ks - 1 slice partials (p x r), the warp sums, 1 / L[j][j] and the column
+// scales
 template <typename T>
-size_t oi_smem_bytes(int64_t p, int r) {
-    return (size_t)(2 * p * r + 2 * (int64_t)r * r) * sizeof(typename tr_elem<T>::acc) + kOiThreads * sizeof(double);
+size_t oi_smem_bytes(int64_t p, int r, int ks) {
+    return (size_t)((2 + (int64_t)(ks - 1)) * p * r + 2 * (int64_t)r * r) * sizeof(typename tr_elem<T>::acc) +
+           (32 + 2 * kOiMaxRank) * sizeof(double);
 }
 
 // ------------------------------------------------------------- cuSOLVER
@@ -844,6 +1050,48 @@ ffdas_error_t get_solver(ffdas_context &ctx, solver_state **out) {
 
 // ------------------------------------------------------------------ driver
 
+// The subspace iteration for bases of up to RM vectors: G in shared memory
+// when it fits the device's opt-in size less the kernel's static shared
+// memory (leading dimension padded to 8 mod 32 elements where that fits),
+// and for complex data as many slices of G Q (up to one thread per row and
+// slice) as the threads and the shared memory allow.
+template <typename T, int RM>
+ffdas_error_t launch_subspace(ffdas_context &h, const T *G, int64_t p, int r, T *basis, int *status) {
+    static const size_t static_smem = [] {
+        cudaFuncAttributes fa{};
+        const bool ok = cudaFuncGetAttributes(&fa, tr_leading_subspace_kernel<T, RM>) == cudaSuccess;
+        cudaGetLastError();
+        return ok ? fa.sharedSizeBytes : SIZE_MAX;
+    }();
+    constexpr bool real = sizeof(typename tr_elem<T>::acc) == sizeof(double);
+    const size_t dyn_max = static_smem < h.smem_optin ? h.smem_optin - static_smem : 0;
+    const auto g_bytes = [&](int64_t ld) { return ((size_t)(p * ld) * sizeof(T) + 15) / 16 * 16; };
+    // complex: slices of rows' inner sums (one thread per row and slice);
+    // real: parts of the tensor-core tasks' inner dimension, about three
+    // tasks per warp and at most kOiTasks
+    const int64_t warps = kOiThreads / 32, tiles = (p + 7) / 8 * ((r + 7) / 8);
+    int ks = real ? (int)std::max<int64_t>(1, std::min<int64_t>({(3 * warps + tiles - 1) / tiles, kOiTasks * warps / tiles,
+                                                                 (p + 3) / 4, (int64_t)kOiMaxSlices}))
+                  : (int)std::max<int64_t>(1, std::min<int64_t>(kOiMaxSlices, kOiThreads / p));
+    int g_ld = 0;
+    const bool aligned = reinterpret_cast<uintptr_t>(G) % 16 == 0;
+    for (int k = ks; k >= 1 && !g_ld && aligned; k--) {
+        const int64_t padded = p + ((8 - p % 32) % 32 + 32) % 32;
+        for (const int64_t ld : {padded, p})
+            if (!g_ld && oi_smem_bytes<T>(p, r, k) + g_bytes(ld) <= dyn_max) g_ld = (int)ld, ks = k;
+    }
+    if (!g_ld)
+        while (ks > 1 && oi_smem_bytes<T>(p, r, ks) > std::max(dyn_max, kSmallBasisSmem)) ks--;
+    const size_t smem = oi_smem_bytes<T>(p, r, ks) + (g_ld ? g_bytes(g_ld) : 0);
+    if (smem > kSmallBasisSmem &&
+        ffdas_raise_smem_limit(reinterpret_cast<const void *>(tr_leading_subspace_kernel<T, RM>), h.device_id,
+                               smem) != cudaSuccess)
+        return FFDAS_ERROR_CUDA_RUNTIME;
+    tr_leading_subspace_kernel<T, RM><<<1, kOiThreads, smem, h.stream>>>(G, (int)p, r, kOiMaxIter, oi_tol<T>(), basis,
+                                                                        status, g_ld, ks);
+    return ffdas_launch_check(h.stream);
+}
+
 constexpr size_t kGramPartialBytes = size_t(256) << 20;
 
 // Row groups of the four-column FP32 pass (0: it does not apply): unit
@@ -864,30 +1112,31 @@ int small4_groups<float>(const float *x, int64_t sp, int64_t sq, int64_t p, int6
 }
 
 template <int RMAX, typename T>
-ffdas_error_t launch_small4(ffdas_context &, const T *, int64_t, int64_t, int64_t, const T *, int, int, int, T *) {
+ffdas_error_t launch_small4(ffdas_context &, const T *, int64_t, int64_t, int64_t, const T *, int, int, int, T *,
+                            const int *) {
     return FFDAS_ERROR_INTERNAL;
 }
 template <int RMAX>
 ffdas_error_t launch_small4(ffdas_context &h, const float *x, int64_t sp, int64_t p, int64_t q, const float *U, int r,
-                            int groups, int subtract, float *out) {
+                            int groups, int subtract, float *out, const int *gate) {
     const int64_t blocks = (q / 4 + 31) / 32;
     if (blocks > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
     const size_t smem = (size_t)(((p * r + 3) & ~int64_t(3)) + (int64_t)groups * r * 32 * 4) * sizeof(float);
     tr_project_small4_kernel<RMAX><<<(unsigned)blocks, 32 * groups, smem, h.stream>>>(x, sp, p, q, U, r, subtract,
-                                                                                     out);
+                                                                                     out, gate);
     return ffdas_launch_check(h.stream);
 }
 
 template <typename T, int RMAX>
 ffdas_error_t launch_small(ffdas_context &h, const T *x, int64_t sp, int64_t sq, int64_t p, int64_t q, const T *U,
-                           int r, int groups, int subtract, T *out) {
+                           int r, int groups, int subtract, T *out, const int *gate) {
     if (const int g4 = small4_groups<T>(x, sp, sq, p, q, r, groups, out))
-        return launch_small4<RMAX>(h, x, sp, p, q, U, r, g4, subtract, out);
+        return launch_small4<RMAX>(h, x, sp, p, q, U, r, g4, subtract, out, gate);
     const int64_t blocks = (q + 31) / 32;
     if (blocks > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
     const size_t smem = (size_t)(p * r + (int64_t)groups * r * 32) * sizeof(T);
     tr_project_small_kernel<T, RMAX><<<(unsigned)blocks, 32 * groups, smem, h.stream>>>(x, sp, sq, p, q, U, r,
-                                                                                       subtract, out);
+                                                                                       subtract, out, gate);
     return ffdas_launch_check(h.stream);
 }
 
@@ -907,13 +1156,9 @@ bool gram_tc_usable<float>(const ffdas_context &h, const float *x, bool rows, in
 
 template <int NB>
 ffdas_error_t launch_gram_tc(ffdas_context &h, const CUtensorMap &map, const gram_tc::params &a, int64_t splits) {
-    static std::once_flag once;
-    static cudaError_t attr = cudaSuccess;
-    std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(gram_tc::gram_tc_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)gram_tc::smem_bytes<NB>());
-    });
-    if (attr != cudaSuccess) return FFDAS_ERROR_CUDA_RUNTIME;
+    if (ffdas_raise_smem_limit(reinterpret_cast<const void *>(gram_tc::gram_tc_kernel<NB>), h.device_id,
+                               gram_tc::smem_bytes<NB>()) != cudaSuccess)
+        return FFDAS_ERROR_CUDA_RUNTIME;
     gram_tc::gram_tc_kernel<NB><<<(unsigned)splits, gram_tc::kThreads, gram_tc::smem_bytes<NB>(), h.stream>>>(map, a);
     return ffdas_launch_check(h.stream);
 }
@@ -963,17 +1208,21 @@ ffdas_error_t launch_gemm(ffdas_context &h, const tr_gemm_args<T> &a, int splits
 
 // out = U (U^H A), or A - U (U^H A) when subtract: the one-pass kernel for
 // bases of up to 32 vectors, else two tiled products through a (r, q)
-// workspace.
+// workspace.  gate (one-pass kernel only): a device flag; the kernel writes
+// nothing unless it reads 1 (the subspace iteration's convergence status).
+template <typename T>
+bool project_takes_gate(int64_t p, int r) { return small_groups<T>(p, r) > 0; }
+
 template <typename T>
 ffdas_error_t project(ffdas_context &h, const T *x, int64_t sp, int64_t sq, int64_t p, int64_t q, const T *U, int r,
-                      int subtract, T *out) {
+                      int subtract, T *out, const int *gate = nullptr) {
     using real = typename tr_elem<T>::real;
     const int groups = small_groups<T>(p, r);
     if (groups > 0) {
-        if (r <= 4) FFDAS_TRY((launch_small<T, 4>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
-        else if (r <= 8) FFDAS_TRY((launch_small<T, 8>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
-        else if (r <= 16) FFDAS_TRY((launch_small<T, 16>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
-        else FFDAS_TRY((launch_small<T, 32>(h, x, sp, sq, p, q, U, r, groups, subtract, out)));
+        if (r <= 4) FFDAS_TRY((launch_small<T, 4>(h, x, sp, sq, p, q, U, r, groups, subtract, out, gate)));
+        else if (r <= 8) FFDAS_TRY((launch_small<T, 8>(h, x, sp, sq, p, q, U, r, groups, subtract, out, gate)));
+        else if (r <= 16) FFDAS_TRY((launch_small<T, 16>(h, x, sp, sq, p, q, U, r, groups, subtract, out, gate)));
+        else FFDAS_TRY((launch_small<T, 32>(h, x, sp, sq, p, q, U, r, groups, subtract, out, gate)));
     } else {
         workspace wbuf(h);
         FFDAS_TRY(wbuf.alloc((size_t)r * (size_t)q * sizeof(T)));
@@ -1080,36 +1329,23 @@ ffdas_error_t truncate_rank_t(ffdas_context &h, int64_t m, int64_t n, const T *x
     // orthogonal iteration first; the dense solver runs only if it does not
     // reach its residual bound
     const bool leading = direct ? start == 0 : stop == p;
-    if (leading && r <= kOiMaxRank && oi_smem_bytes<T>(p, r) <= kSmallBasisSmem) {
-        // G in shared memory too when it fits the device's opt-in limit
-        // (the dynamic limit is the device's opt-in size less the kernel's static shared memory)
-        static std::once_flag once;
-        static size_t dyn_max = 0;
-        std::call_once(once, [&] {
-            cudaFuncAttributes fa{};
-            if (cudaFuncGetAttributes(&fa, tr_leading_subspace_kernel<T>) == cudaSuccess &&
-                h.smem_optin > fa.sharedSizeBytes) {
-                const size_t want = h.smem_optin - fa.sharedSizeBytes;
-                if (cudaFuncSetAttribute(tr_leading_subspace_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)want) == cudaSuccess)
-                    dyn_max = want;
-            }
-            cudaGetLastError();
-        });
-        const size_t g_bytes = ((size_t)p * p * sizeof(T) + 15) / 16 * 16;
-        const int g_shared = oi_smem_bytes<T>(p, r) + g_bytes <= dyn_max ? 1 : 0;
-        const size_t oi_smem = oi_smem_bytes<T>(p, r) + (g_shared ? g_bytes : 0);
-        tr_leading_subspace_kernel<T><<<1, kOiThreads, oi_smem, h.stream>>>(
-            gram.get<T>(), (int)p, r, kOiMaxIter, oi_tol<T>(), basis.get<T>(), info.get<int>() + 1, g_shared);
-        FFDAS_TRY(ffdas_launch_check(h.stream));
+    if (leading && r <= kOiMaxRank && oi_smem_bytes<T>(p, r, 1) <= kSmallBasisSmem) {
+        if (r <= 4) FFDAS_TRY((launch_subspace<T, 4>(h, gram.get<T>(), p, r, basis.get<T>(), info.get<int>() + 1)));
+        else if (r <= 8) FFDAS_TRY((launch_subspace<T, 8>(h, gram.get<T>(), p, r, basis.get<T>(), info.get<int>() + 1)));
+        else FFDAS_TRY((launch_subspace<T, 16>(h, gram.get<T>(), p, r, basis.get<T>(), info.get<int>() + 1)));
         h.last.variant = kRouteSubspace;
         h.last.grid = gram_grid;
         h.last.kernels = 4;
+        // the one-pass projection is queued behind the iteration and reads
+        // its status on the device (no host round trip between them); the
+        // host reads the status once, at the end, for the fallback
+        const bool gated = project_takes_gate<T>(p, r);
+        if (gated) FFDAS_TRY(project(h, x, sp, sq, p, q, basis.get<T>(), r, direct ? 0 : 1, out, info.get<int>() + 1));
         int converged = 0;
         FFDAS_CUDA(cudaMemcpyAsync(&converged, info.get<int>() + 1, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
         FFDAS_CUDA(cudaStreamSynchronize(h.stream));
         if (converged == 1) {
-            FFDAS_TRY(project(h, x, sp, sq, p, q, basis.get<T>(), r, direct ? 0 : 1, out));
+            if (!gated) FFDAS_TRY(project(h, x, sp, sq, p, q, basis.get<T>(), r, direct ? 0 : 1, out));
             return FFDAS_SUCCESS;
         }
     }
