@@ -580,6 +580,8 @@ __device__ __forceinline__ double oi_shfl(double a, int o) { return __shfl_xor_s
 __device__ __forceinline__ double2 oi_shfl(double2 a, int o) {
     return make_double2(__shfl_xor_sync(0xffffffffu, a.x, o), __shfl_xor_sync(0xffffffffu, a.y, o));
 }
+__device__ __forceinline__ double oi_from(float a) { return a; }
+__device__ __forceinline__ double oi_from(double a) { return a; }
 __device__ __forceinline__ double2 oi_from(float2 a) { return make_double2(a.x, a.y); }
 __device__ __forceinline__ double2 oi_from(double2 a) { return a; }
 __device__ __forceinline__ void oi_to(float &o, double a) { o = (float)a; }
@@ -800,8 +802,6 @@ __device__ __forceinline__ void oi_copy_wait() { asm volatile("cp.async.wait_all
 // B[l%4][l/4] and D[l/4][2(l%4) + 0..1].  G column-major with leading
 // dimension ld; Q, Y row-major p x r.
 constexpr int kOiTasks = 4;
-__device__ __forceinline__ double oi_widen(float f) { return f; }
-__device__ __forceinline__ double oi_widen(double d) { return d; }
 template <typename T>
 __device__ void oi_gq_dmma(const T *G, int ld, const double *Q, double *Y, double *P, int p, int r, int parts) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -831,7 +831,7 @@ __device__ void oi_gq_dmma(const T *G, int ld, const double *Q, double *Y, doubl
 #pragma unroll
             for (int u = 0; u < kOiTasks; u++) {
                 const int k = k0[u] + 4 * s, i = row[u] + g, n = col[u] + g;
-                a[u] = on[u] && i < p && k < p ? oi_widen(G[i + (int64_t)k * ld]) : 0.0;
+                a[u] = on[u] && i < p && k < p ? oi_from(G[i + (int64_t)k * ld]) : 0.0;
                 b[u] = on[u] && n < r && k < p ? Q[k * r + n] : 0.0;
             }
 #pragma unroll

@@ -262,6 +262,49 @@ def test_iteration_falls_back_without_a_gap():
         assert np.abs(res - ref).max() / np.abs(x.cpu().numpy()).max() <= 1e-9
 
 
+def _start_basis(p, r):
+    # the subspace iteration's deterministic start values: entry (i, j) of
+    # the p x r start matrix is hash(2 (i r + j) + 1) in [-1, 1)
+    def h(k):
+        k &= 0xFFFFFFFF
+        k ^= k >> 16
+        k = (k * 0x7FEB352D) & 0xFFFFFFFF
+        k ^= k >> 15
+        k = (k * 0x846CA68B) & 0xFFFFFFFF
+        k ^= k >> 16
+        return k * (2.0 / 4294967296.0) - 1.0
+    return np.array([[h(2 * (i * r + j) + 1) for j in range(r)] for i in range(p)])
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_iteration_with_the_leading_vector_orthogonal_to_the_start(dtype):
+    # the dominant eigenvector v1 of G is orthogonal to the start basis, and
+    # span(v2..v6) is an invariant subspace the iteration reaches after one
+    # step.  It is not accepted: rounding leaves v1 a component of about eps
+    # in the basis, each step multiplies it by lambda_1 / lambda_6 (1024
+    # here), and the residual ||G Q - Q H|| carries it (times lambda_1) above
+    # the bound until the basis has turned to v1.  The call removes the 5
+    # leading ranks, v1 among them
+    rng = np.random.default_rng(17)
+    m, n, r = 64, 4096, 5
+    start = _start_basis(m, r)
+    q_start, _ = np.linalg.qr(start)
+    v = rng.standard_normal((m, r + 1))
+    v[:, 0] -= q_start @ (q_start.T @ v[:, 0])          # v1 orthogonal to the start span
+    v, _ = np.linalg.qr(v)
+    assert np.abs(q_start.T @ v[:, 0]).max() < 1e-12
+    w, _ = np.linalg.qr(rng.standard_normal((n, r + 1)))
+    sig = np.array([8.0, 4.0, 2.0, 1.0, 0.5, 0.25])
+    x_np = (v * sig) @ w.T         # rank 6: nothing but rounding ties v1 to the start basis
+    x = _cuda(x_np, dtype)
+    res = ffdas_b200.truncate_rank(x, r).cpu().numpy()
+    xs = x.cpu().numpy()
+    ref = tro.truncate_rank_f64(xs, r)
+    tol = 1e-9 if dtype == torch.float64 else 2e-5
+    assert np.abs(res - ref).max() / np.abs(xs).max() <= tol, _route()
+    assert _route() in (10, 11, 12), _route()
+
+
 # ------------------------------------------ tensor-core (tcgen05) Gram
 
 def _engine_call(engine, x, start, stop=None):
