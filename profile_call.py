@@ -14,7 +14,12 @@ weights).
     python profile_call.py rank_filter --calls 3
 
 runs truncate_rank(x, 5) on the seeded 200-frame 400x256 FP32 slow-time
-ensemble (workloads.slow_time_ensemble) instead.
+ensemble (workloads.slow_time_ensemble) instead, and
+
+    python profile_call.py sparse_select --calls 3
+
+runs sparse_select(w, 32, offsets=o) on 64 events x 400x256 pixels (a seeded
+0/1 beam mask plus 1e-3 jitter, as `bench.py` configs.sparse_select).
 """
 from __future__ import annotations
 
@@ -30,7 +35,7 @@ from ffdas_b200.library import get_library_handle
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=sorted(W.CONFIGS) + ["rank_filter"])
+    ap.add_argument("workload", choices=sorted(W.CONFIGS) + ["rank_filter", "sparse_select"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--frames", type=int, default=None, help="ensemble: number of frames")
     ap.add_argument("--calls", type=int, default=4)
@@ -45,6 +50,17 @@ def main() -> int:
             y = truncate_rank(x, 5)
         torch.cuda.synchronize()
         print(json.dumps({"rank_filter": list(x.shape), "max_abs_out": float(y.abs().max())}))
+        return 0
+    if args.workload == "sparse_select":
+        import ffdas_b200
+        g = torch.Generator().manual_seed(41)
+        shape = (64, 400, 256)
+        w = ((torch.rand(shape, generator=g) < 0.3).float() + torch.rand(shape, generator=g) * 1e-3).to(dev)
+        o = (torch.rand(shape, generator=g) * 1000).to(dev)
+        for _ in range(args.calls):
+            idx, _, _ = ffdas_b200.sparse_select(w, 32, offsets=o)
+        torch.cuda.synchronize()
+        print(json.dumps({"sparse_select": list(w.shape), "first_rank_events": int(idx[0].max())}))
         return 0
     kw = {"frames": args.frames} if args.frames is not None else {}
     wl = W.CONFIGS[args.workload](device=dev, scale=args.scale, **kw)

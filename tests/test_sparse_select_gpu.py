@@ -61,6 +61,25 @@ def test_ties_nan_and_binary_masks():
     np.testing.assert_array_equal(idx.cpu().numpy()[:, 1, 0], np.arange(8))   # all ties: lowest events
 
 
+@pytest.mark.parametrize("S,k", [(64, 32), (33, 32), (100, 32), (200, 7)])
+def test_signed_zeros_infinities_and_long_event_axes(S, k):
+    # -0 and +0 tie (lower event first), infinities and NaN in both signs,
+    # and event axes longer than 64 (the one-thread-per-voxel kernel)
+    g = torch.Generator().manual_seed(S + 31 * k)
+    w = torch.randn((S, 301), generator=g)
+    pick = torch.randint(0, 8, (S, 301), generator=g)
+    for code, val in enumerate([0.0, -0.0, float("inf"), -float("inf"), float("nan"), -float("nan"), 1.0]):
+        w = torch.where(pick == code, torch.full_like(w, val), w)
+    offs = torch.rand((S, 301), generator=g) * 100
+    idx, sw, so = ffdas_b200.sparse_select(w.to(DEV), k, offsets=offs.to(DEV))
+    exp = _expected(w.numpy(), k)
+    np.testing.assert_array_equal(idx.cpu().numpy(), exp)
+    got_w = sw.cpu().numpy()
+    exp_w = np.take_along_axis(w.numpy(), exp, axis=0)
+    np.testing.assert_array_equal(got_w.view(np.uint32), exp_w.view(np.uint32))   # the stored bits, -0 and NaN too
+    np.testing.assert_array_equal(so.cpu().numpy(), np.take_along_axis(offs.numpy(), exp, axis=0))
+
+
 def test_das_sparse_on_selected_lists_equals_masked_das():
     # bindings/python/examples/sparse_compounding.py:146-166: the two images agree
     g = torch.Generator().manual_seed(11)
