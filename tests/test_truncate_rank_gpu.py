@@ -262,6 +262,23 @@ def test_iteration_falls_back_without_a_gap():
         assert np.abs(res - ref).max() / np.abs(x.cpu().numpy()).max() <= 1e-9
 
 
+@pytest.mark.parametrize("dtype, cplx, tol, m, r",
+                         [d + (200, 5) for d in DTYPES] + [d + (240, 12) for d in DTYPES if not d[1]])
+def test_subspace_iteration_with_g_in_global_memory(dtype, cplx, tol, m, r):
+    # G too large for shared memory (200^2 x 8 bytes and up; 240^2 x 4 for
+    # FP32): the iteration reads G from global memory, on the tensor-core
+    # product for real data and the sliced one for complex; bases of up to 8
+    # and (real data; a complex 240 x 12 basis exceeds the iteration's 48 KB
+    # of shared memory and goes to the dense solver) of 9..16 vectors
+    x_np = tro.clutter_ensemble(m, 1600, rank=r, complex_=cplx, seed=m + r, decay=1.6)
+    x = _cuda(x_np, dtype)
+    res = ffdas_b200.truncate_rank(x, r).cpu().numpy()
+    assert _route() == 10, _route()
+    xs = x.cpu().numpy()
+    ref = tro.truncate_rank_f64(xs, r)
+    assert np.abs(res - ref).max() / np.abs(xs).max() <= tol
+
+
 def _start_basis(p, r):
     # the subspace iteration's deterministic start values: entry (i, j) of
     # the p x r start matrix is hash(2 (i r + j) + 1) in [-1, 1)
