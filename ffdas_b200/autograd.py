@@ -4,8 +4,10 @@ Forward calls ffdas_das / ffdas_das_sparse; backward calls ffdas_das_backward,
 which recomputes each interpolation tap (no stored indices) and returns the
 gradients with respect to channel data (two-tap adjoint scatter), weights,
 delays (through the interpolant's slope) and voxel / channel positions.
-Real channel data only (float32, float16, bfloat16), without directivity or
-phase rotation; the gradient of x is returned in x's dtype and layout.
+Real channel data only (float32, float16, bfloat16), without phase rotation;
+element directivity (srcdir) masks taps as in the forward, and the mask has
+no gradient (it is piecewise constant in the positions).  The gradient of x
+is returned in x's dtype and layout.
 """
 from __future__ import annotations
 
@@ -28,9 +30,8 @@ class DASFunction(torch.autograd.Function):
         handle = get_library_handle(xt.device)
         # The forward builds its interpolation-pair rows into a buffer kept for
         # the backward (ffdas_set_pair_buffer), which then skips building them
-        # again; only where the backward can run (real data, no directivity).
-        keep = (opts["srcdir"] is None and opts["wavenum"] == 0.0 and not xt.is_complex()
-                and xt.dtype in _FFDAS_DTYPE)
+        # again; only where the backward can run (real data, no phase rotation).
+        keep = opts["wavenum"] == 0.0 and not xt.is_complex() and xt.dtype in _FFDAS_DTYPE
         if keep:
             nbytes = _lib.pair_bytes(_x_desc(xt, opts["channels_trailing"]), _compute_type(xt, False, False))
             ctx.pairs = torch.empty(nbytes, dtype=torch.uint8, device=xt.device)
@@ -52,8 +53,8 @@ class DASFunction(torch.autograd.Function):
     def backward(ctx, gout):
         x, srcpos, dstpos, offsets, weights, idx = ctx.saved_tensors
         opts = ctx.opts
-        if opts["srcdir"] is not None or opts["wavenum"] != 0.0 or x.is_complex():
-            raise NotImplementedError("das backward supports real data without srcdir/wavenum")
+        if opts["wavenum"] != 0.0 or x.is_complex():
+            raise NotImplementedError("das backward supports real data without phase rotation (wavenum 0)")
         need = ctx.needs_input_grad
         dev = x.device
         gout = gout.contiguous().float()
@@ -79,6 +80,7 @@ class DASFunction(torch.autograd.Function):
         g_desc = _lib.TensorDesc(list(gout.shape), list(gout.stride()), DataType.R_32F)
         f32 = lambda t: _astype(t.detach(), torch.float32, dev, "input")  # noqa: E731
         srcpos_t, dstpos_t, offsets_t, weights_t = f32(srcpos), f32(dstpos), f32(offsets), f32(weights)
+        srcdir_t = f32(_to_torch(opts["srcdir"])) if opts["srcdir"] is not None else None
         idx_t = _astype(idx, torch.int32, dev, "sparse_indices") if ctx.has_sparse else None
         handle = get_library_handle(dev)
         handle.set_stream(torch.cuda.current_stream(dev).cuda_stream)
@@ -87,7 +89,7 @@ class DASFunction(torch.autograd.Function):
             handle.set_pair_buffer(ctx.pairs.data_ptr(), ctx.pairs.numel())
         try:
             _lib.check(_lib.load().ffdas_das_backward(
-                handle.h, ptr(srcpos_t), None, 0.0, x_desc.desc, ptr(xt), ptr(dstpos_t), ptr(offsets_t),
+                handle.h, ptr(srcpos_t), ptr(srcdir_t), 0.0, x_desc.desc, ptr(xt), ptr(dstpos_t), ptr(offsets_t),
                 ptr(weights_t), int(idx_t.shape[0]) if idx_t is not None else 0, ptr(idx_t), g_desc.desc,
                 ptr(gout), ptr(gx), ptr(goff), ptr(gw), ptr(gdst), ptr(gsrc)))
         finally:

@@ -31,6 +31,7 @@ struct bwd_params {
     int64_t V;
     int D0, D1, D2, T0, T1, T2, n0, n1;
     const float *srcpos, *dstpos, *offsets, *weights;
+    const float4 *srcdir;       // element directivity (C x 4), or null
     const int *sparse_idx;
     const float *gout;          // (B, V) with batch stride gout_bstride
     int64_t gout_bstride;
@@ -126,7 +127,10 @@ __global__ void __launch_bounds__(kBwdThreads) das_bwd_kernel(const bwd_params p
         for (int c = cbeg; c < cend; c++) {
             const float cx = __ldg(p.srcpos + 3 * c), cy = __ldg(p.srcpos + 3 * c + 1),
                         cz = __ldg(p.srcpos + 3 * c + 2);
-            const recv_geom gm = receive_geometry(vx, vy, vz, cx, cy, cz);
+            recv_geom gm = receive_geometry(vx, vy, vz, cx, cy, cz);
+            // outside the element's directivity cone the tap leaves the
+            // record, as in the forward: no contribution, no gradient
+            if (p.srcdir) apply_directivity(gm, vx, vy, vz, cx, cy, cz, __ldg(p.srcdir + c));
             const st *Pc = P + (int64_t)c * p.S * p.npad;
             float q = 0.f;      // sum_j w_j sum_b g_b d_b  (for the position gradients)
             uint32_t kk[SC];
@@ -487,7 +491,8 @@ __global__ void __launch_bounds__(kBwsThreads) das_bwd_sorted_kernel(const bwd_p
                 cx[u] = __ldg(p.srcpos + 3 * (c + u));
                 cy[u] = __ldg(p.srcpos + 3 * (c + u) + 1);
                 cz[u] = __ldg(p.srcpos + 3 * (c + u) + 2);
-                const recv_geom gm = receive_geometry(vp.x, vp.y, vp.z, cx[u], cy[u], cz[u]);
+                recv_geom gm = receive_geometry(vp.x, vp.y, vp.z, cx[u], cy[u], cz[u]);
+                if (p.srcdir) apply_directivity(gm, vp.x, vp.y, vp.z, cx[u], cy[u], cz[u], __ldg(p.srcdir + c + u));
                 ri[u] = gm.rinv;
                 ts[u] = split_tau(__fmaf_rn(gm.rsq, gm.rinv, ofs));
                 pr[u] = Pb[row + (uint32_t)(c + u) * cstride + min(ts[u].k, kmax)];
@@ -498,7 +503,8 @@ __global__ void __launch_bounds__(kBwsThreads) das_bwd_sorted_kernel(const bwd_p
         for (; c < cend; c++) {
             const float cx = __ldg(p.srcpos + 3 * c), cy = __ldg(p.srcpos + 3 * c + 1),
                         cz = __ldg(p.srcpos + 3 * c + 2);
-            const recv_geom gm = receive_geometry(vp.x, vp.y, vp.z, cx, cy, cz);
+            recv_geom gm = receive_geometry(vp.x, vp.y, vp.z, cx, cy, cz);
+            if (p.srcdir) apply_directivity(gm, vp.x, vp.y, vp.z, cx, cy, cz, __ldg(p.srcdir + c));
             const tau_split ts = split_tau(__fmaf_rn(gm.rsq, gm.rinv, ofs));
             channel(c, cx, cy, cz, gm.rinv, ts, Pb[row + (uint32_t)c * cstride + min(ts.k, kmax)]);
         }
@@ -565,7 +571,9 @@ void *reusable_pairs(const ffdas_context &h, const ffdas_tensor_desc &xd, const 
 ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tensor_desc &gd,
                            const void *gout, float *gx, float *goff, float *gw, float *gdst, float *gsrc) {
     const ffdas_tensor_desc &xd = *a.x_desc;
-    if (a.srcdir != nullptr || a.wavenum != 0.f) return FFDAS_ERROR_INVALID_ARGUMENT;
+    // real data without phase rotation; directivity (a mask per element and
+    // voxel) is applied as in the forward by the gather and sorted adjoints
+    if (a.wavenum != 0.f) return FFDAS_ERROR_INVALID_ARGUMENT;
     // the adjoint of a channel-scaled forward is not provided: clear the scale
     if (h.chan_scale) return FFDAS_ERROR_INVALID_ARGUMENT;
     if (gd.dtype != FFDAS_R_32F) return FFDAS_ERROR_UNSUPPORTED_TYPE;
@@ -618,6 +626,7 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
     bp.n1 = (pb.D1 + bp.T1 - 1) / bp.T1;
     const int n2 = (pb.D2 + bp.T2 - 1) / bp.T2;
     bp.srcpos = a.srcpos; bp.dstpos = a.dstpos; bp.offsets = a.offsets; bp.weights = a.weights;
+    bp.srcdir = reinterpret_cast<const float4 *>(a.srcdir);
     bp.sparse_idx = a.sparse ? a.sparse_indices : nullptr;
     bp.gout = static_cast<const float *>(gout);
     bp.gout_bstride = pb.out_bstride;
@@ -626,7 +635,7 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
     pb.sparse = a.sparse;
     // The backward kernel does not follow a forward schedule choice: only
     // variant 3 asks for the gather adjoint on dense problems.
-    if (!a.sparse && staged_supported(pb, kind) && !(h.has_config && h.config.variant == 3)) {
+    if (!a.sparse && !a.srcdir && staged_supported(pb, kind) && !(h.has_config && h.config.variant == 3)) {
         // Dense problems: TMA-staged adjoint, one CTA per voxel tile x batch item.
         if (h.has_config && h.config.variant == 2 && (h.config.tile_x || h.config.tile_y)) {
             const int tx = h.config.tile_x ? h.config.tile_x : 1, ty = h.config.tile_y ? h.config.tile_y : 1,

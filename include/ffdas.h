@@ -284,11 +284,14 @@ FFDAS_API ffdas_error_t ffdas_das_sparse(
  *   grad_weights : (S or n, V) FP32, overwritten
  *   grad_dstpos  : (V, 3) FP32, overwritten
  *   grad_srcpos  : (C, 3) FP32, overwritten
- * srcdir and wavenum must be NULL / 0 (no directivity, real data).
+ * wavenum must be 0 (real data, no phase rotation).  srcdir (element
+ * directivity) masks taps as in the forward; the mask has no gradient, and
+ * dense calls with it run the gather adjoint.
  * ffdas_get_last_kernel_info then reports variant 4 (TMA-staged adjoint,
- * dense calls), 3 (gather adjoint: dense calls under schedule variant 3, and
- * das_sparse under variant 3 or when the lists' tables do not fit) or 7
- * (das_sparse: a lane per list entry, entries bucketed by event). */
+ * dense calls), 3 (gather adjoint: dense calls under schedule variant 3 or
+ * with directivity, and das_sparse under variant 3 or when the lists' tables
+ * do not fit) or 7 (das_sparse: a lane per list entry, entries bucketed by
+ * event). */
 FFDAS_API ffdas_error_t ffdas_das_backward(
     ffdas_handle_t handle,
     const float *srcpos,

@@ -134,6 +134,67 @@ def test_sparse_gradients_uneven_lists(kernel, C, weights_grad):
         assert info["grid"] == (8 if C == 128 else 2), info
 
 
+def _directivity(src, dst, frac=0.4):
+    # elements facing +z with an acceptance threshold between two of the
+    # problem's (voxel, element) cosines, so that no pair sits on the cone's
+    # edge (there float32 and float64 could disagree on the mask)
+    d = dst.reshape(-1, 1, 3).double() - src.reshape(1, -1, 3).double()
+    cos = (d[..., 2] / d.norm(dim=-1)).flatten().sort().values
+    i = int(frac * cos.numel())
+    thr = float(0.5 * (cos[i] + cos[i + 1]))
+    assert float(cos[i + 1] - cos[i]) > 1e-6
+    sd = torch.zeros((src.shape[0], 4))
+    sd[:, 2] = 1.0
+    sd[:, 3] = thr
+    return sd
+
+
+@pytest.mark.parametrize("B", [1, 3])
+def test_directivity_gradients_match_float64_reference(B):
+    # element directivity masks taps as in the forward (the reference's
+    # dir_check, das_alg1_kernels.cuh:72-76); the gradients follow the kept
+    # taps (gather adjoint)
+    cpu = list(_problem(5, B=B))
+    sd = _directivity(cpu[1], cpu[2])
+    gpu = [t.to(DEV).requires_grad_(True) for t in cpu]
+    ref = [t.double().requires_grad_(True) for t in cpu]
+    g = torch.randn((B, *cpu[2].shape[:-1]), generator=torch.Generator().manual_seed(6))
+    out = das_autograd(*gpu, srcdir=sd.to(DEV))
+    out.backward(g.to(DEV))
+    out_ref = das_ref(*ref, srcdir=sd)
+    out_ref.backward(g.double())
+    masked = das_ref(*[t.detach().double() for t in cpu])
+    assert oracle.rel_l2(out_ref.detach().numpy(), masked.numpy()) > 1e-2     # the mask removes taps
+    assert oracle.rel_l2(out.detach().cpu().numpy(), out_ref.detach().numpy()) < 2e-5
+    for name, a, b in zip(["x", "srcpos", "dstpos", "offsets", "weights"], gpu, ref):
+        err = oracle.rel_l2(a.grad.cpu().numpy(), b.grad.numpy())
+        assert err < 2e-4, (name, err)
+
+
+def test_directivity_sparse_gradients_match_float64_reference():
+    # das_sparse with directivity: the sorted-list adjoint applies the mask
+    cpu = list(_problem(7, B=1, S=6))
+    sd = _directivity(cpu[1], cpu[2], 0.5)
+    g0 = torch.Generator().manual_seed(8)
+    k = 3
+    idx = torch.stack([torch.randperm(6, generator=g0)[:k] for _ in range(cpu[2][..., 0].numel())], -1)
+    idx = idx.reshape(k, *cpu[2].shape[:-1]).int()
+    offs = cpu[3][:k].clone()
+    w = cpu[4][:k].clone()
+    args = [cpu[0], cpu[1], cpu[2], offs, w]
+    gpu = [t.to(DEV).requires_grad_(True) for t in args]
+    ref = [t.double().requires_grad_(True) for t in args]
+    g = torch.randn((1, *cpu[2].shape[:-1]), generator=torch.Generator().manual_seed(9))
+    out = ffdas_b200.das_sparse(*gpu, idx.to(DEV), srcdir=sd.to(DEV))
+    out.backward(g.to(DEV))
+    out_ref = das_ref(*ref, sparse_indices=idx, srcdir=sd)
+    out_ref.backward(g.double())
+    assert oracle.rel_l2(out.detach().cpu().numpy(), out_ref.detach().numpy()) < 2e-5
+    for name, a, b in zip(["x", "srcpos", "dstpos", "offsets", "weights"], gpu, ref):
+        err = oracle.rel_l2(a.grad.cpu().numpy(), b.grad.numpy())
+        assert err < 2e-4, (name, err)
+
+
 def test_central_finite_differences_fp64():
     x, src, dst, offs, w = _problem(6, B=2)
     loss_ref = lambda o, ww: -(das_ref(x.double(), src.double(), dst.double(), o, ww) ** 4).sum()  # noqa: E731

@@ -4,14 +4,17 @@ Same formula as the reference kernel (src/das/das_alg1_kernels.cuh:48-106):
 tau = offsets[e,v] + sqrt(max(|dst[v]-src[c]|^2, 1e-7)), k = floor(tau),
 t = tau - k, valid iff 0 <= k < N-1, out += w * (x[k] + t (x[k+1] - x[k])).
 Gradients flow through t (not through the floor), exactly the derivative the
-backward kernels implement.  Real data, no directivity.  Small sizes only.
+backward kernels implement.  Real data; optional element directivity
+(srcdir rows (nx, ny, nz, cos_min): a tap counts only where
+(dst - src) . n / |dst - src| > cos_min, src/das/das_alg1_kernels.cuh:72-76),
+a mask without gradient.  Small sizes only.
 """
 from __future__ import annotations
 
 import torch
 
 
-def das_ref(x, srcpos, dstpos, offsets, weights, sparse_indices=None):
+def das_ref(x, srcpos, dstpos, offsets, weights, sparse_indices=None, srcdir=None):
     """x ([B,] C, S, N); returns ([B,] *spatial) float64."""
     have_batch = x.ndim == 4
     xb = x if have_batch else x[None]
@@ -30,6 +33,10 @@ def das_ref(x, srcpos, dstpos, offsets, weights, sparse_indices=None):
     kf = torch.floor(tau.detach())
     t = tau - kf
     valid = (kf >= 0) & (kf < N - 1)
+    if srcdir is not None:
+        sd = srcdir.reshape(C, 4).double().detach()
+        proj = (d.detach() * sd[None, :, :3]).sum(-1) / r.detach()     # (V, C)
+        valid = valid & (proj > sd[None, :, 3])[None]
     k = kf.clamp(0, max(N - 2, 0)).long()
     if sparse_indices is None:
         s = torch.arange(E)[:, None, None].expand(E, V, C)
