@@ -4,10 +4,11 @@ Forward calls ffdas_das / ffdas_das_sparse; backward calls ffdas_das_backward,
 which recomputes each interpolation tap (no stored indices) and returns the
 gradients with respect to channel data (two-tap adjoint scatter), weights,
 delays (through the interpolant's slope) and voxel / channel positions.
-Real channel data only (float32, float16, bfloat16), without phase rotation;
-element directivity (srcdir) masks taps as in the forward, and the mask has
-no gradient (it is piecewise constant in the positions).  The gradient of x
-is returned in x's dtype and layout.
+Real channel data (float32, float16, bfloat16) without phase rotation, and
+complex IQ data (complex64, complex32) with any wavenum; element directivity
+(srcdir) masks taps as in the forward, and the mask has no gradient (it is
+piecewise constant in the positions).  The gradient of x is returned in x's
+dtype and layout.
 """
 from __future__ import annotations
 
@@ -21,6 +22,12 @@ from .das import _FFDAS_DTYPE, _astype, _check_spatial, _compute_type, _run, _to
 from .library import get_library_handle
 
 
+def _backward_supported(x: torch.Tensor, wavenum: float) -> bool:
+    if x.is_complex():
+        return x.dtype in (torch.complex64, torch.complex32)
+    return wavenum == 0.0 and x.dtype in (torch.float32, torch.float16, torch.bfloat16, torch.int16)
+
+
 class DASFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, srcpos, dstpos, offsets, weights, sparse_indices, opts: dict):
@@ -30,8 +37,8 @@ class DASFunction(torch.autograd.Function):
         handle = get_library_handle(xt.device)
         # The forward builds its interpolation-pair rows into a buffer kept for
         # the backward (ffdas_set_pair_buffer), which then skips building them
-        # again; only where the backward can run (real data, no phase rotation).
-        keep = opts["wavenum"] == 0.0 and not xt.is_complex() and xt.dtype in _FFDAS_DTYPE
+        # again; only where the backward can run.
+        keep = _backward_supported(xt, opts["wavenum"])
         if keep:
             nbytes = _lib.pair_bytes(_x_desc(xt, opts["channels_trailing"]), _compute_type(xt, False, False))
             ctx.pairs = torch.empty(nbytes, dtype=torch.uint8, device=xt.device)
@@ -53,18 +60,20 @@ class DASFunction(torch.autograd.Function):
     def backward(ctx, gout):
         x, srcpos, dstpos, offsets, weights, idx = ctx.saved_tensors
         opts = ctx.opts
-        if opts["wavenum"] != 0.0 or x.is_complex():
-            raise NotImplementedError("das backward supports real data without phase rotation (wavenum 0)")
+        if not _backward_supported(x, opts["wavenum"]):
+            raise NotImplementedError("das backward supports real data without phase rotation (wavenum 0) "
+                                      "and complex64 / complex32 data")
         need = ctx.needs_input_grad
         dev = x.device
-        gout = gout.contiguous().float()
+        cplx = x.is_complex()
+        gout = gout.contiguous().to(torch.complex64 if cplx else torch.float32)
         xt = x.detach()
         lead = xt.shape if xt.ndim == 4 else (1, *xt.shape)
         if opts["channels_trailing"]:
             B, S, C, N = lead
         else:
             B, C, S, N = lead
-        gx = torch.zeros((B, C, S, N), dtype=torch.float32, device=dev) if need[0] else None
+        gx = torch.zeros((B, C, S, N), dtype=torch.complex64 if cplx else torch.float32, device=dev) if need[0] else None
         goff = torch.empty(offsets.shape, dtype=torch.float32, device=dev) if need[3] else None
         gw = torch.empty(weights.shape, dtype=torch.float32, device=dev) if need[4] else None
         gdst = torch.empty(dstpos.shape, dtype=torch.float32, device=dev) if need[2] else None
@@ -77,7 +86,7 @@ class DASFunction(torch.autograd.Function):
             dims[c], dims[c + 1] = dims[c + 1], dims[c]
             strides[c], strides[c + 1] = strides[c + 1], strides[c]
         x_desc = _lib.TensorDesc(dims, strides, _FFDAS_DTYPE[xt.dtype])
-        g_desc = _lib.TensorDesc(list(gout.shape), list(gout.stride()), DataType.R_32F)
+        g_desc = _lib.TensorDesc(list(gout.shape), list(gout.stride()), DataType.C_32F if cplx else DataType.R_32F)
         f32 = lambda t: _astype(t.detach(), torch.float32, dev, "input")  # noqa: E731
         srcpos_t, dstpos_t, offsets_t, weights_t = f32(srcpos), f32(dstpos), f32(offsets), f32(weights)
         srcdir_t = f32(_to_torch(opts["srcdir"])) if opts["srcdir"] is not None else None
@@ -89,7 +98,8 @@ class DASFunction(torch.autograd.Function):
             handle.set_pair_buffer(ctx.pairs.data_ptr(), ctx.pairs.numel())
         try:
             _lib.check(_lib.load().ffdas_das_backward(
-                handle.h, ptr(srcpos_t), ptr(srcdir_t), 0.0, x_desc.desc, ptr(xt), ptr(dstpos_t), ptr(offsets_t),
+                handle.h, ptr(srcpos_t), ptr(srcdir_t), float(opts["wavenum"]), x_desc.desc, ptr(xt), ptr(dstpos_t),
+                ptr(offsets_t),
                 ptr(weights_t), int(idx_t.shape[0]) if idx_t is not None else 0, ptr(idx_t), g_desc.desc,
                 ptr(gout), ptr(gx), ptr(goff), ptr(gw), ptr(gdst), ptr(gsrc)))
         finally:

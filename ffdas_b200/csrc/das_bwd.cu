@@ -294,6 +294,136 @@ static ffdas_error_t launch_bwd_k(ffdas_context &h, const bwd_params &bp, int BT
     }
 }
 
+// ------------------------------------------------ complex (IQ) adjoint ---
+// The forward adds, per tap, A v with A = w (cos, sin)(wavenum tau) (the
+// reference's weight, src/das/das_alg1_kernels.cuh:79-86) and v = x_k + t
+// (x_{k+1} - x_k).  With g the output gradient (d loss / d Re + i d loss /
+// d Im, the convention of complex autograd): x_k gets (1 - t) conj(A) g and
+// x_{k+1} gets t conj(A) g; the weight Re(conj(g) (cos, sin) v); the delay
+// Re(conj(g) A (i wavenum v + d)), d = x_{k+1} - x_k, which the positions
+// take through d tau / d v = (v - c) / r.  A thread per voxel walks its
+// events and channels (as the forward gather does); the channel-data
+// gradient goes to global memory with float atomics (real and imaginary
+// parts), the channel positions take a warp sum per channel.
+template <int K>
+__device__ __forceinline__ float2 pair_slope_c(const typename pair_traits<K>::storage &pr);
+template <> __device__ __forceinline__ float2 pair_slope_c<ST_C32>(const float4 &pr) {
+    return make_float2(pr.z, pr.w);
+}
+template <> __device__ __forceinline__ float2 pair_slope_c<ST_C16>(const uint2 &pr) {
+    uint2 q = pr;
+    const float2 a = __half22float2(*reinterpret_cast<__half2 *>(&q.x));
+    const float2 b = __half22float2(*reinterpret_cast<__half2 *>(&q.y));
+    return make_float2(b.x - a.x, b.y - a.y);
+}
+
+template <int K, bool SPARSE>
+__global__ void __launch_bounds__(kBwdThreads) das_bwd_complex_kernel(const bwd_params p, float wavenum) {
+    using tr = pair_traits<K>;
+    using st = typename tr::storage;
+    const int lane = threadIdx.x & 31;
+    const int64_t v = (int64_t)blockIdx.x * kBwdThreads + threadIdx.x;
+    const bool active = v < p.V;
+    const float2 *gout = reinterpret_cast<const float2 *>(p.gout);
+    float2 *gx = reinterpret_cast<float2 *>(p.gx);
+    float vx = 0.f, vy = 0.f, vz = 0.f;
+    if (active) {
+        vx = __ldg(p.dstpos + 3 * v); vy = __ldg(p.dstpos + 3 * v + 1); vz = __ldg(p.dstpos + 3 * v + 2);
+    }
+    const st *__restrict__ P = static_cast<const st *>(p.P);
+    const uint32_t kmax_pair = (uint32_t)(p.npad - 1);
+    const int64_t row_b = (int64_t)p.C * p.S * p.npad;
+    float gpx = 0.f, gpy = 0.f, gpz = 0.f;
+    for (int e = 0; e < p.n_events; e++) {
+        float ofs = 1e30f, w = 0.f;
+        int s = 0;
+        if (active) {
+            const int64_t idx = (int64_t)e * p.V + v;
+            ofs = __ldg(p.offsets + idx);
+            w = __ldg(p.weights + idx);
+            s = e;
+            if constexpr (SPARSE) {
+                s = __ldg(p.sparse_idx + idx);
+                if ((unsigned)s >= (unsigned)p.S) { s = 0; w = 0.f; ofs = 1e30f; }
+            }
+        }
+        float gwa = 0.f, goa = 0.f;
+        for (int c = 0; c < p.C; c++) {
+            const float cx = __ldg(p.srcpos + 3 * c), cy = __ldg(p.srcpos + 3 * c + 1),
+                        cz = __ldg(p.srcpos + 3 * c + 2);
+            recv_geom gm = receive_geometry(vx, vy, vz, cx, cy, cz);
+            if (p.srcdir) apply_directivity(gm, vx, vy, vz, cx, cy, cz, __ldg(p.srcdir + c));
+            const float tau = __fmaf_rn(gm.rsq, gm.rinv, ofs);
+            const tau_split ts = split_tau(tau);
+            float sn, cs;
+            __sincosf(wavenum * tau, &sn, &cs);
+            const float2 A = make_float2(cs * w, sn * w);
+            const st *row = P + ((int64_t)c * p.S + s) * p.npad + min(ts.k, kmax_pair);
+            const bool in_record = active && ts.k < (uint32_t)(p.N - 1);
+            float q = 0.f;
+            for (int b = 0; b < p.B; b++) {
+                const float2 g = active ? gout[(int64_t)b * p.gout_bstride + v] : make_float2(0.f, 0.f);
+                const st pr = row[(int64_t)b * row_b];
+                const float2 val = tr::tap(pr, ts.t);
+                const float2 d = pair_slope_c<K>(pr);
+                // Re(conj(g) (cos, sin) val)
+                const float2 pv = make_float2(cs * val.x - sn * val.y, cs * val.y + sn * val.x);
+                gwa += g.x * pv.x + g.y * pv.y;
+                // Re(conj(g) A (i wavenum val + d))
+                const float2 z = make_float2(d.x - wavenum * val.y, d.y + wavenum * val.x);
+                const float2 Az = make_float2(A.x * z.x - A.y * z.y, A.x * z.y + A.y * z.x);
+                q += g.x * Az.x + g.y * Az.y;
+                if (gx && in_record && w != 0.f) {
+                    // conj(A) g, split over the two samples
+                    const float2 cg = make_float2(A.x * g.x + A.y * g.y, A.x * g.y - A.y * g.x);
+                    float2 *gr = gx + ((int64_t)b * p.C + c) * (int64_t)p.S * p.N + (int64_t)s * p.N + ts.k;
+                    atomicAdd(&gr->x, cg.x - cg.x * ts.t);
+                    atomicAdd(&gr->y, cg.y - cg.y * ts.t);
+                    atomicAdd(&(gr + 1)->x, cg.x * ts.t);
+                    atomicAdd(&(gr + 1)->y, cg.y * ts.t);
+                }
+            }
+            goa += q;
+            const float qr = q * gm.rinv;
+            const float ex = (vx - cx) * qr, ey = (vy - cy) * qr, ez = (vz - cz) * qr;
+            gpx += ex; gpy += ey; gpz += ez;
+            if (p.gsrc) {
+                float sx = -ex, sy = -ey, sz = -ez;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    sx += __shfl_xor_sync(0xffffffffu, sx, o);
+                    sy += __shfl_xor_sync(0xffffffffu, sy, o);
+                    sz += __shfl_xor_sync(0xffffffffu, sz, o);
+                }
+                if (lane == 0 && (sx != 0.f || sy != 0.f || sz != 0.f)) {
+                    atomicAdd(p.gsrc + 3 * c, sx);
+                    atomicAdd(p.gsrc + 3 * c + 1, sy);
+                    atomicAdd(p.gsrc + 3 * c + 2, sz);
+                }
+            }
+        }
+        if (active) {
+            const int64_t idx = (int64_t)e * p.V + v;
+            if (p.gw) p.gw[idx] = gwa;
+            if (p.goff) p.goff[idx] = goa;
+        }
+    }
+    if (active && p.gdst) {
+        p.gdst[3 * v] = gpx; p.gdst[3 * v + 1] = gpy; p.gdst[3 * v + 2] = gpz;
+    }
+}
+
+template <int K>
+static ffdas_error_t launch_bwd_complex(ffdas_context &h, const bwd_params &bp, bool sparse, float wavenum) {
+    const int64_t blocks = (bp.V + kBwdThreads - 1) / kBwdThreads;
+    if (blocks > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
+    if (sparse)
+        das_bwd_complex_kernel<K, true><<<(unsigned)blocks, kBwdThreads, 0, h.stream>>>(bp, wavenum);
+    else
+        das_bwd_complex_kernel<K, false><<<(unsigned)blocks, kBwdThreads, 0, h.stream>>>(bp, wavenum);
+    return ffdas_launch_check(h.stream);
+}
+
 // ---------------------------------------- das_sparse adjoint, sorted lists ---
 // The gather adjoint above gives each lane a voxel and walks its list, so at
 // a list slot the lanes of a warp name different events and the two-tap
@@ -571,14 +701,17 @@ void *reusable_pairs(const ffdas_context &h, const ffdas_tensor_desc &xd, const 
 ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tensor_desc &gd,
                            const void *gout, float *gx, float *goff, float *gw, float *gdst, float *gsrc) {
     const ffdas_tensor_desc &xd = *a.x_desc;
-    // real data without phase rotation; directivity (a mask per element and
-    // voxel) is applied as in the forward by the gather and sorted adjoints
-    if (a.wavenum != 0.f) return FFDAS_ERROR_INVALID_ARGUMENT;
+    // real data without phase rotation, or complex data (complex64 or
+    // complex32 pairs) with any wavenum and a complex64 output gradient;
+    // directivity (a mask per element and voxel) is applied as in the forward
     // the adjoint of a channel-scaled forward is not provided: clear the scale
     if (h.chan_scale) return FFDAS_ERROR_INVALID_ARGUMENT;
-    if (gd.dtype != FFDAS_R_32F) return FFDAS_ERROR_UNSUPPORTED_TYPE;
-    const int kind = select_storage(xd.dtype, FFDAS_R_32F, a.compute_type, xd.ndim == 4 ? (int)xd.dims[0] : 1);
-    if (kind != ST_F32 && kind != ST_F16 && kind != ST_BF16) return FFDAS_ERROR_UNSUPPORTED_TYPE;
+    const bool cplx = xd.dtype == FFDAS_C_32F || xd.dtype == FFDAS_C_16F;
+    if (gd.dtype != (cplx ? FFDAS_C_32F : FFDAS_R_32F)) return FFDAS_ERROR_UNSUPPORTED_TYPE;
+    if (!cplx && a.wavenum != 0.f) return FFDAS_ERROR_INVALID_ARGUMENT;
+    const int kind = select_storage(xd.dtype, gd.dtype, a.compute_type, xd.ndim == 4 ? (int)xd.dims[0] : 1);
+    if (cplx ? (kind != ST_C32 && kind != ST_C16) : (kind != ST_F32 && kind != ST_F16 && kind != ST_BF16))
+        return FFDAS_ERROR_UNSUPPORTED_TYPE;
     if (!fits_int32_indexing(xd) || !fits_int32_indexing(gd)) return FFDAS_ERROR_INVALID_DIMS;
     das_problem pb;
     FFDAS_TRY(make_problem(xd, gd, pb));
@@ -596,7 +729,7 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
 
     const int64_t npad = pair_row_length(pb.N);
     const int64_t rows = (int64_t)pb.B * pb.C * pb.S;
-    const size_t sb = (kind == ST_F32) ? 8 : 4;
+    const size_t sb = kind == ST_C32 ? 16 : (kind == ST_F32 || kind == ST_C16) ? 8 : 4;
     // the pair rows of the forward call on this x when it left them in the
     // handle's pair buffer, else built again
     workspace P(h);
@@ -633,6 +766,19 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
     bp.gx = gx; bp.goff = goff; bp.gw = gw; bp.gdst = gdst; bp.gsrc = gsrc;
 
     pb.sparse = a.sparse;
+    if (cplx) {   // complex data: the gather-form complex adjoint, one thread per voxel
+        if (gsrc) FFDAS_CUDA(cudaMemsetAsync(gsrc, 0, (size_t)pb.C * 3 * sizeof(float), h.stream));
+        h.last = ffdas_kernel_info_t{};
+        h.last.variant = 8;
+        h.last.storage = kind;
+        h.last.kernels = h.last_pairs_reused ? 1 : 2;   // (ingest,) adjoint
+        h.last.grid = (pb.V + kBwdThreads - 1) / kBwdThreads;
+        h.mark_start();
+        const ffdas_error_t err = kind == ST_C32 ? launch_bwd_complex<ST_C32>(h, bp, a.sparse, a.wavenum)
+                                                 : launch_bwd_complex<ST_C16>(h, bp, a.sparse, a.wavenum);
+        h.mark_stop();
+        return err;
+    }
     // The backward kernel does not follow a forward schedule choice: only
     // variant 3 asks for the gather adjoint on dense problems.
     if (!a.sparse && !a.srcdir && staged_supported(pb, kind) && !(h.has_config && h.config.variant == 3)) {

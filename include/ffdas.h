@@ -277,21 +277,27 @@ FFDAS_API ffdas_error_t ffdas_das_sparse(
 );
 
 /* New: adjoint of ffdas_das (sparse_indices == NULL) or ffdas_das_sparse.
- * Real FP32/FP16/BF16 channel data with FP32 output only.  grad_out has the
- * layout of `out`.  Each grad pointer may be NULL (not computed).  Shapes:
- *   grad_x       : x_desc layout, FP32, accumulated (+=) so the caller zeroes it
+ * Real FP32/FP16/BF16 channel data with an FP32 output, or complex64 /
+ * complex32 channel data with a complex64 output (any wavenum).  grad_out
+ * has the layout and type of `out`.  Each grad pointer may be NULL (not
+ * computed).  Shapes:
+ *   grad_x       : x_desc layout, FP32 (complex data: interleaved complex64),
+ *                  accumulated (+=) so the caller zeroes it
  *   grad_offsets : (S or n, V) FP32, overwritten
  *   grad_weights : (S or n, V) FP32, overwritten
  *   grad_dstpos  : (V, 3) FP32, overwritten
  *   grad_srcpos  : (C, 3) FP32, overwritten
- * wavenum must be 0 (real data, no phase rotation).  srcdir (element
+ * Real data needs wavenum 0.  Complex data: x_k gets (1 - t) conj(A) g and
+ * x_{k+1} gets t conj(A) g for the tap weight A = w (cos, sin)(wavenum tau),
+ * g = d loss / d Re(out) + i d loss / d Im(out); the real inputs get the
+ * real part of conj(g) times their derivative of out.  srcdir (element
  * directivity) masks taps as in the forward; the mask has no gradient, and
  * dense calls with it run the gather adjoint.
  * ffdas_get_last_kernel_info then reports variant 4 (TMA-staged adjoint,
  * dense calls), 3 (gather adjoint: dense calls under schedule variant 3 or
  * with directivity, and das_sparse under variant 3 or when the lists' tables
- * do not fit) or 7 (das_sparse: a lane per list entry, entries bucketed by
- * event). */
+ * do not fit), 7 (das_sparse: a lane per list entry, entries bucketed by
+ * event) or 8 (complex data: a thread per voxel). */
 FFDAS_API ffdas_error_t ffdas_das_backward(
     ffdas_handle_t handle,
     const float *srcpos,

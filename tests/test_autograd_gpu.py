@@ -195,6 +195,46 @@ def test_directivity_sparse_gradients_match_float64_reference():
         assert err < 2e-4, (name, err)
 
 
+@pytest.mark.parametrize("sparse, B, wavenum", [(False, 1, 0.0), (False, 2, 0.07), (True, 1, 0.05)])
+def test_complex_gradients_match_float64_reference(sparse, B, wavenum):
+    # complex IQ data with the phase rotation: the gradients of x (conj(A) g
+    # split over the two taps), weights, delays (through the phase and the
+    # slope) and both position sets against complex autograd of the float64
+    # statement; with directivity in the last case
+    cpu = list(_problem(11, B=B, S=4))
+    g0 = torch.Generator().manual_seed(12)
+    cpu[0] = torch.complex(cpu[0], torch.randn(cpu[0].shape, generator=g0))
+    idx = None
+    if sparse:
+        k = 3
+        V = cpu[2][..., 0].numel()
+        idx = torch.stack([torch.randperm(4, generator=g0)[:k] for _ in range(V)], -1)
+        idx = idx.reshape(k, *cpu[2].shape[:-1]).int()
+        cpu[3], cpu[4] = cpu[3][:k].clone(), cpu[4][:k].clone()
+    sd = _directivity(cpu[1], cpu[2], 0.3) if sparse else None
+    gpu = [t.to(DEV).requires_grad_(True) for t in cpu]
+    ref = [(t.to(torch.complex128) if t.is_complex() else t.double()).requires_grad_(True) for t in cpu]
+    g = torch.complex(torch.randn((B, *cpu[2].shape[:-1]), generator=g0),
+                      torch.randn((B, *cpu[2].shape[:-1]), generator=g0))
+    out = das_autograd(*gpu, idx.to(DEV) if sparse else None, srcdir=None if sd is None else sd.to(DEV),
+                       wavenum=wavenum)
+    out.backward(g.to(DEV))
+    out_ref = das_ref(*ref, sparse_indices=idx, srcdir=sd, wavenum=wavenum)
+    out_ref.backward(g.to(torch.complex128))
+    assert oracle.rel_l2(out.detach().cpu().numpy(), out_ref.detach().numpy()) < 2e-5
+    for name, a, b in zip(["x", "srcpos", "dstpos", "offsets", "weights"], gpu, ref):
+        err = oracle.rel_l2(a.grad.cpu().numpy(), b.grad.numpy())
+        assert err < 2e-4, (name, err)
+
+
+def test_complex128_has_no_backward():
+    cpu = list(_problem(13, B=1))
+    x = torch.complex(cpu[0], cpu[0]).to(torch.complex128).to(DEV).requires_grad_(True)
+    out = das_autograd(x, *[t.to(DEV) for t in cpu[1:]])
+    with pytest.raises(NotImplementedError):
+        out.abs().sum().backward()
+
+
 def test_central_finite_differences_fp64():
     x, src, dst, offs, w = _problem(6, B=2)
     loss_ref = lambda o, ww: -(das_ref(x.double(), src.double(), dst.double(), o, ww) ** 4).sum()  # noqa: E731

@@ -4,7 +4,9 @@ Same formula as the reference kernel (src/das/das_alg1_kernels.cuh:48-106):
 tau = offsets[e,v] + sqrt(max(|dst[v]-src[c]|^2, 1e-7)), k = floor(tau),
 t = tau - k, valid iff 0 <= k < N-1, out += w * (x[k] + t (x[k+1] - x[k])).
 Gradients flow through t (not through the floor), exactly the derivative the
-backward kernels implement.  Real data; optional element directivity
+backward kernels implement.  Real data, or complex data with the phase
+rotation out += w exp(i wavenum tau) L (src/das/das_alg1_kernels.cuh:79-86);
+optional element directivity
 (srcdir rows (nx, ny, nz, cos_min): a tap counts only where
 (dst - src) . n / |dst - src| > cos_min, src/das/das_alg1_kernels.cuh:72-76),
 a mask without gradient.  Small sizes only.
@@ -14,8 +16,8 @@ from __future__ import annotations
 import torch
 
 
-def das_ref(x, srcpos, dstpos, offsets, weights, sparse_indices=None, srcdir=None):
-    """x ([B,] C, S, N); returns ([B,] *spatial) float64."""
+def das_ref(x, srcpos, dstpos, offsets, weights, sparse_indices=None, srcdir=None, wavenum=0.0):
+    """x ([B,] C, S, N); returns ([B,] *spatial) float64 (complex128 for complex x)."""
     have_batch = x.ndim == 4
     xb = x if have_batch else x[None]
     B, C, S, N = xb.shape
@@ -45,12 +47,16 @@ def das_ref(x, srcpos, dstpos, offsets, weights, sparse_indices=None, srcdir=Non
         valid = valid & (s >= 0) & (s < S)
         s = s.clamp(0, S - 1)
     c = torch.arange(C)[None, None, :].expand(E, V, C)
-    xd = xb.double()
+    cplx = xb.is_complex()
+    xd = xb.to(torch.complex128) if cplx else xb.double()
+    phase = torch.exp(1j * float(wavenum) * tau) if cplx else None
     outs = []
     for b in range(B):
         x0 = xd[b][c, s, k]
         x1 = xd[b][c, s, (k + 1).clamp(max=N - 1)]
         L = x0 + t * (x1 - x0)
+        if cplx:
+            L = L * phase
         L = torch.where(valid, L, torch.zeros_like(L))
         outs.append((w[:, :, None] * L).sum(dim=(0, 2)))
     out = torch.stack(outs).reshape(B, *spatial)
