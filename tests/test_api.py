@@ -156,3 +156,18 @@ def test_truncate_rank_out_shape_rejected():
 def test_truncate_rank_needs_cuda():
     with pytest.raises(ValueError, match="CUDA"):
         ffdas_b200.truncate_rank(torch.ones((4, 8)), 0)
+
+
+def test_backward_coverage_by_dtype():
+    # the adjoint kernels take real data without phase rotation and complex64
+    # / complex32 data with any wavenum; everything else raises
+    # NotImplementedError in the autograd backward (and keeps no pair rows)
+    from ffdas_b200.autograd import _backward_supported
+    for dt in (torch.float32, torch.float16, torch.bfloat16):
+        assert _backward_supported(torch.zeros(1, dtype=dt), 0.0)
+        assert not _backward_supported(torch.zeros(1, dtype=dt), 0.1)
+    assert not _backward_supported(torch.zeros(1, dtype=torch.float64), 0.0)
+    for dt in (torch.complex64, torch.complex32):
+        assert _backward_supported(torch.zeros(1, dtype=dt), 0.0)
+        assert _backward_supported(torch.zeros(1, dtype=dt), 0.3)
+    assert not _backward_supported(torch.zeros(1, dtype=torch.complex128), 0.0)
