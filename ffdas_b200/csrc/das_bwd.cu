@@ -302,9 +302,11 @@ static ffdas_error_t launch_bwd_k(ffdas_context &h, const bwd_params &bp, int BT
 // x_{k+1} gets t conj(A) g; the weight Re(conj(g) (cos, sin) v); the delay
 // Re(conj(g) A (i wavenum v + d)), d = x_{k+1} - x_k, which the positions
 // take through d tau / d v = (v - c) / r.  A thread per voxel walks its
-// events and channels (as the forward gather does); the channel-data
-// gradient goes to global memory with float atomics (real and imaginary
-// parts), the channel positions take a warp sum per channel.
+// events and the channels of its slice (blockIdx.y; slices add the
+// voxel-side gradients with atomics into zeroed outputs), as the forward
+// gather does; the channel-data gradient goes to global memory with one
+// float2 atomic per sample, the channel positions take a warp sum per
+// channel.
 template <int K>
 __device__ __forceinline__ float2 pair_slope_c(const typename pair_traits<K>::storage &pr);
 template <> __device__ __forceinline__ float2 pair_slope_c<ST_C32>(const float4 &pr) {
@@ -334,6 +336,9 @@ __global__ void __launch_bounds__(kBwdThreads) das_bwd_complex_kernel(const bwd_
     const uint32_t kmax_pair = (uint32_t)(p.npad - 1);
     const int64_t row_b = (int64_t)p.C * p.S * p.npad;
     float gpx = 0.f, gpy = 0.f, gpz = 0.f;
+    const bool multi = gridDim.y > 1;
+    const int cbeg = p.cchunk ? (int)blockIdx.y * p.cchunk : 0;
+    const int cend = p.cchunk ? min(p.C, cbeg + p.cchunk) : p.C;
     for (int e = 0; e < p.n_events; e++) {
         float ofs = 1e30f, w = 0.f;
         int s = 0;
@@ -348,7 +353,7 @@ __global__ void __launch_bounds__(kBwdThreads) das_bwd_complex_kernel(const bwd_
             }
         }
         float gwa = 0.f, goa = 0.f;
-        for (int c = 0; c < p.C; c++) {
+        for (int c = cbeg; c < cend; c++) {
             const float cx = __ldg(p.srcpos + 3 * c), cy = __ldg(p.srcpos + 3 * c + 1),
                         cz = __ldg(p.srcpos + 3 * c + 2);
             recv_geom gm = receive_geometry(vx, vy, vz, cx, cy, cz);
@@ -377,10 +382,10 @@ __global__ void __launch_bounds__(kBwdThreads) das_bwd_complex_kernel(const bwd_
                     // conj(A) g, split over the two samples
                     const float2 cg = make_float2(A.x * g.x + A.y * g.y, A.x * g.y - A.y * g.x);
                     float2 *gr = gx + ((int64_t)b * p.C + c) * (int64_t)p.S * p.N + (int64_t)s * p.N + ts.k;
-                    atomicAdd(&gr->x, cg.x - cg.x * ts.t);
-                    atomicAdd(&gr->y, cg.y - cg.y * ts.t);
-                    atomicAdd(&(gr + 1)->x, cg.x * ts.t);
-                    atomicAdd(&(gr + 1)->y, cg.y * ts.t);
+                    // one 8-byte vector atomic per sample (global memory,
+                    // compute capability 9.0 and up)
+                    atomicAdd(gr, make_float2(cg.x - cg.x * ts.t, cg.y - cg.y * ts.t));
+                    atomicAdd(gr + 1, make_float2(cg.x * ts.t, cg.y * ts.t));
                 }
             }
             goa += q;
@@ -404,23 +409,32 @@ __global__ void __launch_bounds__(kBwdThreads) das_bwd_complex_kernel(const bwd_
         }
         if (active) {
             const int64_t idx = (int64_t)e * p.V + v;
-            if (p.gw) p.gw[idx] = gwa;
-            if (p.goff) p.goff[idx] = goa;
+            if (multi) {
+                if (p.gw) atomicAdd(p.gw + idx, gwa);
+                if (p.goff) atomicAdd(p.goff + idx, goa);
+            } else {
+                if (p.gw) p.gw[idx] = gwa;
+                if (p.goff) p.goff[idx] = goa;
+            }
         }
     }
     if (active && p.gdst) {
-        p.gdst[3 * v] = gpx; p.gdst[3 * v + 1] = gpy; p.gdst[3 * v + 2] = gpz;
+        if (multi) {
+            atomicAdd(p.gdst + 3 * v, gpx); atomicAdd(p.gdst + 3 * v + 1, gpy); atomicAdd(p.gdst + 3 * v + 2, gpz);
+        } else {
+            p.gdst[3 * v] = gpx; p.gdst[3 * v + 1] = gpy; p.gdst[3 * v + 2] = gpz;
+        }
     }
 }
 
 template <int K>
-static ffdas_error_t launch_bwd_complex(ffdas_context &h, const bwd_params &bp, bool sparse, float wavenum) {
-    const int64_t blocks = (bp.V + kBwdThreads - 1) / kBwdThreads;
-    if (blocks > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
+static ffdas_error_t launch_bwd_complex(ffdas_context &h, const bwd_params &bp, bool sparse, float wavenum,
+                                       int64_t blocks, int slices) {
+    const dim3 grid((unsigned)blocks, (unsigned)slices);
     if (sparse)
-        das_bwd_complex_kernel<K, true><<<(unsigned)blocks, kBwdThreads, 0, h.stream>>>(bp, wavenum);
+        das_bwd_complex_kernel<K, true><<<grid, kBwdThreads, 0, h.stream>>>(bp, wavenum);
     else
-        das_bwd_complex_kernel<K, false><<<(unsigned)blocks, kBwdThreads, 0, h.stream>>>(bp, wavenum);
+        das_bwd_complex_kernel<K, false><<<grid, kBwdThreads, 0, h.stream>>>(bp, wavenum);
     return ffdas_launch_check(h.stream);
 }
 
@@ -767,15 +781,35 @@ ffdas_error_t das_backward(ffdas_context &h, const das_call &a, const ffdas_tens
 
     pb.sparse = a.sparse;
     if (cplx) {   // complex data: the gather-form complex adjoint, one thread per voxel
+        const int64_t blocks = (pb.V + kBwdThreads - 1) / kBwdThreads;
+        if (blocks > INT32_MAX) return FFDAS_ERROR_DIMS_TOO_LARGE;
+        // channel slices (8+ channels each) until about 8 CTAs per SM
+        int slices = 1;
+        while (blocks * slices * 2 <= (int64_t)std::max(h.sm_count, 1) * 8 && pb.C >= 16 * slices && slices < 64)
+            slices *= 2;
+        bwd_params cp = bp;
+        cp.cchunk = 0;
+        if (slices > 1) {
+            const int chunk = (pb.C + slices - 1) / slices;
+            slices = (pb.C + chunk - 1) / chunk;
+            cp.cchunk = slices > 1 ? chunk : 0;
+        }
+        if (slices > 1) {   // the slices add into the voxel-side gradients
+            const size_t ve = (size_t)pb.n_events * pb.V * sizeof(float);
+            if (gw) FFDAS_CUDA(cudaMemsetAsync(gw, 0, ve, h.stream));
+            if (goff) FFDAS_CUDA(cudaMemsetAsync(goff, 0, ve, h.stream));
+            if (gdst) FFDAS_CUDA(cudaMemsetAsync(gdst, 0, (size_t)pb.V * 3 * sizeof(float), h.stream));
+        }
         if (gsrc) FFDAS_CUDA(cudaMemsetAsync(gsrc, 0, (size_t)pb.C * 3 * sizeof(float), h.stream));
         h.last = ffdas_kernel_info_t{};
         h.last.variant = 8;
         h.last.storage = kind;
         h.last.kernels = h.last_pairs_reused ? 1 : 2;   // (ingest,) adjoint
-        h.last.grid = (pb.V + kBwdThreads - 1) / kBwdThreads;
+        h.last.grid = blocks * slices;
         h.mark_start();
-        const ffdas_error_t err = kind == ST_C32 ? launch_bwd_complex<ST_C32>(h, bp, a.sparse, a.wavenum)
-                                                 : launch_bwd_complex<ST_C16>(h, bp, a.sparse, a.wavenum);
+        const ffdas_error_t err =
+            kind == ST_C32 ? launch_bwd_complex<ST_C32>(h, cp, a.sparse, a.wavenum, blocks, slices)
+                           : launch_bwd_complex<ST_C16>(h, cp, a.sparse, a.wavenum, blocks, slices);
         h.mark_stop();
         return err;
     }
