@@ -684,6 +684,26 @@ def bwd_extras(args, h) -> dict:
     binfo_s = h.last_kernel_info()
     with_w[0] = False
     msb_s_nw = timed(bwd_s, args.steps, args.warmup, stream, 1)
+
+    # complex IQ data with the phase rotation: the autofocus workload's
+    # channel data as its analytic signal (complex64), wavenum 0.05, every
+    # gradient (the complex adjoint, a thread per voxel)
+    xc = W.analytic_signal(xa).to(torch.complex64)
+    wn = 0.05
+    msf_c = timed(lambda: ffdas_b200.das(xc, *args_f, wavenum=wn), args.steps, args.warmup, stream, 1)
+    gout_c = torch.complex(gout, torch.roll(gout, 1, dims=-1)).contiguous()
+    gxc = torch.zeros(xc.shape, dtype=torch.complex64, device=dev)
+    xdsc_c = _lib.TensorDesc(list(xc.shape), None, DataType.C_32F)
+    gdsc_c = _lib.TensorDesc(list(gout_c.shape), None, DataType.C_32F)
+
+    def bwd_c():
+        h.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+        _lib.check(L.ffdas_das_backward(h.h, af["srcpos"].data_ptr(), None, wn, xdsc_c.desc, xc.data_ptr(),
+                                        af["dstpos"].data_ptr(), af["offsets"].data_ptr(), af["weights"].data_ptr(),
+                                        0, None, gdsc_c.desc, gout_c.data_ptr(), gxc.data_ptr(), go.data_ptr(),
+                                        gw.data_ptr(), gd.data_ptr(), gs.data_ptr()))
+    msb_c = timed(bwd_c, args.steps, args.warmup, stream, 1)
+    binfo_c = h.last_kernel_info()
     return {"bwd_fwd": {"ratio": msb / msf, "fwd_ms": msf, "bwd_ms": msb,
                         "bwd_ms_own_pairs": msb_own, "ratio_own_pairs": msb_own / msf,
                         "pairs": "the backward reads the pair rows the forward built (ffdas_set_pair_buffer), as "
@@ -702,7 +722,11 @@ def bwd_extras(args, h) -> dict:
                                "workload": "das_sparse, 128 ch, 64 focused transmits, 1536 samples, 400x256 "
                                            "pixels, lists of 1..32 transmits padded to 32; backward = grads of x, "
                                            "offsets, weights, voxel and channel positions (and the same "
-                                           "without the weight gradient)"}}
+                                           "without the weight gradient)"},
+            "bwd_fwd_complex": {"ratio": msb_c / msf_c, "fwd_ms": msf_c, "bwd_ms": msb_c, "bwd_kernel": binfo_c,
+                                "workload": "autofocus channel data as its analytic signal (complex64), wavenum "
+                                            "0.05; backward = grads of x, offsets, weights, voxel and channel "
+                                            "positions"}}
 
 
 
