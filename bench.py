@@ -671,19 +671,23 @@ def bwd_extras(args, h) -> dict:
     gds, gss = torch.empty_like(sf["dstpos"]), torch.empty_like(sf["srcpos"])
     xdsc_s = _lib.TensorDesc(list(xs.shape), None, DataType.R_32F)
     gdsc_s = _lib.TensorDesc(list(gout_s.shape), None, DataType.R_32F)
-    with_w = [True]
+    with_w, with_x = [True], [True]
 
     def bwd_s():
         h.set_stream(torch.cuda.current_stream(dev).cuda_stream)
         _lib.check(L.ffdas_das_backward(h.h, sf["srcpos"].data_ptr(), None, 0.0, xdsc_s.desc, xs.data_ptr(),
                                         sf["dstpos"].data_ptr(), sf["offsets"].data_ptr(),
                                         sf["weights"].data_ptr(), int(idx_s.shape[0]), idx_s.data_ptr(),
-                                        gdsc_s.desc, gout_s.data_ptr(), gxs.data_ptr(), gos.data_ptr(),
-                                        gws.data_ptr() if with_w[0] else None, gds.data_ptr(), gss.data_ptr()))
+                                        gdsc_s.desc, gout_s.data_ptr(), gxs.data_ptr() if with_x[0] else None,
+                                        gos.data_ptr(), gws.data_ptr() if with_w[0] else None, gds.data_ptr(),
+                                        gss.data_ptr()))
     msb_s = timed(bwd_s, args.steps, args.warmup, stream, 1)
     binfo_s = h.last_kernel_info()
     with_w[0] = False
     msb_s_nw = timed(bwd_s, args.steps, args.warmup, stream, 1)
+    # the gradients an autofocus step takes (delays and both position sets)
+    with_x[0] = False
+    msb_s_af = timed(bwd_s, args.steps, args.warmup, stream, 1)
 
     # complex IQ data with the phase rotation: the autofocus workload's
     # channel data as its analytic signal (complex64), wavenum 0.05, every
@@ -718,11 +722,13 @@ def bwd_extras(args, h) -> dict:
                                     "backward = grads of x, offsets, weights, voxel and channel positions"},
             "bwd_fwd_sparse": {"ratio": msb_s / msf_s, "fwd_ms": msf_s, "bwd_ms": msb_s,
                                "bwd_ms_without_weight_grad": msb_s_nw, "ratio_without_weight_grad": msb_s_nw / msf_s,
+                               "bwd_ms_autofocus_grads": msb_s_af, "ratio_autofocus_grads": msb_s_af / msf_s,
                                "bwd_kernel": binfo_s,
                                "workload": "das_sparse, 128 ch, 64 focused transmits, 1536 samples, 400x256 "
                                            "pixels, lists of 1..32 transmits padded to 32; backward = grads of x, "
                                            "offsets, weights, voxel and channel positions (and the same "
-                                           "without the weight gradient)"},
+                                           "without the weight gradient; autofocus_grads: offsets and the "
+                                           "two position sets only)"},
             "bwd_fwd_complex": {"ratio": msb_c / msf_c, "fwd_ms": msf_c, "bwd_ms": msb_c, "bwd_kernel": binfo_c,
                                 "workload": "autofocus channel data as its analytic signal (complex64), wavenum "
                                             "0.05; backward = grads of x, offsets, weights, voxel and channel "
